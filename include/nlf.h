@@ -1,0 +1,125 @@
+/* nlfiber-b200: C ABI of the B200 (sm_100a) voxel homogenization hot path.
+ *
+ * One shared library, libnlf.so, replaces the hot path of the reference package nlfiber
+ * (redcican/nonlinear-fiber-homogenization): the small-strain corrector solve of nlfiber/linear.py and the
+ * matrix-free neo-Hookean residual / tangent matvec inside nlfiber/mech.py's Newton-CG.
+ *
+ * Conventions shared by every entry point
+ *  - Plain pointers and sizes only. Any array argument may be a HOST pointer (the library copies it in or
+ *    out on `stream`, synchronously for outputs) or a DEVICE pointer of the current device (used in place);
+ *    the kind is detected per pointer.
+ *  - Arrays use the reference layouts, C order, float64: a density or stiffness-scale field is (nx, ny, nz);
+ *    a corrector / nodal field is (m, nx, ny, nz, 3) per cell; batched calls prepend the cell axis.
+ *    2D (plane strain) cells are nz = 1 (nlfiber/linear.py:100-106).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).
+ *  - Return codes: 0 ok; 1 not converged (outputs and iteration counts are still written; the reference
+ *    returns silently with it == maxit, nlfiber/linear.py:188,217); 2 breakdown (non-finite values);
+ *    -1 bad argument; -2 CUDA error; -3 device wait timed out. The message of the last error of the
+ *    calling thread is returned by nlf_last_error(). Nothing aborts the process.
+ */
+#ifndef NLF_H_
+#define NLF_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NLF_API __attribute__((visibility("default")))
+
+typedef struct nlf_linear nlf_linear;
+typedef struct nlf_mech nlf_mech;
+
+/* Solver precision. */
+#define NLF_PREC_FP64 0  /* the reference algorithm in FP64: the drop-in and the plain GPU baseline */
+#define NLF_PREC_MIXED 1 /* FP32 operator + PCG inside FP64 iterative refinement; FP64 dots */
+
+/* Preconditioner. */
+#define NLF_PC_FFT 0        /* the reference's unit-stiffness FFT inverse (nlfiber/linear.py:154-170) */
+#define NLF_PC_FFT_SCALED 1 /* S^-1/2 K0^-1 S^-1/2 with S the mean stiffness scale of the 8 elements
+                               around each node (same converged solution, far fewer iterations at high
+                               contrast) */
+
+typedef struct nlf_solve_opts {
+  int precision;     /* NLF_PREC_* */
+  int precond;       /* NLF_PC_* */
+  double tol;        /* stop when every case of a cell has ||r|| <= tol ||b|| (< 0: use the handle's tol) */
+  int maxit;         /* total PCG iterations per cell (< 0: use the handle's maxit) */
+  double inner_tol;  /* NLF_PREC_MIXED: relative residual reduction of one FP32 inner solve */
+  int inner_maxit;   /* NLF_PREC_MIXED: iteration cap of one FP32 inner solve */
+  int max_sweeps;    /* NLF_PREC_MIXED: cap on FP64 refinement sweeps */
+  int check_every;   /* host convergence poll period in iterations (>= 1) */
+  int use_graphs;    /* capture the PCG iteration in a CUDA graph and replay it */
+} nlf_solve_opts;
+
+NLF_API const char* nlf_last_error(void);
+NLF_API const char* nlf_version(void);
+NLF_API void nlf_default_opts(nlf_solve_opts* opts);
+
+/* ---- small-strain homogenization (nlfiber/linear.py) --------------------------------------------------- */
+
+/* nlfiber/linear.py:102-113 LinearHomogenization.__init__(shape, E, nu, emin, p, dtype, tol, maxit):
+ * element matrices, preconditioner symbol and workspaces for one grid shape. */
+NLF_API int nlf_linear_create(nlf_linear** h, int nx, int ny, int nz, double E, double nu, double emin,
+                              double p, double tol, int maxit);
+NLF_API int nlf_linear_destroy(nlf_linear* h);
+
+/* nlfiber/linear.py:137-141 stiffness_scale: s = emin + (1 - emin) clip01(rho)^p for ncell cells. */
+NLF_API int nlf_stiffness_scale(nlf_linear* h, int ncell, const double* rho, double* s, void* stream);
+
+/* nlfiber/linear.py:143-144 apply_K: y = K(s) u for `nvec` nodal fields sharing one s (FP64). */
+NLF_API int nlf_apply_K(nlf_linear* h, const double* s, int nvec, const double* u, double* y, void* stream);
+
+/* apply_K in a chosen arithmetic: precision NLF_PREC_FP64 (as nlf_apply_K) or NLF_PREC_MIXED (the FP32
+ * operator of the mixed-precision solver; inputs and outputs stay float64 arrays). */
+NLF_API int nlf_apply_K_ex(nlf_linear* h, const double* s, int nvec, const double* u, double* y, int precision,
+                           void* stream);
+
+/* nlfiber/linear.py:146-149 load: f_I = a(E_I, .) for Es (m, 6); f is (m, nx, ny, nz, 3). */
+NLF_API int nlf_load(nlf_linear* h, const double* s, const double* Es, int m, double* f, void* stream);
+
+/* nlfiber/linear.py:167-170 precond: z = irfftn(Kinv rfftn(r)) for `nvec` fields (FP64). */
+NLF_API int nlf_precond(nlf_linear* h, int nvec, const double* r, double* z, void* stream);
+
+/* precond in a chosen arithmetic and preconditioner: precond NLF_PC_FFT (s ignored, may be NULL) or
+ * NLF_PC_FFT_SCALED (s: the cell's stiffness scale (nx, ny, nz); z = w irfftn(Kinv rfftn(w r)) with
+ * w = (mean of s over the 8 elements around each node)^-1/2). */
+NLF_API int nlf_precond_ex(nlf_linear* h, int nvec, const double* r, double* z, int precision, int precond,
+                           const double* s, void* stream);
+
+/* nlfiber/linear.py:205-217 solve(s, Es, u0) -> (u, it) for ncell cells of this shape, m cases each.
+ * s: (ncell, nx, ny, nz); Es: (m, 6); u0: (ncell, m, nx, ny, nz, 3) or NULL (zeros); u: same shape, out;
+ * iters: (ncell,) out. opts NULL = FP64 reference algorithm with the handle's tol and maxit. */
+NLF_API int nlf_linear_solve(nlf_linear* h, int ncell, const double* s, const double* Es, int m,
+                             const double* u0, double* u, int* iters, const nlf_solve_opts* opts,
+                             void* stream);
+
+/* nlfiber/linear.py:208-210 _solve_rhs(s, b): PCG from zero for right-hand sides b (ncell, m, ..., 3). */
+NLF_API int nlf_linear_solve_rhs(nlf_linear* h, int ncell, const double* s, int m, const double* b,
+                                 double* u, int* iters, const nlf_solve_opts* opts, void* stream);
+
+/* nlfiber/linear.py:220-229 bilinear(s, Es, u) -> C (ncell, m, m). */
+NLF_API int nlf_bilinear(nlf_linear* h, int ncell, const double* s, const double* Es, int m,
+                         const double* u, double* C, void* stream);
+
+/* dC_IJ/drho_e with the correctors held fixed: the value of the reference's VJP of bilinear through
+ * stiffness_scale (nlfiber/linear.py:10-12,137-141,220-229,259-264). rho: (ncell, nx, ny, nz);
+ * dC: (ncell, m, m, nx, ny, nz). */
+NLF_API int nlf_dC_drho(nlf_linear* h, int ncell, const double* rho, const double* Es, int m,
+                        const double* u, double* dC, void* stream);
+
+/* nlfiber/linear.py:231-236 C_full(rho, u0) for a batch: rho -> s -> 6 unit strains -> PCG -> C.
+ * u0, u, dC may be NULL (cold start / corrector not returned / no sensitivities).
+ * C: (ncell, 6, 6); u: (ncell, 6, nx, ny, nz, 3); dC: (ncell, 6, 6, nx, ny, nz); iters: (ncell,). */
+NLF_API int nlf_C_full(nlf_linear* h, int ncell, const double* rho, const double* u0, double* C,
+                       double* u, double* dC, int* iters, const nlf_solve_opts* opts, void* stream);
+
+/* Kinv of the reference's preconditioner (nlfiber/linear.py:154-165), real symmetric 3x3 per wavenumber:
+ * out (nx, ny, nz/2+1, 6) in the order xx yy zz yz xz xy. */
+NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NLF_H_ */

@@ -1,0 +1,375 @@
+// Matrix-free periodic Q1 stiffness operator, load vector and C / dC assembly.
+//
+// apply  y = K(s) x = scatter(s_e Ke gather(x))            nlfiber/linear.py:80-92,143-144
+// load   f_I = scatter(s_e (E_I G))                          nlfiber/linear.py:146-149
+// C      C_IJ = mean_e s_e b_e(E_I + u_I, E_J + u_J)          nlfiber/linear.py:220-229
+// dC/drho (correctors held fixed)                            nlfiber/linear.py:10-12,137-141,259-264
+//
+// The apply kernel marches a CTA along x (the slowest axis) over a TY x TZ tile of the (y, z) plane. Each
+// thread owns one element of the (TY+1) x (TZ+1) element layer that touches the tile (one element row and
+// column of halo). Per layer it reads the 4 new corner nodes from a shared node plane (the other 4 are the
+// previous layer's, kept in registers), computes the 24 element forces with the mode form of Ke, adds the
+// forces on the finished plane to the top-corner forces carried from the previous layer, and publishes them
+// to shared memory; each output node then sums its 4 in-plane element contributions. Every output node is
+// written once, with a fixed summation order (deterministic), and the whole 27-point stencil stays on chip.
+#include "nlf_internal.h"
+
+namespace nlf {
+
+template <typename T, int TY, int TZ>
+__global__ void __launch_bounds__(((TY + 1) * (TZ + 1) + 31) / 32 * 32)
+k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int n0, int n1, int n2, int m,
+        int lx, const CellState* __restrict__ cs, ModeC<T> kc, double* __restrict__ partial) {
+  constexpr int HY = TY + 2, HZ = TZ + 2, EY = TY + 1, EZ = TZ + 1;
+  constexpr int NE = EY * EZ;
+  constexpr int NT = (NE + 31) / 32 * 32;
+  constexpr int NP = HY * HZ;
+  __shared__ T pl[3][NP];
+  __shared__ T sl[NE];
+  __shared__ T g[4][3][NE];
+  __shared__ int gys[HY], gzs[HZ];
+  __shared__ double red[32 * 4];
+  (void)EY;
+
+  const int vec = blockIdx.z, cell = vec / m;
+  if (cs && !cs[cell].active) return;
+  const long N = (long)n0 * n1 * n2;
+  const int ntz = (n2 + TZ - 1) / TZ;
+  const int z0 = (blockIdx.x % ntz) * TZ, y0 = (blockIdx.x / ntz) * TY;
+  const int xb = blockIdx.y * lx, xe = min(xb + lx, n0);
+  const T* __restrict__ xv = x + (long)vec * 3 * N;
+  T* __restrict__ yv = y + (long)vec * 3 * N;
+  const T* __restrict__ sv = s + (long)cell * N;
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < HY; i += NT) gys[i] = wrap(y0 - 1 + i, n1);
+  for (int i = tid; i < HZ; i += NT) gzs[i] = wrap(z0 - 1 + i, n2);
+
+  const bool ev = tid < NE;
+  const int ey = tid / EZ, ez = tid - (tid / EZ) * EZ;
+  int cidx[4];  // in-plane corner q = ay + 2 az of this element, in node-plane coordinates
+#pragma unroll
+  for (int q = 0; q < 4; ++q) cidx[q] = (ey + (q & 1)) * HZ + ez + (q >> 1);
+
+  T lo[3][4], ft[3][4];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  __syncthreads();
+
+  // prologue: node plane xb - 1 (the lower plane of the first element layer)
+  {
+    const long base = (long)wrap(xb - 1, n0) * n1;
+    for (int i = tid; i < 3 * NP; i += NT) {
+      const int c = i / NP, r = i - c * NP;
+      const int hy = r / HZ, hz = r - hy * HZ;
+      pl[c][r] = __ldg(xv + c * N + (base + gys[hy]) * n2 + gzs[hz]);
+    }
+  }
+  __syncthreads();
+  if (ev) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        lo[c][q] = pl[c][cidx[q]];
+        ft[c][q] = T(0);
+      }
+  }
+
+  for (int k = xb - 1; k < xe; ++k) {
+    __syncthreads();  // all reads of pl (previous layer) and g (previous output) are done
+    {
+      const long base = (long)wrap(k + 1, n0) * n1;
+      for (int i = tid; i < 3 * NP; i += NT) {
+        const int c = i / NP, r = i - c * NP;
+        const int hy = r / HZ, hz = r - hy * HZ;
+        pl[c][r] = __ldg(xv + c * N + (base + gys[hy]) * n2 + gzs[hz]);
+      }
+      const long sbase = (long)wrap(k, n0) * n1;
+      for (int i = tid; i < NE; i += NT) {
+        const int a = i / EZ, b = i - a * EZ;
+        sl[i] = __ldg(sv + (sbase + gys[a]) * n2 + gzs[b]);
+      }
+    }
+    __syncthreads();
+    if (ev) {
+      T v[3][8], f[3][8], hi[3][4];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          hi[c][q] = pl[c][cidx[q]];
+          v[c][2 * q] = lo[c][q];
+          v[c][2 * q + 1] = hi[c][q];
+        }
+      const ModeC<T> ks = scale_modec(kc, sl[tid]);
+      element_force(v, ks, f);
+      if (k >= xb) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) g[q][c][tid] = ft[c][q] + f[c][2 * q];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ft[c][q] = f[c][2 * q + 1];
+          lo[c][q] = hi[c][q];
+        }
+    }
+    __syncthreads();
+    if (k >= xb && tid < TY * TZ) {
+      const int ty = tid / TZ, tz = tid - (tid / TZ) * TZ;
+      const int yy = y0 + ty, zz = z0 + tz;
+      if (yy < n1 && zz < n2) {
+        // node (ty+1, tz+1) in plane coords is corner q = ay + 2az of element (ty+1-ay, tz+1-az)
+        const int e00 = (ty + 1) * EZ + (tz + 1);
+        const long idx = ((long)k * n1 + yy) * n2 + zz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T o = (g[0][c][e00] + g[1][c][e00 - EZ]) + (g[2][c][e00 - 1] + g[3][c][e00 - EZ - 1]);
+          yv[c * N + idx] = o;
+          if (partial) {
+            acc[c] += (double)o;
+            acc[3] += (double)__ldg(xv + c * N + idx) * (double)o;
+          }
+        }
+      }
+    }
+  }
+  if (partial) {
+    block_sum<4>(acc, red);
+    if (tid == 0) {
+      const long blk = blockIdx.x + (long)gridDim.x * blockIdx.y;
+      const long nblk = (long)gridDim.x * gridDim.y;
+      double* o = partial + ((long)vec * nblk + blk) * 4;
+      o[0] = acc[0];
+      o[1] = acc[1];
+      o[2] = acc[2];
+      o[3] = acc[3];
+    }
+  }
+}
+
+template <typename T>
+struct ApplyTile;
+template <>
+struct ApplyTile<float> {
+  static constexpr int TY = 8, TZ = 32;
+};
+template <>
+struct ApplyTile<double> {
+  static constexpr int TY = 8, TZ = 16;
+};
+
+template <typename T>
+int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y, const CellState* cs,
+                 double* partial, int* nblk_out, cudaStream_t st) {
+  constexpr int TY = ApplyTile<T>::TY, TZ = ApplyTile<T>::TZ;
+  constexpr int NT = ((TY + 1) * (TZ + 1) + 31) / 32 * 32;
+  const Geom& g = h.g;
+  const int tiles = ((g.n2 + TZ - 1) / TZ) * ((g.n1 + TY - 1) / TY);
+  // enough CTAs for ~4 waves on the SMs, at least 8 planes per march
+  long want = 4L * h.nsm;
+  int chunks = (int)((want + (long)tiles * nvec - 1) / ((long)tiles * nvec));
+  chunks = max(1, min(chunks, max(1, g.n0 / 8)));
+  const int lx = (g.n0 + chunks - 1) / chunks;
+  chunks = (g.n0 + lx - 1) / lx;
+  if (nblk_out) *nblk_out = tiles * chunks;
+  dim3 grid(tiles, chunks, nvec);
+  k_apply<T, TY, TZ><<<grid, NT, 0, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs,
+                                          make_modec<T>(h.lam, h.mu), partial);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+template int launch_apply<float>(const LinearHandle&, const float*, int, int, const float*, float*,
+                                 const CellState*, double*, int*, cudaStream_t);
+template int launch_apply<double>(const LinearHandle&, const double*, int, int, const double*, double*,
+                                  const CellState*, double*, int*, cudaStream_t);
+
+// ---- load: f[cell][I][c][n] = sign * sum_a s(n - off_a) fe[I][3a + c] -----------------------------------
+__global__ void k_load(const double* __restrict__ s, const double* __restrict__ fe, int m, int n0, int n1,
+                       int n2, double* __restrict__ f, double sign) {
+  const long N = (long)n0 * n1 * n2;
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int cell = blockIdx.y;
+  if (n >= N) return;
+  const int k = (int)(n % n2), j = (int)((n / n2) % n1), i = (int)(n / ((long)n1 * n2));
+  const double* sv = s + (long)cell * N;
+  double se[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int ii = wrap(i - (a & 1), n0), jj = wrap(j - ((a >> 1) & 1), n1), kk = wrap(k - (a >> 2), n2);
+    se[a] = sv[((long)ii * n1 + jj) * n2 + kk];
+  }
+  for (int I = 0; I < m; ++I) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) acc += se[a] * fe[I * 24 + 3 * a + c];
+      f[(((long)cell * m + I) * 3 + c) * N + n] = sign * acc;
+    }
+  }
+}
+
+int launch_load(const LinearHandle& h, const double* s, const double* fe, int m, int ncell, double* f,
+                double sign, cudaStream_t st) {
+  const long N = h.g.N;
+  dim3 grid((unsigned)((N + 255) / 256), ncell);
+  k_load<<<grid, 256, 0, st>>>(s, fe, m, h.g.n0, h.g.n1, h.g.n2, f, sign);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// ---- C and dC/drho ----------------------------------------------------------------------------------------
+// b_IJ(e) = E_I D E_J + E_I . D eps_J + E_J . D eps_I + u_I^T Ke u_J, with eps the element-mean strain of the
+// corrector (G u = D mean(B) u, nlfiber/linear.py:112) and u^T Ke u in mode form (c'_I . M c'_J).
+constexpr int kMaxM = 6;
+constexpr int kMaxPairs = kMaxM * (kMaxM + 1) / 2;
+
+__device__ __forceinline__ void gather_modes(const double* __restrict__ u, long N, const long (&nid)[8],
+                                             double (&c)[3][8]) {
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+#pragma unroll
+    for (int a = 0; a < 8; ++a) c[cc][a] = u[cc * N + nid[a]];
+    butterfly8(c[cc]);
+  }
+}
+
+__device__ __forceinline__ void mean_stress(const double (&c)[3][8], double lam, double mu, double (&sig)[6]) {
+  // Voigt strain (engineering shear) of the constant-strain mode: H[c][d] = c'[c][1<<d] / 4
+  const double e0 = 0.25 * c[0][1], e1 = 0.25 * c[1][2], e2 = 0.25 * c[2][4];
+  const double g12 = 0.25 * (c[1][4] + c[2][2]), g02 = 0.25 * (c[0][4] + c[2][1]),
+               g01 = 0.25 * (c[0][2] + c[1][1]);
+  const double tr = lam * (e0 + e1 + e2);
+  sig[0] = tr + 2.0 * mu * e0;
+  sig[1] = tr + 2.0 * mu * e1;
+  sig[2] = tr + 2.0 * mu * e2;
+  sig[3] = mu * g12;
+  sig[4] = mu * g02;
+  sig[5] = mu * g01;
+}
+
+__global__ void __launch_bounds__(128) k_bilinear(const double* __restrict__ s, const double* __restrict__ Es,
+                                                  const double* __restrict__ EDE, int m, int n0, int n1,
+                                                  int n2, double lam, double mu, const double* __restrict__ u,
+                                                  double* __restrict__ Cpart, const double* __restrict__ rho,
+                                                  double emin, double pexp, double* __restrict__ dC) {
+  __shared__ double red[32 * kMaxPairs];
+  const long N = (long)n0 * n1 * n2;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int cell = blockIdx.y;
+  const bool valid = e < N;
+  double acc[kMaxPairs];
+#pragma unroll
+  for (int q = 0; q < kMaxPairs; ++q) acc[q] = 0.0;
+  if (valid) {
+    const int k = (int)(e % n2), j = (int)((e / n2) % n1), i = (int)(e / ((long)n1 * n2));
+    long nid[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int ii = wrap(i + (a & 1), n0), jj = wrap(j + ((a >> 1) & 1), n1), kk = wrap(k + (a >> 2), n2);
+      nid[a] = ((long)ii * n1 + jj) * n2 + kk;
+    }
+    const double se = s[(long)cell * N + e];
+    double ds = 0.0;
+    if (dC) {
+      const double r = rho[(long)cell * N + e];
+      const double rc = r > 1.0 ? 1.0 : (r < 0.0 ? 0.0 : r);
+      ds = (r > 1.0 || r < 0.0) ? 0.0 : (1.0 - emin) * pexp * pow(rc, pexp - 1.0);
+      ds /= (double)N;
+    }
+    const ModeC<double> unit = make_modec<double>(lam, mu);
+    const double* ub = u + (long)cell * m * 3 * N;
+    int q = 0;
+    for (int I = 0; I < m; ++I) {
+      double cI[3][8], fI[3][8], sI[6];
+      gather_modes(ub + (long)I * 3 * N, N, nid, cI);
+      mode_force(cI, unit, fI);
+      mean_stress(cI, lam, mu, sI);
+      for (int J = I; J < m; ++J, ++q) {
+        double cJ[3][8], sJ[6];
+        if (J == I) {
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int a = 0; a < 8; ++a) cJ[cc][a] = cI[cc][a];
+#pragma unroll
+          for (int v = 0; v < 6; ++v) sJ[v] = sI[v];
+        } else {
+          gather_modes(ub + (long)J * 3 * N, N, nid, cJ);
+          mean_stress(cJ, lam, mu, sJ);
+        }
+        double b = EDE[I * m + J];
+#pragma unroll
+        for (int v = 0; v < 6; ++v) b += Es[I * 6 + v] * sJ[v] + Es[J * 6 + v] * sI[v];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+          for (int a = 1; a < 8; ++a) b += cJ[cc][a] * fI[cc][a];
+        // accumulate into the pair slot (unrolled index keeps acc in registers)
+#pragma unroll
+        for (int t = 0; t < kMaxPairs; ++t)
+          if (t == q) acc[t] += se * b;
+        if (dC) {
+          double* o = dC + ((long)cell * m * m) * N;
+          o[((long)I * m + J) * N + e] = ds * b;
+          o[((long)J * m + I) * N + e] = ds * b;
+        }
+      }
+    }
+  }
+  block_sum<kMaxPairs>(acc, red);
+  if (threadIdx.x == 0) {
+    double* o = Cpart + ((long)cell * gridDim.x + blockIdx.x) * kMaxPairs;
+#pragma unroll
+    for (int t = 0; t < kMaxPairs; ++t) o[t] = acc[t];
+  }
+}
+
+__global__ void k_reduce_C(const double* __restrict__ Cpart, int nblk, int m, double invN,
+                           double* __restrict__ C) {
+  const int cell = blockIdx.x;
+  const int npair = m * (m + 1) / 2;
+  for (int t = threadIdx.x; t < npair; t += blockDim.x) {
+    double a = 0.0;
+    for (int b = 0; b < nblk; ++b) a += Cpart[((long)cell * nblk + b) * kMaxPairs + t];
+    // pair t -> (I, J), I <= J, in the order of k_bilinear
+    int I = 0, rem = t;
+    while (rem >= m - I) {
+      rem -= m - I;
+      ++I;
+    }
+    const int J = I + rem;
+    C[((long)cell * m + I) * m + J] = a * invN;
+    C[((long)cell * m + J) * m + I] = a * invN;
+  }
+}
+
+int launch_bilinear(const LinearHandle& h, const double* s, const double* EsEDE, int m, int ncell,
+                    const double* u, double* Cpart, int* nblk, const double* rho, double* dC, cudaStream_t st) {
+  if (m > kMaxM) {
+    set_error("bilinear: at most %d load cases per cell (got %d)", kMaxM, m);
+    return NLF_EBADARG;
+  }
+  const long N = h.g.N;
+  const int nb = (int)((N + 127) / 128);
+  *nblk = nb;
+  dim3 grid(nb, ncell);
+  k_bilinear<<<grid, 128, 0, st>>>(s, EsEDE, EsEDE + m * 6, m, h.g.n0, h.g.n1, h.g.n2, h.lam, h.mu, u, Cpart,
+                                   rho, h.emin, h.p, dC);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+int launch_reduce_C(const LinearHandle& h, const double* Cpart, int nblk, int m, int ncell, double* C,
+                    cudaStream_t st) {
+  k_reduce_C<<<ncell, 32, 0, st>>>(Cpart, nblk, m, 1.0 / (double)h.g.N, C);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+}  // namespace nlf

@@ -1,0 +1,465 @@
+// FFT preconditioner of the periodic corrector solve: z = irfftn(Kinv(k) rfftn(r)) (nlfiber/linear.py:154-170),
+// optionally with node scaling w = S^-1/2 on both sides (z = w .* irfftn(Kinv rfftn(w .* r))).
+//
+// Three passes over a half spectrum stored [vec][comp][ky][x][kz], kz in [0, nz/2]:
+//   A  one CTA per (vec, comp, x-plane): real plane -> 2D transform along z (real, packed as a half-length
+//      complex FFT) and y, in shared memory; writes (ky, x, kz) rows.
+//   B  one CTA per (vec, ky, kz-chunk): the three components' x-lines -> forward FFT along x, 3x3 Kinv
+//      multiply per wavenumber, inverse FFT along x, in shared memory.
+//   C  one CTA per (vec, comp, x-plane): inverse y then inverse real z, scale by 1/N (and w), write the real
+//      field and the reduction partials the PCG needs (sum z, (r, z), sum r, (r, r)).
+// Power-of-two lines use an iterative radix-2 FFT; other lengths (small test grids) a direct DFT.
+// Kinv is the reference's symbol: the FFT of the unit-stiffness impulse response, which is the real symmetric
+// sum over the 27 stencil blocks W_d cos(k.d); K(0) = I; Kinv = inv(K + 1e-12 |tr K| I); Kinv(0) = 0.
+#include <cmath>
+#include "nlf_internal.h"
+
+namespace nlf {
+
+// Transform `nlines` lines of length n in shared memory. Line l starts at
+// (l / inner_n) * outer_stride + (l % inner_n) * inner_stride, elements are `es` apart. tw[k] = e^{-2 pi i k/n}.
+// `scratch` (nlines * n entries) is used by non-power-of-two lengths only. Ends with __syncthreads().
+template <typename T>
+__device__ void lines_fft(cplx<T>* buf, int n, int nlines, int inner_n, int outer_stride, int inner_stride,
+                          int es, const cplx<T>* __restrict__ tw, bool inv, cplx<T>* scratch) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (n == 1) return;
+  if (is_pow2(n)) {
+    const int lg = ilog2(n);
+    for (int idx = tid; idx < nlines * n; idx += nt) {
+      const int l = idx >> lg, j = idx & (n - 1);
+      const int r = (int)(__brev((unsigned)j) >> (32 - lg));
+      if (j < r) {
+        const int b = (l / inner_n) * outer_stride + (l % inner_n) * inner_stride;
+        const cplx<T> t = buf[b + j * es];
+        buf[b + j * es] = buf[b + r * es];
+        buf[b + r * es] = t;
+      }
+    }
+    __syncthreads();
+    const int nh = n >> 1;
+    for (int half = 1, lh = 0; half < n; half <<= 1, ++lh) {
+      const int tstep = n / (2 * half);
+      for (int idx = tid; idx < nlines * nh; idx += nt) {
+        const int l = idx / nh, t = idx - l * nh;
+        const int pos = t & (half - 1), grp = t >> lh;
+        const int i0 = grp * 2 * half + pos, i1 = i0 + half;
+        const int b = (l / inner_n) * outer_stride + (l % inner_n) * inner_stride;
+        cplx<T> w = tw[pos * tstep];
+        if (inv) w.y = -w.y;
+        const cplx<T> a = buf[b + i0 * es];
+        const cplx<T> c = cmul(buf[b + i1 * es], w);
+        buf[b + i0 * es] = cadd(a, c);
+        buf[b + i1 * es] = csub(a, c);
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int idx = tid; idx < nlines * n; idx += nt) {
+      const int l = idx / n, j = idx - l * n;
+      const int b = (l / inner_n) * outer_stride + (l % inner_n) * inner_stride;
+      scratch[idx] = buf[b + j * es];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nlines * n; idx += nt) {
+      const int l = idx / n, k = idx - l * n;
+      const int b = (l / inner_n) * outer_stride + (l % inner_n) * inner_stride;
+      cplx<T> acc{T(0), T(0)};
+      int e = 0;
+      for (int j = 0; j < n; ++j) {
+        cplx<T> w = tw[e];
+        if (inv) w.y = -w.y;
+        acc = cadd(acc, cmul(scratch[l * n + j], w));
+        e += k;
+        if (e >= n) e -= n;
+      }
+      buf[b + k * es] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Packed real FFT post-processing along rows of length n (even), M = n/2: Z (first M entries of each row,
+// the FFT of x[2j] + i x[2j+1]) -> X_k, k = 0..M (row entries 0..M). wn[k] = e^{-2 pi i k / n}.
+template <typename T>
+__device__ void real_post(cplx<T>* buf, int rows, int rs, int n, const cplx<T>* __restrict__ wn) {
+  const int M = n >> 1, H = M / 2 + 1;
+  for (int idx = threadIdx.x; idx < rows * H; idx += blockDim.x) {
+    const int row = idx / H, k = idx - row * H;
+    cplx<T>* z = buf + row * rs;
+    if (k == 0) {
+      const cplx<T> z0 = z[0];
+      z[0] = {z0.x + z0.y, T(0)};
+      z[M] = {z0.x - z0.y, T(0)};
+    } else if (2 * k == M) {
+      z[k] = cconj(z[k]);
+    } else {
+      const cplx<T> a = z[k], b = z[M - k];
+      // E_k = (a + conj b)/2, O_k = -i (a - conj b)/2
+      const cplx<T> Ek{(a.x + b.x) * T(0.5), (a.y - b.y) * T(0.5)};
+      const cplx<T> Ok{(a.y + b.y) * T(0.5), -(a.x - b.x) * T(0.5)};
+      const cplx<T> Em{(b.x + a.x) * T(0.5), (b.y - a.y) * T(0.5)};
+      const cplx<T> Om{(b.y + a.y) * T(0.5), -(b.x - a.x) * T(0.5)};
+      z[k] = cadd(Ek, cmul(wn[k], Ok));
+      z[M - k] = cadd(Em, cmul(wn[M - k], Om));
+    }
+  }
+  __syncthreads();
+}
+
+// Inverse of real_post: X_k (k = 0..M) -> Z_k = E_k + i O_k (k < M), E_k = (X_k + conj X_{M-k})/2,
+// O_k = (X_k - conj X_{M-k}) conj(wn[k]) / 2.
+template <typename T>
+__device__ void real_pre(cplx<T>* buf, int rows, int rs, int n, const cplx<T>* __restrict__ wn) {
+  const int M = n >> 1, H = M / 2 + 1;
+  for (int idx = threadIdx.x; idx < rows * H; idx += blockDim.x) {
+    const int row = idx / H, k = idx - row * H;
+    cplx<T>* z = buf + row * rs;
+    if (k == 0) {
+      // X_0 and X_M of a real signal are real; their imaginary parts are rounding and are dropped (as irfft does)
+      const T a = z[0].x, b = z[M].x;
+      z[0] = {(a + b) * T(0.5), (a - b) * T(0.5)};
+    } else if (2 * k == M) {
+      z[k] = cconj(z[k]);
+    } else {
+      const cplx<T> a = z[k], b = z[M - k];
+      const cplx<T> Ek{(a.x + b.x) * T(0.5), (a.y - b.y) * T(0.5)};
+      const cplx<T> Dk{(a.x - b.x) * T(0.5), (a.y + b.y) * T(0.5)};
+      const cplx<T> Ok = cmul(Dk, cconj(wn[k]));
+      const cplx<T> Em{(b.x + a.x) * T(0.5), (b.y - a.y) * T(0.5)};
+      const cplx<T> Dm{(b.x - a.x) * T(0.5), (b.y + a.y) * T(0.5)};
+      const cplx<T> Om = cmul(Dm, cconj(wn[M - k]));
+      z[k] = {Ek.x - Ok.y, Ek.y + Ok.x};
+      z[M - k] = {Em.x - Om.y, Em.y + Om.x};
+    }
+  }
+  __syncthreads();
+}
+
+struct FftDims {
+  int n0, n1, n2, n2h, rs;  // rs: shared row stride of a (y, z) plane
+  long N, NS;
+  int off0, off1, off2, off2h;
+};
+
+// ---- pass A --------------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T>* __restrict__ spec, FftDims d,
+                        int m, const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs) {
+  extern __shared__ unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* scratch = buf + d.n1 * d.rs;
+  const int x = blockIdx.x, c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  const T* rp = r + ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
+  const T* wp = w ? w + (long)(vec / m) * d.N + (long)x * d.n1 * d.n2 : nullptr;
+  const bool packed = (d.n2 % 2) == 0;
+  if (packed) {
+    const int M = d.n2 / 2;
+    for (int idx = threadIdx.x; idx < d.n1 * M; idx += blockDim.x) {
+      const int y = idx / M, j = idx - y * M;
+      T a = rp[y * d.n2 + 2 * j], b = rp[y * d.n2 + 2 * j + 1];
+      if (wp) {
+        a *= wp[y * d.n2 + 2 * j];
+        b *= wp[y * d.n2 + 2 * j + 1];
+      }
+      buf[y * d.rs + j] = {a, b};
+    }
+    __syncthreads();
+    lines_fft(buf, M, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, false, scratch);
+    real_post(buf, d.n1, d.rs, d.n2, tw + d.off2);
+  } else {
+    for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
+      const int y = idx / d.n2, z = idx - y * d.n2;
+      T a = rp[idx];
+      if (wp) a *= wp[idx];
+      buf[y * d.rs + z] = {a, T(0)};
+    }
+    __syncthreads();
+    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, false, scratch);
+  }
+  // y transform on the n2h columns
+  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, false, scratch);
+  cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
+  for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
+    const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
+    sp[((long)ky * d.n0 + x) * d.n2h + kz] = buf[ky * d.rs + kz];
+  }
+}
+
+// ---- pass B --------------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, FftDims d, int kc, int m,
+                        const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs) {
+  extern __shared__ unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);  // [3][n0][kc]
+  cplx<T>* scratch = buf + 3 * d.n0 * kc;
+  const int ky = blockIdx.x, kz0 = blockIdx.y * kc, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  const int nkz = min(kc, d.n2h - kz0);
+  for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
+    const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
+    const int x = rem / kc, kz = rem - x * kc;
+    cplx<T> v{T(0), T(0)};
+    if (kz < nkz) v = spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + x) * d.n2h + kz0 + kz];
+    buf[idx] = v;
+  }
+  __syncthreads();
+  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, false, scratch);
+  for (int idx = threadIdx.x; idx < d.n0 * kc; idx += blockDim.x) {
+    const int kx = idx / kc, kz = idx - kx * kc;
+    if (kz < nkz) {
+      const T* K = kinv + (((long)kx * d.n1 + ky) * d.n2h + kz0 + kz) * 6;
+      const T kxx = K[0], kyy = K[1], kzz = K[2], kyz = K[3], kxz = K[4], kxy = K[5];
+      const cplx<T> a = buf[idx], b = buf[d.n0 * kc + idx], c = buf[2 * d.n0 * kc + idx];
+      buf[idx] = {kxx * a.x + kxy * b.x + kxz * c.x, kxx * a.y + kxy * b.y + kxz * c.y};
+      buf[d.n0 * kc + idx] = {kxy * a.x + kyy * b.x + kyz * c.x, kxy * a.y + kyy * b.y + kyz * c.y};
+      buf[2 * d.n0 * kc + idx] = {kxz * a.x + kyz * b.x + kzz * c.x, kxz * a.y + kyz * b.y + kzz * c.y};
+    }
+  }
+  __syncthreads();
+  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, true, scratch);
+  for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
+    const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
+    const int x = rem / kc, kz = rem - x * kc;
+    if (kz < nkz) spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + x) * d.n2h + kz0 + kz] = buf[idx];
+  }
+}
+
+// ---- pass C --------------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ w, const T* __restrict__ r,
+                        T* __restrict__ z, FftDims d, int m, const cplx<T>* __restrict__ tw,
+                        const CellState* __restrict__ cs, double* __restrict__ partial) {
+  extern __shared__ unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* scratch = buf + d.n1 * d.rs;
+  __shared__ double red[32 * 4];
+  const int x = blockIdx.x, c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  const cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
+  for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
+    const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
+    buf[ky * d.rs + kz] = sp[((long)ky * d.n0 + x) * d.n2h + kz];
+  }
+  __syncthreads();
+  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, true, scratch);
+  const bool packed = (d.n2 % 2) == 0;
+  if (packed) {
+    real_pre(buf, d.n1, d.rs, d.n2, tw + d.off2);
+    lines_fft(buf, d.n2 / 2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, true, scratch);
+  } else {
+    // rebuild the full row from Hermitian symmetry, then a length-n2 inverse DFT
+    for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
+      const int y = idx / d.n2, k = idx - y * d.n2;
+      if (k >= d.n2h) buf[y * d.rs + k] = cconj(buf[y * d.rs + (d.n2 - k)]);
+    }
+    __syncthreads();
+    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, true, scratch);
+  }
+  // the packed z transform has length n2/2, so its unnormalised inverse carries n0 n1 n2/2
+  const T norm = T((packed ? 2.0 : 1.0) / (double)d.N);
+  const long pbase = ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
+  const T* wp = w ? w + (long)(vec / m) * d.N + (long)x * d.n1 * d.n2 : nullptr;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
+    const int y = idx / d.n2, zz = idx - y * d.n2;
+    T v;
+    if (packed) {
+      const cplx<T> q = buf[y * d.rs + (zz >> 1)];
+      v = (zz & 1) ? q.y : q.x;
+    } else {
+      v = buf[y * d.rs + zz].x;
+    }
+    v *= norm;
+    if (wp) v *= wp[idx];
+    z[pbase + idx] = v;
+    if (partial) {
+      const double rv = (double)r[pbase + idx];
+      acc[0] += (double)v;
+      acc[1] += rv * (double)v;
+      acc[2] += rv;
+      acc[3] += rv * rv;
+    }
+  }
+  if (partial) {
+    block_sum<4>(acc, red);
+    if (threadIdx.x == 0) {
+      double* o = partial + (((long)vec * 3 + c) * d.n0 + x) * 4;
+      o[0] = acc[0];
+      o[1] = acc[1];
+      o[2] = acc[2];
+      o[3] = acc[3];
+    }
+  }
+}
+
+static FftDims fft_dims(const LinearHandle& h) {
+  FftDims d;
+  d.n0 = h.g.n0;
+  d.n1 = h.g.n1;
+  d.n2 = h.g.n2;
+  d.n2h = h.g.n2h;
+  d.rs = (d.n2 % 2 == 0) ? d.n2h : d.n2;
+  d.N = h.g.N;
+  d.NS = h.g.NS;
+  d.off0 = h.tw.off0;
+  d.off1 = h.tw.off1;
+  d.off2 = h.tw.off2;
+  d.off2h = h.tw.off2h;
+  return d;
+}
+
+static bool any_non_pow2(const FftDims& d) {
+  return !is_pow2(d.n0) || !is_pow2(d.n1) || (d.n2 % 2 == 0 ? !is_pow2(d.n2 / 2) : d.n2 > 1);
+}
+
+template <typename T>
+static int pick_kc(const FftDims& d, int smem_cap) {
+  const bool np2 = any_non_pow2(d);
+  int kc = d.n2h;
+  auto need = [&](int k) { return (size_t)3 * d.n0 * k * sizeof(cplx<T>) * (np2 ? 2 : 1); };
+  while (kc > 1 && need(kc) > (size_t)smem_cap) kc = (kc + 1) / 2;
+  return kc;
+}
+
+template <typename T>
+static cplx<T>* twiddles(const LinearHandle& h);
+template <>
+cplx<double>* twiddles<double>(const LinearHandle& h) { return h.t64.tw; }
+template <>
+cplx<float>* twiddles<float>(const LinearHandle& h) { return h.t32.tw; }
+template <typename T>
+static const T* kinv_table(const LinearHandle& h);
+template <>
+const double* kinv_table<double>(const LinearHandle& h) { return h.t64.kinv; }
+template <>
+const float* kinv_table<float>(const LinearHandle& h) { return h.t32.kinv; }
+
+template <typename T>
+int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
+                   const CellState* cs, double* partial, cudaStream_t st) {
+  const FftDims d = fft_dims(h);
+  const bool np2 = any_non_pow2(d);
+  const int cap = h.smem_optin > 0 ? h.smem_optin : 48 * 1024;
+  const size_t plane = (size_t)d.n1 * d.rs * sizeof(cplx<T>) * (np2 ? 2 : 1);
+  if (plane > (size_t)cap) {
+    set_error("precond: a (%d x %d) plane needs %zu B of shared memory (> %d)", d.n1, d.n2, plane, cap);
+    return NLF_EBADARG;
+  }
+  const int kc = pick_kc<T>(d, cap);
+  const size_t smemb = (size_t)3 * d.n0 * kc * sizeof(cplx<T>) * (np2 ? 2 : 1);
+  const cplx<T>* tw = twiddles<T>(h);
+  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_a<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemb));
+  const int nt = 256;
+  k_fft_a<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(r, w, spec, d, m, tw, cs);
+  NLF_CHECK_LAUNCH();
+  k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h), d, kc, m, tw,
+                                                                        cs);
+  NLF_CHECK_LAUNCH();
+  k_fft_c<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(spec, w, r, z, d, m, tw, cs, partial);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+template int launch_precond<float>(const LinearHandle&, int, int, const float*, float*, cplx<float>*,
+                                   const float*, const CellState*, double*, cudaStream_t);
+template int launch_precond<double>(const LinearHandle&, int, int, const double*, double*, cplx<double>*,
+                                    const double*, const CellState*, double*, cudaStream_t);
+
+// ---- tables ----------------------------------------------------------------------------------------------------
+__global__ void k_kinv(const double* __restrict__ W27, int n0, int n1, int n2, int n2h, double* __restrict__ k64,
+                       float* __restrict__ k32) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long NS = (long)n0 * n1 * n2h;
+  if (idx >= NS) return;
+  const int kz = (int)(idx % n2h), ky = (int)((idx / n2h) % n1), kx = (int)(idx / ((long)n2h * n1));
+  double K[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) K[q] = 0.0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) {
+        // cos(2 pi (kx dx / n0 + ky dy / n1 + kz dz / n2)), with the phase reduced to [0, 1) turns
+        double ph = (double)((kx * dx) % n0 + n0) / n0 + (double)((ky * dy) % n1 + n1) / n1 +
+                    (double)((kz * dz) % n2 + n2) / n2;
+        ph -= floor(ph);
+        const double cs = cospi(2.0 * ph);
+        const double* Wd = W27 + ((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) * 9;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) K[q] += Wd[q] * cs;
+      }
+  double out[6];
+  if (idx == 0) {
+    for (int q = 0; q < 6; ++q) out[q] = 0.0;
+  } else {
+    // symmetric part (the antisymmetric part cancels analytically) + regularisation
+    const double a = K[0], b = 0.5 * (K[1] + K[3]), c = 0.5 * (K[2] + K[6]);
+    const double d = K[4], e = 0.5 * (K[5] + K[7]), f = K[8];
+    const double reg = 1e-12 * fabs(a + d + f);
+    const double A = a + reg, D = d + reg, F = f + reg;
+    // inverse of [[A b c] [b D e] [c e F]]
+    const double c00 = D * F - e * e, c01 = c * e - b * F, c02 = b * e - c * D;
+    const double c11 = A * F - c * c, c12 = b * c - A * e, c22 = A * D - b * b;
+    const double det = A * c00 + b * c01 + c * c02;
+    const double id = 1.0 / det;
+    out[0] = c00 * id;  // xx
+    out[1] = c11 * id;  // yy
+    out[2] = c22 * id;  // zz
+    out[3] = c12 * id;  // yz
+    out[4] = c02 * id;  // xz
+    out[5] = c01 * id;  // xy
+  }
+  for (int q = 0; q < 6; ++q) {
+    k64[idx * 6 + q] = out[q];
+    k32[idx * 6 + q] = (float)out[q];
+  }
+}
+
+int build_tables(LinearHandle& h) {
+  const Geom& g = h.g;
+  // twiddles: lengths n0, n1, n2, n2/2 (full circles, e^{-2 pi i k / L}, k < L)
+  std::vector<double> twr, twi;
+  auto add = [&](int L) {
+    const int off = (int)twr.size();
+    for (int k = 0; k < L; ++k) {
+      const double a = -2.0 * 3.14159265358979323846 * (double)k / (double)L;
+      twr.push_back(std::cos(a));
+      twi.push_back(std::sin(a));
+    }
+    return off;
+  };
+  h.tw.off0 = add(g.n0);
+  h.tw.off1 = add(g.n1);
+  h.tw.off2 = add(g.n2);
+  h.tw.off2h = add(g.n2 % 2 == 0 ? g.n2 / 2 : 1);
+  h.tw.total = (int)twr.size();
+  std::vector<cplx<double>> t64(twr.size());
+  std::vector<cplx<float>> t32(twr.size());
+  for (size_t i = 0; i < twr.size(); ++i) {
+    t64[i] = {twr[i], twi[i]};
+    t32[i] = {(float)twr[i], (float)twi[i]};
+  }
+  NLF_CUDA_TRY(cudaMalloc(&h.t64.tw, t64.size() * sizeof(cplx<double>)));
+  NLF_CUDA_TRY(cudaMalloc(&h.t32.tw, t32.size() * sizeof(cplx<float>)));
+  NLF_CUDA_TRY(cudaMemcpy(h.t64.tw, t64.data(), t64.size() * sizeof(cplx<double>), cudaMemcpyHostToDevice));
+  NLF_CUDA_TRY(cudaMemcpy(h.t32.tw, t32.data(), t32.size() * sizeof(cplx<float>), cudaMemcpyHostToDevice));
+  NLF_CUDA_TRY(cudaMalloc(&h.t64.kinv, g.NS * 6 * sizeof(double)));
+  NLF_CUDA_TRY(cudaMalloc(&h.t32.kinv, g.NS * 6 * sizeof(float)));
+  double* dW = nullptr;
+  NLF_CUDA_TRY(cudaMalloc(&dW, sizeof(h.W27)));
+  NLF_CUDA_TRY(cudaMemcpy(dW, h.W27, sizeof(h.W27), cudaMemcpyHostToDevice));
+  k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW, g.n0, g.n1, g.n2, g.n2h, h.t64.kinv, h.t32.kinv);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(dW);
+  if (e != cudaSuccess) {
+    set_error("kinv table: %s", cudaGetErrorString(e));
+    return NLF_ECUDA;
+  }
+  return NLF_OK;
+}
+
+}  // namespace nlf

@@ -1,0 +1,112 @@
+// Internal declarations of the nlfiber-b200 library: the linear handle, its workspace and the launchers.
+#pragma once
+#include <vector>
+#include "nlf_common.cuh"
+#include "nlf_element.cuh"
+#include "../../include/nlf.h"
+
+namespace nlf {
+
+// Grid geometry of one handle. N = n0 * n1 * n2; the half spectrum has n2h = n2 / 2 + 1 z-frequencies.
+struct Geom {
+  int n0, n1, n2;  // x (slowest), y, z (fastest)
+  int n2h;         // n2 / 2 + 1
+  long N;          // voxels
+  long NS;         // half-spectrum entries per component: n0 * n1 * n2h
+};
+
+// FP64 scalars of one PCG vector (one cell and load case).
+struct VecState {
+  double bn;       // ||b|| + 1e-300
+  double rz;       // (r, z)
+  double alpha, beta;
+  double rr;       // (r, r)
+  double scale;    // refinement scale of the right-hand side (mixed precision)
+  double mean[3];  // per-component mean for the next projection
+  double pad;
+};
+
+// Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188).
+struct CellState {
+  int it;
+  int active;
+  int status;
+  int pad;
+};
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int reserve(size_t n);
+  void release();
+};
+
+template <typename T>
+struct Tables {
+  T* kinv = nullptr;     // (n0, n1, n2h, 6)
+  cplx<T>* tw = nullptr;  // twiddles, see tw_off
+};
+
+struct Twiddle {
+  int off0, off1, off2, off2h;  // offsets of the length-n0, n1, n2, n2/2 tables (each of its length)
+  int total;
+};
+
+struct LinearHandle {
+  Geom g;
+  double E, nu, emin, p, tol, lam, mu;
+  int maxit;
+  double Ke[24][24];
+  double Gm[6][24];
+  double Dm[6][6];
+  double W27[27][9];  // unit-stiffness stencil blocks W_d, d = (dx+1)*9 + (dy+1)*3 + (dz+1)
+  Twiddle tw;
+  Tables<double> t64;
+  Tables<float> t32;
+  DevBuf ws;          // solver workspace
+  DevBuf io;          // staging for host <-> device copies
+  DevBuf io2;
+  DevBuf part;        // reduction partials
+  DevBuf kinv_rgb;    // spare
+  int dev = 0;
+  int nsm = 148;
+  int smem_optin = 0;
+};
+
+// ---- launchers (all asynchronous on `st`) ----
+// element operator
+template <typename T>
+int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y,
+                 const CellState* cs, double* partial, int* nblk_out, cudaStream_t st);
+int launch_load(const LinearHandle& h, const double* s, const double* fe /*(m,24) on device*/, int m,
+                int ncell, double* f, double sign, cudaStream_t st);
+int launch_bilinear(const LinearHandle& h, const double* s, const double* Es /*device (m,6)*/, int m,
+                    int ncell, const double* u, double* Cpart, int* nblk, const double* rho, double* dC,
+                    cudaStream_t st);
+int launch_reduce_C(const LinearHandle& h, const double* Cpart, int nblk, int m, int ncell, double* C,
+                    cudaStream_t st);
+
+// FFT preconditioner: z = w .* irfftn(Kinv rfftn(w .* r)) (w == nullptr: unscaled)
+template <typename T>
+int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
+                   const CellState* cs, double* partial /*[nvec][3][n0][4]: sum z, (r,z), sum r, (r,r)*/,
+                   cudaStream_t st);
+int build_tables(LinearHandle& h);
+
+// vector kernels
+template <typename T>
+int launch_sum3(const LinearHandle& h, int nvec, const T* x, double* partial /*[nvec][3][nb]*/, int* nb,
+                cudaStream_t st);
+int launch_scale_fields(const LinearHandle& h, int ncell, const double* rho, double* s64, float* s32,
+                        double* w64, float* w32, int want_rho_is_s, cudaStream_t st);
+
+// stiffness scale only (s = emin + (1 - emin) clip01(rho)^p)
+int launch_stiffness_scale(const LinearHandle& h, long count, const double* rho, double* s, cudaStream_t st);
+
+template <typename Tin, typename Tout>
+int launch_aos_to_soa(long N, int nvec, const Tin* in, Tout* out, double scale, cudaStream_t st);
+template <typename Tin, typename Tout>
+int launch_soa_to_aos(long N, int nvec, const Tin* in, Tout* out, cudaStream_t st);
+
+}  // namespace nlf

@@ -1,0 +1,881 @@
+// Handle, batched PCG drivers and the C ABI of the small-strain homogenization path (nlfiber/linear.py).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "nlf_vec.cuh"
+
+namespace nlf {
+
+// ---- errors ----------------------------------------------------------------------------------------------------
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int DevBuf::reserve(size_t n) {
+  if (n <= bytes) return NLF_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  const size_t want = n + n / 8;  // grow with slack
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ptr = nullptr;
+    set_error("workspace: cudaMalloc(%zu B) failed: %s", want, cudaGetErrorString(e));
+    return NLF_ECUDA;
+  }
+  bytes = want;
+  return NLF_OK;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+// Bump allocator over a workspace; a first pass with base == nullptr measures the size.
+struct Arena {
+  char* base;
+  size_t off = 0;
+  explicit Arena(void* b) : base((char*)b) {}
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+static bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// ---- host element matrices (nlfiber/linear.py:21-77,108-112) ----------------------------------------------------
+static void element_matrices(LinearHandle& h) {
+  const double g1[2] = {0.5 - 1.0 / (2.0 * std::sqrt(3.0)), 0.5 + 1.0 / (2.0 * std::sqrt(3.0))};
+  double gp[8][3], dN[8][8][3];
+  for (int g = 0; g < 8; ++g) {
+    gp[g][0] = g1[g & 1];
+    gp[g][1] = g1[(g >> 1) & 1];
+    gp[g][2] = g1[(g >> 2) & 1];
+  }
+  for (int g = 0; g < 8; ++g)
+    for (int a = 0; a < 8; ++a) {
+      const int i = a & 1, j = (a >> 1) & 1, k = (a >> 2) & 1;
+      const double x = gp[g][0], y = gp[g][1], z = gp[g][2];
+      const double fx = i ? x : 1 - x, fy = j ? y : 1 - y, fz = k ? z : 1 - z;
+      const double sx = i ? 1 : -1, sy = j ? 1 : -1, sz = k ? 1 : -1;
+      dN[g][a][0] = sx * fy * fz;
+      dN[g][a][1] = fx * sy * fz;
+      dN[g][a][2] = fx * fy * sz;
+    }
+  double D[6][6] = {};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) D[i][j] = h.lam;
+  for (int i = 0; i < 3; ++i) D[i][i] = h.lam + 2 * h.mu;
+  for (int i = 3; i < 6; ++i) D[i][i] = h.mu;
+  std::memcpy(h.Dm, D, sizeof(D));
+  std::memset(h.Ke, 0, sizeof(h.Ke));
+  std::memset(h.Gm, 0, sizeof(h.Gm));
+  for (int g = 0; g < 8; ++g) {
+    double B[6][24] = {};
+    for (int a = 0; a < 8; ++a) {
+      const double dx = dN[g][a][0], dy = dN[g][a][1], dz = dN[g][a][2];
+      const int c = 3 * a;
+      B[0][c] = dx;
+      B[1][c + 1] = dy;
+      B[2][c + 2] = dz;
+      B[3][c + 1] = dz;
+      B[3][c + 2] = dy;
+      B[4][c + 0] = dz;
+      B[4][c + 2] = dx;
+      B[5][c + 0] = dy;
+      B[5][c + 1] = dx;
+    }
+    double DB[6][24] = {};
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 24; ++j)
+        for (int k = 0; k < 6; ++k) DB[i][j] += D[i][k] * B[k][j];
+    for (int i = 0; i < 24; ++i)
+      for (int j = 0; j < 24; ++j)
+        for (int k = 0; k < 6; ++k) h.Ke[i][j] += B[k][i] * DB[k][j] / 8.0;
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 24; ++j) h.Gm[i][j] += DB[i][j] / 8.0;
+  }
+  // 27-point stencil blocks of the unit-stiffness operator: W_d = sum_{a,b: off_a - off_b = d} Ke_ab
+  std::memset(h.W27, 0, sizeof(h.W27));
+  for (int a = 0; a < 8; ++a)
+    for (int b = 0; b < 8; ++b) {
+      const int dx = (a & 1) - (b & 1), dy = ((a >> 1) & 1) - ((b >> 1) & 1), dz = (a >> 2) - (b >> 2);
+      double* W = h.W27[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) W[r * 3 + c] += h.Ke[3 * a + r][3 * b + c];
+    }
+}
+
+// ---- PCG ---------------------------------------------------------------------------------------------------------
+struct PcgCtl {
+  double tol;
+  int maxit;
+  int check_every;
+};
+
+template <typename T>
+struct PcgSet {
+  int ncell = 0, m = 0, nvec = 0;
+  T *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *z = nullptr;
+  cplx<T>* spec = nullptr;
+  const T* s = nullptr;
+  const T* w = nullptr;
+  VecState* vs = nullptr;
+  CellState* cs = nullptr;
+  double *part_ap = nullptr, *part_pc = nullptr, *part_st = nullptr;
+  int* d_count = nullptr;
+};
+
+struct Pinned {
+  int* count = nullptr;
+  Pinned() { cudaMallocHost(&count, sizeof(int)); }
+  ~Pinned() {
+    if (count) cudaFreeHost(count);
+  }
+};
+
+template <typename T>
+static void carve_pcg(Arena& A, const LinearHandle& h, PcgSet<T>& P, int ncell, int m) {
+  P.ncell = ncell;
+  P.m = m;
+  P.nvec = ncell * m;
+  const size_t V = (size_t)P.nvec * 3 * h.g.N;
+  P.x = A.take<T>(V);
+  P.r = A.take<T>(V);
+  P.p = A.take<T>(V);
+  P.Ap = A.take<T>(V);
+  P.z = A.take<T>(V);
+  P.spec = A.take<cplx<T>>((size_t)P.nvec * 3 * h.g.NS);
+  P.vs = A.take<VecState>(P.nvec);
+  P.cs = A.take<CellState>(ncell);
+  // apply partials: tiles * x-chunks <= 4096 blocks per vec
+  P.part_ap = A.take<double>((size_t)P.nvec * 4096 * 4);
+  P.part_pc = A.take<double>((size_t)P.nvec * 3 * h.g.n0 * 4);
+  P.part_st = A.take<double>((size_t)P.nvec * 3 * kStatsBlocks * 2);
+  P.d_count = A.take<int>(4);
+}
+
+template <typename T>
+static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl, cudaStream_t st) {
+  const long N = h.g.N;
+  int nblk = 0;
+  NLF_TRY(launch_mark(P.cs, P.ncell, st));
+  NLF_TRY(launch_apply<T>(h, P.s, P.m, P.nvec, P.p, P.Ap, P.cs, P.part_ap, &nblk, st));
+  NLF_TRY(launch_fin_apply(P.nvec, P.m, P.part_ap, nblk, N, P.vs, P.cs, 0, st));
+  NLF_TRY(launch_xr<T>(N, P.nvec, P.m, P.x, P.r, P.p, P.Ap, P.vs, P.cs, st));
+  NLF_TRY(launch_precond<T>(h, P.nvec, P.m, P.r, P.z, P.spec, P.w, P.cs, P.part_pc, st));
+  NLF_TRY(launch_fin_pc(P.ncell, P.m, h.g.n0, N, P.part_pc, P.vs, P.cs, ctl.tol, ctl.maxit, 0, st));
+  NLF_TRY(launch_p<T>(N, P.nvec, P.m, P.p, P.z, P.vs, P.cs, 0, st));
+  return NLF_OK;
+}
+
+static int count_active(const CellState* cs, int ncell, int* d_count, int* h_count, cudaStream_t st) {
+  NLF_TRY(launch_count_active(cs, ncell, d_count, st));
+  NLF_CUDA_TRY(cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return *h_count;
+}
+
+// Lock-step PCG for K x = b on the mean-free subspace (nlfiber/linear.py:173-203), batched over cells.
+// b: [nvec][3][N] in Tb, already mean-free. x: initial guess if x_given (projected here), else zero.
+// mask: device per-cell flags of the cells to solve (nullptr: all).
+template <typename T, typename Tb>
+static int pcg(const LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, const PcgCtl& ctl, const int* mask,
+               int* h_count, cudaStream_t st) {
+  const long N = h.g.N;
+  NLF_TRY(launch_cs_init(P.cs, P.ncell, mask, st));
+  NLF_TRY(launch_stats<Tb>(h, P.nvec, P.m, b, P.cs, P.part_st, P.vs, 1, st));
+  if (x_given) {
+    NLF_TRY(launch_stats<T>(h, P.nvec, P.m, P.x, P.cs, P.part_st, P.vs, 0, st));
+    NLF_TRY(launch_sub_mean<T>(h, P.nvec, P.m, P.x, P.vs, P.cs, st));
+  } else {
+    NLF_CUDA_TRY(cudaMemsetAsync(P.x, 0, (size_t)P.nvec * 3 * N * sizeof(T), st));
+  }
+  int nblk = 0;
+  NLF_TRY(launch_apply<T>(h, P.s, P.m, P.nvec, P.x, P.Ap, P.cs, P.part_ap, &nblk, st));
+  NLF_TRY(launch_fin_apply(P.nvec, P.m, P.part_ap, nblk, N, P.vs, P.cs, 1, st));
+  NLF_TRY((launch_r_init<Tb, T>(N, P.nvec, P.m, P.r, b, P.Ap, P.vs, P.cs, st)));
+  NLF_TRY(launch_precond<T>(h, P.nvec, P.m, P.r, P.z, P.spec, P.w, P.cs, P.part_pc, st));
+  NLF_TRY(launch_fin_pc(P.ncell, P.m, h.g.n0, N, P.part_pc, P.vs, P.cs, ctl.tol, ctl.maxit, 1, st));
+  NLF_TRY(launch_p<T>(N, P.nvec, P.m, P.p, P.z, P.vs, P.cs, 1, st));
+  int act = count_active(P.cs, P.ncell, P.d_count, h_count, st);
+  if (act < 0) return act;
+  int done = 0;
+  const int every = ctl.check_every > 0 ? ctl.check_every : 1;
+  while (act > 0 && done < ctl.maxit) {
+    for (int k = 0; k < every; ++k) NLF_TRY(pcg_iteration<T>(h, P, ctl, st));
+    done += every;
+    act = count_active(P.cs, P.ncell, P.d_count, h_count, st);
+    if (act < 0) return act;
+  }
+  return NLF_OK;
+}
+
+static bool poison_workspace() {
+  static const bool on = [] {
+    const char* e = std::getenv("NLF_POISON_WORKSPACE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+// ---- a whole solve on staged device inputs ---------------------------------------------------------------------
+struct SolveIn {
+  int ncell, m;
+  const double* s64;  // [ncell][N]
+  const double* b64;  // [ncell][m][3][N], mean-free (nullptr: build from fe = Es G)
+  const double* fe;   // device (m, 24) when b64 == nullptr
+  const double* x0;   // AoS (ncell, m, N, 3) device FP64 or nullptr
+};
+
+static nlf_solve_opts resolve_opts(const LinearHandle& h, const nlf_solve_opts* o) {
+  nlf_solve_opts r;
+  nlf_default_opts(&r);
+  if (o) r = *o;
+  if (r.tol < 0) r.tol = h.tol;
+  if (r.maxit < 0) r.maxit = h.maxit;
+  if (r.check_every < 1) r.check_every = 1;
+  if (r.inner_maxit < 1) r.inner_maxit = 1;
+  if (r.max_sweeps < 1) r.max_sweeps = 1;
+  return r;
+}
+
+// Runs the solve; writes the FP64 corrector (SoA) to `xout` ([ncell][m][3][N]) and iterations to iters_h.
+static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& o, double* xout, int* iters_h,
+                      cudaStream_t st) {
+  const int ncell = in.ncell, m = in.m, nvec = ncell * m;
+  const long N = h.g.N;
+  const size_t V = (size_t)nvec * 3 * N;
+  const bool mixed = o.precision == NLF_PREC_MIXED;
+  const bool scaled = o.precond == NLF_PC_FFT_SCALED;
+  Pinned pin;
+  if (!pin.count) {
+    set_error("cudaMallocHost failed");
+    return NLF_ECUDA;
+  }
+  std::vector<int> it_total(ncell, 0);
+  std::vector<CellState> csh(ncell);
+  for (int pass = 0; pass < 2; ++pass) {
+    Arena A(pass ? h.ws.ptr : nullptr);
+    double* b64 = A.take<double>(V);
+    double* w64 = scaled && !mixed ? A.take<double>((size_t)ncell * N) : nullptr;
+    float* s32 = mixed ? A.take<float>((size_t)ncell * N) : nullptr;
+    float* w32 = mixed && scaled ? A.take<float>((size_t)ncell * N) : nullptr;
+    PcgSet<double> P64;
+    PcgSet<float> P32;
+    double* ax64 = nullptr;
+    VecState* vs_o = nullptr;
+    CellState* cs_o = nullptr;
+    double* part_ap = nullptr;
+    double* part_st = nullptr;
+    int* mask = nullptr;
+    if (!mixed) {
+      carve_pcg<double>(A, h, P64, ncell, m);
+    } else {
+      carve_pcg<float>(A, h, P32, ncell, m);
+      ax64 = A.take<double>(V);
+      vs_o = A.take<VecState>(nvec);
+      cs_o = A.take<CellState>(ncell);
+      part_ap = A.take<double>((size_t)nvec * 4096 * 4);
+      part_st = A.take<double>((size_t)nvec * 3 * kStatsBlocks * 2);
+      mask = A.take<int>(ncell);
+    }
+    if (pass == 0) {
+      NLF_TRY(h.ws.reserve(A.off));
+      continue;
+    }
+    // NLF_POISON_WORKSPACE=1 fills the workspace with NaN first, so that any read of a value the solve has
+    // not written shows up in its result (a debugging aid used by the tests).
+    if (poison_workspace()) NLF_CUDA_TRY(cudaMemsetAsync(h.ws.ptr, 0xFF, A.off, st));
+    // right-hand side b = -proj(load) (nlfiber/linear.py:176,206)
+    if (in.b64) {
+      NLF_CUDA_TRY(cudaMemcpyAsync(b64, in.b64, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+      NLF_TRY(launch_load(h, in.s64, in.fe, m, ncell, b64, -1.0, st));
+    }
+    {
+      // project b (all cells active for this)
+      CellState* cs = mixed ? cs_o : P64.cs;
+      VecState* vs = mixed ? vs_o : P64.vs;
+      double* ps = mixed ? part_st : P64.part_st;
+      NLF_TRY(launch_cs_init(cs, ncell, nullptr, st));
+      NLF_TRY(launch_stats<double>(h, nvec, m, b64, cs, ps, vs, 0, st));
+      NLF_TRY(launch_sub_mean<double>(h, nvec, m, b64, vs, cs, st));
+    }
+    if (!mixed) {
+      P64.s = in.s64;
+      P64.w = w64;
+      if (scaled) NLF_TRY(launch_node_scaling(h, ncell, in.s64, nullptr, w64, nullptr, st));
+      const bool xg = in.x0 != nullptr;
+      if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, P64.x, 1.0, st)));
+      PcgCtl ctl{o.tol, o.maxit, o.check_every};
+      NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, st)));
+      NLF_CUDA_TRY(cudaMemcpyAsync(xout, P64.x, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P64.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
+      NLF_CUDA_TRY(cudaStreamSynchronize(st));
+      int status = NLF_OK;
+      for (int c = 0; c < ncell; ++c) {
+        iters_h[c] = csh[c].it;
+        if (csh[c].active) status = NLF_NOT_CONVERGED;
+      }
+      std::vector<VecState> vsh(nvec);
+      NLF_CUDA_TRY(cudaMemcpy(vsh.data(), P64.vs, nvec * sizeof(VecState), cudaMemcpyDeviceToHost));
+      for (int v = 0; v < nvec; ++v)
+        if (!std::isfinite(vsh[v].rr)) status = NLF_BREAKDOWN;
+      return status;
+    }
+    // ---- mixed precision: FP32 PCG inside FP64 iterative refinement ----
+    NLF_TRY(launch_node_scaling(h, ncell, in.s64, s32, nullptr, w32, st));
+    P32.s = s32;
+    P32.w = w32;
+    double* x64 = xout;
+    NLF_TRY(launch_stats<double>(h, nvec, m, b64, cs_o, part_st, vs_o, 1, st));  // bn
+    if (in.x0) {
+      NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, x64, 1.0, st)));
+      NLF_TRY(launch_stats<double>(h, nvec, m, x64, cs_o, part_st, vs_o, 0, st));
+      NLF_TRY(launch_sub_mean<double>(h, nvec, m, x64, vs_o, cs_o, st));
+    } else {
+      NLF_CUDA_TRY(cudaMemsetAsync(x64, 0, V * sizeof(double), st));
+    }
+    std::vector<VecState> vsh(nvec);
+    std::vector<int> conv(ncell, 0), maskh(ncell, 0);
+    int status = NLF_OK;
+    for (int sweep = 0;; ++sweep) {
+      // r64 = b - proj(K x) in FP64 (the refinement residual)
+      NLF_TRY(launch_cs_init(cs_o, ncell, nullptr, st));
+      int nblk = 0;
+      NLF_TRY(launch_apply<double>(h, in.s64, m, nvec, x64, ax64, cs_o, part_ap, &nblk, st));
+      NLF_TRY(launch_fin_apply(nvec, m, part_ap, nblk, N, vs_o, cs_o, 1, st));
+      NLF_TRY((launch_r_init<double, double>(N, nvec, m, ax64, b64, ax64, vs_o, cs_o, st)));
+      NLF_TRY(launch_stats<double>(h, nvec, m, ax64, cs_o, part_st, vs_o, 2, st));
+      NLF_CUDA_TRY(cudaMemcpyAsync(vsh.data(), vs_o, nvec * sizeof(VecState), cudaMemcpyDeviceToHost, st));
+      NLF_CUDA_TRY(cudaStreamSynchronize(st));
+      int nact = 0;
+      for (int c = 0; c < ncell; ++c) {
+        bool ok = true;
+        for (int I = 0; I < m; ++I) {
+          const VecState& v = vsh[c * m + I];
+          if (!std::isfinite(v.rr)) status = NLF_BREAKDOWN;
+          if (std::sqrt(v.rr) > o.tol * v.bn) ok = false;
+        }
+        conv[c] = ok;
+        maskh[c] = !ok && it_total[c] < o.maxit && sweep < o.max_sweeps;
+        nact += maskh[c];
+      }
+      if (nact == 0 || status == NLF_BREAKDOWN) break;
+      NLF_CUDA_TRY(cudaMemcpyAsync(mask, maskh.data(), ncell * sizeof(int), cudaMemcpyHostToDevice, st));
+      NLF_TRY(launch_cs_init(cs_o, ncell, mask, st));
+      NLF_TRY(launch_r_to32(N, nvec, m, ax64, P32.z, vs_o, cs_o, st));  // P32.z holds the FP32 rhs for init
+      // the FP32 inner solve reads its rhs from a buffer it does not overwrite: use Ap's slot via a copy
+      float* rhs32 = reinterpret_cast<float*>(ax64);  // ax64 is free until the next sweep
+      NLF_CUDA_TRY(cudaMemcpyAsync(rhs32, P32.z, V * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      int cap = o.inner_maxit;
+      for (int c = 0; c < ncell; ++c)
+        if (maskh[c]) cap = std::min(cap, std::max(1, o.maxit - it_total[c]));
+      PcgCtl ctl{o.inner_tol, cap, o.check_every};
+      NLF_TRY((pcg<float, float>(h, P32, rhs32, false, ctl, mask, pin.count, st)));
+      NLF_TRY(launch_x_update(N, nvec, m, x64, P32.x, vs_o, cs_o, st));
+      NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P32.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
+      NLF_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int c = 0; c < ncell; ++c)
+        if (maskh[c]) it_total[c] += csh[c].it;
+    }
+    for (int c = 0; c < ncell; ++c) {
+      iters_h[c] = it_total[c];
+      if (!conv[c] && status == NLF_OK) status = NLF_NOT_CONVERGED;
+    }
+    return status;
+  }
+  return NLF_OK;
+}
+
+}  // namespace nlf
+
+using namespace nlf;
+
+struct nlf_linear {
+  LinearHandle h;
+};
+
+// ---- staging helpers --------------------------------------------------------------------------------------------
+namespace {
+
+// Device view of an input array: the pointer itself when it is device memory, else a copy in `buf`.
+struct InView {
+  const double* d = nullptr;
+};
+
+int stage_in(const double* src, size_t count, DevBuf& buf, size_t buf_off, InView& v, cudaStream_t st) {
+  if (!src) {
+    v.d = nullptr;
+    return NLF_OK;
+  }
+  if (is_device_ptr(src)) {
+    v.d = src;
+    return NLF_OK;
+  }
+  double* dst = reinterpret_cast<double*>((char*)buf.ptr + buf_off);
+  NLF_CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, st));
+  v.d = dst;
+  return NLF_OK;
+}
+
+int copy_out(double* dst, const double* dsrc, size_t count, cudaStream_t st) {
+  NLF_CUDA_TRY(cudaMemcpyAsync(dst, dsrc, count * sizeof(double), is_device_ptr(dst) ? cudaMemcpyDeviceToDevice
+                                                                                      : cudaMemcpyDeviceToHost,
+                               st));
+  return NLF_OK;
+}
+
+size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+bool bad_handle(nlf_linear* h) {
+  if (!h) {
+    set_error("null handle");
+    return true;
+  }
+  return false;
+}
+
+void es_to_fe(const LinearHandle& h, const double* Es, int m, std::vector<double>& fe) {
+  fe.assign((size_t)m * 24, 0.0);
+  for (int I = 0; I < m; ++I)
+    for (int j = 0; j < 24; ++j) {
+      double a = 0.0;
+      for (int i = 0; i < 6; ++i) a += Es[I * 6 + i] * h.Gm[i][j];
+      fe[(size_t)I * 24 + j] = a;
+    }
+}
+
+int host_copy_small(const double* src, size_t count, std::vector<double>& out) {
+  out.resize(count);
+  if (is_device_ptr(src)) {
+    NLF_CUDA_TRY(cudaMemcpy(out.data(), src, count * sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(out.data(), src, count * sizeof(double));
+  }
+  return NLF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+NLF_API const char* nlf_last_error(void) { return g_err; }
+NLF_API const char* nlf_version(void) { return "nlfiber-b200 0.1 (sm_100a)"; }
+
+NLF_API void nlf_default_opts(nlf_solve_opts* o) {
+  if (!o) return;
+  o->precision = NLF_PREC_FP64;
+  o->precond = NLF_PC_FFT;
+  o->tol = -1.0;
+  o->maxit = -1;
+  o->inner_tol = 1e-3;
+  o->inner_maxit = 200;
+  o->max_sweeps = 20;
+  o->check_every = 8;
+  o->use_graphs = 0;
+}
+
+NLF_API int nlf_linear_create(nlf_linear** out, int nx, int ny, int nz, double E, double nu, double emin, double p,
+                              double tol, int maxit) {
+  if (!out || nx < 1 || ny < 1 || nz < 1 || nx > 1024 || ny > 1024 || nz > 1024 || !(E > 0) || !(nu > -1.0) ||
+      !(nu < 0.5) || maxit < 0) {
+    set_error("nlf_linear_create: bad arguments (shape %d x %d x %d, E %g, nu %g, maxit %d)", nx, ny, nz, E, nu,
+              maxit);
+    return NLF_EBADARG;
+  }
+  *out = nullptr;
+  nlf_linear* H = new nlf_linear();
+  LinearHandle& h = H->h;
+  h.g.n0 = nx;
+  h.g.n1 = ny;
+  h.g.n2 = nz;
+  h.g.n2h = nz / 2 + 1;
+  h.g.N = (long)nx * ny * nz;
+  h.g.NS = (long)nx * ny * h.g.n2h;
+  h.E = E;
+  h.nu = nu;
+  h.emin = emin;
+  h.p = p;
+  h.tol = tol;
+  h.maxit = maxit;
+  h.lam = E * nu / ((1 + nu) * (1 - 2 * nu));
+  h.mu = E / (2 * (1 + nu));
+  element_matrices(h);
+  cudaError_t e = cudaGetDevice(&h.dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h.dev);
+  if (e != cudaSuccess) {
+    set_error("nlf_linear_create: %s", cudaGetErrorString(e));
+    delete H;
+    return NLF_ECUDA;
+  }
+  int st = build_tables(h);
+  if (st != NLF_OK) {
+    nlf_linear_destroy(H);
+    return st;
+  }
+  *out = H;
+  return NLF_OK;
+}
+
+NLF_API int nlf_linear_destroy(nlf_linear* H) {
+  if (!H) return NLF_OK;
+  LinearHandle& h = H->h;
+  cudaFree(h.t64.kinv);
+  cudaFree(h.t32.kinv);
+  cudaFree(h.t64.tw);
+  cudaFree(h.t32.tw);
+  h.ws.release();
+  h.io.release();
+  h.io2.release();
+  h.part.release();
+  delete H;
+  return NLF_OK;
+}
+
+NLF_API int nlf_stiffness_scale(nlf_linear* H, int ncell, const double* rho, double* s, void* stream) {
+  if (bad_handle(H) || ncell < 0 || !rho || !s) {
+    set_error("nlf_stiffness_scale: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t cnt = (size_t)ncell * h.g.N;
+  NLF_TRY(h.io.reserve(al(cnt * 8) * 2));
+  InView r;
+  NLF_TRY(stage_in(rho, cnt, h.io, 0, r, st));
+  double* sd = is_device_ptr(s) ? s : reinterpret_cast<double*>((char*)h.io.ptr + al(cnt * 8));
+  NLF_TRY(launch_stiffness_scale(h, (long)cnt, r.d, sd, st));
+  if (sd != s) NLF_TRY(copy_out(s, sd, cnt, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_apply_K_ex(nlf_linear* H, const double* s, int nvec, const double* u, double* y, int precision,
+                           void* stream) {
+  if (bad_handle(H) || nvec < 1 || !s || !u || !y ||
+      (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED)) {
+    set_error("nlf_apply_K: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const size_t V = (size_t)nvec * 3 * N;
+  NLF_TRY(h.io.reserve(2 * al(N * 8) + 3 * al(V * 8)));
+  char* b = (char*)h.io.ptr;
+  InView sv, uv;
+  NLF_TRY(stage_in(s, N, h.io, 0, sv, st));
+  NLF_TRY(stage_in(u, V, h.io, al(N * 8), uv, st));
+  double* xs = reinterpret_cast<double*>(b + al(N * 8) + al(V * 8));
+  double* ys = reinterpret_cast<double*>(b + al(N * 8) + 2 * al(V * 8));
+  double* yd = is_device_ptr(y) ? y : xs;
+  if (precision == NLF_PREC_FP64) {
+    NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, uv.d, xs, 1.0, st)));
+    NLF_TRY(launch_apply<double>(h, sv.d, nvec, nvec, xs, ys, nullptr, nullptr, nullptr, st));
+    NLF_TRY((launch_soa_to_aos<double, double>(N, nvec, ys, yd, st)));
+  } else {
+    float* x32 = reinterpret_cast<float*>(xs);
+    float* y32 = reinterpret_cast<float*>(ys);
+    float* s32 = reinterpret_cast<float*>(b + al(N * 8) + 3 * al(V * 8));
+    NLF_TRY(launch_node_scaling(h, 1, sv.d, s32, nullptr, nullptr, st));
+    NLF_TRY((launch_aos_to_soa<double, float>(N, nvec, uv.d, x32, 1.0, st)));
+    NLF_TRY(launch_apply<float>(h, s32, nvec, nvec, x32, y32, nullptr, nullptr, nullptr, st));
+    NLF_TRY((launch_soa_to_aos<float, double>(N, nvec, y32, yd, st)));
+  }
+  if (yd != y) NLF_TRY(copy_out(y, yd, V, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_apply_K(nlf_linear* H, const double* s, int nvec, const double* u, double* y, void* stream) {
+  return nlf_apply_K_ex(H, s, nvec, u, y, NLF_PREC_FP64, stream);
+}
+
+NLF_API int nlf_load(nlf_linear* H, const double* s, const double* Es, int m, double* f, void* stream) {
+  if (bad_handle(H) || m < 1 || !s || !Es || !f) {
+    set_error("nlf_load: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const size_t V = (size_t)m * 3 * N;
+  std::vector<double> Esh, fe;
+  NLF_TRY(host_copy_small(Es, (size_t)m * 6, Esh));
+  es_to_fe(h, Esh.data(), m, fe);
+  NLF_TRY(h.io.reserve(al(N * 8) + al(fe.size() * 8) + 2 * al(V * 8)));
+  char* b = (char*)h.io.ptr;
+  InView sv;
+  NLF_TRY(stage_in(s, N, h.io, 0, sv, st));
+  double* fed = reinterpret_cast<double*>(b + al(N * 8));
+  NLF_CUDA_TRY(cudaMemcpyAsync(fed, fe.data(), fe.size() * 8, cudaMemcpyHostToDevice, st));
+  double* fs = reinterpret_cast<double*>(b + al(N * 8) + al(fe.size() * 8));
+  double* fa = reinterpret_cast<double*>(b + al(N * 8) + al(fe.size() * 8) + al(V * 8));
+  NLF_TRY(launch_load(h, sv.d, fed, m, 1, fs, 1.0, st));
+  double* fd = is_device_ptr(f) ? f : fa;
+  NLF_TRY((launch_soa_to_aos<double, double>(N, m, fs, fd, st)));
+  if (fd != f) NLF_TRY(copy_out(f, fd, V, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_precond_ex(nlf_linear* H, int nvec, const double* r, double* z, int precision, int precond,
+                           const double* s, void* stream) {
+  if (bad_handle(H) || nvec < 1 || !r || !z || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) ||
+      (precond != NLF_PC_FFT && precond != NLF_PC_FFT_SCALED) || (precond == NLF_PC_FFT_SCALED && !s)) {
+    set_error("nlf_precond: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const size_t V = (size_t)nvec * 3 * N;
+  const size_t S = (size_t)nvec * 3 * h.g.NS * 2;
+  NLF_TRY(h.io.reserve(3 * al(V * 8) + al(S * 8) + 3 * al(N * 8)));
+  char* b = (char*)h.io.ptr;
+  InView rv, sv;
+  NLF_TRY(stage_in(r, V, h.io, 0, rv, st));
+  const size_t o_s = 3 * al(V * 8) + al(S * 8);
+  NLF_TRY(stage_in(s, N, h.io, o_s, sv, st));
+  void* wbuf = b + o_s + al(N * 8);
+  const bool scaled = precond == NLF_PC_FFT_SCALED;
+  double* rs = reinterpret_cast<double*>(b + al(V * 8));
+  double* zs = reinterpret_cast<double*>(b + 2 * al(V * 8));
+  double* zd = is_device_ptr(z) ? z : rs;
+  if (precision == NLF_PREC_FP64) {
+    double* w = scaled ? reinterpret_cast<double*>(wbuf) : nullptr;
+    if (scaled) NLF_TRY(launch_node_scaling(h, 1, sv.d, nullptr, w, nullptr, st));
+    cplx<double>* spec = reinterpret_cast<cplx<double>*>(b + 3 * al(V * 8));
+    NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, rv.d, rs, 1.0, st)));
+    NLF_TRY(launch_precond<double>(h, nvec, nvec, rs, zs, spec, w, nullptr, nullptr, st));  // one cell
+    NLF_TRY((launch_soa_to_aos<double, double>(N, nvec, zs, zd, st)));
+  } else {
+    float* w = scaled ? reinterpret_cast<float*>(wbuf) : nullptr;
+    if (scaled) NLF_TRY(launch_node_scaling(h, 1, sv.d, nullptr, nullptr, w, st));
+    cplx<float>* spec = reinterpret_cast<cplx<float>*>(b + 3 * al(V * 8));
+    float* r32 = reinterpret_cast<float*>(rs);
+    float* z32 = reinterpret_cast<float*>(zs);
+    NLF_TRY((launch_aos_to_soa<double, float>(N, nvec, rv.d, r32, 1.0, st)));
+    NLF_TRY(launch_precond<float>(h, nvec, nvec, r32, z32, spec, w, nullptr, nullptr, st));  // one cell
+    NLF_TRY((launch_soa_to_aos<float, double>(N, nvec, z32, zd, st)));
+  }
+  if (zd != z) NLF_TRY(copy_out(z, zd, V, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_precond(nlf_linear* H, int nvec, const double* r, double* z, void* stream) {
+  return nlf_precond_ex(H, nvec, r, z, NLF_PREC_FP64, NLF_PC_FFT, nullptr, stream);
+}
+
+static int solve_entry(nlf_linear* H, int ncell, const double* s, const double* Es, const double* bsrc, int m,
+                       const double* u0, double* u, int* iters, const nlf_solve_opts* opts, void* stream) {
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const int nvec = ncell * m;
+  const size_t V = (size_t)nvec * 3 * N;
+  const nlf_solve_opts o = resolve_opts(h, opts);
+  std::vector<double> fe;
+  if (Es) {
+    std::vector<double> Esh;
+    NLF_TRY(host_copy_small(Es, (size_t)m * 6, Esh));
+    es_to_fe(h, Esh.data(), m, fe);
+  }
+  // io: s | fe | b (SoA) | u0 (AoS) | x (SoA) | u (AoS)
+  const size_t o_s = 0, o_fe = al((size_t)ncell * N * 8), o_b = o_fe + al(m * 24 * 8 + 8);
+  const size_t o_u0 = o_b + (bsrc ? al(V * 8) : 0);
+  const size_t o_x = o_u0 + (u0 && !is_device_ptr(u0) ? al(V * 8) : 0);
+  const size_t o_u = o_x + al(V * 8);
+  NLF_TRY(h.io.reserve(o_u + al(V * 8)));
+  char* b = (char*)h.io.ptr;
+  InView sv, u0v;
+  NLF_TRY(stage_in(s, (size_t)ncell * N, h.io, o_s, sv, st));
+  double* fed = reinterpret_cast<double*>(b + o_fe);
+  if (Es) NLF_CUDA_TRY(cudaMemcpyAsync(fed, fe.data(), fe.size() * 8, cudaMemcpyHostToDevice, st));
+  double* bsoa = nullptr;
+  if (bsrc) {
+    InView bv;
+    NLF_TRY(stage_in(bsrc, V, h.io, o_x, bv, st));  // staging through the x slot, converted below
+    bsoa = reinterpret_cast<double*>(b + o_b);
+    NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, bv.d, bsoa, 1.0, st)));
+  }
+  NLF_TRY(stage_in(u0, V, h.io, o_u0, u0v, st));
+  double* xs = reinterpret_cast<double*>(b + o_x);
+  SolveIn in{ncell, m, sv.d, bsoa, fed, u0v.d};
+  std::vector<int> it(ncell, 0);
+  int status = solve_core(h, in, o, xs, it.data(), st);
+  if (status < 0) return status;
+  double* ud = is_device_ptr(u) ? u : reinterpret_cast<double*>(b + o_u);
+  NLF_TRY((launch_soa_to_aos<double, double>(N, nvec, xs, ud, st)));
+  if (ud != u) NLF_TRY(copy_out(u, ud, V, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  if (iters) {
+    if (is_device_ptr(iters)) {
+      NLF_CUDA_TRY(cudaMemcpy(iters, it.data(), ncell * sizeof(int), cudaMemcpyHostToDevice));
+    } else {
+      std::memcpy(iters, it.data(), ncell * sizeof(int));
+    }
+  }
+  return status;
+}
+
+NLF_API int nlf_linear_solve(nlf_linear* H, int ncell, const double* s, const double* Es, int m, const double* u0,
+                             double* u, int* iters, const nlf_solve_opts* opts, void* stream) {
+  if (bad_handle(H) || ncell < 1 || m < 1 || !s || !Es || !u) {
+    set_error("nlf_linear_solve: bad arguments");
+    return NLF_EBADARG;
+  }
+  return solve_entry(H, ncell, s, Es, nullptr, m, u0, u, iters, opts, stream);
+}
+
+NLF_API int nlf_linear_solve_rhs(nlf_linear* H, int ncell, const double* s, int m, const double* b, double* u,
+                                 int* iters, const nlf_solve_opts* opts, void* stream) {
+  if (bad_handle(H) || ncell < 1 || m < 1 || !s || !b || !u) {
+    set_error("nlf_linear_solve_rhs: bad arguments");
+    return NLF_EBADARG;
+  }
+  return solve_entry(H, ncell, s, nullptr, b, m, nullptr, u, iters, opts, stream);
+}
+
+static int bilinear_entry(nlf_linear* H, int ncell, const double* s, const double* rho, const double* Es, int m,
+                          const double* u, double* C, double* dC, void* stream) {
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const int nvec = ncell * m;
+  const size_t V = (size_t)nvec * 3 * N;
+  std::vector<double> Esh;
+  NLF_TRY(host_copy_small(Es, (size_t)m * 6, Esh));
+  std::vector<double> EsEDE((size_t)m * 6 + (size_t)m * m);
+  for (int i = 0; i < m * 6; ++i) EsEDE[i] = Esh[i];
+  for (int I = 0; I < m; ++I)
+    for (int J = 0; J < m; ++J) {
+      double a = 0.0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) a += Esh[I * 6 + i] * h.Dm[i][j] * Esh[J * 6 + j];
+      EsEDE[(size_t)m * 6 + I * m + J] = a;
+    }
+  const int nb = (int)((N + 127) / 128);
+  const size_t o_s = 0, o_r = al((size_t)ncell * N * 8), o_u = o_r + al((size_t)ncell * N * 8);
+  const size_t o_us = o_u + al(V * 8), o_e = o_us + al(V * 8), o_cp = o_e + al(EsEDE.size() * 8);
+  const size_t o_c = o_cp + al((size_t)ncell * nb * 21 * 8);
+  const size_t o_dc = o_c + al((size_t)ncell * m * m * 8);
+  const size_t dcount = dC ? (size_t)ncell * m * m * N : 0;
+  NLF_TRY(h.io.reserve(o_dc + al(dcount * 8) + 256));
+  char* b = (char*)h.io.ptr;
+  InView sv, rv, uv;
+  double* sd = nullptr;
+  if (rho) {
+    NLF_TRY(stage_in(rho, (size_t)ncell * N, h.io, o_r, rv, st));
+    sd = reinterpret_cast<double*>(b + o_s);
+    NLF_TRY(launch_stiffness_scale(h, (long)ncell * N, rv.d, sd, st));
+  } else {
+    NLF_TRY(stage_in(s, (size_t)ncell * N, h.io, o_s, sv, st));
+    sd = const_cast<double*>(sv.d);
+  }
+  NLF_TRY(stage_in(u, V, h.io, o_u, uv, st));
+  double* us = reinterpret_cast<double*>(b + o_us);
+  NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, uv.d, us, 1.0, st)));
+  double* ed = reinterpret_cast<double*>(b + o_e);
+  NLF_CUDA_TRY(cudaMemcpyAsync(ed, EsEDE.data(), EsEDE.size() * 8, cudaMemcpyHostToDevice, st));
+  double* cp = reinterpret_cast<double*>(b + o_cp);
+  double* cd = reinterpret_cast<double*>(b + o_c);
+  double* dcd = dC ? (is_device_ptr(dC) ? dC : reinterpret_cast<double*>(b + o_dc)) : nullptr;
+  int nblk = 0;
+  NLF_TRY(launch_bilinear(h, sd, ed, m, ncell, us, cp, &nblk, rho ? rv.d : nullptr, dcd, st));
+  NLF_TRY(launch_reduce_C(h, cp, nblk, m, ncell, cd, st));
+  if (C) NLF_TRY(copy_out(C, cd, (size_t)ncell * m * m, st));
+  if (dC && dcd != dC) NLF_TRY(copy_out(dC, dcd, dcount, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_bilinear(nlf_linear* H, int ncell, const double* s, const double* Es, int m, const double* u,
+                         double* C, void* stream) {
+  if (bad_handle(H) || ncell < 1 || m < 1 || m > 6 || !s || !Es || !u || !C) {
+    set_error("nlf_bilinear: bad arguments (1 <= m <= 6)");
+    return NLF_EBADARG;
+  }
+  return bilinear_entry(H, ncell, s, nullptr, Es, m, u, C, nullptr, stream);
+}
+
+NLF_API int nlf_dC_drho(nlf_linear* H, int ncell, const double* rho, const double* Es, int m, const double* u,
+                        double* dC, void* stream) {
+  if (bad_handle(H) || ncell < 1 || m < 1 || m > 6 || !rho || !Es || !u || !dC) {
+    set_error("nlf_dC_drho: bad arguments (1 <= m <= 6)");
+    return NLF_EBADARG;
+  }
+  return bilinear_entry(H, ncell, nullptr, rho, Es, m, u, nullptr, dC, stream);
+}
+
+NLF_API int nlf_C_full(nlf_linear* H, int ncell, const double* rho, const double* u0, double* C, double* u,
+                       double* dC, int* iters, const nlf_solve_opts* opts, void* stream) {
+  if (bad_handle(H) || ncell < 1 || !rho || !C) {
+    set_error("nlf_C_full: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const int m = 6;
+  const size_t V = (size_t)ncell * m * 3 * N;
+  // separate staging (io2) so that the solve's own io staging does not clobber rho / s / u
+  NLF_TRY(h.io2.reserve(2 * al((size_t)ncell * N * 8) + al(V * 8)));
+  char* b = (char*)h.io2.ptr;
+  InView rv;
+  NLF_TRY(stage_in(rho, (size_t)ncell * N, h.io2, 0, rv, st));
+  double* sd = reinterpret_cast<double*>(b + al((size_t)ncell * N * 8));
+  NLF_TRY(launch_stiffness_scale(h, (long)ncell * N, rv.d, sd, st));
+  double* ud = (u && is_device_ptr(u)) ? u : reinterpret_cast<double*>(b + 2 * al((size_t)ncell * N * 8));
+  double eye[36] = {};
+  for (int i = 0; i < 6; ++i) eye[i * 6 + i] = 1.0;
+  int status = nlf_linear_solve(H, ncell, sd, eye, m, u0, ud, iters, opts, stream);
+  if (status < 0) return status;
+  int s2 = bilinear_entry(H, ncell, sd, dC ? rv.d : nullptr, eye, m, ud, C, dC, stream);
+  if (s2 < 0) return s2;
+  if (u && ud != u) {
+    NLF_TRY(copy_out(u, ud, V, st));
+    NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  return status;
+}
+
+NLF_API int nlf_precond_symbol(nlf_linear* H, double* kinv6) {
+  if (bad_handle(H) || !kinv6) {
+    set_error("nlf_precond_symbol: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  NLF_CUDA_TRY(cudaMemcpy(kinv6, h.t64.kinv, h.g.NS * 6 * sizeof(double),
+                          is_device_ptr(kinv6) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+  return NLF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,457 @@
+// Elementwise and reduction kernels of the batched lock-step PCG (nlfiber/linear.py:173-203).
+//
+// Every vector is [vec][comp][N]; vec = cell * m + case. Reductions write per-CTA FP64 partials that a
+// finalize kernel sums in a fixed order (deterministic). A cell whose CellState.active is 0 is skipped by
+// every kernel, which reproduces the reference's lock-step `while_loop` per cell inside a batch of cells.
+#include "nlf_vec.cuh"
+
+namespace nlf {
+
+// ---- layout conversion -------------------------------------------------------------------------------------
+template <typename Tin, typename Tout>
+__global__ void k_aos_to_soa(long N, const Tin* __restrict__ in, Tout* __restrict__ out, double scale) {
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long vec = blockIdx.y;
+  if (n >= N) return;
+  const Tin* p = in + (vec * N + n) * 3;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[(vec * 3 + c) * N + n] = (Tout)((double)p[c] * scale);
+}
+
+template <typename Tin, typename Tout>
+__global__ void k_soa_to_aos(long N, const Tin* __restrict__ in, Tout* __restrict__ out) {
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long vec = blockIdx.y;
+  if (n >= N) return;
+  Tout* p = out + (vec * N + n) * 3;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) p[c] = (Tout)in[(vec * 3 + c) * N + n];
+}
+
+template <typename Tin, typename Tout>
+int launch_aos_to_soa(long N, int nvec, const Tin* in, Tout* out, double scale, cudaStream_t st) {
+  if (nvec == 0) return NLF_OK;
+  k_aos_to_soa<Tin, Tout><<<dim3((unsigned)((N + 255) / 256), nvec), 256, 0, st>>>(N, in, out, scale);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template <typename Tin, typename Tout>
+int launch_soa_to_aos(long N, int nvec, const Tin* in, Tout* out, cudaStream_t st) {
+  if (nvec == 0) return NLF_OK;
+  k_soa_to_aos<Tin, Tout><<<dim3((unsigned)((N + 255) / 256), nvec), 256, 0, st>>>(N, in, out);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template int launch_aos_to_soa<double, double>(long, int, const double*, double*, double, cudaStream_t);
+template int launch_aos_to_soa<double, float>(long, int, const double*, float*, double, cudaStream_t);
+template int launch_soa_to_aos<double, double>(long, int, const double*, double*, cudaStream_t);
+template int launch_soa_to_aos<float, double>(long, int, const float*, double*, cudaStream_t);
+
+// ---- stiffness scale, node scaling of the scaled preconditioner -----------------------------------------------
+__device__ __forceinline__ double clip01(double r) { return r > 1.0 ? 1.0 : (r < 0.0 ? 0.0 : r); }
+
+__global__ void k_stiffness_scale(long count, const double* __restrict__ rho, double* __restrict__ s, double emin,
+                                  double p) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < count) s[i] = emin + (1.0 - emin) * pow(clip01(rho[i]), p);
+}
+
+int launch_stiffness_scale(const LinearHandle& h, long count, const double* rho, double* s, cudaStream_t st) {
+  if (count == 0) return NLF_OK;
+  k_stiffness_scale<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, rho, s, h.emin, h.p);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// s32 = (float) s; w = 1 / sqrt(mean of s over the 8 elements around each node)
+__global__ void k_node_scaling(int n0, int n1, int n2, const double* __restrict__ s, float* __restrict__ s32,
+                               double* __restrict__ w64, float* __restrict__ w32) {
+  const long N = (long)n0 * n1 * n2;
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int cell = blockIdx.y;
+  if (n >= N) return;
+  const double* sv = s + (long)cell * N;
+  if (s32) s32[(long)cell * N + n] = (float)sv[n];
+  if (w64 || w32) {
+    const int k = (int)(n % n2), j = (int)((n / n2) % n1), i = (int)(n / ((long)n1 * n2));
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int ii = wrap(i - (a & 1), n0), jj = wrap(j - ((a >> 1) & 1), n1), kk = wrap(k - (a >> 2), n2);
+      acc += sv[((long)ii * n1 + jj) * n2 + kk];
+    }
+    const double w = 1.0 / sqrt(acc * 0.125);
+    if (w64) w64[(long)cell * N + n] = w;
+    if (w32) w32[(long)cell * N + n] = (float)w;
+  }
+}
+
+int launch_node_scaling(const LinearHandle& h, int ncell, const double* s, float* s32, double* w64, float* w32,
+                        cudaStream_t st) {
+  if (ncell == 0) return NLF_OK;
+  k_node_scaling<<<dim3((unsigned)((h.g.N + 255) / 256), ncell), 256, 0, st>>>(h.g.n0, h.g.n1, h.g.n2, s, s32,
+                                                                               w64, w32);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// ---- statistics: per (vec, comp) sum and sum of squares ------------------------------------------------------
+template <typename T>
+__global__ void k_stats(long N, const T* __restrict__ x, const CellState* __restrict__ cs, int m,
+                        double* __restrict__ partial) {
+  __shared__ double red[32 * 2];
+  const int c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  const T* p = x + ((long)vec * 3 + c) * N;
+  double acc[2] = {0.0, 0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double v = (double)p[i];
+    acc[0] += v;
+    acc[1] += v * v;
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) {
+    double* o = partial + (((long)vec * 3 + c) * gridDim.x + blockIdx.x) * 2;
+    o[0] = acc[0];
+    o[1] = acc[1];
+  }
+}
+
+// what: 0 -> mean[c] = sum_c / N; 1 -> bn = sqrt(sum of squares) + 1e-300; 2 -> rr = sum of squares
+__global__ void k_fin_stats(const double* __restrict__ partial, int nb, long N, int nvec, VecState* __restrict__ vs,
+                            const CellState* __restrict__ cs, int m, int what) {
+  const int vec = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (vec >= nvec) return;
+  if (cs && !cs[vec / m].active) return;
+  double s[3] = {0, 0, 0}, q = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    for (int b = lane; b < nb; b += 32) {
+      const double* o = partial + (((long)vec * 3 + c) * nb + b) * 2;
+      s[c] += o[0];
+      q += o[1];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s[0] += __shfl_down_sync(0xffffffffu, s[0], o);
+    s[1] += __shfl_down_sync(0xffffffffu, s[1], o);
+    s[2] += __shfl_down_sync(0xffffffffu, s[2], o);
+    q += __shfl_down_sync(0xffffffffu, q, o);
+  }
+  if (lane == 0) {
+    if (what == 0) {
+      vs[vec].mean[0] = s[0] / (double)N;
+      vs[vec].mean[1] = s[1] / (double)N;
+      vs[vec].mean[2] = s[2] / (double)N;
+    } else if (what == 1) {
+      vs[vec].bn = sqrt(q) + 1e-300;
+    } else {
+      vs[vec].rr = q;
+    }
+  }
+}
+
+template <typename T>
+int launch_stats(const LinearHandle& h, int nvec, int m, const T* x, const CellState* cs, double* partial,
+                 VecState* vs, int what, cudaStream_t st) {
+  if (nvec == 0) return NLF_OK;
+  const int nb = kStatsBlocks;
+  k_stats<T><<<dim3(nb, 3, nvec), 256, 0, st>>>(h.g.N, x, cs, m, partial);
+  NLF_CHECK_LAUNCH();
+  k_fin_stats<<<(nvec + 7) / 8, 256, 0, st>>>(partial, nb, h.g.N, nvec, vs, cs, m, what);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template int launch_stats<float>(const LinearHandle&, int, int, const float*, const CellState*, double*, VecState*,
+                                 int, cudaStream_t);
+template int launch_stats<double>(const LinearHandle&, int, int, const double*, const CellState*, double*,
+                                  VecState*, int, cudaStream_t);
+
+// x[c] -= mean[c]
+template <typename T>
+__global__ void k_sub_mean(long N, T* __restrict__ x, const VecState* __restrict__ vs,
+                           const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const T mu = (T)vs[vec].mean[c];
+  T* p = x + ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) p[i] -= mu;
+}
+
+template <typename T>
+int launch_sub_mean(const LinearHandle& h, int nvec, int m, T* x, const VecState* vs, const CellState* cs,
+                    cudaStream_t st) {
+  if (nvec == 0) return NLF_OK;
+  const int nb = (int)std::min<long>((h.g.N + 255) / 256, 256);
+  k_sub_mean<T><<<dim3(nb, 3, nvec), 256, 0, st>>>(h.g.N, x, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template int launch_sub_mean<float>(const LinearHandle&, int, int, float*, const VecState*, const CellState*,
+                                    cudaStream_t);
+template int launch_sub_mean<double>(const LinearHandle&, int, int, double*, const VecState*, const CellState*,
+                                     cudaStream_t);
+
+// ---- PCG steps ---------------------------------------------------------------------------------------------
+// After the apply: mean[c] of Ap, pAp = (p, Ap - mean) and alpha = rz / pAp (pAp == 0 -> 1).
+// init = 1: only the means (r = b - proj(A x) at the start).
+__global__ void k_fin_apply(const double* __restrict__ partial, int nblk, long N, int nvec, VecState* __restrict__ vs,
+                            const CellState* __restrict__ cs, int m, int init) {
+  const int vec = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (vec >= nvec) return;
+  if (cs && !cs[vec / m].active) return;
+  double a[4] = {0, 0, 0, 0};
+  for (int b = lane; b < nblk; b += 32) {
+    const double* o = partial + ((long)vec * nblk + b) * 4;
+    a[0] += o[0];
+    a[1] += o[1];
+    a[2] += o[2];
+    a[3] += o[3];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_down_sync(0xffffffffu, a[k], o);
+  if (lane == 0) {
+    VecState& v = vs[vec];
+    v.mean[0] = a[0] / (double)N;
+    v.mean[1] = a[1] / (double)N;
+    v.mean[2] = a[2] / (double)N;
+    if (!init) {
+      const double pAp = a[3];  // (p, Ap - mean Ap) = (p, Ap) since p is mean-free
+      v.alpha = v.rz / (pAp == 0.0 ? 1.0 : pAp);
+    }
+  }
+}
+
+// x += alpha p; r -= alpha (Ap - mean)
+template <typename T>
+__global__ void k_xr(long N, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ Ap,
+                     const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const T al = (T)vs[vec].alpha, mu = (T)vs[vec].mean[c];
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    x[off + i] += al * p[off + i];
+    r[off + i] -= al * (Ap[off + i] - mu);
+  }
+}
+
+// r = b - (Ax - mean)
+template <typename Tb, typename T>
+__global__ void k_r_init(long N, T* __restrict__ r, const Tb* __restrict__ b, const T* __restrict__ Ax,
+                         const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const double mu = vs[vec].mean[c];
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    r[off + i] = (T)((double)b[off + i] - ((double)Ax[off + i] - mu));
+}
+
+// After the preconditioner: mean[c] of z, rz1 = (r, z - mean z), rr = (r, r); per-cell lock-step control.
+// One block per cell, one warp per case. init = 1: rz = rz1, it stays 0. Otherwise beta = rz1 / rz, it += 1.
+// active = it < maxit && any case with sqrt(rr) > tol * bn (nlfiber/linear.py:185-188).
+__global__ void k_fin_pc(const double* __restrict__ partial, int n0, long N, VecState* __restrict__ vs,
+                         CellState* __restrict__ cs, int m, double tol, int maxit, int init) {
+  __shared__ int go;
+  const int cell = blockIdx.x;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (!cs[cell].active) return;
+  if (threadIdx.x == 0) go = 0;
+  __syncthreads();
+  if (wid < m) {
+    const int vec = cell * m + wid;
+    double a[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[c][k] = 0.0;
+    for (int c = 0; c < 3; ++c)
+      for (int x = lane; x < n0; x += 32) {
+        const double* o = partial + (((long)vec * 3 + c) * n0 + x) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a[c][k] += o[k];
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[c][k] += __shfl_down_sync(0xffffffffu, a[c][k], o);
+    if (lane == 0) {
+      VecState& v = vs[vec];
+      double rz1 = 0.0, rr = 0.0;
+      for (int c = 0; c < 3; ++c) {
+        const double mz = a[c][0] / (double)N;
+        v.mean[c] = mz;
+        rz1 += a[c][1] - mz * a[c][2];
+        rr += a[c][3];
+      }
+      if (!init) v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
+      v.rz = rz1;
+      v.rr = rr;
+      if (sqrt(rr) > tol * v.bn) atomicOr(&go, 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CellState& s = cs[cell];
+    if (!init) s.it += 1;
+    s.active = (s.it < maxit) && go;
+  }
+}
+
+// p = (z - mean z) + beta p   (init: p = z - mean z). Runs for cells active at the start of the iteration,
+// which is signalled by `was` (the pre-iteration flag kept in CellState.status bit 1).
+template <typename T>
+__global__ void k_p(long N, T* __restrict__ p, const T* __restrict__ z, const VecState* __restrict__ vs,
+                    const CellState* __restrict__ cs, int m, int init) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !(cs[vec / m].status & 2)) return;
+  const T be = (T)vs[vec].beta, mu = (T)vs[vec].mean[c];
+  const long off = ((long)vec * 3 + c) * N;
+  if (init) {  // p is not read: it holds stale workspace contents
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+      p[off + i] = z[off + i] - mu;
+  } else {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+      p[off + i] = (z[off + i] - mu) + be * p[off + i];
+  }
+}
+
+// status bit 1 <- active (marks the cells that run the current iteration, for k_p after k_fin_pc)
+__global__ void k_mark(CellState* cs, int ncell) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncell) cs[c].status = (cs[c].status & ~2) | (cs[c].active ? 2 : 0);
+}
+
+__global__ void k_cs_init(CellState* cs, int ncell, const int* __restrict__ mask) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncell) {
+    cs[c].it = 0;
+    cs[c].active = mask ? mask[c] : 1;
+    cs[c].status = cs[c].active ? 2 : 0;
+  }
+}
+
+__global__ void k_count_active(const CellState* __restrict__ cs, int ncell, int* __restrict__ out) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int local = 0;
+  for (int c = threadIdx.x; c < ncell; c += blockDim.x) local += cs[c].active ? 1 : 0;
+  atomicAdd(&cnt, local);
+  __syncthreads();
+  if (threadIdx.x == 0) *out = cnt;
+}
+
+// ---- mixed precision refinement -----------------------------------------------------------------------------
+// scale = sqrt(rr) (1 if 0); r32 = r64 / scale
+__global__ void k_r_to32(long N, const double* __restrict__ r64, float* __restrict__ r32, VecState* __restrict__ vs,
+                         const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const double rr = vs[vec].rr;
+  const double sc = rr > 0.0 ? sqrt(rr) : 1.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && c == 0) vs[vec].scale = sc;
+  const double inv = 1.0 / sc;
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    r32[off + i] = (float)(r64[off + i] * inv);
+}
+
+// x64 += scale * x32
+__global__ void k_x_update(long N, double* __restrict__ x64, const float* __restrict__ x32,
+                           const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const double sc = vs[vec].scale;
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    x64[off + i] += sc * (double)x32[off + i];
+}
+
+// ---- launch helpers ----------------------------------------------------------------------------------------
+static inline dim3 vec_grid(long N, int nvec) {
+  return dim3((unsigned)std::min<long>((N + 255) / 256, 512), 3, nvec);
+}
+
+int launch_fin_apply(int nvec, int m, const double* partial, int nblk, long N, VecState* vs, const CellState* cs,
+                     int init, cudaStream_t st) {
+  k_fin_apply<<<(nvec + 7) / 8, 256, 0, st>>>(partial, nblk, N, nvec, vs, cs, m, init);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template <typename T>
+int launch_xr(long N, int nvec, int m, T* x, T* r, const T* p, const T* Ap, const VecState* vs, const CellState* cs,
+              cudaStream_t st) {
+  k_xr<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, x, r, p, Ap, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template <typename Tb, typename T>
+int launch_r_init(long N, int nvec, int m, T* r, const Tb* b, const T* Ax, const VecState* vs, const CellState* cs,
+                  cudaStream_t st) {
+  k_r_init<Tb, T><<<vec_grid(N, nvec), 256, 0, st>>>(N, r, b, Ax, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_fin_pc(int ncell, int m, int n0, long N, const double* partial, VecState* vs, CellState* cs, double tol,
+                  int maxit, int init, cudaStream_t st) {
+  k_fin_pc<<<ncell, 32 * m, 0, st>>>(partial, n0, N, vs, cs, m, tol, maxit, init);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template <typename T>
+int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, const CellState* cs, int init,
+             cudaStream_t st) {
+  k_p<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, p, z, vs, cs, m, init);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_mark(CellState* cs, int ncell, cudaStream_t st) {
+  k_mark<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_cs_init(CellState* cs, int ncell, const int* mask, cudaStream_t st) {
+  k_cs_init<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell, mask);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_count_active(const CellState* cs, int ncell, int* out, cudaStream_t st) {
+  k_count_active<<<1, 256, 0, st>>>(cs, ncell, out);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_r_to32(long N, int nvec, int m, const double* r64, float* r32, VecState* vs, const CellState* cs,
+                  cudaStream_t st) {
+  k_r_to32<<<vec_grid(N, nvec), 256, 0, st>>>(N, r64, r32, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+int launch_x_update(long N, int nvec, int m, double* x64, const float* x32, const VecState* vs, const CellState* cs,
+                    cudaStream_t st) {
+  k_x_update<<<vec_grid(N, nvec), 256, 0, st>>>(N, x64, x32, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+template int launch_xr<float>(long, int, int, float*, float*, const float*, const float*, const VecState*,
+                              const CellState*, cudaStream_t);
+template int launch_xr<double>(long, int, int, double*, double*, const double*, const double*, const VecState*,
+                               const CellState*, cudaStream_t);
+template int launch_r_init<double, double>(long, int, int, double*, const double*, const double*, const VecState*,
+                                           const CellState*, cudaStream_t);
+template int launch_r_init<float, float>(long, int, int, float*, const float*, const float*, const VecState*,
+                                         const CellState*, cudaStream_t);
+template int launch_p<float>(long, int, int, float*, const float*, const VecState*, const CellState*, int,
+                             cudaStream_t);
+template int launch_p<double>(long, int, int, double*, const double*, const VecState*, const CellState*, int,
+                              cudaStream_t);
+
+}  // namespace nlf

@@ -1,0 +1,181 @@
+"""Parity of the CUDA small-strain path (libnlf.so through nlfiber_b200.linear) with the NumPy FP64 oracle
+(a restatement of nlfiber/linear.py) and the reference's own known-answer tests (tests/test_core.py:78-142 of
+the reference). Tolerances are written per test; FP64 operators agree with the oracle to rounding."""
+import os
+
+# every solve starts from a NaN-filled workspace, so reads of unwritten values fail the tests
+os.environ.setdefault("NLF_POISON_WORKSPACE", "1")
+
+import numpy as np  # noqa: E402
+import pytest  # noqa: E402
+
+from oracle import density_ref as OD
+from oracle import linear_ref as OL
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "linear_golden.npz")
+
+
+@pytest.fixture(scope="module")
+def L():
+    from nlfiber_b200 import linear
+    return linear
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+SHAPES = [(8, 8, 8), (6, 6, 6), (4, 8, 16), (12, 10, 6), (16, 16, 16), (32, 32, 32), (8, 8, 1), (5, 7, 3)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_apply_load_precond_symbol(L, shape):
+    rng = np.random.default_rng(1)
+    s = 1e-3 + rng.random(shape)
+    u = rng.standard_normal((3,) + shape + (3,))
+    lh, oh = L.LinearHomogenization(shape), OL.LinearHomogenization(shape)
+    assert rel(lh.apply_K(s, u), np.stack([oh.apply_K(s, x) for x in u])) < 1e-13
+    Es = rng.standard_normal((4, 6))
+    assert rel(lh.load(s, Es), oh.load(s, Es)) < 1e-13
+    assert rel(lh.Kinv, oh.Kinv) < 1e-12
+    assert rel(lh.precond(u), oh.precond(u)) < 1e-12
+
+
+def _scaled_oracle(oh, s, r):
+    sn = sum(np.roll(s, shift=tuple(off), axis=(0, 1, 2)) for off in OL.NODES) / 8.0
+    w = (1.0 / np.sqrt(sn))[..., None]
+    return w * oh.precond(w * r)
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (6, 6, 6), (8, 8, 1)])
+def test_fp32_and_scaled_operators(L, shape):
+    """The FP32 operators of the mixed-precision solver agree with the FP64 oracle to FP32 rounding
+    (rel 2e-6); the FP64 scaled preconditioner to FP64 rounding."""
+    rng = np.random.default_rng(2)
+    s = 1e-3 + rng.random(shape)
+    u = rng.standard_normal((2,) + shape + (3,))
+    lh, oh = L.LinearHomogenization(shape), OL.LinearHomogenization(shape)
+    Ku = np.stack([oh.apply_K(s, x) for x in u])
+    assert rel(lh.apply_K(s, u, precision="mixed"), Ku) < 2e-6
+    assert rel(lh.precond(u, precision="mixed"), oh.precond(u)) < 2e-6
+    zs = _scaled_oracle(oh, s, u)
+    assert rel(lh.precond(u, precond="scaled", s=s), zs) < 1e-12
+    assert rel(lh.precond(u, precision="mixed", precond="scaled", s=s), zs) < 2e-6
+
+
+def test_mixed_low_contrast_matches_fp64(L):
+    rho = OD.grey_cell(4)
+    lh = L.LinearHomogenization(rho.shape, tol=1e-10)
+    C, _, it = lh.C_full(rho)
+    Cm, _, itm = lh.C_full(rho, precision="mixed")
+    assert rel(Cm, C) < 1e-9, (rel(Cm, C), itm)
+
+
+def test_fp64_pcg_trajectory_matches_oracle(L):
+    """Same algorithm, same iterates: 25 iterations with tol = 0 agree to rounding."""
+    rho = OD.grey_cell(4)
+    lh = L.LinearHomogenization(rho.shape, tol=0.0, maxit=25)
+    oh = OL.LinearHomogenization(rho.shape, tol=0.0, maxit=25)
+    s = oh.stiffness_scale(rho)
+    Es = np.eye(6)[[0, 3]]
+    u, it = lh.solve(s, Es)
+    uo, ito = oh.solve(s, Es)
+    assert it == ito == 25
+    assert rel(u, uo) < 1e-9
+
+
+def test_C_full_and_dC_match_oracle(L):
+    rho = OD.grey_cell(4)
+    lh, oh = L.LinearHomogenization(rho.shape), OL.LinearHomogenization(rho.shape)
+    C, u, it = lh.C_full(rho)
+    Co, uo, ito = oh.C_full(rho)
+    assert abs(it - ito) <= 1
+    assert rel(C, Co) < 1e-10
+    assert rel(u, uo) < 1e-6
+    dC = lh.dC_drho(rho, np.eye(6), u)
+    dCo = oh.dC_drho(rho, np.eye(6), u)
+    assert rel(dC, dCo) < 1e-12
+    assert rel(lh.bilinear(oh.stiffness_scale(rho), np.eye(6), u), oh.bilinear(oh.stiffness_scale(rho), np.eye(6), u)) < 1e-13
+
+
+def test_golden_fixtures(L):
+    g = np.load(GOLDEN)
+    rho = g["grey8_rho"]
+    C, _, it = L.LinearHomogenization(rho.shape).C_full(rho)
+    assert rel(C, g["grey8_C"]) < 1e-10
+    assert abs(it - int(g["grey8_it"])) <= 1
+    rho2 = g["plane8_rho"]
+    c2, _, _ = L.LinearHomogenization(rho2.shape).invariants(rho2)
+    assert rel(c2, g["plane8_c"]) < 1e-9
+
+
+def test_uniform_solid_is_isotropic_material(L):
+    """tests/test_core.py:88-91 of the reference."""
+    C, _, _ = L.LinearHomogenization((4, 4, 4), E=2.0, nu=0.25).C_full(np.ones((4, 4, 4)))
+    np.testing.assert_allclose(C, L.iso_D(2.0, 0.25), atol=1e-10)
+
+
+def test_full_vs_cubic_path_and_symmetry(L):
+    """tests/test_core.py:78-86 of the reference."""
+    rho = OD.grey_cell(4)
+    lh = L.LinearHomogenization(rho.shape)
+    C, _, _ = lh.C_full(rho)
+    np.testing.assert_allclose(C, C.T, atol=1e-12)
+    assert L.cubic_leakage(C) < 1e-8
+    c, _, _ = lh.invariants(rho)
+    np.testing.assert_allclose(c, L.cubic_invariants(C), rtol=1e-8)
+
+
+def test_plane_strain_equals_extruded_3d(L):
+    """tests/test_core.py:93-99 of the reference."""
+    rho2 = OD.grey_cell(4, d=2)
+    c2, _, _ = L.LinearHomogenization(rho2.shape).invariants(rho2)
+    rho3 = np.repeat(rho2[..., None], 3, axis=2)
+    C3, _, _ = L.LinearHomogenization(rho3.shape).C_full(rho3)
+    np.testing.assert_allclose(c2, [C3[0, 0], C3[1, 0], C3[5, 5]], rtol=1e-8)
+
+
+def test_hashin_shtrikman_bounds_cell(L):
+    """tests/test_core.py:135-142 of the reference."""
+    rho = OD.binary_cell(6, v=0.3).astype(float)
+    C, _, _ = L.LinearHomogenization(rho.shape).C_full(rho)
+    c11, c12, c44 = L.cubic_invariants(C)
+    K = (c11 + 2 * c12) / 3
+    Khs, Ghs = L.hashin_shtrikman(rho.mean())
+    assert K < Khs and c44 < Ghs
+
+
+def test_batched_equals_single_and_deterministic(L):
+    cells = np.stack([OD.random_cell(i, n_o=4, beta=8.0)[0] for i in range(3)])
+    lh = L.LinearHomogenization(cells.shape[1:])
+    r = lh.C_full_batched(cells, want_u=True)
+    r2 = lh.C_full_batched(cells, want_u=True)
+    assert np.array_equal(r["C"], r2["C"]) and np.array_equal(r["u"], r2["u"])
+    for i in range(3):
+        C, u, it = lh.C_full(cells[i])
+        assert np.array_equal(C, r["C"][i]) and it == r["it"][i]
+
+
+def test_high_contrast_variants_reach_the_fp64_C(L):
+    """emin = 1e-9 Schwarz-P 16^3: the scaled preconditioner (FP64 and FP32-in-FP64 refinement) and the
+    reference preconditioner (long run) reach the same C; every entry within 1e-8 of max |C|."""
+    rho = OD.schwarz_p_cell(8)
+    lh = L.LinearHomogenization(rho.shape, emin=1e-9, tol=1e-11, maxit=4000)
+    Cs, _, its = lh.C_full(rho, precond="scaled")
+    Cm, _, itm = lh.C_full(rho, precond="scaled", precision="mixed")
+    Cr, _, itr = lh.C_full(rho, tol=0.0, maxit=4000)
+    assert rel(Cm, Cs) < 1e-8, (rel(Cm, Cs), itm)
+    assert rel(Cr, Cs) < 1e-8, (rel(Cr, Cs), itr)
+    assert its < 200 and itm < 400
+
+
+def test_not_converged_is_silent_and_bad_args_raise(L):
+    rho = OD.grey_cell(4)
+    lh = L.LinearHomogenization(rho.shape, maxit=3)
+    _, _, it = lh.C_full(rho)
+    assert it == 3
+    from nlfiber_b200 import _lib
+    with pytest.raises(_lib.NlfError):
+        L.LinearHomogenization((0, 4, 4))
