@@ -1,0 +1,372 @@
+"""Throughput benchmark of the voxel homogenization hot path on B200.
+
+Metric: cells/s at 64^3 to relative C error <= 1e-8, where C error = max_IJ |C_IJ - C*_IJ| / max |C*| against
+C*, the FP64 C of the same cell solved to a tight residual. A step is one batched C_full (rho -> s -> six unit
+strains -> PCG -> C) over the GPU's batch of cells. Cells are seeded synthetic 64^3 cells (the reference's
+random_start generator on a 32^3 octant, v ~ U[0.2, 0.5], filter r = 1.5, beta = 16, solid E = 1, nu = 0.3,
+void floor 1e-9); no dataset is involved.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--calibrate-plain]
+
+--impl reference times the reference's algorithm on the host cores (the NumPy FP64 restatement in oracle/;
+the reference itself needs JAX, which is not installed) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "nonlinear-fiber-homogenization_b200")
+for _p in (ROOT, PKG_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "cells/s at 64^3 to rel C err 1e-8: batched mixed+learned vs plain FP64 PCG"
+UNIT = "cells/s"
+MATERIAL = dict(E=1.0, nu=0.3, emin=1e-9, p=3.0)
+# solver settings of the measured path: batched lock-step FP64 PCG with the node-scaled FFT preconditioner;
+# `tol` is the relative residual ||b - K u|| / ||b||. (The FP32-in-FP64-refinement path cannot reach 1e-8 on
+# cells with solid islands held only by the 1e-9 void: their rigid motions are below FP32 resolution.)
+FAST = dict(precision="fp64", precond="scaled", tol=1e-9, maxit=3000, check_every=16)
+CSTAR = dict(precision="fp64", precond="scaled", tol=1e-12, maxit=4000, check_every=32)
+# iterations the reference algorithm (FP64 PCG, unit-stiffness FFT preconditioner, nlfiber/linear.py:154-203)
+# needs per 64^3 cell of this workload to bring C within 1e-8 of C*, from `--calibrate-plain` on B200 (the plain
+# FP64 GPU path runs the reference's iterates): cells 0-3 needed > 32000, 4000, 32000 and 16000; the mean,
+# counting the first at its 32000 lower bound, is 21000. The plain GPU baseline and the CPU arm scale their
+# measured per-iteration times by it.
+REF_ITERS_64 = 21000
+
+
+def _gen(i, n_o):
+    from nlfiber_b200 import density as D
+    return D.random_cell(i, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0]
+
+
+def gen_cells(seeds, n_o, procs=8):
+    """Seeded synthetic cells (host NumPy), generated in spawned workers before any CUDA call."""
+    if len(seeds) == 1 or procs <= 1:
+        return np.stack([_gen(i, n_o) for i in seeds])
+    with mp.get_context("spawn").Pool(min(procs, len(seeds))) as pool:
+        return np.stack(pool.starmap(_gen, [(i, n_o) for i in seeds]))
+
+
+def rel_err(C, Cs):
+    C, Cs = np.asarray(C), np.asarray(Cs)
+    return np.abs(C - Cs).reshape(len(C), -1).max(1) / np.abs(Cs).reshape(len(Cs), -1).max(1)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.path = index, None, None
+
+    def start(self):
+        try:
+            self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def unit_bytes(kind, N, NS, m):
+    """Algorithmic bytes per unit of work (one vector = one cell and load case, N voxels) of a kernel class: what
+    the kernel must read and write at least once. Half spectrum: NS = nx ny (nz/2+1) complex per component."""
+    w = 8 if kind.endswith("f64") else 4
+    cw = 2 * w
+    return {
+        "apply": N * (6 * w + w / m),                      # x in, y out (3 components each), s shared by m cases
+        "fft_a": N * 3 * w + NS * 3 * cw + N * w / m,       # r in, half spectrum out, node scaling
+        "fft_b": 2 * NS * 3 * cw,                           # half spectrum in and out (Kinv table is shared)
+        "fft_c": NS * 3 * cw + 2 * N * 3 * w + N * w / m,   # spectrum in, r in (dots), z out, node scaling
+    }.get(kind.rsplit("_", 1)[0])
+
+
+def roofline(prof, N, NS, m, peaks, peak_kind):
+    tot = sum(v[0] for v in prof.values())
+    best, best_ms = None, -1.0
+    for k, (ms, la, un) in prof.items():
+        if unit_bytes(k, N, NS, m) is not None and ms > best_ms:
+            best, best_ms = k, ms
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "units": v[2], "share": round(v[0] / tot, 4)}
+               for k, v in prof.items() if v[1]}
+    if best is None or best_ms <= 0:
+        return None, kernels
+    ms, la, un = prof[best]
+    bytes_total = un * unit_bytes(best, N, NS, m)
+    achieved = bytes_total / (ms * 1e-3) / 1e9
+    peak = float(peaks["hbm_gbs"])
+    return {"kernel": best, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "peak_kind": "of measured copy bandwidth" if peak_kind == "measured" else "of fallback 6650 GB/s",
+            "avg_launch_ms": round(ms / max(la, 1), 4),
+            "algorithmic_bytes_per_launch": round(bytes_total / max(la, 1)), "traffic": None}, kernels
+
+
+def cpu_reference(cells, sample_iters=2):
+    """The reference algorithm (FP64 PCG with the unit-stiffness FFT preconditioner; the NumPy restatement in
+    oracle/) on one cell, all host threads. Times the setup (stiffness scale, load, first residual and
+    preconditioner, C assembly) and `sample_iters` PCG iterations, and scales to REF_ITERS_64 iterations."""
+    from oracle import linear_ref as OL
+    rho = cells[0]
+    lh = OL.LinearHomogenization(rho.shape, **MATERIAL, tol=0.0)
+    t0 = time.perf_counter()
+    s = lh.stiffness_scale(rho)
+    b = -lh.load(s, np.eye(6))
+    t1 = time.perf_counter()
+    x, _ = lh._cg(s, b, np.zeros_like(b), maxit=0)
+    t2 = time.perf_counter()
+    lh._cg(s, b, np.zeros_like(b), maxit=sample_iters)
+    t3 = time.perf_counter()
+    lh.bilinear(s, np.eye(6), x)
+    t4 = time.perf_counter()
+    setup = (t1 - t0) + (t2 - t1) + (t4 - t3)
+    per_it = max((t3 - t2) - (t2 - t1), 1e-9) / sample_iters
+    cell_s = setup + REF_ITERS_64 * per_it
+    sample = (f"1 cell {rho.shape[0]}^3 x 6 cases: setup, C assembly and {sample_iters} FP64 PCG iterations timed "
+              f"({t4 - t0:.1f} s), iterations scaled to {REF_ITERS_64} (the reference algorithm's count to C "
+              f"err 1e-8 on this workload)")
+    return 1.0 / cell_s, sample, t4 - t0
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cells = gen_cells([0], args.n // 2, procs=1)
+    t_all = time.perf_counter()
+    for _ in range(args.warmup):
+        cpu_reference(cells, sample_iters=1)
+    vals, sample = [], ""
+    for _ in range(max(1, args.steps)):
+        v, sample, _ = cpu_reference(cells)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"seeded synthetic {args.n}^3 cells x 6 unit strains, C_full, emin 1e-9",
+                       "grid": args.n, "cases": 6},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": round(time.perf_counter() - t_all, 1)}
+    print(json.dumps(line), flush=True)
+
+
+def plain_fp64_time(L, rho_d, n, stream, iters=200):
+    """Seconds per PCG iteration per cell of the plain FP64 GPU PCG (the reference algorithm, unit-stiffness FFT
+    preconditioner), measured on one cell."""
+    import torch
+    lh = L.LinearHomogenization((n, n, n), **MATERIAL, tol=0.0, maxit=iters, precision="fp64", precond="fft",
+                                check_every=64)
+    lh.stream = stream
+    C = torch.empty((1, 6, 6), dtype=torch.float64, device="cuda")
+    lh.C_full_batched(rho_d[:1], out_C=C, maxit=8)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    lh.C_full_batched(rho_d[:1], out_C=C)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / iters
+
+
+def calibrate_plain(L, rho_d, Cstar, n, stream, ncell=4, caps=(1000, 2000, 4000, 8000, 16000, 32000)):
+    """Iterations the plain FP64 GPU PCG needs per cell to bring C within 1e-8 of C*: C error after each cap."""
+    import torch
+    lh = L.LinearHomogenization((n, n, n), **MATERIAL, tol=0.0, maxit=1, precision="fp64", precond="fft",
+                                check_every=64)
+    lh.stream = stream
+    C = torch.empty((ncell, 6, 6), dtype=torch.float64, device="cuda")
+    table = {}
+    for cap in caps:
+        lh.C_full_batched(rho_d[:ncell], out_C=C, maxit=cap)
+        table[cap] = rel_err(C.cpu().numpy(), Cstar[:ncell]).tolist()
+        print(json.dumps({"calibrate_plain_cap": cap, "c_err": table[cap]}), flush=True)
+    need = []
+    for i in range(ncell):
+        hit = [cap for cap in caps if table[cap][i] <= 1e-8]
+        need.append(hit[0] if hit else None)
+    return {"needed_iterations": need, "c_err_by_cap": table}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=32, help="cells per GPU")
+    ap.add_argument("--n", type=int, default=64, help="grid side")
+    ap.add_argument("--skip-plain", action="store_true", help="skip the plain FP64 GPU baseline")
+    ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--calibrate-plain", action="store_true",
+                    help="measure the plain FP64 PCG iteration count to C err 1e-8 (slow) and exit")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    n_o = args.n // 2
+    seeds = list(range(rank * args.cells, (rank + 1) * args.cells))
+    t_gen = time.perf_counter()
+    cells = gen_cells(seeds, n_o)
+    t_gen = time.perf_counter() - t_gen
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from nlfiber_b200 import _lib
+    from nlfiber_b200 import linear as L
+
+    n, B = args.n, args.cells
+    N = n ** 3
+    NS = n * n * (n // 2 + 1)
+    stream = torch.cuda.current_stream().cuda_stream
+    rho_d = torch.from_numpy(cells).cuda()
+    C_d = torch.empty((B, 6, 6), dtype=torch.float64, device="cuda")
+
+    # C*: FP64, scaled preconditioner, tight residual
+    ref = L.LinearHomogenization((n, n, n), **MATERIAL, **CSTAR)
+    ref.stream = stream
+    Cstar = ref.C_full_batched(rho_d, out_C=torch.empty_like(C_d))["C"].cpu().numpy()
+    del ref
+    if args.calibrate_plain:
+        if rank == 0:
+            print(json.dumps({"calibrate_plain": calibrate_plain(L, rho_d, Cstar, n, stream)}), flush=True)
+        return
+
+    lh = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
+    lh.stream = stream
+    for _ in range(args.warmup):
+        lh.C_full_batched(rho_d, out_C=C_d)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = ClockSampler(vis.split(",")[local] if vis else torch.cuda.current_device())
+    clocks.start()
+    _lib.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    its = None
+    for _ in range(args.steps):
+        its = lh.C_full_batched(rho_d, out_C=C_d)["it"]
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = _lib.profile_report()
+    _lib.profile(False)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    err = rel_err(C_d.cpu().numpy(), Cstar)
+    value = world * B * args.steps / (ms / 1e3)
+
+    # end to end through the same API with pinned host buffers (H2D of rho and D2H of C inside the region)
+    rho_h = torch.from_numpy(cells).pin_memory()
+    C_h = torch.empty((B, 6, 6), dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, args.steps // 2)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record()
+    for _ in range(e2e_steps):
+        lh.C_full_batched(rho_h, out_C=C_h)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * B * e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * N * 8,
+           "d2h_bytes_per_step": B * 36 * 8, "c_err_max": float(rel_err(C_h.numpy(), Cstar).max())}
+
+    peaks, peak_kind = measured_peaks()
+    roof, kernels = roofline(prof, N, NS, 6, peaks, peak_kind)
+    launches = sum(v[1] for v in prof.values())
+
+    plain, cpu = None, None
+    if rank == 0 and not args.skip_plain:
+        t_it = plain_fp64_time(L, rho_d, n, stream)
+        plain = {"sec_per_iteration_per_cell": t_it, "iterations_to_1e-8": REF_ITERS_64,
+                 "cells_per_s": 1.0 / (t_it * REF_ITERS_64),
+                 "note": "time per iteration measured here; iteration count from --calibrate-plain"}
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        v, sample, _ = cpu_reference(cells)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{B} seeded synthetic {n}^3 cells per GPU x 6 unit strains, C_full, emin 1e-9",
+                   "grid": n, "cells_per_gpu": B, "cases": 6, "solver": "FP64 PCG, node-scaled FFT "
+                   "preconditioner, batched lock-step per cell", "tol": FAST["tol"],
+                   "l2": "working set > L2 (126 MB) every step; no flush needed", "parallelism": f"dp{world}"},
+        "c_err_max": float(err.max()), "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
+        "roofline": roof, "kernels": kernels, "gpu_launches": launches, "clocks": clk, "e2e": e2e,
+        "cpu_baseline": cpu, "plain_fp64_gpu": plain,
+        "speedup_vs_plain_fp64": (value / world / plain["cells_per_s"]) if plain else None,
+        "input_gen_s": round(t_gen, 1),
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

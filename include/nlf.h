@@ -119,6 +119,19 @@ NLF_API int nlf_C_full(nlf_linear* h, int ncell, const double* rho, const double
  * out (nx, ny, nz/2+1, 6) in the order xx yy zz yz xz xy. */
 NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
 
+/* ---- kernel profiler ------------------------------------------------------------------------------------- */
+
+/* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library
+ * is bracketed by CUDA events on its stream and the units of work that actually ran (vectors of active cells)
+ * are counted on the device. Process-wide and not thread-safe; off by default. No counterpart in the
+ * reference (which has no tracing, nlfiber/qoi.py:81,106 only records wall-clock seconds). */
+NLF_API int nlf_profile(int on);
+/* Per kernel class k < n (n >= the number of classes): total event-timed milliseconds, launches and units.
+ * Synchronizes the device. Returns the number of classes. */
+NLF_API int nlf_profile_report(double* total_ms, long long* launches, unsigned long long* units, int n);
+/* Name of kernel class k ("apply_f32", "fft_a_f32", ...); "" when out of range. */
+NLF_API const char* nlf_profile_name(int kind);
+
 #ifdef __cplusplus
 }
 #endif

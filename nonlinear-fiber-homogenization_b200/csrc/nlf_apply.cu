@@ -13,13 +13,15 @@
 // to shared memory; each output node then sums its 4 in-plane element contributions. Every output node is
 // written once, with a fixed summation order (deterministic), and the whole 27-point stencil stays on chip.
 #include "nlf_internal.h"
+#include "nlf_prof.cuh"
 
 namespace nlf {
 
 template <typename T, int TY, int TZ>
 __global__ void __launch_bounds__(((TY + 1) * (TZ + 1) + 31) / 32 * 32)
 k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int n0, int n1, int n2, int m,
-        int lx, const CellState* __restrict__ cs, ModeC<T> kc, double* __restrict__ partial) {
+        int lx, const CellState* __restrict__ cs, ModeC<T> kc, double* __restrict__ partial,
+        unsigned long long* __restrict__ units, int ukind) {
   constexpr int HY = TY + 2, HZ = TZ + 2, EY = TY + 1, EZ = TZ + 1;
   constexpr int NE = EY * EZ;
   constexpr int NT = (NE + 31) / 32 * 32;
@@ -33,6 +35,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 
   const int vec = blockIdx.z, cell = vec / m;
   if (cs && !cs[cell].active) return;
+  prof_count(units, ukind);
   const long N = (long)n0 * n1 * n2;
   const int ntz = (n2 + TZ - 1) / TZ;
   const int z0 = (blockIdx.x % ntz) * TZ, y0 = (blockIdx.x / ntz) * TY;
@@ -177,8 +180,10 @@ int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x,
   chunks = (g.n0 + lx - 1) / lx;
   if (nblk_out) *nblk_out = tiles * chunks;
   dim3 grid(tiles, chunks, nvec);
+  const int kind = sizeof(T) == 4 ? PK_APPLY32 : PK_APPLY64;
+  ProfScope ps(kind, st);
   k_apply<T, TY, TZ><<<grid, NT, 0, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs,
-                                          make_modec<T>(h.lam, h.mu), partial);
+                                          make_modec<T>(h.lam, h.mu), partial, prof_units(), kind);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
@@ -218,6 +223,7 @@ int launch_load(const LinearHandle& h, const double* s, const double* fe, int m,
                 double sign, cudaStream_t st) {
   const long N = h.g.N;
   dim3 grid((unsigned)((N + 255) / 256), ncell);
+  ProfScope ps(PK_LOAD, st);
   k_load<<<grid, 256, 0, st>>>(s, fe, m, h.g.n0, h.g.n1, h.g.n2, f, sign);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -359,6 +365,7 @@ int launch_bilinear(const LinearHandle& h, const double* s, const double* EsEDE,
   const int nb = (int)((N + 127) / 128);
   *nblk = nb;
   dim3 grid(nb, ncell);
+  ProfScope ps(PK_BILINEAR, st);
   k_bilinear<<<grid, 128, 0, st>>>(s, EsEDE, EsEDE + m * 6, m, h.g.n0, h.g.n1, h.g.n2, h.lam, h.mu, u, Cpart,
                                    rho, h.emin, h.p, dC);
   NLF_CHECK_LAUNCH();
@@ -367,6 +374,7 @@ int launch_bilinear(const LinearHandle& h, const double* s, const double* EsEDE,
 
 int launch_reduce_C(const LinearHandle& h, const double* Cpart, int nblk, int m, int ncell, double* C,
                     cudaStream_t st) {
+  ProfScope ps(PK_OTHER, st);
   k_reduce_C<<<ncell, 32, 0, st>>>(Cpart, nblk, m, 1.0 / (double)h.g.N, C);
   NLF_CHECK_LAUNCH();
   return NLF_OK;

@@ -13,6 +13,7 @@
 // sum over the 27 stencil blocks W_d cos(k.d); K(0) = I; Kinv = inv(K + 1e-12 |tr K| I); Kinv(0) = 0.
 #include <cmath>
 #include "nlf_internal.h"
+#include "nlf_prof.cuh"
 
 namespace nlf {
 
@@ -145,12 +146,14 @@ struct FftDims {
 // ---- pass A --------------------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T>* __restrict__ spec, FftDims d,
-                        int m, const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs) {
+                        int m, const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs,
+                        unsigned long long* __restrict__ units, int ukind) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* scratch = buf + d.n1 * d.rs;
   const int x = blockIdx.x, c = blockIdx.y, vec = blockIdx.z;
   if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
   const T* rp = r + ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
   const T* wp = w ? w + (long)(vec / m) * d.N + (long)x * d.n1 * d.n2 : nullptr;
   const bool packed = (d.n2 % 2) == 0;
@@ -190,12 +193,14 @@ __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T
 // ---- pass B --------------------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, FftDims d, int kc, int m,
-                        const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs) {
+                        const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs,
+                        unsigned long long* __restrict__ units, int ukind) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);  // [3][n0][kc]
   cplx<T>* scratch = buf + 3 * d.n0 * kc;
   const int ky = blockIdx.x, kz0 = blockIdx.y * kc, vec = blockIdx.z;
   if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
   const int nkz = min(kc, d.n2h - kz0);
   for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
     const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
@@ -230,13 +235,15 @@ __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, 
 template <typename T>
 __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ w, const T* __restrict__ r,
                         T* __restrict__ z, FftDims d, int m, const cplx<T>* __restrict__ tw,
-                        const CellState* __restrict__ cs, double* __restrict__ partial) {
+                        const CellState* __restrict__ cs, double* __restrict__ partial,
+                        unsigned long long* __restrict__ units, int ukind) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* scratch = buf + d.n1 * d.rs;
   __shared__ double red[32 * 4];
   const int x = blockIdx.x, c = blockIdx.y, vec = blockIdx.z;
   if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
   const cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
   for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
     const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
@@ -354,13 +361,27 @@ int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cpl
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemb));
   const int nt = 256;
-  k_fft_a<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(r, w, spec, d, m, tw, cs);
-  NLF_CHECK_LAUNCH();
-  k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h), d, kc, m, tw,
-                                                                        cs);
-  NLF_CHECK_LAUNCH();
-  k_fft_c<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(spec, w, r, z, d, m, tw, cs, partial);
-  NLF_CHECK_LAUNCH();
+  const bool f32 = sizeof(T) == 4;
+  unsigned long long* units = prof_units();
+  {
+    const int kind = f32 ? PK_FFTA32 : PK_FFTA64;
+    ProfScope ps(kind, st);
+    k_fft_a<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(r, w, spec, d, m, tw, cs, units, kind);
+    NLF_CHECK_LAUNCH();
+  }
+  {
+    const int kind = f32 ? PK_FFTB32 : PK_FFTB64;
+    ProfScope ps(kind, st);
+    k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h), d, kc, m, tw,
+                                                                          cs, units, kind);
+    NLF_CHECK_LAUNCH();
+  }
+  {
+    const int kind = f32 ? PK_FFTC32 : PK_FFTC64;
+    ProfScope ps(kind, st);
+    k_fft_c<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(spec, w, r, z, d, m, tw, cs, partial, units, kind);
+    NLF_CHECK_LAUNCH();
+  }
   return NLF_OK;
 }
 

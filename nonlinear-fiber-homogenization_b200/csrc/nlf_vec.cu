@@ -4,6 +4,7 @@
 // finalize kernel sums in a fixed order (deterministic). A cell whose CellState.active is 0 is skipped by
 // every kernel, which reproduces the reference's lock-step `while_loop` per cell inside a batch of cells.
 #include "nlf_vec.cuh"
+#include "nlf_prof.cuh"
 
 namespace nlf {
 
@@ -31,6 +32,7 @@ __global__ void k_soa_to_aos(long N, const Tin* __restrict__ in, Tout* __restric
 template <typename Tin, typename Tout>
 int launch_aos_to_soa(long N, int nvec, const Tin* in, Tout* out, double scale, cudaStream_t st) {
   if (nvec == 0) return NLF_OK;
+  ProfScope ps_(PK_OTHER, st);
   k_aos_to_soa<Tin, Tout><<<dim3((unsigned)((N + 255) / 256), nvec), 256, 0, st>>>(N, in, out, scale);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -38,6 +40,7 @@ int launch_aos_to_soa(long N, int nvec, const Tin* in, Tout* out, double scale, 
 template <typename Tin, typename Tout>
 int launch_soa_to_aos(long N, int nvec, const Tin* in, Tout* out, cudaStream_t st) {
   if (nvec == 0) return NLF_OK;
+  ProfScope ps_(PK_OTHER, st);
   k_soa_to_aos<Tin, Tout><<<dim3((unsigned)((N + 255) / 256), nvec), 256, 0, st>>>(N, in, out);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -58,6 +61,7 @@ __global__ void k_stiffness_scale(long count, const double* __restrict__ rho, do
 
 int launch_stiffness_scale(const LinearHandle& h, long count, const double* rho, double* s, cudaStream_t st) {
   if (count == 0) return NLF_OK;
+  ProfScope ps_(PK_OTHER, st);
   k_stiffness_scale<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, rho, s, h.emin, h.p);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -89,6 +93,7 @@ __global__ void k_node_scaling(int n0, int n1, int n2, const double* __restrict_
 int launch_node_scaling(const LinearHandle& h, int ncell, const double* s, float* s32, double* w64, float* w32,
                         cudaStream_t st) {
   if (ncell == 0) return NLF_OK;
+  ProfScope ps_(PK_OTHER, st);
   k_node_scaling<<<dim3((unsigned)((h.g.N + 255) / 256), ncell), 256, 0, st>>>(h.g.n0, h.g.n1, h.g.n2, s, s32,
                                                                                w64, w32);
   NLF_CHECK_LAUNCH();
@@ -157,8 +162,10 @@ int launch_stats(const LinearHandle& h, int nvec, int m, const T* x, const CellS
                  VecState* vs, int what, cudaStream_t st) {
   if (nvec == 0) return NLF_OK;
   const int nb = kStatsBlocks;
+  ProfScope ps_(PK_STATS, st);
   k_stats<T><<<dim3(nb, 3, nvec), 256, 0, st>>>(h.g.N, x, cs, m, partial);
   NLF_CHECK_LAUNCH();
+  ProfScope ps2_(PK_FIN, st);
   k_fin_stats<<<(nvec + 7) / 8, 256, 0, st>>>(partial, nb, h.g.N, nvec, vs, cs, m, what);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -184,6 +191,7 @@ int launch_sub_mean(const LinearHandle& h, int nvec, int m, T* x, const VecState
                     cudaStream_t st) {
   if (nvec == 0) return NLF_OK;
   const int nb = (int)std::min<long>((h.g.N + 255) / 256, 256);
+  ProfScope ps_(PK_OTHER, st);
   k_sub_mean<T><<<dim3(nb, 3, nvec), 256, 0, st>>>(h.g.N, x, vs, cs, m);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -382,6 +390,7 @@ static inline dim3 vec_grid(long N, int nvec) {
 
 int launch_fin_apply(int nvec, int m, const double* partial, int nblk, long N, VecState* vs, const CellState* cs,
                      int init, cudaStream_t st) {
+  ProfScope ps_(PK_FIN, st);
   k_fin_apply<<<(nvec + 7) / 8, 256, 0, st>>>(partial, nblk, N, nvec, vs, cs, m, init);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -389,6 +398,7 @@ int launch_fin_apply(int nvec, int m, const double* partial, int nblk, long N, V
 template <typename T>
 int launch_xr(long N, int nvec, int m, T* x, T* r, const T* p, const T* Ap, const VecState* vs, const CellState* cs,
               cudaStream_t st) {
+  ProfScope ps_(PK_XR, st);
   k_xr<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, x, r, p, Ap, vs, cs, m);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -396,12 +406,14 @@ int launch_xr(long N, int nvec, int m, T* x, T* r, const T* p, const T* Ap, cons
 template <typename Tb, typename T>
 int launch_r_init(long N, int nvec, int m, T* r, const Tb* b, const T* Ax, const VecState* vs, const CellState* cs,
                   cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_r_init<Tb, T><<<vec_grid(N, nvec), 256, 0, st>>>(N, r, b, Ax, vs, cs, m);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_fin_pc(int ncell, int m, int n0, long N, const double* partial, VecState* vs, CellState* cs, double tol,
                   int maxit, int init, cudaStream_t st) {
+  ProfScope ps_(PK_FIN, st);
   k_fin_pc<<<ncell, 32 * m, 0, st>>>(partial, n0, N, vs, cs, m, tol, maxit, init);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -409,33 +421,39 @@ int launch_fin_pc(int ncell, int m, int n0, long N, const double* partial, VecSt
 template <typename T>
 int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, const CellState* cs, int init,
              cudaStream_t st) {
+  ProfScope ps_(PK_P, st);
   k_p<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, p, z, vs, cs, m, init);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_mark(CellState* cs, int ncell, cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_mark<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_cs_init(CellState* cs, int ncell, const int* mask, cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_cs_init<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell, mask);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_count_active(const CellState* cs, int ncell, int* out, cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_count_active<<<1, 256, 0, st>>>(cs, ncell, out);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_r_to32(long N, int nvec, int m, const double* r64, float* r32, VecState* vs, const CellState* cs,
                   cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_r_to32<<<vec_grid(N, nvec), 256, 0, st>>>(N, r64, r32, vs, cs, m);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 int launch_x_update(long N, int nvec, int m, double* x64, const float* x32, const VecState* vs, const CellState* cs,
                     cudaStream_t st) {
+  ProfScope ps_(PK_OTHER, st);
   k_x_update<<<vec_grid(N, nvec), 256, 0, st>>>(N, x64, x32, vs, cs, m);
   NLF_CHECK_LAUNCH();
   return NLF_OK;

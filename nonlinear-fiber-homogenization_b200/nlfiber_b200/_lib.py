@@ -21,6 +21,7 @@ EXPORTS = (
     "nlf_last_error", "nlf_version", "nlf_default_opts", "nlf_linear_create", "nlf_linear_destroy",
     "nlf_stiffness_scale", "nlf_apply_K", "nlf_load", "nlf_precond", "nlf_linear_solve", "nlf_linear_solve_rhs",
     "nlf_bilinear", "nlf_dC_drho", "nlf_C_full", "nlf_precond_symbol", "nlf_apply_K_ex", "nlf_precond_ex",
+    "nlf_profile", "nlf_profile_report", "nlf_profile_name",
 )
 
 
@@ -63,6 +64,9 @@ def _load():
         "nlf_dC_drho": (I, [P, I, P, P, I, P, P, P]),
         "nlf_C_full": (I, [P, I, P, P, P, P, P, P, P, P]),
         "nlf_precond_symbol": (I, [P, P]),
+        "nlf_profile": (I, [I]),
+        "nlf_profile_report": (I, [P, P, P, I]),
+        "nlf_profile_name": (ctypes.c_char_p, [I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -115,3 +119,18 @@ def as_f64(a):
             raise TypeError("device tensors must be float64")
         return a.contiguous()
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def profile(on=True):
+    """Turn the library's kernel profiler on (and reset it) or off."""
+    check(lib.nlf_profile(1 if on else 0))
+
+
+def profile_report():
+    """{kernel class: (total_ms, launches, units)} of the launches recorded since profile(True)."""
+    n = 32
+    ms = np.zeros(n)
+    la = np.zeros(n, dtype=np.int64)
+    un = np.zeros(n, dtype=np.uint64)
+    k = check(lib.nlf_profile_report(ms.ctypes.data, la.ctypes.data, un.ctypes.data, n))
+    return {lib.nlf_profile_name(i).decode(): (float(ms[i]), int(la[i]), int(un[i])) for i in range(k)}

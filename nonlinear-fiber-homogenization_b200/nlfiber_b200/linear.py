@@ -117,6 +117,7 @@ class LinearHomogenization:
                                     self.maxit))
         self._h = h
         self._Kinv = None
+        self.stream = None  # cudaStream_t handle (int) used by every call; None = the legacy default stream
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -160,7 +161,7 @@ class LinearHomogenization:
         rho = self._cell(rho)
         out = np.empty(rho.shape)
         ncell = int(np.prod(rho.shape)) // self.N
-        check(lib.nlf_stiffness_scale(self._h, ncell, ptr(rho), ptr(out), None))
+        check(lib.nlf_stiffness_scale(self._h, ncell, ptr(rho), ptr(out), self.stream))
         return out
 
     def apply_K(self, s, u, precision="fp64"):
@@ -170,7 +171,7 @@ class LinearHomogenization:
         u = as_f64(u)
         nvec = int(np.prod(u.shape)) // (3 * self.N)
         out = np.empty(u.shape)
-        check(lib.nlf_apply_K_ex(self._h, ptr(s), nvec, ptr(u), ptr(out), _PREC[precision], None))
+        check(lib.nlf_apply_K_ex(self._h, ptr(s), nvec, ptr(u), ptr(out), _PREC[precision], self.stream))
         return out
 
     def load(self, s, Es):
@@ -178,7 +179,7 @@ class LinearHomogenization:
         s = self._cell(s)
         Es = as_f64(np.atleast_2d(Es))
         out = np.empty((Es.shape[0],) + self.shape + (3,))
-        check(lib.nlf_load(self._h, ptr(s), ptr(Es), Es.shape[0], ptr(out), None))
+        check(lib.nlf_load(self._h, ptr(s), ptr(Es), Es.shape[0], ptr(out), self.stream))
         return out
 
     def residual(self, s, Es, u):
@@ -193,7 +194,7 @@ class LinearHomogenization:
         nvec = int(np.prod(r.shape)) // (3 * self.N)
         out = np.empty(r.shape)
         s = None if s is None else self._cell(s)
-        check(lib.nlf_precond_ex(self._h, nvec, ptr(r), ptr(out), _PREC[precision], _PC[precond], ptr(s), None))
+        check(lib.nlf_precond_ex(self._h, nvec, ptr(r), ptr(out), _PREC[precision], _PC[precond], ptr(s), self.stream))
         return out
 
     # --- solver ---------------------------------------------------------------------------------------------
@@ -209,7 +210,7 @@ class LinearHomogenization:
         it = np.zeros(ncell, dtype=np.int32)
         o = self.opts(**opt)
         st = check(lib.nlf_linear_solve(self._h, ncell, ptr(s), ptr(Es), m, ptr(u0), ptr(u), ptr(it),
-                                        ctypes.byref(o), None))
+                                        ctypes.byref(o), self.stream))
         return u, it, st
 
     def solve(self, s, Es, u0=None, **opt):
@@ -227,7 +228,7 @@ class LinearHomogenization:
         u = np.empty(b.shape)
         it = np.zeros(1, dtype=np.int32)
         o = self.opts(**opt)
-        check(lib.nlf_linear_solve_rhs(self._h, 1, ptr(s), m, ptr(b), ptr(u), ptr(it), ctypes.byref(o), None))
+        check(lib.nlf_linear_solve_rhs(self._h, 1, ptr(s), m, ptr(b), ptr(u), ptr(it), ctypes.byref(o), self.stream))
         return u, int(it[0])
 
     def correctors(self, s, Es, u0):
@@ -242,7 +243,7 @@ class LinearHomogenization:
         u = as_f64(u)
         m = Es.shape[0]
         C = np.empty((m, m))
-        check(lib.nlf_bilinear(self._h, 1, ptr(s), ptr(Es), m, ptr(u), ptr(C), None))
+        check(lib.nlf_bilinear(self._h, 1, ptr(s), ptr(Es), m, ptr(u), ptr(C), self.stream))
         return C
 
     def dC_drho(self, rho, Es, u):
@@ -253,22 +254,23 @@ class LinearHomogenization:
         u = as_f64(u)
         m = Es.shape[0]
         out = np.empty((m, m) + self.shape)
-        check(lib.nlf_dC_drho(self._h, 1, ptr(rho), ptr(Es), m, ptr(u), ptr(out), None))
+        check(lib.nlf_dC_drho(self._h, 1, ptr(rho), ptr(Es), m, ptr(u), ptr(out), self.stream))
         return out
 
-    def C_full_batched(self, rho, u0=None, want_u=False, want_dC=False, **opt):
+    def C_full_batched(self, rho, u0=None, want_u=False, want_dC=False, out_C=None, **opt):
         """C (ncell, 6, 6) of ncell cells of this shape in one batched solve. Returns a dict with C, it, status
-        and, when asked, u (ncell, 6, nx, ny, nz, 3) and dC (ncell, 6, 6, nx, ny, nz)."""
+        and, when asked, u (ncell, 6, nx, ny, nz, 3) and dC (ncell, 6, 6, nx, ny, nz). rho and out_C may be
+        CUDA float64 torch tensors (device resident) or pinned host tensors."""
         rho = as_f64(rho)
         ncell = int(np.prod(rho.shape)) // self.N
-        C = np.empty((ncell, 6, 6))
+        C = np.empty((ncell, 6, 6)) if out_C is None else out_C
         u = np.empty((ncell, 6) + self.shape + (3,)) if want_u else None
         dC = np.empty((ncell, 6, 6) + self.shape) if want_dC else None
         it = np.zeros(ncell, dtype=np.int32)
         u0 = None if u0 is None else as_f64(u0)
         o = self.opts(**opt)
         st = check(lib.nlf_C_full(self._h, ncell, ptr(rho), ptr(u0), ptr(C), ptr(u), ptr(dC), ptr(it),
-                                  ctypes.byref(o), None))
+                                  ctypes.byref(o), self.stream))
         return dict(C=C, u=u, dC=dC, it=it, status=st)
 
     def C_full(self, rho, u0=None, **opt):
