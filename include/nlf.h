@@ -109,6 +109,18 @@ NLF_API int nlf_bilinear(nlf_linear* h, int ncell, const double* s, const double
 NLF_API int nlf_dC_drho(nlf_linear* h, int ncell, const double* rho, const double* Es, int m,
                         const double* u, double* dC, void* stream);
 
+/* C_IJ assembly that allocates nothing (no counterpart in the reference). For callers that may not call
+ * cudaMalloc while they run (a handler inside a framework that owns all device memory, code inside another
+ * library's callback, a service with pre-reserved memory) and already hold device arrays: s (ncell, nx, ny, nz),
+ * u (ncell, m, nx, ny, nz, 3) and C (ncell, m, m) must be device pointers of the current device; Es (m, 6) is a
+ * host array. Same values as nlf_bilinear. No handle: the grid shape and material are arguments. At most 64
+ * cells and 6 load cases per call (-1 with a message beyond). The partial sums live in a fixed 672 KiB device
+ * array held by every GPU that loads the library; calls that overlap on the GPU race on it, so serialise them.
+ * The first call on a device looks up that array's address; make it before any stream capture. Asynchronous on
+ * `stream`: C is ready when the stream reaches it. */
+NLF_API int nlf_bilinear_noalloc(int nx, int ny, int nz, double E, double nu, int ncell, const double* s,
+                                 const double* Es, int m, const double* u, double* C, void* stream);
+
 /* nlfiber/linear.py:231-236 C_full(rho, u0) for a batch: rho -> s -> 6 unit strains -> PCG -> C.
  * u0, u, dC may be NULL (cold start / corrector not returned / no sensitivities).
  * C: (ncell, 6, 6); u: (ncell, 6, nx, ny, nz, 3); dC: (ncell, 6, 6, nx, ny, nz); iters: (ncell,). */

@@ -21,7 +21,7 @@ EXPORTS = (
     "nlf_last_error", "nlf_version", "nlf_default_opts", "nlf_linear_create", "nlf_linear_destroy",
     "nlf_stiffness_scale", "nlf_apply_K", "nlf_load", "nlf_precond", "nlf_linear_solve", "nlf_linear_solve_rhs",
     "nlf_bilinear", "nlf_dC_drho", "nlf_C_full", "nlf_precond_symbol", "nlf_apply_K_ex", "nlf_precond_ex",
-    "nlf_profile", "nlf_profile_report", "nlf_profile_name",
+    "nlf_profile", "nlf_profile_report", "nlf_profile_name", "nlf_bilinear_noalloc",
 )
 
 
@@ -67,6 +67,7 @@ def _load():
         "nlf_profile": (I, [I]),
         "nlf_profile_report": (I, [P, P, P, I]),
         "nlf_profile_name": (ctypes.c_char_p, [I]),
+        "nlf_bilinear_noalloc": (I, [I, I, I, D, D, I, P, P, I, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
