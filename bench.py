@@ -242,6 +242,10 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--calibrate-plain", action="store_true",
                     help="measure the plain FP64 PCG iteration count to C err 1e-8 (slow) and exit")
+    ap.add_argument("--ncu", action="store_true",
+                    help="small fixed profiling case for ncu: one warm-up and one C_full of --cells cells with "
+                         "--iters PCG iterations, no C*, no baselines")
+    ap.add_argument("--iters", type=int, default=20)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -271,6 +275,18 @@ def main():
     stream = torch.cuda.current_stream().cuda_stream
     rho_d = torch.from_numpy(cells).cuda()
     C_d = torch.empty((B, 6, 6), dtype=torch.float64, device="cuda")
+
+    if args.ncu:
+        kw = dict(FAST, tol=0.0, maxit=args.iters)
+        for prec in ("fp64", "mixed"):
+            lh = L.LinearHomogenization((n, n, n), **MATERIAL, **dict(kw, precision=prec, inner_maxit=args.iters,
+                                                                        inner_tol=0.0, max_sweeps=1))
+            lh.stream = stream
+            for _ in range(2):
+                lh.C_full_batched(rho_d, out_C=C_d)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": f"{B} cells {n}^3, {args.iters} PCG iterations, fp64 and mixed"}))
+        return
 
     # C*: FP64, scaled preconditioner, tight residual
     ref = L.LinearHomogenization((n, n, n), **MATERIAL, **CSTAR)
