@@ -17,8 +17,8 @@
 
 namespace nlf {
 
-template <typename T, int TY, int TZ>
-__global__ void __launch_bounds__(((TY + 1) * (TZ + 1) + 31) / 32 * 32)
+template <typename T, int TY, int TZ, int MINB>
+__global__ void __launch_bounds__(((TY + 1) * (TZ + 1) + 31) / 32 * 32, MINB)
 k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int n0, int n1, int n2, int m,
         int lx, const CellState* __restrict__ cs, ModeC<T> kc, double* __restrict__ partial,
         unsigned long long* __restrict__ units, int ukind) {
@@ -26,7 +26,8 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   constexpr int NE = EY * EZ;
   constexpr int NT = (NE + 31) / 32 * 32;
   constexpr int NP = HY * HZ;
-  __shared__ T pl[3][NP];
+  constexpr int PF = (3 * NP + NT - 1) / NT;  // plane values each thread prefetches per layer
+  __shared__ T pl[2][3][NP];                  // node plane j lives in pl[j & 1]
   __shared__ T sl[NE];
   __shared__ T g[4][3][NE];
   __shared__ int gys[HY], gzs[HZ];
@@ -37,6 +38,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   if (cs && !cs[cell].active) return;
   prof_count(units, ukind);
   const long N = (long)n0 * n1 * n2;
+  const long P = (long)n1 * n2;
   const int ntz = (n2 + TZ - 1) / TZ;
   const int z0 = (blockIdx.x % ntz) * TZ, y0 = (blockIdx.x / ntz) * TY;
   const int xb = blockIdx.y * lx, xe = min(xb + lx, n0);
@@ -47,62 +49,71 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 
   for (int i = tid; i < HY; i += NT) gys[i] = wrap(y0 - 1 + i, n1);
   for (int i = tid; i < HZ; i += NT) gzs[i] = wrap(z0 - 1 + i, n2);
+  __syncthreads();
 
+  // per-thread offsets (within a node plane) of the plane values this thread loads, and of its element's s
+  long poff[PF];
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    const int idx = tid + i * NT;
+    poff[i] = -1;
+    if (idx < 3 * NP) {
+      const int c = idx / NP, r = idx - c * NP;
+      const int hy = r / HZ, hz = r - hy * HZ;
+      poff[i] = c * N + (long)gys[hy] * n2 + gzs[hz];
+    }
+  }
   const bool ev = tid < NE;
   const int ey = tid / EZ, ez = tid - (tid / EZ) * EZ;
+  const long soff = ev ? (long)gys[ey] * n2 + gzs[ez] : 0;
   int cidx[4];  // in-plane corner q = ay + 2 az of this element, in node-plane coordinates
 #pragma unroll
   for (int q = 0; q < 4; ++q) cidx[q] = (ey + (q & 1)) * HZ + ez + (q >> 1);
+  const bool outp = tid < TY * TZ;
+  const int ty = tid / TZ, tz = tid - (tid / TZ) * TZ;
+  const int own = (ty + 1) * HZ + tz + 1;  // the output node in node-plane coordinates
 
-  T lo[3][4], ft[3][4];
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  __syncthreads();
-
-  // prologue: node plane xb - 1 (the lower plane of the first element layer)
-  {
-    const long base = (long)wrap(xb - 1, n0) * n1;
-    for (int i = tid; i < 3 * NP; i += NT) {
-      const int c = i / NP, r = i - c * NP;
-      const int hy = r / HZ, hz = r - hy * HZ;
-      pl[c][r] = __ldg(xv + c * N + (base + gys[hy]) * n2 + gzs[hz]);
+  // prologue: node planes xb - 1 and xb, element scales of layer xb - 1
+#pragma unroll
+  for (int i = 0; i < PF; ++i)
+    if (poff[i] >= 0) {
+      const int idx = tid + i * NT;
+      pl[(xb - 1) & 1][0][idx] = __ldg(xv + (long)wrap(xb - 1, n0) * P + poff[i]);
+      pl[xb & 1][0][idx] = __ldg(xv + (long)wrap(xb, n0) * P + poff[i]);
     }
-  }
+  if (ev) sl[tid] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
   __syncthreads();
-  if (ev) {
+
+  T ft[3][4];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+  for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        lo[c][q] = pl[c][cidx[q]];
-        ft[c][q] = T(0);
-      }
-  }
+    for (int q = 0; q < 4; ++q) ft[c][q] = T(0);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
   for (int k = xb - 1; k < xe; ++k) {
-    __syncthreads();  // all reads of pl (previous layer) and g (previous output) are done
-    {
-      const long base = (long)wrap(k + 1, n0) * n1;
-      for (int i = tid; i < 3 * NP; i += NT) {
-        const int c = i / NP, r = i - c * NP;
-        const int hy = r / HZ, hz = r - hy * HZ;
-        pl[c][r] = __ldg(xv + c * N + (base + gys[hy]) * n2 + gzs[hz]);
-      }
-      const long sbase = (long)wrap(k, n0) * n1;
-      for (int i = tid; i < NE; i += NT) {
-        const int a = i / EZ, b = i - a * EZ;
-        sl[i] = __ldg(sv + (sbase + gys[a]) * n2 + gzs[b]);
-      }
+    // prefetch node plane k + 2 and the scales of layer k + 1 into registers; they land while this layer's
+    // elements are computed and are stored after the first barrier
+    T pre[PF];
+    T pres = T(0);
+    const bool more = k + 1 < xe;
+    if (more) {
+      const long base = (long)wrap(k + 2, n0) * P;
+#pragma unroll
+      for (int i = 0; i < PF; ++i) pre[i] = poff[i] >= 0 ? __ldg(xv + base + poff[i]) : T(0);
+      if (ev) pres = __ldg(sv + (long)wrap(k + 1, n0) * P + soff);
     }
-    __syncthreads();
+    const T(*lo)[NP] = pl[k & 1];
+    const T(*hi)[NP] = pl[(k + 1) & 1];
+    T xo[3] = {T(0), T(0), T(0)};
     if (ev) {
-      T v[3][8], f[3][8], hi[3][4];
+      T v[3][8], f[3][8];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          hi[c][q] = pl[c][cidx[q]];
-          v[c][2 * q] = lo[c][q];
-          v[c][2 * q + 1] = hi[c][q];
+          v[c][2 * q] = lo[c][cidx[q]];
+          v[c][2 * q + 1] = hi[c][cidx[q]];
         }
       const ModeC<T> ks = scale_modec(kc, sl[tid]);
       element_force(v, ks, f);
@@ -115,30 +126,37 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          ft[c][q] = f[c][2 * q + 1];
-          lo[c][q] = hi[c][q];
-        }
+        for (int q = 0; q < 4; ++q) ft[c][q] = f[c][2 * q + 1];
     }
-    __syncthreads();
-    if (k >= xb && tid < TY * TZ) {
-      const int ty = tid / TZ, tz = tid - (tid / TZ) * TZ;
+    if (partial && outp && k >= xb) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xo[c] = lo[c][own];
+    }
+    __syncthreads();  // g complete; every read of pl[k & 1] and sl is done
+    if (k >= xb && outp) {
       const int yy = y0 + ty, zz = z0 + tz;
       if (yy < n1 && zz < n2) {
-        // node (ty+1, tz+1) in plane coords is corner q = ay + 2az of element (ty+1-ay, tz+1-az)
+        // node (ty+1, tz+1) is corner q = ay + 2az of element (ty+1-ay, tz+1-az)
         const int e00 = (ty + 1) * EZ + (tz + 1);
-        const long idx = ((long)k * n1 + yy) * n2 + zz;
+        const long idx = (long)k * P + (long)yy * n2 + zz;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const T o = (g[0][c][e00] + g[1][c][e00 - EZ]) + (g[2][c][e00 - 1] + g[3][c][e00 - EZ - 1]);
           yv[c * N + idx] = o;
           if (partial) {
             acc[c] += (double)o;
-            acc[3] += (double)__ldg(xv + c * N + idx) * (double)o;
+            acc[3] += (double)xo[c] * (double)o;
           }
         }
       }
     }
+    if (more) {
+#pragma unroll
+      for (int i = 0; i < PF; ++i)
+        if (poff[i] >= 0) pl[k & 1][0][tid + i * NT] = pre[i];  // plane k + 2 replaces plane k
+      if (ev) sl[tid] = pres;
+    }
+    __syncthreads();  // next layer's planes and scales are in place; g is free again
   }
   if (partial) {
     block_sum<4>(acc, red);
@@ -158,17 +176,17 @@ template <typename T>
 struct ApplyTile;
 template <>
 struct ApplyTile<float> {
-  static constexpr int TY = 8, TZ = 32;
+  static constexpr int TY = 8, TZ = 32, MINB = 2;
 };
 template <>
 struct ApplyTile<double> {
-  static constexpr int TY = 8, TZ = 16;
+  static constexpr int TY = 8, TZ = 16, MINB = 3;
 };
 
 template <typename T>
 int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y, const CellState* cs,
                  double* partial, int* nblk_out, cudaStream_t st) {
-  constexpr int TY = ApplyTile<T>::TY, TZ = ApplyTile<T>::TZ;
+  constexpr int TY = ApplyTile<T>::TY, TZ = ApplyTile<T>::TZ, MINB = ApplyTile<T>::MINB;
   constexpr int NT = ((TY + 1) * (TZ + 1) + 31) / 32 * 32;
   const Geom& g = h.g;
   const int tiles = ((g.n2 + TZ - 1) / TZ) * ((g.n1 + TY - 1) / TY);
@@ -182,7 +200,7 @@ int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x,
   dim3 grid(tiles, chunks, nvec);
   const int kind = sizeof(T) == 4 ? PK_APPLY32 : PK_APPLY64;
   ProfScope ps(kind, st);
-  k_apply<T, TY, TZ><<<grid, NT, 0, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs,
+  k_apply<T, TY, TZ, MINB><<<grid, NT, 0, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs,
                                           make_modec<T>(h.lam, h.mu), partial, prof_units(), kind);
   NLF_CHECK_LAUNCH();
   return NLF_OK;

@@ -65,6 +65,9 @@ __host__ __device__ __forceinline__ int ilog2(int n) {
   return l;
 }
 
+// x / d with a shift when d is a power of two (the usual grid sides)
+__device__ __forceinline__ int fdiv(int x, int d) { return is_pow2(d) ? (x >> (31 - __clz(d))) : x / d; }
+
 // Block-wide sum of K doubles; result valid in thread 0. `sh` needs 32*K doubles.
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* sh) {

@@ -11,20 +11,148 @@
 // Power-of-two lines use an iterative radix-2 FFT; other lengths (small test grids) a direct DFT.
 // Kinv is the reference's symbol: the FFT of the unit-stiffness impulse response, which is the real symmetric
 // sum over the 27 stencil blocks W_d cos(k.d); K(0) = I; Kinv = inv(K + 1e-12 |tr K| I); Kinv(0) = 0.
+#include <algorithm>
 #include <cmath>
 #include "nlf_internal.h"
 #include "nlf_prof.cuh"
 
 namespace nlf {
 
+// r-point DFT (r in {2, 4, 8}) of a[0..r) in registers; INV selects e^{+2 pi i jk/r}.
+template <typename T, bool INV>
+__device__ __forceinline__ void dft4(cplx<T>& a0, cplx<T>& a1, cplx<T>& a2, cplx<T>& a3) {
+  const cplx<T> s0 = cadd(a0, a2), d0 = csub(a0, a2), s1 = cadd(a1, a3), d1 = csub(a1, a3);
+  // forward: X1 = d0 - i d1, X3 = d0 + i d1; inverse swaps them
+  const cplx<T> id1{-d1.y, d1.x};
+  a0 = cadd(s0, s1);
+  a2 = csub(s0, s1);
+  a1 = INV ? cadd(d0, id1) : csub(d0, id1);
+  a3 = INV ? csub(d0, id1) : cadd(d0, id1);
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ void dft_small(cplx<T> (&a)[8], int r) {
+  if (r == 2) {
+    const cplx<T> t = csub(a[0], a[1]);
+    a[0] = cadd(a[0], a[1]);
+    a[1] = t;
+  } else if (r == 4) {
+    dft4<T, INV>(a[0], a[1], a[2], a[3]);
+  } else {
+    // split into even / odd 4-point DFTs, then X_k = E_k + W^k O_k, X_{k+4} = E_k - W^k O_k
+    cplx<T> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6], o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<T, INV>(e0, e1, e2, e3);
+    dft4<T, INV>(o0, o1, o2, o3);
+    const T c = T(0.70710678118654752440084436210485);
+    // W^1 o1, W^2 o2, W^3 o3 with W = e^{-+2 pi i / 8}
+    cplx<T> w1, w2, w3;
+    if (!INV) {
+      w1 = {c * (o1.x + o1.y), c * (o1.y - o1.x)};
+      w2 = {o2.y, -o2.x};
+      w3 = {c * (o3.y - o3.x), -c * (o3.x + o3.y)};
+    } else {
+      w1 = {c * (o1.x - o1.y), c * (o1.x + o1.y)};
+      w2 = {-o2.y, o2.x};
+      w3 = {-c * (o3.x + o3.y), c * (o3.x - o3.y)};
+    }
+    a[0] = cadd(e0, o0);
+    a[4] = csub(e0, o0);
+    a[1] = cadd(e1, w1);
+    a[5] = csub(e1, w1);
+    a[2] = cadd(e2, w2);
+    a[6] = csub(e2, w2);
+    a[3] = cadd(e3, w3);
+    a[7] = csub(e3, w3);
+  }
+}
+
+// One Stockham autosort stage of radix r over `nlines` lines (src -> dst, same layout). Ns is the product of the
+// radices of the previous stages. Butterfly j reads x[j + t n/r], twiddles by e^{-+2 pi i t k/(Ns r)} with
+// k = j mod Ns, and writes the r outputs to (j / Ns) Ns r + k + t Ns.
+template <typename T, bool INV>
+__device__ void stockham_stage(const cplx<T>* src, cplx<T>* dst, int n, int r, int Ns, int nlines, int inner_n,
+                               int outer_stride, int inner_stride, int es, const cplx<T>* __restrict__ tw) {
+  const int nr = n / r, tstride = n / (Ns * r), total = nlines * nr;
+  const int lgNs = ilog2(Ns);
+  for (int wi = threadIdx.x; wi < total; wi += blockDim.x) {
+    int l, j;
+    if (es == 1) {
+      l = fdiv(wi, nr);
+      j = wi - l * nr;
+    } else {  // strided lines: neighbouring threads take neighbouring lines (contiguous in memory)
+      j = fdiv(wi, nlines);
+      l = wi - j * nlines;
+    }
+    const int lo = fdiv(l, inner_n);
+    const int b = lo * outer_stride + (l - lo * inner_n) * inner_stride;
+    const int k = j & (Ns - 1);
+    cplx<T> a[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t < r) {
+        a[t] = src[b + (j + t * nr) * es];
+        if (t > 0 && k > 0) {
+          cplx<T> w = tw[t * k * tstride];
+          if (INV) w.y = -w.y;
+          a[t] = cmul(a[t], w);
+        }
+      }
+    }
+    dft_small<T, INV>(a, r);
+    const int base = ((j >> lgNs) * r << lgNs) + k;
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < r) dst[b + (base + t * Ns) * es] = a[t];
+  }
+}
+
+// Power-of-two transform by Stockham stages of radix 8/4/2 (an even number of stages when n >= 4, so the result
+// ends in `buf`), ping-ponging with `scratch` (same size and layout as buf). Ends with __syncthreads().
+template <typename T>
+__device__ void lines_fft_stockham(cplx<T>* buf, int n, int nlines, int inner_n, int outer_stride,
+                                   int inner_stride, int es, const cplx<T>* __restrict__ tw, bool inv,
+                                   cplx<T>* scratch) {
+  const int e = ilog2(n);
+  int S = (e + 2) / 3;
+  if ((S & 1) && e >= 2) ++S;
+  cplx<T>* src = buf;
+  cplx<T>* dst = scratch;
+  int Ns = 1;
+  for (int st = 0; st < S; ++st) {
+    const int ex = e / S + (st < e % S ? 1 : 0);
+    const int r = 1 << ex;
+    if (inv)
+      stockham_stage<T, true>(src, dst, n, r, Ns, nlines, inner_n, outer_stride, inner_stride, es, tw);
+    else
+      stockham_stage<T, false>(src, dst, n, r, Ns, nlines, inner_n, outer_stride, inner_stride, es, tw);
+    __syncthreads();
+    cplx<T>* t = src;
+    src = dst;
+    dst = t;
+    Ns *= r;
+  }
+  if (src != buf) {  // odd stage count (n == 2): copy back
+    for (int idx = threadIdx.x; idx < nlines * n; idx += blockDim.x) {
+      const int l = idx / n, j = idx - l * n;
+      const int b = (l / inner_n) * outer_stride + (l % inner_n) * inner_stride;
+      buf[b + j * es] = src[b + j * es];
+    }
+    __syncthreads();
+  }
+}
+
 // Transform `nlines` lines of length n in shared memory. Line l starts at
 // (l / inner_n) * outer_stride + (l % inner_n) * inner_stride, elements are `es` apart. tw[k] = e^{-2 pi i k/n}.
 // `scratch` (nlines * n entries) is used by non-power-of-two lengths only. Ends with __syncthreads().
 template <typename T>
 __device__ void lines_fft(cplx<T>* buf, int n, int nlines, int inner_n, int outer_stride, int inner_stride,
-                          int es, const cplx<T>* __restrict__ tw, bool inv, cplx<T>* scratch) {
+                          int es, const cplx<T>* __restrict__ tw, bool inv, cplx<T>* scratch, bool pingpong) {
   const int tid = threadIdx.x, nt = blockDim.x;
   if (n == 1) return;
+  if (is_pow2(n) && pingpong) {
+    lines_fft_stockham(buf, n, nlines, inner_n, outer_stride, inner_stride, es, tw, inv, scratch);
+    return;
+  }
   if (is_pow2(n)) {
     const int lg = ilog2(n);
     for (int idx = tid; idx < nlines * n; idx += nt) {
@@ -137,8 +265,20 @@ __device__ void real_pre(cplx<T>* buf, int rows, int rs, int n, const cplx<T>* _
   __syncthreads();
 }
 
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+
 struct FftDims {
   int n0, n1, n2, n2h, rs;  // rs: shared row stride of a (y, z) plane
+  bool pp;                  // power-of-two lines ping-pong with an equal-size scratch (Stockham)
   long N, NS;
   int off0, off1, off2, off2h;
 };
@@ -159,17 +299,22 @@ __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T
   const bool packed = (d.n2 % 2) == 0;
   if (packed) {
     const int M = d.n2 / 2;
+    using V2 = typename Vec2<T>::type;
+    const V2* rp2 = reinterpret_cast<const V2*>(rp);  // pair j of row y is element y M + j (N and n2 even)
+    const V2* wp2 = reinterpret_cast<const V2*>(wp);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < d.n1 * M; idx += blockDim.x) {
-      const int y = idx / M, j = idx - y * M;
-      T a = rp[y * d.n2 + 2 * j], b = rp[y * d.n2 + 2 * j + 1];
+      const int y = fdiv(idx, M), j = idx - y * M;
+      V2 ab = rp2[idx];
       if (wp) {
-        a *= wp[y * d.n2 + 2 * j];
-        b *= wp[y * d.n2 + 2 * j + 1];
+        const V2 ww = wp2[idx];
+        ab.x *= ww.x;
+        ab.y *= ww.y;
       }
-      buf[y * d.rs + j] = {a, b};
+      buf[y * d.rs + j] = {ab.x, ab.y};
     }
     __syncthreads();
-    lines_fft(buf, M, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, false, scratch);
+    lines_fft(buf, M, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, false, scratch, d.pp);
     real_post(buf, d.n1, d.rs, d.n2, tw + d.off2);
   } else {
     for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
@@ -179,11 +324,12 @@ __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T
       buf[y * d.rs + z] = {a, T(0)};
     }
     __syncthreads();
-    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, false, scratch);
+    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, false, scratch, d.pp);
   }
   // y transform on the n2h columns
-  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, false, scratch);
+  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, false, scratch, d.pp);
   cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
     const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
     sp[((long)ky * d.n0 + x) * d.n2h + kz] = buf[ky * d.rs + kz];
@@ -202,6 +348,7 @@ __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, 
   if (cs && !cs[vec / m].active) return;
   prof_count(units, ukind);
   const int nkz = min(kc, d.n2h - kz0);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
     const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
     const int x = rem / kc, kz = rem - x * kc;
@@ -210,7 +357,8 @@ __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, 
     buf[idx] = v;
   }
   __syncthreads();
-  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, false, scratch);
+  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, false, scratch, d.pp);
+#pragma unroll 2
   for (int idx = threadIdx.x; idx < d.n0 * kc; idx += blockDim.x) {
     const int kx = idx / kc, kz = idx - kx * kc;
     if (kz < nkz) {
@@ -223,7 +371,8 @@ __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, 
     }
   }
   __syncthreads();
-  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, true, scratch);
+  lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, true, scratch, d.pp);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
     const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
     const int x = rem / kc, kz = rem - x * kc;
@@ -245,16 +394,17 @@ __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ 
   if (cs && !cs[vec / m].active) return;
   prof_count(units, ukind);
   const cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
     const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
     buf[ky * d.rs + kz] = sp[((long)ky * d.n0 + x) * d.n2h + kz];
   }
   __syncthreads();
-  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, true, scratch);
+  lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, true, scratch, d.pp);
   const bool packed = (d.n2 % 2) == 0;
   if (packed) {
     real_pre(buf, d.n1, d.rs, d.n2, tw + d.off2);
-    lines_fft(buf, d.n2 / 2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, true, scratch);
+    lines_fft(buf, d.n2 / 2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, true, scratch, d.pp);
   } else {
     // rebuild the full row from Hermitian symmetry, then a length-n2 inverse DFT
     for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
@@ -262,31 +412,51 @@ __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ 
       if (k >= d.n2h) buf[y * d.rs + k] = cconj(buf[y * d.rs + (d.n2 - k)]);
     }
     __syncthreads();
-    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, true, scratch);
+    lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, true, scratch, d.pp);
   }
   // the packed z transform has length n2/2, so its unnormalised inverse carries n0 n1 n2/2
   const T norm = T((packed ? 2.0 : 1.0) / (double)d.N);
   const long pbase = ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
   const T* wp = w ? w + (long)(vec / m) * d.N + (long)x * d.n1 * d.n2 : nullptr;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
-    const int y = idx / d.n2, zz = idx - y * d.n2;
-    T v;
-    if (packed) {
-      const cplx<T> q = buf[y * d.rs + (zz >> 1)];
-      v = (zz & 1) ? q.y : q.x;
-    } else {
-      v = buf[y * d.rs + zz].x;
+  if (packed) {  // one complex entry = the pair (2j, 2j+1) of a row: vector loads and stores of two reals
+    using V2 = typename Vec2<T>::type;
+    const int M = d.n2 / 2;
+    const V2* wp2 = reinterpret_cast<const V2*>(wp);
+    const V2* rp2 = reinterpret_cast<const V2*>(r + pbase);
+    V2* zp2 = reinterpret_cast<V2*>(z + pbase);
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < d.n1 * M; idx += blockDim.x) {
+      const int y = fdiv(idx, M), j = idx - y * M;
+      const cplx<T> q = buf[y * d.rs + j];
+      V2 v{q.x * norm, q.y * norm};
+      if (wp) {
+        const V2 ww = wp2[idx];
+        v.x *= ww.x;
+        v.y *= ww.y;
+      }
+      zp2[idx] = v;
+      if (partial) {
+        const V2 rv = rp2[idx];
+        acc[0] += (double)v.x + (double)v.y;
+        acc[1] += (double)rv.x * (double)v.x + (double)rv.y * (double)v.y;
+        acc[2] += (double)rv.x + (double)rv.y;
+        acc[3] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+      }
     }
-    v *= norm;
-    if (wp) v *= wp[idx];
-    z[pbase + idx] = v;
-    if (partial) {
-      const double rv = (double)r[pbase + idx];
-      acc[0] += (double)v;
-      acc[1] += rv * (double)v;
-      acc[2] += rv;
-      acc[3] += rv * rv;
+  } else {
+    for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
+      const int y = idx / d.n2, zz = idx - y * d.n2;
+      T v = buf[y * d.rs + zz].x * norm;
+      if (wp) v *= wp[idx];
+      z[pbase + idx] = v;
+      if (partial) {
+        const double rv = (double)r[pbase + idx];
+        acc[0] += (double)v;
+        acc[1] += rv * (double)v;
+        acc[2] += rv;
+        acc[3] += rv * rv;
+      }
     }
   }
   if (partial) {
@@ -321,13 +491,13 @@ static bool any_non_pow2(const FftDims& d) {
   return !is_pow2(d.n0) || !is_pow2(d.n1) || (d.n2 % 2 == 0 ? !is_pow2(d.n2 / 2) : d.n2 > 1);
 }
 
+// kz chunk of pass B: the largest balanced chunk whose buffers (x2 with a ping-pong scratch) stay under `target`
 template <typename T>
-static int pick_kc(const FftDims& d, int smem_cap) {
-  const bool np2 = any_non_pow2(d);
-  int kc = d.n2h;
-  auto need = [&](int k) { return (size_t)3 * d.n0 * k * sizeof(cplx<T>) * (np2 ? 2 : 1); };
-  while (kc > 1 && need(kc) > (size_t)smem_cap) kc = (kc + 1) / 2;
-  return kc;
+static int pick_kc(const FftDims& d, size_t target, int mult) {
+  int chunks = 1;
+  auto need = [&](int k) { return (size_t)3 * d.n0 * k * sizeof(cplx<T>) * mult; };
+  while (chunks < d.n2h && need((d.n2h + chunks - 1) / chunks) > target) ++chunks;
+  return (d.n2h + chunks - 1) / chunks;
 }
 
 template <typename T>
@@ -346,16 +516,20 @@ const float* kinv_table<float>(const LinearHandle& h) { return h.t32.kinv; }
 template <typename T>
 int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
                    const CellState* cs, double* partial, cudaStream_t st) {
-  const FftDims d = fft_dims(h);
+  FftDims d = fft_dims(h);
   const bool np2 = any_non_pow2(d);
-  const int cap = h.smem_optin > 0 ? h.smem_optin : 48 * 1024;
-  const size_t plane = (size_t)d.n1 * d.rs * sizeof(cplx<T>) * (np2 ? 2 : 1);
+  const int cap = (h.smem_optin > 0 ? h.smem_optin : 48 * 1024) - 2048;  // room for static shared memory
+  const size_t plane1 = (size_t)d.n1 * d.rs * sizeof(cplx<T>);
+  // Stockham ping-pong needs a scratch plane; non-power-of-two lines need it for the DFT anyway
+  d.pp = 2 * plane1 <= (size_t)cap;
+  const size_t plane = plane1 * ((d.pp || np2) ? 2 : 1);
   if (plane > (size_t)cap) {
     set_error("precond: a (%d x %d) plane needs %zu B of shared memory (> %d)", d.n1, d.n2, plane, cap);
     return NLF_EBADARG;
   }
-  const int kc = pick_kc<T>(d, cap);
-  const size_t smemb = (size_t)3 * d.n0 * kc * sizeof(cplx<T>) * (np2 ? 2 : 1);
+  const int mult = (d.pp || np2) ? 2 : 1;
+  const int kc = pick_kc<T>(d, std::min<size_t>(64 * 1024, (size_t)cap), mult);
+  const size_t smemb = (size_t)3 * d.n0 * kc * sizeof(cplx<T>) * mult;
   const cplx<T>* tw = twiddles<T>(h);
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_a<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
