@@ -131,6 +131,35 @@ NLF_API int nlf_C_full(nlf_linear* h, int ncell, const double* rho, const double
  * out (nx, ny, nz/2+1, 6) in the order xx yy zz yz xz xy. */
 NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
 
+/* ---- finite-strain homogenization (nlfiber/mech.py) ------------------------------------------------------- */
+
+/* nlfiber/mech.py:91-103 Cell(rho, E, nu, material, wls, emin, p) without the density: material 0 = linear,
+ * 1 = neo-Hookean; wls_b <= 0 means no void interpolation (wls=None). */
+NLF_API int nlf_mech_create(nlf_mech** h, int nx, int ny, int nz, double E, double nu, int material, double wls_b,
+                            double wls_r0, double emin, double p);
+NLF_API int nlf_mech_destroy(nlf_mech* h);
+/* mech.py:101-113,292-294: s = emin + (1 - emin) clip01(rho)^p and the WLS gamma on the device; optional copies of
+ * s, gamma (nx, ny, nz) and the preconditioner scale sws = exp(mean log s). */
+NLF_API int nlf_mech_set_rho(nlf_mech* h, const double* rho, double* s, double* gamma, double* sws, void* stream);
+/* mech.py:141-152,166-169,191-192 energy / jax.grad: W = wq sum_g sum_e s psi_eff(Fbar + H_g); gw = dW/dw
+ * (nx, ny, nz, 3) and P = dW/dFbar (3, 3, the mean stress) when not NULL. */
+NLF_API int nlf_mech_energy(nlf_mech* h, const double* w, const double* Fbar, double* W, double* gw, double* P,
+                            void* stream);
+/* mech.py:154-164,227-238 tangent_g + hvp_A, matrix-free: the second derivative of W at (w, Fbar) applied to the
+ * direction (v (nx, ny, nz, 3), dFbar (3, 3)) -> (hv (nx, ny, nz, 3), hP (3, 3)). */
+NLF_API int nlf_mech_hvp(nlf_mech* h, const double* w, const double* Fbar, const double* v, const double* dFbar,
+                         double* hv, double* hP, void* stream);
+/* mech.py:172-189 precond_w: inverse of the homogeneous unit-stiffness operator (N x the linear symbol). */
+NLF_API int nlf_mech_precond_w(nlf_mech* h, const double* r, double* z, void* stream);
+/* mech.py:127-129 grad_w: displacement gradient at the Gauss points, H (8, nx, ny, nz, 3, 3). */
+NLF_API int nlf_mech_grad_w(nlf_mech* h, const double* w, double* H, void* stream);
+/* mech.py:264-290 _cg_impl at the linearization point (w, Fbar) with k free macro components
+ * free_idx = (a0, b0, a1, b1, ...): PCG for H x = b on z-vectors (3N + k: w then the macro unknowns), with the
+ * reference's guards (negative curvature exit, x = M b if it happens at the first iteration). */
+NLF_API int nlf_mech_cg(nlf_mech* h, const double* w, const double* Fbar, int k, const int* free_idx, const double* b,
+                        const double* dmac, double sws, double tol, int maxit, double* x, int* it, int* conv, int* neg,
+                        int check_every, void* stream);
+
 /* ---- kernel profiler ------------------------------------------------------------------------------------- */
 
 /* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library

@@ -420,6 +420,10 @@ struct nlf_linear {
   LinearHandle h;
 };
 
+namespace nlf {
+LinearHandle& linear_handle(nlf_linear* h) { return h->h; }
+}  // namespace nlf
+
 // ---- staging helpers --------------------------------------------------------------------------------------------
 namespace {
 

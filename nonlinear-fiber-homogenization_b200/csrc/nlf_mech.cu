@@ -1,0 +1,920 @@
+// Finite-strain periodic homogenization (nlfiber/mech.py): energy, residual, mean stress, matrix-free tangent
+// matvec and the preconditioned CG of the Newton step, on the GPU in FP64.
+//
+// The reference gets the residual by autodiff of the energy and stores the Gauss-point tangent, 648 doubles per
+// element (mech.py:154-169,227-238). Here the first Piola stress P = d psi_eff / dF and the tangent action
+// dP = d2 psi_eff / dF dF : dF are closed forms evaluated at each of the 8 Gauss points from the state, so a
+// tangent matvec reads the state and the direction and nothing else:
+//   psi_eff(F) = psi(F_g) - psi_lin(F_g) + psi_lin(F),   F_g = I + gamma (F - I)       (mech.py:134-139)
+//   P_eff      = gamma (P(F_g) - sig_lin(F_g)) + sig_lin(F)
+//   dP_eff     = gamma^2 (dP(F_g; dF) - dsig_lin(dF)) + dsig_lin(dF)
+//   neo-Hookean: P = mu (F - F^-T) + lam lnJ F^-T,
+//                dP = mu dF + (mu - lam lnJ) F^-T dF^T F^-T + lam (F^-T : dF) F^-T.
+// Element forces go to a [24][N] buffer; a gather kernel sums the 8 contributions of each node in a fixed order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "nlf_vec.cuh"
+#include "nlf_prof.cuh"
+
+namespace nlf {
+
+__constant__ double cDN[8][8][3];  // shape-function gradients [gauss][node][dim] (nlfiber/linear.py:33-41)
+
+struct MechDev {
+  int n0, n1, n2;
+  long N;
+  double lam, mu, wq;
+  int material;  // 0 linear, 1 neo-Hookean
+  int use_gamma;
+  const double* s;
+  const double* gamma;
+};
+
+// ---- material laws ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double det3(const double (&F)[9]) {
+  return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+         F[2] * (F[3] * F[7] - F[4] * F[6]);
+}
+
+// G = F^-T = cof(F) / det F
+__device__ __forceinline__ void inv_t3(const double (&F)[9], double J, double (&G)[9]) {
+  const double iJ = 1.0 / J;
+  G[0] = (F[4] * F[8] - F[5] * F[7]) * iJ;
+  G[1] = -(F[3] * F[8] - F[5] * F[6]) * iJ;
+  G[2] = (F[3] * F[7] - F[4] * F[6]) * iJ;
+  G[3] = -(F[1] * F[8] - F[2] * F[7]) * iJ;
+  G[4] = (F[0] * F[8] - F[2] * F[6]) * iJ;
+  G[5] = -(F[0] * F[7] - F[1] * F[6]) * iJ;
+  G[6] = (F[1] * F[5] - F[2] * F[4]) * iJ;
+  G[7] = -(F[0] * F[5] - F[2] * F[3]) * iJ;
+  G[8] = (F[0] * F[4] - F[1] * F[3]) * iJ;
+}
+
+__device__ __forceinline__ double psi_lin(const double (&F)[9], double lam, double mu) {
+  const double e0 = F[0] - 1.0, e1 = F[4] - 1.0, e2 = F[8] - 1.0;
+  const double e01 = 0.5 * (F[1] + F[3]), e02 = 0.5 * (F[2] + F[6]), e12 = 0.5 * (F[5] + F[7]);
+  const double tr = e0 + e1 + e2;
+  return 0.5 * lam * tr * tr + mu * (e0 * e0 + e1 * e1 + e2 * e2 + 2.0 * (e01 * e01 + e02 * e02 + e12 * e12));
+}
+
+// P += c * sig_lin(F) (sym gradient of F - I)
+__device__ __forceinline__ void add_sig_lin(const double (&F)[9], double lam, double mu, double c, double (&P)[9]) {
+  const double tr = lam * (F[0] + F[4] + F[8] - 3.0);
+  P[0] += c * (tr + 2.0 * mu * (F[0] - 1.0));
+  P[4] += c * (tr + 2.0 * mu * (F[4] - 1.0));
+  P[8] += c * (tr + 2.0 * mu * (F[8] - 1.0));
+  const double s01 = mu * (F[1] + F[3]), s02 = mu * (F[2] + F[6]), s12 = mu * (F[5] + F[7]);
+  P[1] += c * s01;
+  P[3] += c * s01;
+  P[2] += c * s02;
+  P[6] += c * s02;
+  P[5] += c * s12;
+  P[7] += c * s12;
+}
+
+// dP += c * dsig_lin(dF)
+__device__ __forceinline__ void add_dsig_lin(const double (&d)[9], double lam, double mu, double c, double (&P)[9]) {
+  const double tr = lam * (d[0] + d[4] + d[8]);
+  P[0] += c * (tr + 2.0 * mu * d[0]);
+  P[4] += c * (tr + 2.0 * mu * d[4]);
+  P[8] += c * (tr + 2.0 * mu * d[8]);
+  const double s01 = mu * (d[1] + d[3]), s02 = mu * (d[2] + d[6]), s12 = mu * (d[5] + d[7]);
+  P[1] += c * s01;
+  P[3] += c * s01;
+  P[2] += c * s02;
+  P[6] += c * s02;
+  P[5] += c * s12;
+  P[7] += c * s12;
+}
+
+__device__ __forceinline__ double psi_nh(const double (&F)[9], double lam, double mu) {
+  const double J = det3(F);
+  double I1 = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) I1 += F[q] * F[q];
+  const double lnJ = log(J);  // NaN for J <= 0, as the reference's jnp.log
+  return 0.5 * mu * (I1 - 3.0) - mu * lnJ + 0.5 * lam * lnJ * lnJ;
+}
+
+__device__ __forceinline__ void add_P_nh(const double (&F)[9], double lam, double mu, double c, double (&P)[9]) {
+  const double J = det3(F);
+  double G[9];
+  inv_t3(F, J, G);
+  const double lnJ = log(J);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) P[q] += c * (mu * (F[q] - G[q]) + lam * lnJ * G[q]);
+}
+
+__device__ __forceinline__ void add_dP_nh(const double (&F)[9], const double (&d)[9], double lam, double mu,
+                                          double c, double (&P)[9]) {
+  const double J = det3(F);
+  double G[9];
+  inv_t3(F, J, G);
+  const double lnJ = log(J);
+  double GdF = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) GdF += G[q] * d[q];
+  // T = G dF^T G: T_ij = sum_kl G_ik dF_lk G_lj
+  double M[9];  // M = G dF^T: M_il = sum_k G_ik dF_lk
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) M[i * 3 + l] = G[i * 3] * d[l * 3] + G[i * 3 + 1] * d[l * 3 + 1] + G[i * 3 + 2] * d[l * 3 + 2];
+  const double cm = mu - lam * lnJ;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double T = M[i * 3] * G[j] + M[i * 3 + 1] * G[3 + j] + M[i * 3 + 2] * G[6 + j];
+      P[i * 3 + j] += c * (mu * d[i * 3 + j] + cm * T + lam * GdF * G[i * 3 + j]);
+    }
+}
+
+// psi_eff, P_eff, dP_eff (mech.py:134-139) at one Gauss point, scaled by c = wq s
+__device__ __forceinline__ double psi_eff(const MechDev& a, const double (&F)[9], double gam) {
+  if (a.material == 0) return psi_lin(F, a.lam, a.mu);
+  if (!a.use_gamma) return psi_nh(F, a.lam, a.mu);
+  double Fg[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Fg[q] = (q % 4 == 0 ? 1.0 : 0.0) + gam * (F[q] - (q % 4 == 0 ? 1.0 : 0.0));
+  return psi_nh(Fg, a.lam, a.mu) - psi_lin(Fg, a.lam, a.mu) + psi_lin(F, a.lam, a.mu);
+}
+
+__device__ __forceinline__ void add_P_eff(const MechDev& a, const double (&F)[9], double gam, double c,
+                                          double (&P)[9]) {
+  if (a.material == 0) {
+    add_sig_lin(F, a.lam, a.mu, c, P);
+    return;
+  }
+  if (!a.use_gamma) {
+    add_P_nh(F, a.lam, a.mu, c, P);
+    return;
+  }
+  double Fg[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Fg[q] = (q % 4 == 0 ? 1.0 : 0.0) + gam * (F[q] - (q % 4 == 0 ? 1.0 : 0.0));
+  add_P_nh(Fg, a.lam, a.mu, c * gam, P);
+  add_sig_lin(Fg, a.lam, a.mu, -c * gam, P);
+  add_sig_lin(F, a.lam, a.mu, c, P);
+}
+
+__device__ __forceinline__ void add_dP_eff(const MechDev& a, const double (&F)[9], const double (&d)[9], double gam,
+                                           double c, double (&P)[9]) {
+  if (a.material == 0) {
+    add_dsig_lin(d, a.lam, a.mu, c, P);
+    return;
+  }
+  if (!a.use_gamma) {
+    add_dP_nh(F, d, a.lam, a.mu, c, P);
+    return;
+  }
+  double Fg[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Fg[q] = (q % 4 == 0 ? 1.0 : 0.0) + gam * (F[q] - (q % 4 == 0 ? 1.0 : 0.0));
+  add_dP_nh(Fg, d, a.lam, a.mu, c * gam * gam, P);
+  add_dsig_lin(d, a.lam, a.mu, c * (1.0 - gam * gam), P);
+}
+
+// ---- element kernel ------------------------------------------------------------------------------------------
+// MODE 0: energy, element forces of P, sum of P (10 partials); 1: element forces of dP, sum of dP (9);
+// 2: energy only (1). Vectors are SoA [3][N]; fe is [24][N] (dof 3a + c of the element's node a).
+constexpr int kMechThreads = 128;
+
+template <int MODE>
+__global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const double* __restrict__ w,
+                                                            const double* __restrict__ Fbar,
+                                                            const double* __restrict__ v,
+                                                            const double* __restrict__ dFm,
+                                                            double* __restrict__ fe, double* __restrict__ partial) {
+  constexpr int NP = MODE == 0 ? 10 : (MODE == 1 ? 9 : 1);
+  __shared__ double red[32 * NP];
+  double acc[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q) acc[q] = 0.0;
+  double Fb[9], dM[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    Fb[q] = Fbar[q];
+    dM[q] = MODE == 1 ? dFm[q] : 0.0;
+  }
+  const long N = a.N;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < N; e += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % a.n2), j = (int)((e / a.n2) % a.n1), i = (int)(e / ((long)a.n1 * a.n2));
+    long nid[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      nid[q] = ((long)wrap(i + (q & 1), a.n0) * a.n1 + wrap(j + ((q >> 1) & 1), a.n1)) * a.n2 +
+               wrap(k + (q >> 2), a.n2);
+    double wn[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) wn[c][q] = w[c * N + nid[q]];
+    double vn[3][8];
+    if (MODE == 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) vn[c][q] = v[c * N + nid[q]];
+    }
+    const double cs = a.wq * a.s[e];
+    const double gam = a.use_gamma ? a.gamma[e] : 1.0;
+    double fa[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) fa[c][q] = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < 8; ++g) {
+      double F[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double h = 0.0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h += wn[c][q] * cDN[g][q][d];
+          F[c * 3 + d] = Fb[c * 3 + d] + h;
+        }
+      double P[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) P[q] = 0.0;
+      if (MODE == 0 || MODE == 2) acc[0] += cs * psi_eff(a, F, gam);
+      if (MODE == 0) add_P_eff(a, F, gam, cs, P);
+      if (MODE == 1) {
+        double dF[9];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            double h = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) h += vn[c][q] * cDN[g][q][d];
+            dF[c * 3 + d] = dM[c * 3 + d] + h;
+          }
+        add_dP_eff(a, F, dF, gam, cs, P);
+      }
+      if (MODE != 2) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[(MODE == 0 ? 1 : 0) + q] += P[q];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            fa[c][q] += P[c * 3] * cDN[g][q][0] + P[c * 3 + 1] * cDN[g][q][1] + P[c * 3 + 2] * cDN[g][q][2];
+      }
+    }
+    if (MODE != 2) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fe[(long)(3 * q + c) * N + e] = fa[c][q];
+    }
+  }
+  block_sum<NP>(acc, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) partial[(long)blockIdx.x * NP + q] = acc[q];
+  }
+}
+
+// out[c][n] = sum_a fe[3a + c][n - off_a]
+__global__ void k_mech_gather(long N, int n0, int n1, int n2, const double* __restrict__ fe, double* __restrict__ out) {
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int k = (int)(n % n2), j = (int)((n / n2) % n1), i = (int)(n / ((long)n1 * n2));
+  double o[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const long e = ((long)wrap(i - (q & 1), n0) * n1 + wrap(j - ((q >> 1) & 1), n1)) * n2 + wrap(k - (q >> 2), n2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] += fe[(long)(3 * q + c) * N + e];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c * N + n] = o[c];
+}
+
+// sum of nb partial rows of width np into out[np] (one block, fixed order)
+__global__ void k_mech_sum(const double* __restrict__ partial, int nb, int np, double* __restrict__ out) {
+  for (int q = threadIdx.x; q < np; q += blockDim.x) {
+    double a = 0.0;
+    for (int b = 0; b < nb; ++b) a += partial[(long)b * np + q];
+    out[q] = a;
+  }
+}
+
+__global__ void k_mech_scale(int n0, int n1, int n2, const double* __restrict__ rho, double emin, double p,
+                             double wb, double r0, double* __restrict__ s, double* __restrict__ gamma,
+                             double* __restrict__ logs) {
+  const long N = (long)n0 * n1 * n2;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= N) return;
+  const double r = rho[e];
+  const double rc = r > 1.0 ? 1.0 : (r < 0.0 ? 0.0 : r);
+  const double v = pow(rc, p);
+  s[e] = emin + (1.0 - emin) * v;  // mech.py:105-106
+  logs[e] = log(s[e]);
+  if (wb > 0.0)  // mech.py:108-113
+    gamma[e] = (tanh(wb * r0) + tanh(wb * (v - r0))) / (tanh(wb * r0) + tanh(wb * (1.0 - r0)));
+}
+
+// displacement gradient at the Gauss points: H[g][n][c][d] = sum_a w_c(e + off_a) DN[g][a][d]
+__global__ void k_mech_gradw(long N, int n0, int n1, int n2, const double* __restrict__ w, double* __restrict__ H) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= N) return;
+  const int k = (int)(e % n2), j = (int)((e / n2) % n1), i = (int)(e / ((long)n1 * n2));
+  double wn[3][8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const long nd = ((long)wrap(i + (q & 1), n0) * n1 + wrap(j + ((q >> 1) & 1), n1)) * n2 + wrap(k + (q >> 2), n2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) wn[c][q] = w[c * N + nd];
+  }
+  for (int g = 0; g < 8; ++g)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double h = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h += wn[c][q] * cDN[g][q][d];
+        H[(((long)g * N + e) * 3 + c) * 3 + d] = h;
+      }
+}
+
+// ---- CG (mech.py:264-290) on z = (w [3][N], macro tail [k]) ------------------------------------------------------
+struct MechCG {
+  double bn, rz, pap, alpha, beta, rr, scale;  // scale = N / sws of the w preconditioner
+  double mAp[3], mz[3];
+  double dmac[9];
+  double tol;
+  int k, it, maxit, done, conv, neg, ran;
+};
+
+constexpr int kCgBlocks = 256;
+
+// partials over the vector: [sum a_w (3), sum a.b (w part)]
+__global__ void k_cg_dot(long N, const double* __restrict__ a, const double* __restrict__ b,
+                         const MechCG* __restrict__ st, double* __restrict__ partial) {
+  __shared__ double red[32 * 4];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (!st->done) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < 3 * N; i += (long)gridDim.x * blockDim.x) {
+      const double x = a[i];
+      acc[i / N] += x;
+      acc[3] += x * b[i];
+    }
+  }
+  block_sum<4>(acc, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) partial[blockIdx.x * 4 + q] = acc[q];
+}
+
+// after Ap = H p: mean of Ap's w part, pAp (tail included, p is mean-free), alpha and the negative-curvature flag
+__global__ void k_cg_fin_pap(long N, const double* __restrict__ partial, int nb, const double* __restrict__ p,
+                             const double* __restrict__ Ap, MechCG* st) {
+  if (threadIdx.x != 0 || st->done) return;
+  double s[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nb; ++b)
+    for (int q = 0; q < 4; ++q) s[q] += partial[b * 4 + q];
+  double pap = s[3];
+  for (int t = 0; t < st->k; ++t) pap += p[3 * N + t] * Ap[3 * N + t];
+  for (int c = 0; c < 3; ++c) st->mAp[c] = s[c] / (double)N;
+  st->pap = pap;
+  st->neg = pap <= 0.0;
+  st->alpha = st->neg ? 0.0 : st->rz / pap;
+  st->ran = 1;
+}
+
+// x1 = x + a p, r1 = r - a (Ap - mean): on negative curvature x = z0 at it == 0 else x unchanged
+__global__ void k_cg_xr(long N, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                        const double* __restrict__ Ap, const double* __restrict__ z0, const MechCG* __restrict__ st) {
+  if (st->done) return;
+  const double a = st->alpha;
+  const long L = 3 * N + st->k;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < L; i += (long)gridDim.x * blockDim.x) {
+    const double ap = i < 3 * N ? Ap[i] - st->mAp[i / N] : Ap[i];
+    r[i] -= a * ap;
+    if (st->neg) {
+      if (st->it == 0) x[i] = z0[i];
+    } else {
+      x[i] += a * p[i];
+    }
+  }
+}
+
+// after the preconditioner (w part unscaled in zf): mean of z, rz1, rr, convergence, beta, counters
+__global__ void k_cg_fin_pc(long N, int n0, const double* __restrict__ partial, const double* __restrict__ r,
+                            MechCG* st, int init) {
+  if (threadIdx.x != 0 || st->done) return;
+  double a[3][4];
+  for (int c = 0; c < 3; ++c)
+    for (int q = 0; q < 4; ++q) {
+      double v = 0.0;
+      for (int x = 0; x < n0; ++x) v += partial[((long)c * n0 + x) * 4 + q];
+      a[c][q] = v;
+    }
+  double rz1 = 0.0, rr = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    st->mz[c] = a[c][0] / (double)N;
+    rz1 += st->scale * (a[c][1] - st->mz[c] * a[c][2]);
+    rr += a[c][3];
+  }
+  for (int t = 0; t < st->k; ++t) {
+    const double rt = r[3 * N + t];
+    rz1 += rt * rt / st->dmac[t];
+    rr += rt * rt;
+  }
+  st->rr = rr;
+  if (init) {
+    st->bn = sqrt(rr) + 1e-300;
+    st->rz = rz1;
+    return;
+  }
+  const bool conv1 = sqrt(rr) <= st->tol * st->bn;
+  st->beta = rz1 / (st->rz == 0.0 ? 1.0 : st->rz);
+  st->rz = rz1;
+  st->it += 1;
+  st->conv = conv1 && !st->neg;
+  st->done = st->neg || conv1 || st->it >= st->maxit;
+}
+
+// p1 = scale (zf - mean) + beta p (w part), r_t / dmac_t + beta p_t (tail); init: p = z0 = M b (also kept in z0)
+__global__ void k_cg_p(long N, double* __restrict__ p, const double* __restrict__ zf, const double* __restrict__ r,
+                       double* __restrict__ z0, const MechCG* __restrict__ st, int init) {
+  if (!init && !st->ran) return;
+  const double be = init ? 0.0 : st->beta;
+  const long L = 3 * N + st->k;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < L; i += (long)gridDim.x * blockDim.x) {
+    const double z = i < 3 * N ? st->scale * (zf[i] - st->mz[i / N]) : r[i] / st->dmac[i - 3 * N];
+    if (init) {
+      p[i] = z;
+      z0[i] = z;
+    } else {
+      p[i] = z + be * p[i];
+    }
+  }
+}
+
+__global__ void k_cg_clear_ran(MechCG* st) { st->ran = 0; }
+
+// b = proj(b): subtract the mean of the w part (in place) using k_cg_dot partials of (b, b)
+__global__ void k_cg_mean_sub(long N, double* __restrict__ b, const double* __restrict__ partial, int nb) {
+  __shared__ double m[3];
+  if (threadIdx.x < 3) {
+    double a = 0.0;
+    for (int q = 0; q < nb; ++q) a += partial[q * 4 + threadIdx.x];
+    m[threadIdx.x] = a / (double)N;
+  }
+  __syncthreads();
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < 3 * N; i += (long)gridDim.x * blockDim.x)
+    b[i] -= m[i / N];
+}
+
+}  // namespace nlf
+
+using namespace nlf;
+
+struct nlf_mech {
+  nlf_linear* lin = nullptr;  // FFT tables and geometry of the preconditioner
+  MechDev d{};
+  double wls_b = 0.0, wls_r0 = 0.0, emin = 0.0, p = 3.0, sws = 1.0;
+  bool rho_set = false;
+  DevBuf state;  // s, gamma, logs
+  DevBuf ws;     // vectors and partials
+  DevBuf io;     // staging
+};
+
+namespace {
+
+size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+bool on_dev(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// device copy of a (count) float64 input: the pointer itself or a staged copy at io + off
+int stage(const double* src, size_t count, DevBuf& io, size_t off, const double** out, cudaStream_t st) {
+  if (!src) {
+    *out = nullptr;
+    return NLF_OK;
+  }
+  if (on_dev(src)) {
+    *out = src;
+    return NLF_OK;
+  }
+  double* dst = reinterpret_cast<double*>((char*)io.ptr + off);
+  NLF_CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, st));
+  *out = dst;
+  return NLF_OK;
+}
+
+int copy_back(double* dst, const double* src, size_t count, cudaStream_t st) {
+  NLF_CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(double),
+                               on_dev(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  return NLF_OK;
+}
+
+LinearHandle& lin_of(nlf_mech* H);
+
+}  // namespace
+
+// access to the linear handle's internals (defined in nlf_linear.cu)
+namespace nlf {
+LinearHandle& linear_handle(nlf_linear* h);
+}
+
+namespace {
+LinearHandle& lin_of(nlf_mech* H) { return nlf::linear_handle(H->lin); }
+
+// one element pass of MODE over the SoA state w (device) with macro Fbar (device 9), direction v, dFm
+template <int MODE>
+int mech_pass(nlf_mech* H, const double* w, const double* Fb, const double* v, const double* dFm, double* fe,
+              double* partial, int* nb, cudaStream_t st) {
+  const long N = H->d.N;
+  const int blocks = (int)std::min<long>((N + kMechThreads - 1) / kMechThreads, 4L * 148 * 4);
+  *nb = blocks;
+  ProfScope ps(PK_OTHER, st);
+  k_mech_elem<MODE><<<blocks, kMechThreads, 0, st>>>(H->d, w, Fb, v, dFm, fe, partial);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+int gather(nlf_mech* H, const double* fe, double* out, cudaStream_t st) {
+  const long N = H->d.N;
+  ProfScope ps(PK_OTHER, st);
+  k_mech_gather<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, H->d.n0, H->d.n1, H->d.n2, fe, out);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+bool bad(nlf_mech* H) {
+  if (!H || !H->rho_set) {
+    set_error("mech handle is null or has no density (call nlf_mech_set_rho)");
+    return true;
+  }
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+NLF_API int nlf_mech_create(nlf_mech** out, int nx, int ny, int nz, double E, double nu, int material,
+                            double wls_b, double wls_r0, double emin, double p) {
+  if (!out || (material != 0 && material != 1)) {
+    set_error("nlf_mech_create: bad arguments (material 0 = linear, 1 = neo-Hookean)");
+    return NLF_EBADARG;
+  }
+  *out = nullptr;
+  nlf_mech* H = new nlf_mech();
+  int stc = nlf_linear_create(&H->lin, nx, ny, nz, E, nu, emin, p, 1e-9, 1);
+  if (stc != NLF_OK) {
+    delete H;
+    return stc;
+  }
+  const LinearHandle& L = lin_of(H);
+  H->d.n0 = nx;
+  H->d.n1 = ny;
+  H->d.n2 = nz;
+  H->d.N = L.g.N;
+  H->d.lam = L.lam;
+  H->d.mu = L.mu;
+  H->d.wq = 1.0 / (8.0 * (double)L.g.N);
+  H->d.material = material;
+  H->d.use_gamma = (material == 1 && wls_b > 0.0) ? 1 : 0;
+  H->wls_b = wls_b;
+  H->wls_r0 = wls_r0;
+  H->emin = emin;
+  H->p = p;
+  // shape-function gradients at the Gauss points (nlfiber/linear.py:22-41)
+  double dN[8][8][3];
+  const double g1[2] = {0.5 - 1.0 / (2.0 * std::sqrt(3.0)), 0.5 + 1.0 / (2.0 * std::sqrt(3.0))};
+  for (int g = 0; g < 8; ++g)
+    for (int a = 0; a < 8; ++a) {
+      const double x = g1[g & 1], y = g1[(g >> 1) & 1], z = g1[(g >> 2) & 1];
+      const int i = a & 1, j = (a >> 1) & 1, k = (a >> 2) & 1;
+      const double fx = i ? x : 1 - x, fy = j ? y : 1 - y, fz = k ? z : 1 - z;
+      const double sx = i ? 1 : -1, sy = j ? 1 : -1, sz = k ? 1 : -1;
+      dN[g][a][0] = sx * fy * fz;
+      dN[g][a][1] = fx * sy * fz;
+      dN[g][a][2] = fx * fy * sz;
+    }
+  cudaError_t e = cudaMemcpyToSymbol(cDN, dN, sizeof(dN));
+  if (e != cudaSuccess) {
+    set_error("nlf_mech_create: %s", cudaGetErrorString(e));
+    nlf_linear_destroy(H->lin);
+    delete H;
+    return NLF_ECUDA;
+  }
+  *out = H;
+  return NLF_OK;
+}
+
+NLF_API int nlf_mech_destroy(nlf_mech* H) {
+  if (!H) return NLF_OK;
+  H->state.release();
+  H->ws.release();
+  H->io.release();
+  nlf_linear_destroy(H->lin);
+  delete H;
+  return NLF_OK;
+}
+
+NLF_API int nlf_mech_set_rho(nlf_mech* H, const double* rho, double* s_out, double* gamma_out, double* sws_out,
+                             void* stream) {
+  if (!H || !rho) {
+    set_error("nlf_mech_set_rho: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = H->d.N;
+  NLF_TRY(H->state.reserve(3 * al(N * 8)));
+  NLF_TRY(H->io.reserve(al(N * 8)));
+  const double* rd = nullptr;
+  NLF_TRY(stage(rho, N, H->io, 0, &rd, st));
+  double* s = reinterpret_cast<double*>(H->state.ptr);
+  double* gam = reinterpret_cast<double*>((char*)H->state.ptr + al(N * 8));
+  double* logs = reinterpret_cast<double*>((char*)H->state.ptr + 2 * al(N * 8));
+  k_mech_scale<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(H->d.n0, H->d.n1, H->d.n2, rd, H->emin, H->p, H->wls_b,
+                                                            H->wls_r0, s, gam, logs);
+  NLF_CHECK_LAUNCH();
+  H->d.s = s;
+  H->d.gamma = gam;
+  // sws = exp(mean log s) (mech.py:292-294), FP64 on the host from the device values
+  std::vector<double> lg(N);
+  NLF_CUDA_TRY(cudaMemcpyAsync(lg.data(), logs, N * 8, cudaMemcpyDeviceToHost, st));
+  if (s_out) NLF_TRY(copy_back(s_out, s, N, st));
+  if (gamma_out && H->wls_b > 0.0) NLF_TRY(copy_back(gamma_out, gam, N, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  double a = 0.0;
+  for (long i = 0; i < N; ++i) a += lg[i];
+  H->sws = std::exp(a / (double)N);
+  if (sws_out) *sws_out = H->sws;
+  H->rho_set = true;
+  return NLF_OK;
+}
+
+// energy W; residual gw = dW/dw (nx, ny, nz, 3) and mean stress P = dW/dFbar (3, 3) when not NULL
+NLF_API int nlf_mech_energy(nlf_mech* H, const double* w, const double* Fbar, double* W, double* gw, double* P,
+                            void* stream) {
+  if (bad(H) || !w || !Fbar || !W) {
+    if (H && H->rho_set) set_error("nlf_mech_energy: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = H->d.N;
+  const size_t o_w = 0, o_ws = al(3 * N * 8), o_fe = o_ws + al(3 * N * 8), o_g = o_fe + al(24 * N * 8);
+  const size_t o_gs = o_g + al(3 * N * 8), o_fb = o_gs + al(3 * N * 8), o_p = o_fb + 256, o_sum = o_p + al(4096 * 10 * 8);
+  NLF_TRY(H->ws.reserve(o_sum + 256));
+  char* b = (char*)H->ws.ptr;
+  NLF_TRY(H->io.reserve(al(3 * N * 8)));
+  const double* wd = nullptr;
+  NLF_TRY(stage(w, 3 * N, H->io, 0, &wd, st));
+  double* ws = reinterpret_cast<double*>(b + o_ws);
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, wd, ws, 1.0, st)));
+  double* fbd = reinterpret_cast<double*>(b + o_fb);
+  NLF_CUDA_TRY(cudaMemcpyAsync(fbd, Fbar, 9 * 8, on_dev(Fbar) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  double* part = reinterpret_cast<double*>(b + o_p);
+  double* sum = reinterpret_cast<double*>(b + o_sum);
+  double* fe = reinterpret_cast<double*>(b + o_fe);
+  int nb = 0;
+  const bool want_g = gw || P;
+  if (want_g) {
+    NLF_TRY(mech_pass<0>(H, ws, fbd, nullptr, nullptr, fe, part, &nb, st));
+    k_mech_sum<<<1, 32, 0, st>>>(part, nb, 10, sum);
+  } else {
+    NLF_TRY(mech_pass<2>(H, ws, fbd, nullptr, nullptr, nullptr, part, &nb, st));
+    k_mech_sum<<<1, 32, 0, st>>>(part, nb, 1, sum);
+  }
+  NLF_CHECK_LAUNCH();
+  double h[10];
+  NLF_CUDA_TRY(cudaMemcpyAsync(h, sum, (want_g ? 10 : 1) * 8, cudaMemcpyDeviceToHost, st));
+  if (gw) {
+    double* gs = reinterpret_cast<double*>(b + o_gs);
+    NLF_TRY(gather(H, fe, gs, st));
+    double* gd = on_dev(gw) ? gw : reinterpret_cast<double*>(b + o_g);
+    NLF_TRY((launch_soa_to_aos<double, double>(N, 1, gs, gd, st)));
+    if (gd != gw) NLF_TRY(copy_back(gw, gd, 3 * N, st));
+  }
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  *W = h[0];
+  if (P) std::memcpy(P, h + 1, 9 * 8);
+  return NLF_OK;
+}
+
+// tangent at (w, Fbar) applied to (v, dFm): hv (nx, ny, nz, 3) and hP (3, 3) = d(mean stress)
+NLF_API int nlf_mech_hvp(nlf_mech* H, const double* w, const double* Fbar, const double* v, const double* dFm,
+                         double* hv, double* hP, void* stream) {
+  if (bad(H) || !w || !Fbar || !v || !dFm || !hv) {
+    if (H && H->rho_set) set_error("nlf_mech_hvp: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = H->d.N;
+  const size_t V = al(3 * N * 8);
+  const size_t o_ws = 0, o_vs = V, o_fe = 2 * V, o_o = o_fe + al(24 * N * 8), o_os = o_o + V, o_fb = o_os + V;
+  const size_t o_p = o_fb + 256, o_sum = o_p + al(4096 * 10 * 8);
+  NLF_TRY(H->ws.reserve(o_sum + 256));
+  NLF_TRY(H->io.reserve(2 * V));
+  char* b = (char*)H->ws.ptr;
+  const double *wd = nullptr, *vd = nullptr;
+  NLF_TRY(stage(w, 3 * N, H->io, 0, &wd, st));
+  NLF_TRY(stage(v, 3 * N, H->io, V, &vd, st));
+  double* ws = reinterpret_cast<double*>(b + o_ws);
+  double* vs = reinterpret_cast<double*>(b + o_vs);
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, wd, ws, 1.0, st)));
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, vd, vs, 1.0, st)));
+  double* fbd = reinterpret_cast<double*>(b + o_fb);
+  NLF_CUDA_TRY(cudaMemcpyAsync(fbd, Fbar, 72, on_dev(Fbar) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  NLF_CUDA_TRY(cudaMemcpyAsync(fbd + 9, dFm, 72, on_dev(dFm) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  double* fe = reinterpret_cast<double*>(b + o_fe);
+  double* part = reinterpret_cast<double*>(b + o_p);
+  double* sum = reinterpret_cast<double*>(b + o_sum);
+  int nb = 0;
+  NLF_TRY(mech_pass<1>(H, ws, fbd, vs, fbd + 9, fe, part, &nb, st));
+  k_mech_sum<<<1, 32, 0, st>>>(part, nb, 9, sum);
+  NLF_CHECK_LAUNCH();
+  double* os = reinterpret_cast<double*>(b + o_os);
+  NLF_TRY(gather(H, fe, os, st));
+  double* od = on_dev(hv) ? hv : reinterpret_cast<double*>(b + o_o);
+  NLF_TRY((launch_soa_to_aos<double, double>(N, 1, os, od, st)));
+  if (od != hv) NLF_TRY(copy_back(hv, od, 3 * N, st));
+  double h[9];
+  NLF_CUDA_TRY(cudaMemcpyAsync(h, sum, 72, cudaMemcpyDeviceToHost, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hP) std::memcpy(hP, h, 72);
+  return NLF_OK;
+}
+
+// mech.py:187-189 precond_w: N x the linear FFT preconditioner (the mech operator carries wq = 1 / (8N))
+NLF_API int nlf_mech_precond_w(nlf_mech* H, const double* r, double* z, void* stream) {
+  if (!H || !r || !z) {
+    set_error("nlf_mech_precond_w: bad arguments");
+    return NLF_EBADARG;
+  }
+  const LinearHandle& L = lin_of(H);
+  NLF_TRY(nlf_precond(H->lin, 1, r, z, stream));
+  // scale in place (z is host or device)
+  const long n = 3 * L.g.N;
+  if (on_dev(z)) {
+    std::vector<double> t(n);
+    NLF_CUDA_TRY(cudaMemcpy(t.data(), z, n * 8, cudaMemcpyDeviceToHost));
+    for (long i = 0; i < n; ++i) t[i] *= (double)L.g.N;
+    NLF_CUDA_TRY(cudaMemcpy(z, t.data(), n * 8, cudaMemcpyHostToDevice));
+  } else {
+    for (long i = 0; i < n; ++i) z[i] *= (double)L.g.N;
+  }
+  return NLF_OK;
+}
+
+// displacement gradient at the Gauss points (mech.py:127-129): H (8, nx, ny, nz, 3, 3)
+NLF_API int nlf_mech_grad_w(nlf_mech* H, const double* w, double* Hout, void* stream) {
+  if (!H || !w || !Hout) {
+    set_error("nlf_mech_grad_w: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = H->d.N;
+  const size_t V = al(3 * N * 8);
+  NLF_TRY(H->ws.reserve(V + al(72 * N * 8)));
+  NLF_TRY(H->io.reserve(V));
+  const double* wd = nullptr;
+  NLF_TRY(stage(w, 3 * N, H->io, 0, &wd, st));
+  double* ws = reinterpret_cast<double*>(H->ws.ptr);
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, wd, ws, 1.0, st)));
+  double* hd = on_dev(Hout) ? Hout : reinterpret_cast<double*>((char*)H->ws.ptr + V);
+  k_mech_gradw<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, H->d.n0, H->d.n1, H->d.n2, ws, hd);
+  NLF_CHECK_LAUNCH();
+  if (hd != Hout) NLF_TRY(copy_back(Hout, hd, 72 * N, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+// mech.py:264-290 _cg_impl at the linearization point (w, Fbar): solve H x = b for z-vectors
+// (w (nx, ny, nz, 3) flattened, then the k macro unknowns Fbar[free[2j], free[2j+1]]).
+// dmac: (k,) macro preconditioner diagonal; sws: stiffness scale of the w preconditioner.
+// Outputs x (3N + k), *it, *conv, *neg (negative curvature met).
+NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k, const int* free_idx,
+                        const double* b, const double* dmac, double sws, double tol, int maxit, double* x, int* it,
+                        int* conv, int* neg, int check_every, void* stream) {
+  if (bad(H) || !w || !Fbar || !b || !x || k < 0 || k > 9 || (k > 0 && (!free_idx || !dmac)) || maxit < 0) {
+    if (H && H->rho_set) set_error("nlf_mech_cg: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  LinearHandle& L = lin_of(H);
+  const long N = H->d.N;
+  const long Lz = 3 * N + k;
+  // workspace: w, b->r, x, p, Ap, zf, z0, fe, spec, partials, state
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += al(bytes);
+    return o;
+  };
+  const size_t o_w = take(3 * N * 8), o_r = take(Lz * 8), o_x = take(Lz * 8), o_p = take(Lz * 8),
+               o_ap = take(Lz * 8), o_zf = take(3 * N * 8), o_z0 = take(Lz * 8), o_fe = take(24 * N * 8),
+               o_sp = take(3 * L.g.NS * 16), o_pa = take(4096 * 10 * 8), o_pc = take(3 * L.g.n0 * 4 * 8),
+               o_fb = take(256), o_st = take(sizeof(MechCG));
+  NLF_TRY(H->ws.reserve(off));
+  NLF_TRY(H->io.reserve(2 * al(Lz * 8)));
+  char* B = (char*)H->ws.ptr;
+  double* ws = reinterpret_cast<double*>(B + o_w);
+  double* r = reinterpret_cast<double*>(B + o_r);
+  double* xs = reinterpret_cast<double*>(B + o_x);
+  double* p = reinterpret_cast<double*>(B + o_p);
+  double* Ap = reinterpret_cast<double*>(B + o_ap);
+  double* zf = reinterpret_cast<double*>(B + o_zf);
+  double* z0 = reinterpret_cast<double*>(B + o_z0);
+  double* fe = reinterpret_cast<double*>(B + o_fe);
+  cplx<double>* spec = reinterpret_cast<cplx<double>*>(B + o_sp);
+  double* part = reinterpret_cast<double*>(B + o_pa);
+  double* ppc = reinterpret_cast<double*>(B + o_pc);
+  double* fbd = reinterpret_cast<double*>(B + o_fb);
+  MechCG* stt = reinterpret_cast<MechCG*>(B + o_st);
+  // inputs: w -> SoA; b -> r (SoA w part + tail)
+  const double *wd = nullptr, *bd = nullptr;
+  NLF_TRY(stage(w, 3 * N, H->io, 0, &wd, st));
+  NLF_TRY(stage(b, Lz, H->io, al(Lz * 8), &bd, st));
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, wd, ws, 1.0, st)));
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 1, bd, r, 1.0, st)));
+  if (k) NLF_CUDA_TRY(cudaMemcpyAsync(r + 3 * N, bd + 3 * N, k * 8, cudaMemcpyDeviceToDevice, st));
+  NLF_CUDA_TRY(cudaMemcpyAsync(fbd, Fbar, 72, on_dev(Fbar) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  MechCG hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.k = k;
+  hs.maxit = maxit;
+  hs.tol = tol;
+  hs.scale = (double)N / sws;
+  for (int j = 0; j < k; ++j) hs.dmac[j] = dmac[j];
+  hs.done = maxit == 0 ? 1 : 0;
+  NLF_CUDA_TRY(cudaMemcpyAsync(stt, &hs, sizeof(hs), cudaMemcpyHostToDevice, st));
+  NLF_CUDA_TRY(cudaMemsetAsync(xs, 0, Lz * 8, st));
+  const int vb = kCgBlocks, vt = 256;
+  // b = proj(b) (mech.py:267)
+  k_cg_dot<<<vb, vt, 0, st>>>(N, r, r, stt, part);
+  k_cg_mean_sub<<<vb, vt, 0, st>>>(N, r, part, vb);
+  NLF_CHECK_LAUNCH();
+  // z0 = M b, p = z0, rz = (b, z0), bn = ||b||
+  NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, nullptr, nullptr, ppc, st));
+  k_cg_fin_pc<<<1, 32, 0, st>>>(N, L.g.n0, ppc, r, stt, 1);
+  k_cg_p<<<vb, vt, 0, st>>>(N, p, zf, r, z0, stt, 1);
+  NLF_CHECK_LAUNCH();
+  // the macro unknowns enter the element pass as dFm = sum_j p_tail[j] E_sel_j; build it on the device
+  int fidx[18] = {};
+  for (int j = 0; j < 2 * k; ++j) fidx[j] = free_idx[j];
+  const int every = check_every > 0 ? check_every : 8;
+  int host_done = hs.done, iters = 0;
+  while (!host_done) {
+    for (int q = 0; q < every; ++q) {
+      k_cg_clear_ran<<<1, 1, 0, st>>>(stt);
+      // Ap = H p; the macro part of p enters as dFm[a][b] = p_tail[j] for (a, b) = free[j] (fbd[9..17])
+      NLF_CUDA_TRY(cudaMemsetAsync(fbd + 9, 0, 72, st));
+      for (int j = 0; j < k; ++j)
+        NLF_CUDA_TRY(cudaMemcpyAsync(fbd + 9 + fidx[2 * j] * 3 + fidx[2 * j + 1], p + 3 * N + j, 8,
+                                     cudaMemcpyDeviceToDevice, st));
+      int nb = 0;
+      NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, st));
+      double* sum9 = part + 4096 * 9;
+      k_mech_sum<<<1, 32, 0, st>>>(part, nb, 9, sum9);
+      NLF_TRY(gather(H, fe, Ap, st));
+      for (int j = 0; j < k; ++j)
+        NLF_CUDA_TRY(cudaMemcpyAsync(Ap + 3 * N + j, sum9 + fidx[2 * j] * 3 + fidx[2 * j + 1], 8,
+                                     cudaMemcpyDeviceToDevice, st));
+      // proj(Ap) and pAp
+      k_cg_dot<<<vb, vt, 0, st>>>(N, Ap, p, stt, part + 4096 * 10 - 4 * vb);
+      k_cg_fin_pap<<<1, 32, 0, st>>>(N, part + 4096 * 10 - 4 * vb, vb, p, Ap, stt);
+      k_cg_xr<<<vb, vt, 0, st>>>(N, xs, r, p, Ap, z0, stt);
+      NLF_CHECK_LAUNCH();
+      NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, nullptr, nullptr, ppc, st));
+      k_cg_fin_pc<<<1, 32, 0, st>>>(N, L.g.n0, ppc, r, stt, 0);
+      k_cg_p<<<vb, vt, 0, st>>>(N, p, zf, r, z0, stt, 0);
+      NLF_CHECK_LAUNCH();
+    }
+    iters += every;
+    NLF_CUDA_TRY(cudaMemcpyAsync(&hs, stt, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    NLF_CUDA_TRY(cudaStreamSynchronize(st));
+    host_done = hs.done || iters >= maxit + every;
+  }
+  // x (SoA + tail) -> caller layout
+  double* xo = on_dev(x) ? x : reinterpret_cast<double*>((char*)H->io.ptr);
+  NLF_TRY((launch_soa_to_aos<double, double>(N, 1, xs, xo, st)));
+  if (k) NLF_CUDA_TRY(cudaMemcpyAsync(xo + 3 * N, xs + 3 * N, k * 8, cudaMemcpyDeviceToDevice, st));
+  if (xo != x) NLF_TRY(copy_back(x, xo, Lz, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  if (it) *it = hs.it;
+  if (conv) *conv = hs.conv;
+  if (neg) *neg = hs.done && !hs.conv && hs.neg;
+  return NLF_OK;
+}
+
+}  // extern "C"

@@ -22,6 +22,8 @@ EXPORTS = (
     "nlf_stiffness_scale", "nlf_apply_K", "nlf_load", "nlf_precond", "nlf_linear_solve", "nlf_linear_solve_rhs",
     "nlf_bilinear", "nlf_dC_drho", "nlf_C_full", "nlf_precond_symbol", "nlf_apply_K_ex", "nlf_precond_ex",
     "nlf_profile", "nlf_profile_report", "nlf_profile_name", "nlf_bilinear_noalloc",
+    "nlf_mech_create", "nlf_mech_destroy", "nlf_mech_set_rho", "nlf_mech_energy", "nlf_mech_hvp",
+    "nlf_mech_precond_w", "nlf_mech_grad_w", "nlf_mech_cg",
 )
 
 
@@ -68,6 +70,14 @@ def _load():
         "nlf_profile_report": (I, [P, P, P, I]),
         "nlf_profile_name": (ctypes.c_char_p, [I]),
         "nlf_bilinear_noalloc": (I, [I, I, I, D, D, I, P, P, I, P, P, P]),
+        "nlf_mech_create": (I, [ctypes.POINTER(P), I, I, I, D, D, I, D, D, D, D]),
+        "nlf_mech_destroy": (I, [P]),
+        "nlf_mech_set_rho": (I, [P, P, P, P, P, P]),
+        "nlf_mech_energy": (I, [P, P, P, P, P, P, P]),
+        "nlf_mech_hvp": (I, [P, P, P, P, P, P, P, P]),
+        "nlf_mech_precond_w": (I, [P, P, P, P]),
+        "nlf_mech_grad_w": (I, [P, P, P, P]),
+        "nlf_mech_cg": (I, [P, P, P, I, P, P, P, D, D, I, P, P, P, P, I, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

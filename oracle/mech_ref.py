@@ -1,0 +1,310 @@
+"""NumPy FP64 restatement of nlfiber/mech.py (finite-strain periodic homogenization). TEST ORACLE ONLY.
+
+The reference obtains the residual and the tangent by JAX autodiff of the energy (mech.py:154-169,227-238);
+here they are the closed forms of the same functions (first Piola stress and its derivative, applied to a
+direction without forming the 81-entry tangent). tests/test_mech_oracle.py checks both against finite
+differences of the energy and the small-strain limit against the linear oracle.
+"""
+import numpy as np
+
+from .linear_ref import NODES, dN_ref, lame
+
+DN = dN_ref()  # [gauss, node, dim]
+I3 = np.eye(3)
+STALL_RTOL = 1e-6  # nlfiber/mech.py:53
+
+
+def clip01(x):
+    return np.where(x > 1.0, 1.0, np.where(x < 0.0, 0.0, x))
+
+
+# --- materials (nlfiber/mech.py:38-52) --------------------------------------------------------------------------
+def psi_linear(F, lam, mu):
+    H = F - I3
+    eps = 0.5 * (H + np.swapaxes(H, -1, -2))
+    tr = np.trace(eps, axis1=-2, axis2=-1)
+    return 0.5 * lam * tr ** 2 + mu * np.sum(eps * eps, axis=(-2, -1))
+
+
+def psi_neohooke(F, lam, mu):
+    J = np.linalg.det(F)
+    I1 = np.sum(F * F, axis=(-2, -1))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        lnJ = np.log(J)
+    return 0.5 * mu * (I1 - 3.0) - mu * lnJ + 0.5 * lam * lnJ ** 2
+
+
+def sig_linear(F, lam, mu):
+    """d psi_linear / dF = lam tr(eps) I + 2 mu eps."""
+    H = F - I3
+    eps = 0.5 * (H + np.swapaxes(H, -1, -2))
+    return lam * np.trace(eps, axis1=-2, axis2=-1)[..., None, None] * I3 + 2 * mu * eps
+
+
+def P_neohooke(F, lam, mu):
+    """d psi_neohooke / dF = mu (F - F^-T) + lam ln J F^-T."""
+    Fit = np.swapaxes(np.linalg.inv(F), -1, -2)
+    lnJ = np.log(np.linalg.det(F))
+    return mu * (F - Fit) + lam * lnJ[..., None, None] * Fit
+
+
+def dP_neohooke(F, dF, lam, mu):
+    """Directional derivative of P_neohooke: mu dF + (mu - lam lnJ) F^-T dF^T F^-T + lam (F^-T : dF) F^-T."""
+    Fit = np.swapaxes(np.linalg.inv(F), -1, -2)
+    lnJ = np.log(np.linalg.det(F))
+    t = Fit @ np.swapaxes(dF, -1, -2) @ Fit
+    return mu * dF + (mu - lam * lnJ)[..., None, None] * t + lam * np.sum(Fit * dF, axis=(-2, -1))[..., None, None] * Fit
+
+
+def dsig_linear(dF, lam, mu):
+    e = 0.5 * (dF + np.swapaxes(dF, -1, -2))
+    return lam * np.trace(e, axis1=-2, axis2=-1)[..., None, None] * I3 + 2 * mu * e
+
+
+class Cell:
+    """nlfiber/mech.py:88-192 (energy, residual, mean stress; tangent as a matvec)."""
+
+    def __init__(self, rho, E=1.0, nu=0.3, material="neohooke", wls=(500.0, 0.01), emin=1e-3, p=3.0):
+        rho = np.asarray(rho, dtype=np.float64)
+        if rho.ndim == 2:
+            rho = rho[..., None]
+        self.rho, self.shape = rho, tuple(rho.shape)
+        self.N = int(np.prod(self.shape))
+        self.E, self.nu, self.material, self.wls, self.emin, self.p = E, nu, material, wls, emin, p
+        self.lam, self.mu = lame(E, nu)
+        self.wq = 1.0 / (8.0 * self.N)
+        self.s = self.emin + (1.0 - self.emin) * clip01(rho) ** self.p  # mech.py:105-106
+        self.gamma = self.gamma_of(rho)
+
+    def gamma_of(self, rho):
+        """mech.py:108-113."""
+        if self.wls is None:
+            return None
+        b, r0 = self.wls
+        v = clip01(rho) ** self.p
+        return (np.tanh(b * r0) + np.tanh(b * (v - r0))) / (np.tanh(b * r0) + np.tanh(b * (1 - r0)))
+
+    # mech.py:124-132
+    def nodal(self, w):
+        return np.stack([np.roll(w, shift=tuple(-o for o in off), axis=(0, 1, 2)) for off in NODES])
+
+    def grad_w(self, w):
+        return np.einsum("aijkc,gad->gijkcd", self.nodal(w), DN)
+
+    def _gam(self):
+        return np.ones(self.shape) if self.gamma is None else self.gamma
+
+    # mech.py:134-139
+    def psi_eff(self, F, gamma):
+        psi = psi_neohooke if self.material == "neohooke" else psi_linear
+        if gamma is None:
+            return psi(F, self.lam, self.mu)
+        g = gamma[..., None, None]
+        Fg = I3 + g * (F - I3)
+        return psi(Fg, self.lam, self.mu) - psi_linear(Fg, self.lam, self.mu) + psi_linear(F, self.lam, self.mu)
+
+    def P_eff(self, F, gamma):
+        """d psi_eff / dF."""
+        Pm = P_neohooke if self.material == "neohooke" else sig_linear
+        if gamma is None:
+            return Pm(F, self.lam, self.mu)
+        g = gamma[..., None, None]
+        Fg = I3 + g * (F - I3)
+        return g * (Pm(Fg, self.lam, self.mu) - sig_linear(Fg, self.lam, self.mu)) + sig_linear(F, self.lam, self.mu)
+
+    def dP_eff(self, F, dF, gamma):
+        """d^2 psi_eff / dF dF : dF."""
+        if self.material == "neohooke":
+            dPm = lambda Fx, d: dP_neohooke(Fx, d, self.lam, self.mu)  # noqa: E731
+        else:
+            dPm = lambda Fx, d: dsig_linear(d, self.lam, self.mu)  # noqa: E731
+        if gamma is None:
+            return dPm(F, dF)
+        g = gamma[..., None, None]
+        Fg = I3 + g * (F - I3)
+        return g * g * (dPm(Fg, dF) - dsig_linear(dF, self.lam, self.mu)) + dsig_linear(dF, self.lam, self.mu)
+
+    # mech.py:141-152
+    def energy(self, w, Fbar):
+        F = np.asarray(Fbar)[None, None, None, None] + self.grad_w(w)
+        return self.wq * float(np.sum(self.s[None] * self.psi_eff(F, None if self.gamma is None else self.gamma[None])))
+
+    def _scatter(self, Pg):
+        """Nodal gradient of sum_g wq s P_g : grad(v): (nx, ny, nz, 3)."""
+        out = np.zeros(self.shape + (3,))
+        for a, off in enumerate(NODES):
+            fa = np.einsum("gijkcd,gd->ijkc", Pg, DN[:, a])
+            out = out + np.roll(fa, shift=tuple(off), axis=(0, 1, 2))
+        return out
+
+    def grad(self, w, Fbar):
+        """(d W / d w, d W / d Fbar) = (residual (nx, ny, nz, 3), mean stress Pbar (3, 3)) (mech.py:166-169,191)."""
+        F = np.asarray(Fbar)[None, None, None, None] + self.grad_w(w)
+        gam = None if self.gamma is None else self.gamma[None]
+        Pg = self.wq * self.s[None, ..., None, None] * self.P_eff(F, gam)
+        return self._scatter(Pg), Pg.sum(axis=(0, 1, 2, 3))
+
+    def mean_stress(self, w, Fbar):
+        return self.grad(w, Fbar)[1]
+
+    def hvp(self, w, Fbar, v, dFmac):
+        """Tangent (second derivative of W at (w, Fbar)) applied to (v, dFmac): (dw part, dFbar part (3, 3))."""
+        F = np.asarray(Fbar)[None, None, None, None] + self.grad_w(w)
+        dF = np.asarray(dFmac)[None, None, None, None] + self.grad_w(v)
+        gam = None if self.gamma is None else self.gamma[None]
+        dP = self.wq * self.s[None, ..., None, None] * self.dP_eff(F, dF, gam)
+        return self._scatter(dP), dP.sum(axis=(0, 1, 2, 3))
+
+    def precond_symbol(self):
+        """mech.py:172-185: Kinv of the homogeneous linear operator with unit stiffness and weight wq."""
+        from .linear_ref import LinearHomogenization
+        lh = LinearHomogenization(self.shape, E=self.E, nu=self.nu)
+        return lh.Kinv * self.N  # the mech operator is the linear one divided by N (wq = 1 / (8 N))
+
+    def precond_w(self, r):
+        """mech.py:187-189."""
+        Kinv = self.precond_symbol() if not hasattr(self, "_Kinv") else self._Kinv
+        self._Kinv = Kinv
+        rh = np.fft.rfftn(r, axes=(0, 1, 2))
+        return np.fft.irfftn(np.einsum("...ac,...c->...a", Kinv, rh), s=self.shape, axes=(0, 1, 2))
+
+
+class Mixed:
+    """nlfiber/mech.py:195-346: mixed macroscopic control, Newton-CG on z = (w, Fbar_free)."""
+
+    def __init__(self, cell, free=((1, 1), (2, 2)), forcing="ew"):
+        self.c = cell
+        self.free = [tuple(f) for f in free]
+        self.forcing = forcing
+        self.shape = cell.shape
+        self.nw = 3 * cell.N
+        self.k = len(self.free)
+
+    def unpack(self, z, Fb):
+        w = z[: self.nw].reshape(self.shape + (3,))
+        F = np.array(Fb, dtype=np.float64)
+        for j, (a, b) in enumerate(self.free):
+            F[a, b] = z[self.nw + j]
+        return w, F
+
+    def z0(self, Fb):
+        Fb = np.asarray(Fb, dtype=np.float64)
+        return np.concatenate([np.zeros(self.nw), np.array([Fb[a, b] for a, b in self.free])])
+
+    def proj(self, v):
+        w = v[: self.nw].reshape(self.shape + (3,))
+        w = w - w.mean(axis=(0, 1, 2))
+        return np.concatenate([w.ravel(), v[self.nw:]])
+
+    def E(self, z, Fb):
+        return self.c.energy(*self.unpack(z, Fb))
+
+    def g(self, z, Fb):
+        gw, P = self.c.grad(*self.unpack(z, Fb))
+        return np.concatenate([gw.ravel(), np.array([P[a, b] for a, b in self.free])])
+
+    def hvp(self, z, Fb, v):
+        w, F = self.unpack(z, Fb)
+        dFm = np.zeros((3, 3))
+        for j, (a, b) in enumerate(self.free):
+            dFm[a, b] = v[self.nw + j]
+        hw, hP = self.c.hvp(w, F, v[: self.nw].reshape(self.shape + (3,)), dFm)
+        return np.concatenate([hw.ravel(), np.array([hP[a, b] for a, b in self.free])])
+
+    def macro_diag(self, z, Fb):
+        """mech.py:252-258."""
+        d = []
+        for j in range(self.k):
+            e = np.zeros(self.nw + self.k)
+            e[self.nw + j] = 1.0
+            d.append(self.hvp(z, Fb, e)[self.nw + j])
+        return np.abs(np.array(d)) + 1e-12
+
+    def _sws(self):
+        """mech.py:292-294."""
+        return float(np.exp(np.mean(np.log(self.c.s))))
+
+    def precond(self, r, dmac, sws):
+        """mech.py:260-262."""
+        w = self.c.precond_w(r[: self.nw].reshape(self.shape + (3,))) / sws
+        return np.concatenate([w.ravel(), r[self.nw:] / dmac])
+
+    def cg(self, z, Fb, b, dmac, sws, tol, maxit):
+        """mech.py:264-290 (the same guards and exits). Returns (x, it, conv, neg)."""
+        M = lambda r: self.proj(self.precond(r, dmac, sws))  # noqa: E731
+        b = self.proj(b)
+        bn = np.linalg.norm(b) + 1e-300
+        z0 = M(b)
+        x, r, p, rz, it, done, conv = np.zeros_like(b), b, z0, float(b @ z0), 0, False, False
+        while not done and it < maxit:
+            Ap = self.proj(self.hvp(z, Fb, p))
+            pAp = float(p @ Ap)
+            neg = pAp <= 0
+            a = 0.0 if neg else rz / pAp
+            x1, r1 = x + a * p, r - a * Ap
+            conv1 = np.linalg.norm(r1) <= tol * bn
+            z1 = M(r1)
+            rz1 = float(r1 @ z1)
+            p1 = z1 + (rz1 / (1.0 if rz == 0 else rz)) * p
+            x1 = z0 if (neg and it == 0) else (x if neg else x1)
+            x, r, p, rz, it, done, conv = x1, r1, p1, rz1, it + 1, neg or conv1, conv1 and not neg
+        return x, it, conv, done and not conv
+
+    def solve(self, Fbar, z0=None, rtol=1e-9, maxnewton=30, cg_tol=1e-6, cg_maxit=20000, g_ref=None):
+        """mech.py:302-346."""
+        Fb = np.asarray(Fbar, dtype=np.float64)
+        z = self.z0(Fb) if z0 is None else np.asarray(z0, dtype=np.float64)
+        g0, log = g_ref, dict(newton=0, cg=0, converged=False, gnorm=[], negative_curvature=False)
+        eta, gprev = None, None
+        sws = self._sws()
+        for k in range(maxnewton):
+            g = self.proj(self.g(z, Fb))
+            gn = float(np.linalg.norm(g))
+            g0 = gn if g0 is None else g0
+            log["gnorm"].append(gn)
+            if gn <= rtol * max(g0, 1e-300) or gn < 1e-14:
+                log["converged"] = True
+                break
+            tol = cg_tol
+            if self.forcing == "ew":
+                e_new = 0.1 if gprev is None else 0.9 * (gn / gprev) ** 2
+                if eta is not None and 0.9 * eta ** 2 > 0.1:
+                    e_new = max(e_new, 0.9 * eta ** 2)
+                eta = min(e_new, 0.1)
+                tol = max(eta, cg_tol, 0.5 * rtol * g0 / gn) if gprev is not None else max(eta, cg_tol)
+            gprev = gn
+            dmac = self.macro_diag(z, Fb) if self.k else np.zeros(0)
+            dz, its, ok, neg = self.cg(z, Fb, -g, dmac, sws, tol, cg_maxit)
+            log["cg"] += its
+            log["negative_curvature"] |= bool(neg)
+            E0, slope = self.E(z, Fb), float(g @ dz)
+            if slope >= 0:
+                dz = -self.proj(self.precond(g, dmac, sws))
+                slope = float(g @ dz)
+            t = linesearch(lambda x: self.E(x, Fb), lambda x: float(np.linalg.norm(self.proj(self.g(x, Fb)))),
+                           z, dz, E0, slope, gn)
+            log["newton"] = k + 1
+            if t is None:
+                log["linesearch_failed"] = True
+                if gn <= STALL_RTOL * g0:
+                    log["converged"] = log["roundoff_floor"] = True
+                break
+            z = z + t * dz
+        w, F = self.unpack(z, Fb)
+        log["z"], log["g0"] = z, g0
+        return w, F, log
+
+
+def linesearch(E, gnorm, x, dx, E0, slope, gn):
+    """mech.py:73-85."""
+    tol = 64 * np.finfo(np.float64).eps * max(abs(E0), 1e-300)
+    t = 1.0
+    while t > 1e-6:
+        Et = E(x + t * dx)
+        if np.isfinite(Et):
+            if Et <= E0 + 1e-4 * t * slope:
+                return t
+            if Et <= E0 + tol and gnorm(x + t * dx) < gn:
+                return t
+        t *= 0.5
+    return None

@@ -1,0 +1,91 @@
+"""Parity of the CUDA finite-strain path (libnlf.so through nlfiber_b200.mech) with the NumPy oracle (a
+restatement of nlfiber/mech.py whose closed forms are checked by finite differences in test_mech_oracle.py):
+energy, residual, mean stress, tangent matvec, preconditioner, the CG iterates and a Newton-CG solve."""
+import os
+
+os.environ.setdefault("NLF_POISON_WORKSPACE", "1")
+
+import numpy as np  # noqa: E402
+import pytest  # noqa: E402
+
+from oracle import density_ref as OD  # noqa: E402
+from oracle import mech_ref as OM  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    from nlfiber_b200 import mech
+    return mech
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("material,wls", [("neohooke", (500.0, 0.01)), ("neohooke", None), ("linear", None)])
+@pytest.mark.parametrize("shape_n", [3, 4])
+def test_energy_residual_tangent(M, material, wls, shape_n):
+    rho = OD.grey_cell(shape_n, beta=3.0)
+    c, o = M.Cell(rho, material=material, wls=wls), OM.Cell(rho, material=material, wls=wls)
+    np.testing.assert_allclose(c.s, o.s, rtol=1e-14)
+    if wls is not None:
+        np.testing.assert_allclose(c.gamma, o.gamma, rtol=1e-13, atol=1e-15)
+    rng = np.random.default_rng(3)
+    w = 0.05 * rng.standard_normal(c.shape + (3,))
+    Fb = np.eye(3) + 0.05 * rng.standard_normal((3, 3))
+    assert rel(c.energy(w, Fb), o.energy(w, Fb)) < 1e-12
+    gw, P = c.grad(w, Fb)
+    gwo, Po = o.grad(w, Fb)
+    assert rel(gw, gwo) < 1e-12 and rel(P, Po) < 1e-12
+    v = rng.standard_normal(c.shape + (3,))
+    dF = rng.standard_normal((3, 3))
+    hv, hP = c.hvp(w, Fb, v, dF)
+    hvo, hPo = o.hvp(w, Fb, v, dF)
+    assert rel(hv, hvo) < 1e-12 and rel(hP, hPo) < 1e-12
+    assert rel(c.grad_w(w), o.grad_w(w)) < 1e-13
+    assert rel(c.precond_w(v), o.precond_w(v)) < 1e-11
+
+
+def test_cg_iterates_match_oracle(M):
+    rho = OD.grey_cell(3, beta=3.0)
+    c, o = M.Cell(rho), OM.Cell(rho)
+    mix, omix = M.Mixed(c, [(1, 1), (2, 2)]), OM.Mixed(o, [(1, 1), (2, 2)])
+    Fb = np.diag([1.03, 1.0, 1.0])
+    rng = np.random.default_rng(4)
+    z = omix.z0(Fb) + np.concatenate([0.01 * rng.standard_normal(omix.nw), np.zeros(2)])
+    g = omix.proj(omix.g(z, Fb))
+    dmac = omix.macro_diag(z, Fb)
+    sws = omix._sws()
+    x, it, conv, neg = mix._cgA(mix.tangent(z, Fb), -g, dmac, sws, 0.0, 25)
+    xo, ito, convo, nego = omix.cg(z, Fb, -g, dmac, sws, 0.0, 25)
+    assert it == ito == 25 and conv == convo and neg == nego
+    assert rel(x, xo) < 1e-8
+    np.testing.assert_allclose(mix.macro_diag(mix.tangent(z, Fb)), dmac, rtol=1e-12)
+
+
+def test_newton_solve_matches_oracle(M):
+    """Uniaxial stretch 3% with free lateral stretches (qoi.LATERAL[0]): same Newton history and state."""
+    rho = OD.grey_cell(3, beta=3.0)
+    c, o = M.Cell(rho), OM.Cell(rho)
+    Fb = np.diag([1.03, 1.0, 1.0])
+    w, F, log = M.Mixed(c, [(1, 1), (2, 2)]).solve(Fb, rtol=1e-10, cg_tol=1e-10)
+    wo, Fo, logo = OM.Mixed(o, [(1, 1), (2, 2)]).solve(Fb, rtol=1e-10, cg_tol=1e-10)
+    assert log["converged"] and logo["converged"]
+    assert log["newton"] == logo["newton"]
+    np.testing.assert_allclose(F, Fo, atol=1e-9)
+    assert rel(c.mean_stress(w, F), o.mean_stress(wo, Fo)) < 1e-8
+
+
+def test_small_strain_limit_is_linear_C(M):
+    from nlfiber_b200 import linear as L
+    rho = OD.grey_cell(3, beta=3.0)
+    c = M.Cell(rho)
+    C, _, _ = L.LinearHomogenization(rho.shape, emin=c.emin, tol=1e-12).C_full(rho)
+    e = 1e-4
+    w, F, log = M.Mixed(c, free=[]).solve(np.diag([1 + e, 1.0, 1.0]), rtol=1e-10, cg_tol=1e-10)
+    assert log["converged"]
+    P = c.mean_stress(w, F)
+    np.testing.assert_allclose([P[0, 0], P[1, 1], P[2, 2]], C[:3, 0] * e, rtol=2e-3)
