@@ -283,35 +283,85 @@ struct FftDims {
   int off0, off1, off2, off2h;
 };
 
+// Optional fusions of the PCG iteration into the passes (all pointers may be null):
+//   A: r <- r - alpha (Ap - mean Ap) before the transform (written back), partials (sum r, sum r^2) per plane
+//   B: Parseval partial of (w r, K0^-1 w r) = (r, z) per CTA (the half spectrum weighted 1 or 2 per kz)
+//   C: partial sum z per plane (mean removal), without reading r
+struct PcgFuse {
+  const void* Ap;         // A: Ap of this iteration (T, same layout as r)
+  const VecState* vs;     // A: alpha and mean Ap per vector
+  double* partA;          // [vec][comp][x-plane][2]
+  double* partB;          // [vec][ky][chunk]
+  double* partC;          // [vec][comp][x-plane]
+};
+
+// global loads issued together before their first use: enough bytes in flight per thread for HBM latency while
+// keeping the plane kernels at 3 CTAs of 256 threads per SM (at most 85 registers)
+template <typename T>
+constexpr int batch() {
+  return sizeof(T) == 8 ? 4 : 8;
+}
+
 // ---- pass A --------------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T>* __restrict__ spec, FftDims d,
-                        int m, const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs,
-                        unsigned long long* __restrict__ units, int ukind) {
+__global__ void __launch_bounds__(256, 3) k_fft_a(T* __restrict__ r, const T* __restrict__ w, cplx<T>* __restrict__ spec, FftDims d, int m,
+                        const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs,
+                        unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* scratch = buf + d.n1 * d.rs;
+  __shared__ double red[32 * 2];
   const int x = blockIdx.x, c = blockIdx.y, vec = blockIdx.z;
   if (cs && !cs[vec / m].active) return;
   prof_count(units, ukind);
-  const T* rp = r + ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
+  T* rp = r + ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2;
   const T* wp = w ? w + (long)(vec / m) * d.N + (long)x * d.n1 * d.n2 : nullptr;
+  const T* ap = fu.Ap ? static_cast<const T*>(fu.Ap) + ((long)vec * 3 + c) * d.N + (long)x * d.n1 * d.n2 : nullptr;
+  T al = T(0), mu = T(0);
+  if (ap) {
+    al = (T)fu.vs[vec].alpha;
+    mu = (T)fu.vs[vec].mean[c];
+  }
+  double acc[2] = {0.0, 0.0};
+  constexpr int kBatch = batch<T>();
   const bool packed = (d.n2 % 2) == 0;
   if (packed) {
-    const int M = d.n2 / 2;
+    const int M = d.n2 / 2, total = d.n1 * M;
     using V2 = typename Vec2<T>::type;
-    const V2* rp2 = reinterpret_cast<const V2*>(rp);  // pair j of row y is element y M + j (N and n2 even)
+    V2* rp2 = reinterpret_cast<V2*>(rp);  // pair j of row y is element y M + j (N and n2 even)
     const V2* wp2 = reinterpret_cast<const V2*>(wp);
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < d.n1 * M; idx += blockDim.x) {
-      const int y = fdiv(idx, M), j = idx - y * M;
-      V2 ab = rp2[idx];
-      if (wp) {
-        const V2 ww = wp2[idx];
-        ab.x *= ww.x;
-        ab.y *= ww.y;
+    const V2* ap2 = reinterpret_cast<const V2*>(ap);
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+      V2 rv[kBatch], av[kBatch], wv[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          rv[u] = rp2[idx];
+          if (ap) av[u] = ap2[idx];
+          if (wp) wv[u] = wp2[idx];
+        }
       }
-      buf[y * d.rs + j] = {ab.x, ab.y};
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          V2 v = rv[u];
+          if (ap) {
+            v.x -= al * (av[u].x - mu);
+            v.y -= al * (av[u].y - mu);
+            rp2[idx] = v;
+          }
+          acc[0] += (double)v.x + (double)v.y;
+          acc[1] += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+          if (wp) {
+            v.x *= wv[u].x;
+            v.y *= wv[u].y;
+          }
+          const int y = fdiv(idx, M), j = idx - y * M;
+          buf[y * d.rs + j] = {v.x, v.y};
+        }
+      }
     }
     __syncthreads();
     lines_fft(buf, M, d.n1, d.n1, 0, d.rs, 1, tw + d.off2h, false, scratch, d.pp);
@@ -319,9 +369,15 @@ __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T
   } else {
     for (int idx = threadIdx.x; idx < d.n1 * d.n2; idx += blockDim.x) {
       const int y = idx / d.n2, z = idx - y * d.n2;
-      T a = rp[idx];
-      if (wp) a *= wp[idx];
-      buf[y * d.rs + z] = {a, T(0)};
+      T v = rp[idx];
+      if (ap) {
+        v -= al * (ap[idx] - mu);
+        rp[idx] = v;
+      }
+      acc[0] += (double)v;
+      acc[1] += (double)v * (double)v;
+      if (wp) v *= wp[idx];
+      buf[y * d.rs + z] = {v, T(0)};
     }
     __syncthreads();
     lines_fft(buf, d.n2, d.n1, d.n1, 0, d.rs, 1, tw + d.off2, false, scratch, d.pp);
@@ -334,30 +390,53 @@ __global__ void k_fft_a(const T* __restrict__ r, const T* __restrict__ w, cplx<T
     const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
     sp[((long)ky * d.n0 + x) * d.n2h + kz] = buf[ky * d.rs + kz];
   }
+  if (fu.partA) {
+    block_sum<2>(acc, red);
+    if (threadIdx.x == 0) {
+      double* o = fu.partA + (((long)vec * 3 + c) * d.n0 + x) * 2;
+      o[0] = acc[0];
+      o[1] = acc[1];
+    }
+  }
 }
 
 // ---- pass B --------------------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, FftDims d, int kc, int m,
                         const cplx<T>* __restrict__ tw, const CellState* __restrict__ cs,
-                        unsigned long long* __restrict__ units, int ukind) {
+                        unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);  // [3][n0][kc]
   cplx<T>* scratch = buf + 3 * d.n0 * kc;
+  __shared__ double red[32];
   const int ky = blockIdx.x, kz0 = blockIdx.y * kc, vec = blockIdx.z;
   if (cs && !cs[vec / m].active) return;
   prof_count(units, ukind);
   const int nkz = min(kc, d.n2h - kz0);
-#pragma unroll 4
-  for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
-    const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
-    const int x = rem / kc, kz = rem - x * kc;
-    cplx<T> v{T(0), T(0)};
-    if (kz < nkz) v = spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + x) * d.n2h + kz0 + kz];
-    buf[idx] = v;
+  const int total = 3 * d.n0 * kc;
+  constexpr int kBatch = batch<T>();
+  for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+    cplx<T> v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int idx = base + u * blockDim.x;
+      v[u] = {T(0), T(0)};
+      if (idx < total) {
+        const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
+        const int xx = rem / kc, kz = rem - xx * kc;
+        if (kz < nkz) v[u] = spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + xx) * d.n2h + kz0 + kz];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < total) buf[idx] = v[u];
+    }
   }
   __syncthreads();
   lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, false, scratch, d.pp);
+  double dot[1] = {0.0};
+  const bool even = (d.n2 % 2) == 0;
 #pragma unroll 2
   for (int idx = threadIdx.x; idx < d.n0 * kc; idx += blockDim.x) {
     const int kx = idx / kc, kz = idx - kx * kc;
@@ -365,27 +444,41 @@ __global__ void k_fft_b(cplx<T>* __restrict__ spec, const T* __restrict__ kinv, 
       const T* K = kinv + (((long)kx * d.n1 + ky) * d.n2h + kz0 + kz) * 6;
       const T kxx = K[0], kyy = K[1], kzz = K[2], kyz = K[3], kxz = K[4], kxy = K[5];
       const cplx<T> a = buf[idx], b = buf[d.n0 * kc + idx], c = buf[2 * d.n0 * kc + idx];
-      buf[idx] = {kxx * a.x + kxy * b.x + kxz * c.x, kxx * a.y + kxy * b.y + kxz * c.y};
-      buf[d.n0 * kc + idx] = {kxy * a.x + kyy * b.x + kyz * c.x, kxy * a.y + kyy * b.y + kyz * c.y};
-      buf[2 * d.n0 * kc + idx] = {kxz * a.x + kyz * b.x + kzz * c.x, kxz * a.y + kyz * b.y + kzz * c.y};
+      const cplx<T> ua{kxx * a.x + kxy * b.x + kxz * c.x, kxx * a.y + kxy * b.y + kxz * c.y};
+      const cplx<T> ub{kxy * a.x + kyy * b.x + kyz * c.x, kxy * a.y + kyy * b.y + kyz * c.y};
+      const cplx<T> uc{kxz * a.x + kyz * b.x + kzz * c.x, kxz * a.y + kyz * b.y + kzz * c.y};
+      if (fu.partB) {
+        // Parseval on the half spectrum: kz = 0 (and nz/2 for even nz) once, the others twice
+        const int kzg = kz0 + kz;
+        const double wt = (kzg == 0 || (even && 2 * kzg == d.n2)) ? 1.0 : 2.0;
+        dot[0] += wt * ((double)a.x * ua.x + (double)a.y * ua.y + (double)b.x * ub.x + (double)b.y * ub.y +
+                        (double)c.x * uc.x + (double)c.y * uc.y);
+      }
+      buf[idx] = ua;
+      buf[d.n0 * kc + idx] = ub;
+      buf[2 * d.n0 * kc + idx] = uc;
     }
   }
   __syncthreads();
   lines_fft(buf, d.n0, 3 * kc, kc, d.n0 * kc, 1, kc, tw + d.off0, true, scratch, d.pp);
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < 3 * d.n0 * kc; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int c = idx / (d.n0 * kc), rem = idx - c * d.n0 * kc;
-    const int x = rem / kc, kz = rem - x * kc;
-    if (kz < nkz) spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + x) * d.n2h + kz0 + kz] = buf[idx];
+    const int xx = rem / kc, kz = rem - xx * kc;
+    if (kz < nkz) spec[((long)vec * 3 + c) * d.NS + ((long)ky * d.n0 + xx) * d.n2h + kz0 + kz] = buf[idx];
+  }
+  if (fu.partB) {
+    block_sum<1>(dot, red);
+    if (threadIdx.x == 0) fu.partB[((long)vec * d.n1 + ky) * gridDim.y + blockIdx.y] = dot[0];
   }
 }
 
 // ---- pass C --------------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ w, const T* __restrict__ r,
+__global__ void __launch_bounds__(256, 3) k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ w, const T* __restrict__ r,
                         T* __restrict__ z, FftDims d, int m, const cplx<T>* __restrict__ tw,
                         const CellState* __restrict__ cs, double* __restrict__ partial,
-                        unsigned long long* __restrict__ units, int ukind) {
+                        unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
   extern __shared__ unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* scratch = buf + d.n1 * d.rs;
@@ -394,10 +487,28 @@ __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ 
   if (cs && !cs[vec / m].active) return;
   prof_count(units, ukind);
   const cplx<T>* sp = spec + ((long)vec * 3 + c) * d.NS;
-#pragma unroll 4
-  for (int idx = threadIdx.x; idx < d.n1 * d.n2h; idx += blockDim.x) {
-    const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
-    buf[ky * d.rs + kz] = sp[((long)ky * d.n0 + x) * d.n2h + kz];
+  constexpr int kBatch = batch<T>();
+  {
+    const int total = d.n1 * d.n2h;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+      cplx<T> v[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
+          v[u] = sp[((long)ky * d.n0 + x) * d.n2h + kz];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          const int ky = idx / d.n2h, kz = idx - ky * d.n2h;
+          buf[ky * d.rs + kz] = v[u];
+        }
+      }
+    }
   }
   __syncthreads();
   lines_fft(buf, d.n1, d.n2h, d.n2h, 0, 1, d.rs, tw + d.off1, true, scratch, d.pp);
@@ -421,27 +532,39 @@ __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ 
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (packed) {  // one complex entry = the pair (2j, 2j+1) of a row: vector loads and stores of two reals
     using V2 = typename Vec2<T>::type;
-    const int M = d.n2 / 2;
+    const int M = d.n2 / 2, total = d.n1 * M;
     const V2* wp2 = reinterpret_cast<const V2*>(wp);
     const V2* rp2 = reinterpret_cast<const V2*>(r + pbase);
     V2* zp2 = reinterpret_cast<V2*>(z + pbase);
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < d.n1 * M; idx += blockDim.x) {
-      const int y = fdiv(idx, M), j = idx - y * M;
-      const cplx<T> q = buf[y * d.rs + j];
-      V2 v{q.x * norm, q.y * norm};
-      if (wp) {
-        const V2 ww = wp2[idx];
-        v.x *= ww.x;
-        v.y *= ww.y;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+      V2 wv[kBatch], rv[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          if (wp) wv[u] = wp2[idx];
+          if (partial) rv[u] = rp2[idx];
+        }
       }
-      zp2[idx] = v;
-      if (partial) {
-        const V2 rv = rp2[idx];
-        acc[0] += (double)v.x + (double)v.y;
-        acc[1] += (double)rv.x * (double)v.x + (double)rv.y * (double)v.y;
-        acc[2] += (double)rv.x + (double)rv.y;
-        acc[3] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int idx = base + u * blockDim.x;
+        if (idx < total) {
+          const int y = fdiv(idx, M), j = idx - y * M;
+          const cplx<T> q = buf[y * d.rs + j];
+          V2 v{q.x * norm, q.y * norm};
+          if (wp) {
+            v.x *= wv[u].x;
+            v.y *= wv[u].y;
+          }
+          zp2[idx] = v;
+          acc[0] += (double)v.x + (double)v.y;
+          if (partial) {
+            acc[1] += (double)rv[u].x * (double)v.x + (double)rv[u].y * (double)v.y;
+            acc[2] += (double)rv[u].x + (double)rv[u].y;
+            acc[3] += (double)rv[u].x * (double)rv[u].x + (double)rv[u].y * (double)rv[u].y;
+          }
+        }
       }
     }
   } else {
@@ -450,23 +573,26 @@ __global__ void k_fft_c(const cplx<T>* __restrict__ spec, const T* __restrict__ 
       T v = buf[y * d.rs + zz].x * norm;
       if (wp) v *= wp[idx];
       z[pbase + idx] = v;
+      acc[0] += (double)v;
       if (partial) {
         const double rv = (double)r[pbase + idx];
-        acc[0] += (double)v;
         acc[1] += rv * (double)v;
         acc[2] += rv;
         acc[3] += rv * rv;
       }
     }
   }
-  if (partial) {
+  if (partial || fu.partC) {
     block_sum<4>(acc, red);
     if (threadIdx.x == 0) {
-      double* o = partial + (((long)vec * 3 + c) * d.n0 + x) * 4;
-      o[0] = acc[0];
-      o[1] = acc[1];
-      o[2] = acc[2];
-      o[3] = acc[3];
+      if (partial) {
+        double* o = partial + (((long)vec * 3 + c) * d.n0 + x) * 4;
+        o[0] = acc[0];
+        o[1] = acc[1];
+        o[2] = acc[2];
+        o[3] = acc[3];
+      }
+      if (fu.partC) fu.partC[((long)vec * 3 + c) * d.n0 + x] = acc[0];
     }
   }
 }
@@ -514,8 +640,8 @@ template <>
 const float* kinv_table<float>(const LinearHandle& h) { return h.t32.kinv; }
 
 template <typename T>
-int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
-                   const CellState* cs, double* partial, cudaStream_t st) {
+static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx<T>* spec, const T* w,
+                        const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk, cudaStream_t st) {
   FftDims d = fft_dims(h);
   const bool np2 = any_non_pow2(d);
   const int cap = (h.smem_optin > 0 ? h.smem_optin : 48 * 1024) - 2048;  // room for static shared memory
@@ -530,6 +656,7 @@ int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cpl
   const int mult = (d.pp || np2) ? 2 : 1;
   const int kc = pick_kc<T>(d, std::min<size_t>(64 * 1024, (size_t)cap), mult);
   const size_t smemb = (size_t)3 * d.n0 * kc * sizeof(cplx<T>) * mult;
+  if (nchunk) *nchunk = (d.n2h + kc - 1) / kc;
   const cplx<T>* tw = twiddles<T>(h);
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_a<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
   NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
@@ -540,24 +667,46 @@ int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cpl
   {
     const int kind = f32 ? PK_FFTA32 : PK_FFTA64;
     ProfScope ps(kind, st);
-    k_fft_a<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(r, w, spec, d, m, tw, cs, units, kind);
+    k_fft_a<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(r, w, spec, d, m, tw, cs, units, kind, fu);
     NLF_CHECK_LAUNCH();
   }
   {
     const int kind = f32 ? PK_FFTB32 : PK_FFTB64;
     ProfScope ps(kind, st);
     k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h), d, kc, m, tw,
-                                                                          cs, units, kind);
+                                                                          cs, units, kind, fu);
     NLF_CHECK_LAUNCH();
   }
   {
     const int kind = f32 ? PK_FFTC32 : PK_FFTC64;
     ProfScope ps(kind, st);
-    k_fft_c<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(spec, w, r, z, d, m, tw, cs, partial, units, kind);
+    k_fft_c<T><<<dim3(d.n0, 3, nvec), nt, plane, st>>>(spec, w, r, z, d, m, tw, cs, partial, units, kind, fu);
     NLF_CHECK_LAUNCH();
   }
   return NLF_OK;
 }
+
+template <typename T>
+int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
+                   const CellState* cs, double* partial, cudaStream_t st) {
+  PcgFuse fu{nullptr, nullptr, nullptr, nullptr, nullptr};
+  return precond_impl<T>(h, nvec, m, const_cast<T*>(r), z, spec, w, cs, partial, fu, nullptr, st);
+}
+
+template <typename T>
+int launch_precond_pcg(const LinearHandle& h, int nvec, int m, T* r, const T* Ap, const VecState* vs, T* z,
+                       cplx<T>* spec, const T* w, const CellState* cs, double* partA, double* partB, double* partC,
+                       int* nchunk, cudaStream_t st) {
+  PcgFuse fu{Ap, vs, partA, partB, partC};
+  return precond_impl<T>(h, nvec, m, r, z, spec, w, cs, nullptr, fu, nchunk, st);
+}
+
+template int launch_precond_pcg<float>(const LinearHandle&, int, int, float*, const float*, const VecState*, float*,
+                                       cplx<float>*, const float*, const CellState*, double*, double*, double*, int*,
+                                       cudaStream_t);
+template int launch_precond_pcg<double>(const LinearHandle&, int, int, double*, const double*, const VecState*,
+                                        double*, cplx<double>*, const double*, const CellState*, double*, double*,
+                                        double*, int*, cudaStream_t);
 
 template int launch_precond<float>(const LinearHandle&, int, int, const float*, float*, cplx<float>*,
                                    const float*, const CellState*, double*, cudaStream_t);

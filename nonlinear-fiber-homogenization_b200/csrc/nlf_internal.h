@@ -92,6 +92,13 @@ template <typename T>
 int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
                    const CellState* cs, double* partial /*[nvec][3][n0][4]: sum z, (r,z), sum r, (r,r)*/,
                    cudaStream_t st);
+// The same transform inside a PCG iteration, fused with the neighbouring vector work: pass A first updates
+// r <- r - alpha (Ap - mean Ap) in place and writes partA [nvec][3][n0][2] (sum r, (r, r)); pass B writes the
+// Parseval partials of (r, z) to partB [nvec][n1][nchunk]; pass C writes sum z to partC [nvec][3][n0].
+template <typename T>
+int launch_precond_pcg(const LinearHandle& h, int nvec, int m, T* r, const T* Ap, const VecState* vs, T* z,
+                       cplx<T>* spec, const T* w, const CellState* cs, double* partA, double* partB, double* partC,
+                       int* nchunk, cudaStream_t st);
 int build_tables(LinearHandle& h);
 
 // vector kernels

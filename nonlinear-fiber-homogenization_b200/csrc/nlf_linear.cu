@@ -145,7 +145,7 @@ struct PcgSet {
   const T* w = nullptr;
   VecState* vs = nullptr;
   CellState* cs = nullptr;
-  double *part_ap = nullptr, *part_pc = nullptr, *part_st = nullptr;
+  double *part_ap = nullptr, *part_pc = nullptr, *part_st = nullptr, *part_b = nullptr;
   int* d_count = nullptr;
 };
 
@@ -174,6 +174,7 @@ static void carve_pcg(Arena& A, const LinearHandle& h, PcgSet<T>& P, int ncell, 
   // apply partials: tiles * x-chunks <= 4096 blocks per vec
   P.part_ap = A.take<double>((size_t)P.nvec * 4096 * 4);
   P.part_pc = A.take<double>((size_t)P.nvec * 3 * h.g.n0 * 4);
+  P.part_b = A.take<double>((size_t)P.nvec * h.g.n1 * h.g.n2h);  // pass-B chunks <= n2h per ky
   P.part_st = A.take<double>((size_t)P.nvec * 3 * kStatsBlocks * 2);
   P.d_count = A.take<int>(4);
 }
@@ -185,10 +186,15 @@ static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl,
   NLF_TRY(launch_mark(P.cs, P.ncell, st));
   NLF_TRY(launch_apply<T>(h, P.s, P.m, P.nvec, P.p, P.Ap, P.cs, P.part_ap, &nblk, st));
   NLF_TRY(launch_fin_apply(P.nvec, P.m, P.part_ap, nblk, N, P.vs, P.cs, 0, st));
-  NLF_TRY(launch_xr<T>(N, P.nvec, P.m, P.x, P.r, P.p, P.Ap, P.vs, P.cs, st));
-  NLF_TRY(launch_precond<T>(h, P.nvec, P.m, P.r, P.z, P.spec, P.w, P.cs, P.part_pc, st));
-  NLF_TRY(launch_fin_pc(P.ncell, P.m, h.g.n0, N, P.part_pc, P.vs, P.cs, ctl.tol, ctl.maxit, 0, st));
-  NLF_TRY(launch_p<T>(N, P.nvec, P.m, P.p, P.z, P.vs, P.cs, 0, st));
+  // r update, (r, r), (r, z) and the sums ride on the FFT passes; x += alpha p rides on the p update
+  double* partA = P.part_pc;
+  double* partC = P.part_pc + (size_t)P.nvec * 3 * h.g.n0 * 2;
+  int nchunk = 0;
+  NLF_TRY(launch_precond_pcg<T>(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.z, P.spec, P.w, P.cs, partA, P.part_b, partC,
+                                &nchunk, st));
+  NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, partC, nchunk, P.vs, P.cs, ctl.tol,
+                              ctl.maxit, st));
+  NLF_TRY(launch_px<T>(N, P.nvec, P.m, P.x, P.p, P.z, P.vs, P.cs, st));
   return NLF_OK;
 }
 

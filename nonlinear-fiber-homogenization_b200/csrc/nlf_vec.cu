@@ -331,6 +331,78 @@ __global__ void k_p(long N, T* __restrict__ p, const T* __restrict__ z, const Ve
   }
 }
 
+// Fused form of k_fin_pc for an iteration whose preconditioner passes also updated r:
+//   partA [vec][3][n0][2]: sum r, (r, r) of the updated residual (FFT pass A)
+//   partB [vec][n1][nchunk]: Parseval partials of (r, z) on the half spectrum, unnormalised (pass B)
+//   partC [vec][3][n0]: sum z (pass C)
+// rz1 = (r, z - mean z) = (r, z) - sum_c mean z_c sum r_c; the control is that of k_fin_pc.
+__global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* __restrict__ partB,
+                               const double* __restrict__ partC, int nchunk, int n0, int n1, long N,
+                               VecState* __restrict__ vs, CellState* __restrict__ cs, int m, double tol, int maxit) {
+  __shared__ int go;
+  const int cell = blockIdx.x;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (!cs[cell].active) return;
+  if (threadIdx.x == 0) go = 0;
+  __syncthreads();
+  if (wid < m) {
+    const int vec = cell * m + wid;
+    double sr[3] = {0, 0, 0}, sz[3] = {0, 0, 0}, rr = 0.0, dot = 0.0;
+    for (int c = 0; c < 3; ++c)
+      for (int x = lane; x < n0; x += 32) {
+        const long i = ((long)vec * 3 + c) * n0 + x;
+        sr[c] += partA[2 * i];
+        rr += partA[2 * i + 1];
+        sz[c] += partC[i];
+      }
+    for (int i = lane; i < n1 * nchunk; i += 32) dot += partB[(long)vec * n1 * nchunk + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sr[c] += __shfl_down_sync(0xffffffffu, sr[c], o);
+        sz[c] += __shfl_down_sync(0xffffffffu, sz[c], o);
+      }
+      rr += __shfl_down_sync(0xffffffffu, rr, o);
+      dot += __shfl_down_sync(0xffffffffu, dot, o);
+    }
+    if (lane == 0) {
+      VecState& v = vs[vec];
+      double rz1 = dot / (double)N;
+      for (int c = 0; c < 3; ++c) {
+        const double mz = sz[c] / (double)N;
+        v.mean[c] = mz;
+        rz1 -= mz * sr[c];
+      }
+      v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
+      v.rz = rz1;
+      v.rr = rr;
+      if (sqrt(rr) > tol * v.bn) atomicOr(&go, 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CellState& s = cs[cell];
+    s.it += 1;
+    s.active = (s.it < maxit) && go;
+  }
+}
+
+// x += alpha p; p = (z - mean z) + beta p, for the cells that ran this iteration (status bit 1)
+template <typename T>
+__global__ void k_px(long N, T* __restrict__ x, T* __restrict__ p, const T* __restrict__ z,
+                     const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !(cs[vec / m].status & 2)) return;
+  const T al = (T)vs[vec].alpha, be = (T)vs[vec].beta, mu = (T)vs[vec].mean[c];
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const T po = p[off + i];
+    x[off + i] += al * po;
+    p[off + i] = (z[off + i] - mu) + be * po;
+  }
+}
+
 // status bit 1 <- active (marks the cells that run the current iteration, for k_p after k_fin_pc)
 __global__ void k_mark(CellState* cs, int ncell) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,6 +498,26 @@ int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, cons
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
+int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
+                        const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
+                        cudaStream_t st) {
+  ProfScope ps_(PK_FIN, st);
+  k_fin_pc_fused<<<ncell, 32 * m, 0, st>>>(partA, partB, partC, nchunk, n0, n1, N, vs, cs, m, tol, maxit);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template <typename T>
+int launch_px(long N, int nvec, int m, T* x, T* p, const T* z, const VecState* vs, const CellState* cs,
+              cudaStream_t st) {
+  ProfScope ps_(PK_P, st);
+  k_px<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, x, p, z, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template int launch_px<float>(long, int, int, float*, float*, const float*, const VecState*, const CellState*,
+                              cudaStream_t);
+template int launch_px<double>(long, int, int, double*, double*, const double*, const VecState*, const CellState*,
+                               cudaStream_t);
 int launch_mark(CellState* cs, int ncell, cudaStream_t st) {
   ProfScope ps_(PK_OTHER, st);
   k_mark<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell);

@@ -28,6 +28,13 @@ int launch_fin_pc(int ncell, int m, int n0, long N, const double* partial, VecSt
 template <typename T>
 int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, const CellState* cs, int init,
              cudaStream_t st);
+// fused iteration: (r, z), sums and the lock-step control from the FFT passes' partials; x and p updates together
+int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
+                        const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
+                        cudaStream_t st);
+template <typename T>
+int launch_px(long N, int nvec, int m, T* x, T* p, const T* z, const VecState* vs, const CellState* cs,
+              cudaStream_t st);
 int launch_mark(CellState* cs, int ncell, cudaStream_t st);
 int launch_cs_init(CellState* cs, int ncell, const int* mask, cudaStream_t st);
 int launch_count_active(const CellState* cs, int ncell, int* out, cudaStream_t st);
