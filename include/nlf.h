@@ -50,7 +50,11 @@ typedef struct nlf_solve_opts {
   int inner_maxit;   /* NLF_PREC_MIXED: iteration cap of one FP32 inner solve */
   int max_sweeps;    /* NLF_PREC_MIXED: cap on FP64 refinement sweeps */
   int check_every;   /* host convergence poll period in iterations (>= 1) */
-  int use_graphs;    /* capture the PCG iteration in a CUDA graph and replay it */
+  int use_graphs;    /* capture check_every PCG iterations in a CUDA graph once per solve and replay it
+                        (ignored while nlf_profile is on) */
+  int slots;         /* NLF_PREC_FP64: cells solved at once (0 or >= ncell: all cells in lock-step). With
+                        0 < slots < ncell a converged cell hands its slot to the next queued cell at the next
+                        poll, so the batch stays full until the queue runs dry. Same per-cell result. */
 } nlf_solve_opts;
 
 NLF_API const char* nlf_last_error(void);

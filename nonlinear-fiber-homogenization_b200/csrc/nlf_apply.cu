@@ -190,12 +190,10 @@ int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x,
   constexpr int NT = ((TY + 1) * (TZ + 1) + 31) / 32 * 32;
   const Geom& g = h.g;
   const int tiles = ((g.n2 + TZ - 1) / TZ) * ((g.n1 + TY - 1) / TY);
-  // enough CTAs for ~4 waves on the SMs, at least 8 planes per march
-  long want = 4L * h.nsm;
-  int chunks = (int)((want + (long)tiles * nvec - 1) / ((long)tiles * nvec));
-  chunks = max(1, min(chunks, max(1, g.n0 / 8)));
-  const int lx = (g.n0 + chunks - 1) / chunks;
-  chunks = (g.n0 + lx - 1) / lx;
+  // marches of 16 planes (one halo plane per 16 re-read). The split depends on the grid alone, so that the
+  // partial sums of a vector, and with them every PCG scalar, are the same whatever else is in the batch.
+  const int lx = g.n0 >= 32 ? 16 : g.n0;
+  const int chunks = (g.n0 + lx - 1) / lx;
   if (nblk_out) *nblk_out = tiles * chunks;
   dim3 grid(tiles, chunks, nvec);
   const int kind = sizeof(T) == 4 ? PK_APPLY32 : PK_APPLY64;

@@ -72,6 +72,10 @@ struct LinearHandle {
   int dev = 0;
   int nsm = 148;
   int smem_optin = 0;
+  // CUDA graph replay of PCG iterations: captured and launched on a handle-owned stream ordered after the
+  // caller's stream by events (capture is not possible on the legacy default stream)
+  cudaStream_t gst = nullptr;
+  cudaEvent_t gev[2] = {nullptr, nullptr};
 };
 
 // ---- launchers (all asynchronous on `st`) ----

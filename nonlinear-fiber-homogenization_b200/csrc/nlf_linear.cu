@@ -6,6 +6,7 @@
 #include <cstring>
 #include <vector>
 #include "nlf_vec.cuh"
+#include "nlf_prof.cuh"
 
 namespace nlf {
 
@@ -205,12 +206,31 @@ static int count_active(const CellState* cs, int ncell, int* d_count, int* h_cou
   return *h_count;
 }
 
-// Lock-step PCG for K x = b on the mean-free subspace (nlfiber/linear.py:173-203), batched over cells.
-// b: [nvec][3][N] in Tb, already mean-free. x: initial guess if x_given (projected here), else zero.
-// mask: device per-cell flags of the cells to solve (nullptr: all).
+// The first cell..cell+count-1 of a PCG set as a set of its own (same partial-sum buffers).
+template <typename T>
+static PcgSet<T> pcg_view(const PcgSet<T>& P, const LinearHandle& h, int cell, int count) {
+  PcgSet<T> v = P;
+  const size_t V = (size_t)P.m * 3 * h.g.N * cell;
+  v.ncell = count;
+  v.nvec = count * P.m;
+  v.x += V;
+  v.r += V;
+  v.p += V;
+  v.Ap += V;
+  v.z += V;
+  v.spec += (size_t)P.m * 3 * h.g.NS * cell;
+  if (v.s) v.s += (size_t)h.g.N * cell;
+  if (v.w) v.w += (size_t)h.g.N * cell;
+  v.vs += (size_t)P.m * cell;
+  v.cs += cell;
+  return v;
+}
+
+// Start of the lock-step PCG (nlfiber/linear.py:173-183): x0 = proj(x) or 0, r = b - proj(A x0), z = M r,
+// p = proj(z), the first (r, z) and the per-cell active flags. b: [nvec][3][N] in Tb, already mean-free.
 template <typename T, typename Tb>
-static int pcg(const LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, const PcgCtl& ctl, const int* mask,
-               int* h_count, cudaStream_t st) {
+static int pcg_init(const LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, const PcgCtl& ctl,
+                    const int* mask, cudaStream_t st) {
   const long N = h.g.N;
   NLF_TRY(launch_cs_init(P.cs, P.ncell, mask, st));
   NLF_TRY(launch_stats<Tb>(h, P.nvec, P.m, b, P.cs, P.part_st, P.vs, 1, st));
@@ -227,12 +247,78 @@ static int pcg(const LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, c
   NLF_TRY(launch_precond<T>(h, P.nvec, P.m, P.r, P.z, P.spec, P.w, P.cs, P.part_pc, st));
   NLF_TRY(launch_fin_pc(P.ncell, P.m, h.g.n0, N, P.part_pc, P.vs, P.cs, ctl.tol, ctl.maxit, 1, st));
   NLF_TRY(launch_p<T>(N, P.nvec, P.m, P.p, P.z, P.vs, P.cs, 1, st));
+  return NLF_OK;
+}
+
+// `k` PCG iterations, either launched one by one on `st` or, with graphs, captured once into `exec` on the
+// handle's own stream and replayed there, ordered after and before the work on `st` by events. The set's
+// pointers must stay the same while `exec` lives.
+struct IterGraph {
+  cudaGraphExec_t exec = nullptr;
+  int k = 0;
+  ~IterGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+static int graph_stream(LinearHandle& h) {
+  if (h.gst) return NLF_OK;
+  NLF_CUDA_TRY(cudaStreamCreateWithFlags(&h.gst, cudaStreamNonBlocking));
+  NLF_CUDA_TRY(cudaEventCreateWithFlags(&h.gev[0], cudaEventDisableTiming));
+  NLF_CUDA_TRY(cudaEventCreateWithFlags(&h.gev[1], cudaEventDisableTiming));
+  return NLF_OK;
+}
+
+template <typename T>
+static int run_iterations(LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl, int k, bool graphs, IterGraph& G,
+                          cudaStream_t st) {
+  if (!graphs || prof_on()) {
+    for (int i = 0; i < k; ++i) NLF_TRY(pcg_iteration<T>(h, P, ctl, st));
+    return NLF_OK;
+  }
+  NLF_TRY(graph_stream(h));
+  if (!G.exec || G.k != k) {
+    if (G.exec) {
+      cudaGraphExecDestroy(G.exec);
+      G.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    NLF_CUDA_TRY(cudaStreamBeginCapture(h.gst, cudaStreamCaptureModeThreadLocal));
+    int rc = NLF_OK;
+    for (int i = 0; i < k && rc == NLF_OK; ++i) rc = pcg_iteration<T>(h, P, ctl, h.gst);
+    const cudaError_t e = cudaStreamEndCapture(h.gst, &graph);
+    if (rc != NLF_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != NLF_OK) return rc;
+      NLF_CUDA_TRY(e);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NLF_CUDA_TRY(ei);
+    G.k = k;
+  }
+  NLF_CUDA_TRY(cudaEventRecord(h.gev[0], st));
+  NLF_CUDA_TRY(cudaStreamWaitEvent(h.gst, h.gev[0], 0));
+  NLF_CUDA_TRY(cudaGraphLaunch(G.exec, h.gst));
+  NLF_CUDA_TRY(cudaEventRecord(h.gev[1], h.gst));
+  NLF_CUDA_TRY(cudaStreamWaitEvent(st, h.gev[1], 0));
+  return NLF_OK;
+}
+
+// Lock-step PCG for K x = b on the mean-free subspace (nlfiber/linear.py:173-203), batched over cells.
+// b: [nvec][3][N] in Tb, already mean-free. x: initial guess if x_given (projected here), else zero.
+// mask: device per-cell flags of the cells to solve (nullptr: all).
+template <typename T, typename Tb>
+static int pcg(LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, const PcgCtl& ctl, const int* mask,
+               int* h_count, bool graphs, cudaStream_t st) {
+  NLF_TRY((pcg_init<T, Tb>(h, P, b, x_given, ctl, mask, st)));
   int act = count_active(P.cs, P.ncell, P.d_count, h_count, st);
   if (act < 0) return act;
   int done = 0;
   const int every = ctl.check_every > 0 ? ctl.check_every : 1;
+  IterGraph G;
   while (act > 0 && done < ctl.maxit) {
-    for (int k = 0; k < every; ++k) NLF_TRY(pcg_iteration<T>(h, P, ctl, st));
+    NLF_TRY(run_iterations<T>(h, P, ctl, every, graphs, G, st));
     done += every;
     act = count_active(P.cs, P.ncell, P.d_count, h_count, st);
     if (act < 0) return act;
@@ -266,7 +352,119 @@ static nlf_solve_opts resolve_opts(const LinearHandle& h, const nlf_solve_opts* 
   if (r.check_every < 1) r.check_every = 1;
   if (r.inner_maxit < 1) r.inner_maxit = 1;
   if (r.max_sweeps < 1) r.max_sweeps = 1;
+  if (r.slots < 0) r.slots = 0;
   return r;
+}
+
+// Status of one finished cell from its cases' VecState: breakdown if a residual is not finite, not converged
+// if a case still has ||r|| > tol ||b|| (it ran out of iterations), else ok.
+static int cell_status(const VecState* v, int m, double tol) {
+  int st = NLF_OK;
+  for (int I = 0; I < m; ++I) {
+    if (!std::isfinite(v[I].rr)) return NLF_BREAKDOWN;
+    if (std::sqrt(v[I].rr) > tol * v[I].bn) st = NLF_NOT_CONVERGED;
+  }
+  return st;
+}
+static int worse(int a, int b) { return (a == NLF_BREAKDOWN || b == NLF_BREAKDOWN) ? NLF_BREAKDOWN : std::max(a, b); }
+
+struct PinnedBuf {
+  void* p = nullptr;
+  explicit PinnedBuf(size_t n) {
+    if (cudaMallocHost(&p, n) != cudaSuccess) p = nullptr;
+  }
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+// FP64 PCG of ncell cells through `o.slots` slots: each slot runs the lock-step PCG of one cell at a time
+// (the same iteration as the all-cells batch, so each cell's result is the same), and at every poll the cells
+// that stopped are copied out and their slots restarted on the next queued cells.
+static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& o, double* xout, int* iters_h,
+                       cudaStream_t st) {
+  const int ncell = in.ncell, m = in.m, S = o.slots;
+  const long N = h.g.N;
+  const size_t Vc = (size_t)m * 3 * N;  // the vectors of one cell
+  const bool scaled = o.precond == NLF_PC_FFT_SCALED;
+  PcgSet<double> P;
+  double *s_sl = nullptr, *w_sl = nullptr, *b_sl = nullptr;
+  for (int pass = 0; pass < 2; ++pass) {
+    Arena A(pass ? h.ws.ptr : nullptr);
+    s_sl = A.take<double>((size_t)S * N);
+    w_sl = scaled ? A.take<double>((size_t)S * N) : nullptr;
+    b_sl = A.take<double>((size_t)S * Vc);
+    carve_pcg<double>(A, h, P, S, m);
+    if (pass == 0) {
+      NLF_TRY(h.ws.reserve(A.off));
+    } else if (poison_workspace()) {
+      NLF_CUDA_TRY(cudaMemsetAsync(h.ws.ptr, 0xFF, A.off, st));
+    }
+  }
+  P.s = s_sl;
+  P.w = w_sl;
+  PinnedBuf pin(S * sizeof(CellState) + (size_t)S * m * sizeof(VecState));
+  if (!pin.p) {
+    set_error("cudaMallocHost failed");
+    return NLF_ECUDA;
+  }
+  CellState* cs_h = static_cast<CellState*>(pin.p);
+  VecState* vs_h = reinterpret_cast<VecState*>(cs_h + S);
+  NLF_CUDA_TRY(cudaMemsetAsync(P.cs, 0, S * sizeof(CellState), st));  // every slot empty and inactive
+  const PcgCtl ctl{o.tol, o.maxit, o.check_every};
+  std::vector<int> slot_cell(S, -1);
+  int next = 0;
+  auto start = [&](int sl) -> int {
+    const int c = next++;
+    slot_cell[sl] = c;
+    double* ss = s_sl + (size_t)sl * N;
+    double* bs = b_sl + (size_t)sl * Vc;
+    PcgSet<double> v = pcg_view(P, h, sl, 1);
+    NLF_CUDA_TRY(cudaMemcpyAsync(ss, in.s64 + (size_t)c * N, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (scaled) NLF_TRY(launch_node_scaling(h, 1, ss, nullptr, w_sl + (size_t)sl * N, nullptr, st));
+    // b = -proj(load) (nlfiber/linear.py:176,206)
+    if (in.b64) {
+      NLF_CUDA_TRY(cudaMemcpyAsync(bs, in.b64 + (size_t)c * Vc, Vc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    } else {
+      NLF_TRY(launch_load(h, ss, in.fe, m, 1, bs, -1.0, st));
+    }
+    NLF_TRY(launch_cs_init(v.cs, 1, nullptr, st));
+    NLF_TRY(launch_stats<double>(h, m, m, bs, v.cs, P.part_st, v.vs, 0, st));
+    NLF_TRY(launch_sub_mean<double>(h, m, m, bs, v.vs, v.cs, st));
+    const bool xg = in.x0 != nullptr;
+    if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, m, in.x0 + (size_t)c * Vc, v.x, 1.0, st)));
+    return pcg_init<double, double>(h, v, bs, xg, ctl, nullptr, st);
+  };
+  for (int sl = 0; sl < S && next < ncell; ++sl) NLF_TRY(start(sl));
+  const int every = ctl.check_every > 0 ? ctl.check_every : 1;
+  IterGraph G;
+  int status = NLF_OK;
+  for (;;) {
+    NLF_CUDA_TRY(cudaMemcpyAsync(cs_h, P.cs, S * sizeof(CellState), cudaMemcpyDeviceToHost, st));
+    NLF_CUDA_TRY(cudaMemcpyAsync(vs_h, P.vs, (size_t)S * m * sizeof(VecState), cudaMemcpyDeviceToHost, st));
+    NLF_CUDA_TRY(cudaStreamSynchronize(st));
+    int nact = 0;
+    for (int sl = 0; sl < S; ++sl) {
+      const int c = slot_cell[sl];
+      if (c < 0) continue;
+      if (cs_h[sl].active) {
+        ++nact;
+        continue;
+      }
+      iters_h[c] = cs_h[sl].it;
+      status = worse(status, cell_status(vs_h + (size_t)sl * m, m, o.tol));
+      NLF_CUDA_TRY(cudaMemcpyAsync(xout + (size_t)c * Vc, P.x + (size_t)sl * Vc, Vc * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st));
+      slot_cell[sl] = -1;
+      if (next < ncell) {
+        NLF_TRY(start(sl));
+        ++nact;
+      }
+    }
+    if (nact == 0) break;
+    NLF_TRY(run_iterations<double>(h, P, ctl, every, o.use_graphs != 0, G, st));
+  }
+  return status;
 }
 
 // Runs the solve; writes the FP64 corrector (SoA) to `xout` ([ncell][m][3][N]) and iterations to iters_h.
@@ -338,19 +536,18 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       const bool xg = in.x0 != nullptr;
       if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, P64.x, 1.0, st)));
       PcgCtl ctl{o.tol, o.maxit, o.check_every};
-      NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, st)));
+      if (o.slots > 0 && o.slots < ncell) return solve_slots(h, in, o, xout, iters_h, st);
+      NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, o.use_graphs != 0, st)));
       NLF_CUDA_TRY(cudaMemcpyAsync(xout, P64.x, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
       NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P64.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
       NLF_CUDA_TRY(cudaStreamSynchronize(st));
+      std::vector<VecState> vsh(nvec);
+      NLF_CUDA_TRY(cudaMemcpy(vsh.data(), P64.vs, nvec * sizeof(VecState), cudaMemcpyDeviceToHost));
       int status = NLF_OK;
       for (int c = 0; c < ncell; ++c) {
         iters_h[c] = csh[c].it;
-        if (csh[c].active) status = NLF_NOT_CONVERGED;
+        status = worse(status, cell_status(&vsh[(size_t)c * m], m, o.tol));
       }
-      std::vector<VecState> vsh(nvec);
-      NLF_CUDA_TRY(cudaMemcpy(vsh.data(), P64.vs, nvec * sizeof(VecState), cudaMemcpyDeviceToHost));
-      for (int v = 0; v < nvec; ++v)
-        if (!std::isfinite(vsh[v].rr)) status = NLF_BREAKDOWN;
       return status;
     }
     // ---- mixed precision: FP32 PCG inside FP64 iterative refinement ----
@@ -402,7 +599,7 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       for (int c = 0; c < ncell; ++c)
         if (maskh[c]) cap = std::min(cap, std::max(1, o.maxit - it_total[c]));
       PcgCtl ctl{o.inner_tol, cap, o.check_every};
-      NLF_TRY((pcg<float, float>(h, P32, rhs32, false, ctl, mask, pin.count, st)));
+      NLF_TRY((pcg<float, float>(h, P32, rhs32, false, ctl, mask, pin.count, o.use_graphs != 0, st)));
       NLF_TRY(launch_x_update(N, nvec, m, x64, P32.x, vs_o, cs_o, st));
       NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P32.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
       NLF_CUDA_TRY(cudaStreamSynchronize(st));
@@ -508,6 +705,7 @@ NLF_API void nlf_default_opts(nlf_solve_opts* o) {
   o->max_sweeps = 20;
   o->check_every = 8;
   o->use_graphs = 0;
+  o->slots = 0;
 }
 
 NLF_API int nlf_linear_create(nlf_linear** out, int nx, int ny, int nz, double E, double nu, double emin, double p,
@@ -556,6 +754,9 @@ NLF_API int nlf_linear_create(nlf_linear** out, int nx, int ny, int nz, double E
 NLF_API int nlf_linear_destroy(nlf_linear* H) {
   if (!H) return NLF_OK;
   LinearHandle& h = H->h;
+  if (h.gst) cudaStreamDestroy(h.gst);
+  for (cudaEvent_t e : h.gev)
+    if (e) cudaEventDestroy(e);
   cudaFree(h.t64.kinv);
   cudaFree(h.t32.kinv);
   cudaFree(h.t64.tw);

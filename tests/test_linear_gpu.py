@@ -158,6 +158,24 @@ def test_batched_equals_single_and_deterministic(L):
         assert np.array_equal(C, r["C"][i]) and it == r["it"][i]
 
 
+def test_slot_refill_and_graphs_equal_lock_step(L):
+    """Five 32^3 cells through two slots (a converged cell hands its slot to the next one), with the iterations
+    replayed from a CUDA graph, give bit for bit the lock-step batch's u, C and iteration counts; the status
+    says converged, and a cap below the needed iterations says not converged (status 1)."""
+    cells = np.stack([OD.random_cell(i, n_o=16, beta=8.0)[0] for i in range(5)])
+    lock = L.LinearHomogenization(cells.shape[1:], precond="scaled", tol=1e-8, maxit=2000, check_every=4)
+    slot = L.LinearHomogenization(cells.shape[1:], precond="scaled", tol=1e-8, maxit=2000, check_every=4,
+                                  slots=2, use_graphs=True)
+    a = lock.C_full_batched(cells, want_u=True)
+    b = slot.C_full_batched(cells, want_u=True)
+    assert a["status"] == 0 and b["status"] == 0
+    assert np.array_equal(a["it"], b["it"]), (a["it"], b["it"])
+    assert np.array_equal(a["u"], b["u"]) and np.array_equal(a["C"], b["C"])
+    assert len(set(a["it"].tolist())) > 1  # the cells really stop at different iterations
+    short = slot.C_full_batched(cells, maxit=int(a["it"].min()) - 1)
+    assert short["status"] == 1 and np.all(short["it"] == a["it"].min() - 1)
+
+
 def test_high_contrast_variants_reach_the_fp64_C(L):
     """emin = 1e-9 Schwarz-P 16^3: the scaled preconditioner (FP64 and FP32-in-FP64 refinement) and the
     reference preconditioner (long run) reach the same C; every entry within 1e-8 of max |C|."""
