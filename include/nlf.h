@@ -164,6 +164,34 @@ NLF_API int nlf_mech_cg(nlf_mech* h, const double* w, const double* Fbar, int k,
                         const double* dmac, double sws, double tol, int maxit, double* x, int* it, int* conv, int* neg,
                         int check_every, void* stream);
 
+/* ---- learned warm start ----------------------------------------------------------------------------------
+ * A 3-level U-Net (widths w0, w1, w2; periodic 3x3x3 convolutions, ReLU, 2x average pooling, nearest
+ * upsampling with skip concatenation, a final 1x1 convolution to 18 channels) maps a density cell to the 6
+ * unit-strain correctors as u / nx (channels-last, case-major: channel 3 I + c). Its prediction is the u0 of
+ * nlf_C_full / nlf_linear_solve. No counterpart in the reference, whose solve always starts from u0 = 0
+ * (nlfiber/linear.py:209-212, the u0 argument of solve and C_full :231-236). The convolutions run as BF16
+ * implicit GEMMs on the tensor cores with FP32 accumulation; parameters, gradients and Adam moments are FP32.
+ * Flat parameter layout: per layer W (ntaps, cout, cin) then b (cout), layers in network order. */
+typedef struct nlf_unet nlf_unet;
+
+/* widths multiples of 16 with w1 + w0 <= 128 and w2 + w1 <= 128; He-normal weights from `seed`. */
+NLF_API int nlf_unet_create(nlf_unet** out, int w0, int w1, int w2, unsigned long long seed);
+NLF_API int nlf_unet_destroy(nlf_unet* net);
+NLF_API long long nlf_unet_param_count(const nlf_unet* net);
+/* FP32 parameters to / from a host or device buffer of nlf_unet_param_count floats; set_params also resets the
+ * Adam state. */
+NLF_API int nlf_unet_get_params(nlf_unet* net, float* out, void* stream);
+NLF_API int nlf_unet_set_params(nlf_unet* net, const float* in, void* stream);
+/* y (nb, nx, ny, nz, 18) = net(rho (nb, nx, ny, nz)); device FP32 buffers; nx, ny, nz divisible by 4. */
+NLF_API int nlf_unet_forward(nlf_unet* net, int nb, int nx, int ny, int nz, const float* rho, float* y,
+                             void* stream);
+/* loss = sum_v weight[v] sum_c (y - target)^2 / 18 and its gradient w.r.t. the parameters (kept for
+ * nlf_unet_adam_step; also copied to `grad` when not NULL, host or device). rho, target, weight: device FP32. */
+NLF_API int nlf_unet_backward(nlf_unet* net, int nb, int nx, int ny, int nz, const float* rho, const float* target,
+                              const float* weight, double* loss, float* grad, void* stream);
+/* One Adam step (Kingma & Ba 2015, bias-corrected) with the gradient of the last nlf_unet_backward. */
+NLF_API int nlf_unet_adam_step(nlf_unet* net, double lr, double beta1, double beta2, double eps, void* stream);
+
 /* ---- kernel profiler ------------------------------------------------------------------------------------- */
 
 /* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library
