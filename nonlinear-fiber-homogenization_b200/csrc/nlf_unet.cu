@@ -38,12 +38,14 @@ __device__ __forceinline__ long nbr(int i, int j, int k, int t, int sign, int n0
 // ---- the tcgen05 main loop -------------------------------------------------------------------------------------
 // nsteps stages of K = 64 (4 MMAs of K = 16) into the TMEM accumulator; ld(stage_smem_addr, step) issues the
 // cp.async copies of one step. A 4-deep ring: the copies of step k + 3 are issued after the MMAs of step k, once
-// the MMAs of step k - 1 (the previous user of that slot) have completed. Returns false, uniformly over the CTA,
-// when an mbarrier wait timed out (*err raised).
+// the MMAs of step k - 1 (the previous user of that slot) have completed. The u-th completion of a slot's
+// mbarrier has parity u & 1, and no slot is committed again before every thread has seen its previous
+// completion. Returns false, uniformly over the CTA, when an mbarrier wait timed out (*err raised).
 template <int NPAD, class Loader>
 __device__ bool mainloop(const Loader& ld, int nsteps, uint32_t su, uint64_t* mbar, uint32_t tmem, uint32_t idesc,
-                         int* err, volatile int* s_fail) {
+                         int* err) {
   constexpr uint32_t SB = kStageA + NPAD * 128;
+  int bad = 0;  // this thread's wait timed out; the CTA leaves together through __syncthreads_or
   for (int s = 0; s < kStages - 1; ++s) {
     if (s < nsteps) ld(su + s * SB, s);
     tc::cp_commit();
@@ -52,8 +54,7 @@ __device__ bool mainloop(const Loader& ld, int nsteps, uint32_t su, uint64_t* mb
     const int st = kb % kStages;
     tc::cp_wait<kStages - 2>();
     tc::fence_proxy_async();
-    __syncthreads();
-    if (*s_fail) return false;
+    if (__syncthreads_or(bad)) return false;
     if (threadIdx.x == 0) {
       tc::fence_after();
       const uint32_t a0 = su + st * SB, b0 = a0 + kStageA;
@@ -65,16 +66,15 @@ __device__ bool mainloop(const Loader& ld, int nsteps, uint32_t su, uint64_t* mb
     const int nx = kb + kStages - 1;
     if (nx < nsteps) {
       if (kb >= 1 && !tc::mbar_wait(tc::smem_u32(&mbar[(kb - 1) % kStages]), ((kb - 1) / kStages) & 1, err))
-        *s_fail = 1;
-      ld(su + (nx % kStages) * SB, nx);
+        bad = 1;
+      if (!bad) ld(su + (nx % kStages) * SB, nx);
     }
     tc::cp_commit();
   }
   const int last = nsteps - 1;
-  if (!tc::mbar_wait(tc::smem_u32(&mbar[last % kStages]), (last / kStages) & 1, err)) *s_fail = 1;
+  if (!bad && !tc::mbar_wait(tc::smem_u32(&mbar[last % kStages]), (last / kStages) & 1, err)) bad = 1;
   tc::cp_wait<0>();
-  __syncthreads();
-  return !*s_fail;
+  return !__syncthreads_or(bad);
 }
 
 template <int NPAD>
@@ -84,7 +84,7 @@ constexpr uint32_t tmem_cols() {
 
 // CTA prologue / epilogue shared by the kernels: TMEM allocation by warp 0, mbarrier init by thread 0.
 template <int NPAD>
-__device__ __forceinline__ uint32_t tc_setup(uint32_t* s_tmem, uint64_t* mbar, volatile int* s_fail) {
+__device__ __forceinline__ uint32_t tc_setup(uint32_t* s_tmem, uint64_t* mbar) {
   if ((threadIdx.x >> 5) == 0) {
     tc::tmem_alloc(tc::smem_u32(s_tmem), tmem_cols<NPAD>());
     tc::tmem_relinquish();
@@ -92,7 +92,6 @@ __device__ __forceinline__ uint32_t tc_setup(uint32_t* s_tmem, uint64_t* mbar, v
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) tc::mbar_init(tc::smem_u32(&mbar[s]), 1);
     tc::mbar_fence_init();
-    *s_fail = 0;
   }
   tc::fence_before();
   __syncthreads();
@@ -164,9 +163,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t mbar[kStages];
   __shared__ uint32_t s_tmem;
-  __shared__ int s_fail;
   const uint32_t su = aligned_smem(smem_raw);
-  const uint32_t tmem = tc_setup<NPAD>(&s_tmem, mbar, &s_fail);
+  const uint32_t tmem = tc_setup<NPAD>(&s_tmem, mbar);
   const int tid = threadIdx.x, warp = tid >> 5;
   const long nvox = (long)a.n0 * a.n1 * a.n2, total = (long)a.nb * nvox;
   const long v = (long)blockIdx.x * 128 + tid;
@@ -190,7 +188,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a) {
     ld.k = (int)(l % a.n2);
   }
   const int nsteps = (ld.kt + 7) / 8;
-  if (mainloop<NPAD>(ld, nsteps, su, mbar, tmem, tc::idesc_bf16(NPAD, 0, 0), a.err, &s_fail)) {
+  if (mainloop<NPAD>(ld, nsteps, su, mbar, tmem, tc::idesc_bf16(NPAD, 0, 0), a.err)) {
     tc::fence_after();
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
@@ -287,9 +285,8 @@ __global__ void __launch_bounds__(128) k_dw_tc(DwArgs a) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t mbar[kStages];
   __shared__ uint32_t s_tmem;
-  __shared__ int s_fail;
   const uint32_t su = aligned_smem(smem_raw);
-  const uint32_t tmem = tc_setup<NPAD>(&s_tmem, mbar, &s_fail);
+  const uint32_t tmem = tc_setup<NPAD>(&s_tmem, mbar);
   const int tid = threadIdx.x, warp = tid >> 5;
   const long nvox = (long)a.n0 * a.n1 * a.n2, total = (long)a.nb * nvox;
   DwLoad<NPAD> ld;
@@ -306,7 +303,7 @@ __global__ void __launch_bounds__(128) k_dw_tc(DwArgs a) {
   ld.vbeg = (long)blockIdx.y * a.vpc;
   ld.vend = ld.vbeg + a.vpc < total ? ld.vbeg + a.vpc : total;
   const int nsteps = (int)((ld.vend - ld.vbeg + 63) / 64);
-  if (mainloop<NPAD>(ld, nsteps, su, mbar, tmem, tc::idesc_bf16(NPAD, 1, 1), a.err, &s_fail)) {
+  if (mainloop<NPAD>(ld, nsteps, su, mbar, tmem, tc::idesc_bf16(NPAD, 1, 1), a.err)) {
     tc::fence_after();
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     float* out = a.part + ((long)blockIdx.y * a.rows_pad + (long)blockIdx.x * 128 + tid) * NPAD;
