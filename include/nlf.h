@@ -55,6 +55,15 @@ typedef struct nlf_solve_opts {
   int slots;         /* NLF_PREC_FP64: cells solved at once (0 or >= ncell: all cells in lock-step). With
                         0 < slots < ncell a converged cell hands its slot to the next queued cell at the next
                         poll, so the batch stays full until the queue runs dry. Same per-cell result. */
+  int scale_x0;      /* with an initial guess u0: start from beta u0 instead, beta (per case) minimising the
+                        energy 1/2 x.Kx - b.x over the multiples of u0 (so never further from the solution in the
+                        energy norm than u0 = 0). 0: the reference's start x0 = proj(u0). */
+  double energy_tol; /* > 0 (solves from strains Es, FP64): energy guard. A cell stops only when, besides the
+                        residual rule, the last 32 terms alpha_j (r_j, z_j) of its PCG sum to at most
+                        energy_tol * N * max_J C_JJ for every case I. That sum estimates ||u_I - u*_I||_K^2 =
+                        N (C_II(u) - C_II*) (Hestenes-Stiefel), which bounds every |C_IJ(u) - C*_IJ|; C_JJ comes
+                        from the same recurrences. It keeps cells whose residual is small but whose C is not
+                        (near-mechanisms of the solid) running; it never stops a cell earlier. 0: residual rule only. */
 } nlf_solve_opts;
 
 NLF_API const char* nlf_last_error(void);

@@ -23,8 +23,16 @@ struct VecState {
   double rr;       // (r, r)
   double scale;    // refinement scale of the right-hand side (mixed precision)
   double mean[3];  // per-component mean for the next projection
-  double pad;
+  double x0scale;  // energy-optimal multiple of the initial guess (scale_x0)
+  double ebase;    // N C_II at the start: (E D E) sum(s) + x0.K x0 - 2 (b, x0)   (energy stopping rule)
+  double esum;     // sum over the iterations so far of alpha_j (r_j, z_j)
 };
+
+// energy stopping rule: E_I D E_I of the cases (m <= 6) and the window of alpha (r, z) terms it sums
+struct Ede {
+  double v[6];
+};
+constexpr int kEnergyWindow = 32;
 
 // Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188).
 struct CellState {

@@ -135,6 +135,9 @@ struct PcgCtl {
   double tol;
   int maxit;
   int check_every;
+  int scale_x0;
+  double energy_tol;  // > 0: energy stopping rule (needs ede)
+  Ede ede;
 };
 
 template <typename T>
@@ -147,6 +150,7 @@ struct PcgSet {
   VecState* vs = nullptr;
   CellState* cs = nullptr;
   double *part_ap = nullptr, *part_pc = nullptr, *part_st = nullptr, *part_b = nullptr;
+  double* ring = nullptr;  // [nvec][kEnergyWindow]
   int* d_count = nullptr;
 };
 
@@ -177,6 +181,7 @@ static void carve_pcg(Arena& A, const LinearHandle& h, PcgSet<T>& P, int ncell, 
   P.part_pc = A.take<double>((size_t)P.nvec * 3 * h.g.n0 * 4);
   P.part_b = A.take<double>((size_t)P.nvec * h.g.n1 * h.g.n2h);  // pass-B chunks <= n2h per ky
   P.part_st = A.take<double>((size_t)P.nvec * 3 * kStatsBlocks * 2);
+  P.ring = A.take<double>((size_t)P.nvec * kEnergyWindow);
   P.d_count = A.take<int>(4);
 }
 
@@ -194,7 +199,7 @@ static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl,
   NLF_TRY(launch_precond_pcg<T>(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.z, P.spec, P.w, P.cs, partA, P.part_b, partC,
                                 &nchunk, st));
   NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, partC, nchunk, P.vs, P.cs, ctl.tol,
-                              ctl.maxit, st));
+                              ctl.maxit, P.ring, ctl.energy_tol, st));
   NLF_TRY(launch_px<T>(N, P.nvec, P.m, P.x, P.p, P.z, P.vs, P.cs, st));
   return NLF_OK;
 }
@@ -223,6 +228,7 @@ static PcgSet<T> pcg_view(const PcgSet<T>& P, const LinearHandle& h, int cell, i
   if (v.w) v.w += (size_t)h.g.N * cell;
   v.vs += (size_t)P.m * cell;
   v.cs += cell;
+  if (v.ring) v.ring += (size_t)P.m * kEnergyWindow * cell;
   return v;
 }
 
@@ -243,6 +249,10 @@ static int pcg_init(const LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_giv
   int nblk = 0;
   NLF_TRY(launch_apply<T>(h, P.s, P.m, P.nvec, P.x, P.Ap, P.cs, P.part_ap, &nblk, st));
   NLF_TRY(launch_fin_apply(P.nvec, P.m, P.part_ap, nblk, N, P.vs, P.cs, 1, st));
+  if (x_given && ctl.scale_x0) NLF_TRY((launch_x0_scale<Tb, T>(h, P.nvec, P.m, b, P.x, P.Ap, P.cs, P.part_st, P.vs, st)));
+  if (ctl.energy_tol > 0.0)
+    NLF_TRY((launch_energy_init<Tb, T>(h, P.ncell, P.m, P.s, ctl.ede, b, P.x, P.Ap, x_given, P.cs, P.part_st, P.vs,
+                                       st)));
   NLF_TRY((launch_r_init<Tb, T>(N, P.nvec, P.m, P.r, b, P.Ap, P.vs, P.cs, st)));
   NLF_TRY(launch_precond<T>(h, P.nvec, P.m, P.r, P.z, P.spec, P.w, P.cs, P.part_pc, st));
   NLF_TRY(launch_fin_pc(P.ncell, P.m, h.g.n0, N, P.part_pc, P.vs, P.cs, ctl.tol, ctl.maxit, 1, st));
@@ -341,6 +351,8 @@ struct SolveIn {
   const double* b64;  // [ncell][m][3][N], mean-free (nullptr: build from fe = Es G)
   const double* fe;   // device (m, 24) when b64 == nullptr
   const double* x0;   // AoS (ncell, m, N, 3) device FP64 or nullptr
+  bool has_ede;       // E_I D E_I known (a solve from strains, m <= 6): the energy stopping rule is available
+  Ede ede;
 };
 
 static nlf_solve_opts resolve_opts(const LinearHandle& h, const nlf_solve_opts* o) {
@@ -411,7 +423,7 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   CellState* cs_h = static_cast<CellState*>(pin.p);
   VecState* vs_h = reinterpret_cast<VecState*>(cs_h + S);
   NLF_CUDA_TRY(cudaMemsetAsync(P.cs, 0, S * sizeof(CellState), st));  // every slot empty and inactive
-  const PcgCtl ctl{o.tol, o.maxit, o.check_every};
+  const PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede};
   std::vector<int> slot_cell(S, -1);
   int next = 0;
   auto start = [&](int sl) -> int {
@@ -535,7 +547,7 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       if (scaled) NLF_TRY(launch_node_scaling(h, ncell, in.s64, nullptr, w64, nullptr, st));
       const bool xg = in.x0 != nullptr;
       if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, P64.x, 1.0, st)));
-      PcgCtl ctl{o.tol, o.maxit, o.check_every};
+      PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede};
       if (o.slots > 0 && o.slots < ncell) return solve_slots(h, in, o, xout, iters_h, st);
       NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, o.use_graphs != 0, st)));
       NLF_CUDA_TRY(cudaMemcpyAsync(xout, P64.x, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -598,7 +610,7 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       int cap = o.inner_maxit;
       for (int c = 0; c < ncell; ++c)
         if (maskh[c]) cap = std::min(cap, std::max(1, o.maxit - it_total[c]));
-      PcgCtl ctl{o.inner_tol, cap, o.check_every};
+      PcgCtl ctl{o.inner_tol, cap, o.check_every, 0, 0.0, Ede{}};
       NLF_TRY((pcg<float, float>(h, P32, rhs32, false, ctl, mask, pin.count, o.use_graphs != 0, st)));
       NLF_TRY(launch_x_update(N, nvec, m, x64, P32.x, vs_o, cs_o, st));
       NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P32.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
@@ -706,6 +718,8 @@ NLF_API void nlf_default_opts(nlf_solve_opts* o) {
   o->check_every = 8;
   o->use_graphs = 0;
   o->slots = 0;
+  o->scale_x0 = 0;
+  o->energy_tol = 0.0;
 }
 
 NLF_API int nlf_linear_create(nlf_linear** out, int nx, int ny, int nz, double E, double nu, double emin, double p,
@@ -939,7 +953,18 @@ static int solve_entry(nlf_linear* H, int ncell, const double* s, const double* 
   }
   NLF_TRY(stage_in(u0, V, h.io, o_u0, u0v, st));
   double* xs = reinterpret_cast<double*>(b + o_x);
-  SolveIn in{ncell, m, sv.d, bsoa, fed, u0v.d};
+  SolveIn in{ncell, m, sv.d, bsoa, fed, u0v.d, false, Ede{}};
+  if (Es && m <= 6) {
+    std::vector<double> Esh;
+    NLF_TRY(host_copy_small(Es, (size_t)m * 6, Esh));
+    in.has_ede = true;
+    for (int I = 0; I < m; ++I) {
+      double a = 0.0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) a += Esh[I * 6 + i] * h.Dm[i][j] * Esh[I * 6 + j];
+      in.ede.v[I] = a;
+    }
+  }
   std::vector<int> it(ncell, 0);
   int status = solve_core(h, in, o, xs, it.data(), st);
   if (status < 0) return status;

@@ -338,11 +338,14 @@ __global__ void k_p(long N, T* __restrict__ p, const T* __restrict__ z, const Ve
 // rz1 = (r, z - mean z) = (r, z) - sum_c mean z_c sum r_c; the control is that of k_fin_pc.
 __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* __restrict__ partB,
                                const double* __restrict__ partC, int nchunk, int n0, int n1, long N,
-                               VecState* __restrict__ vs, CellState* __restrict__ cs, int m, double tol, int maxit) {
+                               VecState* __restrict__ vs, CellState* __restrict__ cs, int m, double tol, int maxit,
+                               double* __restrict__ ring, double etol) {
   __shared__ int go;
+  __shared__ double s_nc[8], s_w[8];
   const int cell = blockIdx.x;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (!cs[cell].active) return;
+  const int itk = cs[cell].it;  // index of the iteration that just ran
   if (threadIdx.x == 0) go = 0;
   __syncthreads();
   if (wid < m) {
@@ -366,6 +369,23 @@ __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* _
       rr += __shfl_down_sync(0xffffffffu, rr, o);
       dot += __shfl_down_sync(0xffffffffu, dot, o);
     }
+    if (etol > 0.0) {
+      // energy rule: the error energy ||x* - x_k||_K^2 = sum_{j >= k} alpha_j (r_j, z_j) (Hestenes-Stiefel),
+      // estimated by the last kEnergyWindow terms; N C_II(x_k) = ebase - esum
+      const double term = vs[vec].alpha * vs[vec].rz;
+      double* rg = ring + (long)vec * kEnergyWindow;
+      const int nw = min(itk + 1, kEnergyWindow), slot = itk % kEnergyWindow;
+      double w = (lane < nw && lane != slot) ? rg[lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+      if (lane == 0) {
+        rg[slot] = term;
+        VecState& v = vs[vec];
+        v.esum += term;
+        s_w[wid] = w + term;
+        s_nc[wid] = v.ebase - v.esum;
+      }
+    }
     if (lane == 0) {
       VecState& v = vs[vec];
       double rz1 = dot / (double)N;
@@ -382,10 +402,55 @@ __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* _
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    bool eok = false;
+    if (etol > 0.0 && itk + 1 >= kEnergyWindow) {
+      double cmax = 0.0;
+      for (int I = 0; I < m; ++I) cmax = fmax(cmax, s_nc[I]);
+      eok = cmax > 0.0;
+      for (int I = 0; I < m; ++I) eok = eok && s_w[I] <= etol * cmax;
+    }
+    // with the energy rule a cell stops only when both the residual rule and the energy rule hold
     CellState& s = cs[cell];
     s.it += 1;
-    s.active = (s.it < maxit) && go;
+    s.active = (s.it < maxit) && (go || (etol > 0.0 && !eok));
   }
+}
+
+// ebase[vec] = ede[I] * sum(s of the cell), esum = 0; one block per cell
+template <typename T>
+__global__ void k_energy_base(const T* __restrict__ s, long N, int m, Ede ede, VecState* __restrict__ vs,
+                              const CellState* __restrict__ cs) {
+  __shared__ double red[32];
+  const int cell = blockIdx.x;
+  if (cs && !cs[cell].active) return;
+  double acc[1] = {0.0};
+  for (long i = threadIdx.x; i < N; i += blockDim.x) acc[0] += (double)s[(long)cell * N + i];
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0)
+    for (int I = 0; I < m; ++I) {
+      vs[cell * m + I].ebase = ede.v[I] * acc[0];
+      vs[cell * m + I].esum = 0.0;
+    }
+}
+
+// ebase += x0.K x0 - 2 (b, x0) from the k_x0_dots partials
+__global__ void k_energy_x0(const double* __restrict__ partial, int nb, int nvec, VecState* __restrict__ vs,
+                            const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (vec >= nvec) return;
+  if (cs && !cs[vec / m].active) return;
+  double bx = 0.0, xax = 0.0;
+  for (int k = lane; k < 3 * nb; k += 32) {
+    bx += partial[((long)vec * 3 * nb + k) * 2];
+    xax += partial[((long)vec * 3 * nb + k) * 2 + 1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    bx += __shfl_down_sync(0xffffffffu, bx, o);
+    xax += __shfl_down_sync(0xffffffffu, xax, o);
+  }
+  if (lane == 0) vs[vec].ebase += xax - 2.0 * bx;
 }
 
 // x += alpha p; p = (z - mean z) + beta p, for the cells that ran this iteration (status bit 1)
@@ -400,6 +465,70 @@ __global__ void k_px(long N, T* __restrict__ x, T* __restrict__ p, const T* __re
     const T po = p[off + i];
     x[off + i] += al * po;
     p[off + i] = (z[off + i] - mu) + be * po;
+  }
+}
+
+// ---- energy-optimal scaling of an initial guess ------------------------------------------------------------
+// partial[vec][c][blk] = ((b, x), (x, Ax - mean Ax)) over the block's share of component c
+template <typename Tb, typename T>
+__global__ void k_x0_dots(long N, const Tb* __restrict__ b, const T* __restrict__ x, const T* __restrict__ Ax,
+                          const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m,
+                          double* __restrict__ partial) {
+  __shared__ double red[32 * 2];
+  const int c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  const long off = ((long)vec * 3 + c) * N;
+  const double mu = vs[vec].mean[c];
+  double acc[2] = {0.0, 0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double xv = (double)x[off + i];
+    acc[0] += (double)b[off + i] * xv;
+    acc[1] += xv * ((double)Ax[off + i] - mu);
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) {
+    double* o = partial + (((long)vec * 3 + c) * gridDim.x + blockIdx.x) * 2;
+    o[0] = acc[0];
+    o[1] = acc[1];
+  }
+}
+
+__global__ void k_x0_fin(const double* __restrict__ partial, int nb, int nvec, VecState* __restrict__ vs,
+                         const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (vec >= nvec) return;
+  if (cs && !cs[vec / m].active) return;
+  double bx = 0.0, xax = 0.0;
+  for (int k = lane; k < 3 * nb; k += 32) {
+    bx += partial[((long)vec * 3 * nb + k) * 2];
+    xax += partial[((long)vec * 3 * nb + k) * 2 + 1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    bx += __shfl_down_sync(0xffffffffu, bx, o);
+    xax += __shfl_down_sync(0xffffffffu, xax, o);
+  }
+  if (lane == 0) {
+    const double beta = (xax > 0.0 && isfinite(bx / xax)) ? bx / xax : 0.0;
+    VecState& v = vs[vec];
+    v.x0scale = beta;
+    v.mean[0] *= beta;
+    v.mean[1] *= beta;
+    v.mean[2] *= beta;
+  }
+}
+
+template <typename T>
+__global__ void k_x0_apply(long N, T* __restrict__ x, T* __restrict__ Ax, const VecState* __restrict__ vs,
+                           const CellState* __restrict__ cs, int m) {
+  const int vec = blockIdx.z, c = blockIdx.y;
+  if (cs && !cs[vec / m].active) return;
+  const T be = (T)vs[vec].x0scale;
+  const long off = ((long)vec * 3 + c) * N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    x[off + i] *= be;
+    Ax[off + i] *= be;
   }
 }
 
@@ -500,9 +629,10 @@ int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, cons
 }
 int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
                         const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
-                        cudaStream_t st) {
+                        double* ring, double etol, cudaStream_t st) {
   ProfScope ps_(PK_FIN, st);
-  k_fin_pc_fused<<<ncell, 32 * m, 0, st>>>(partA, partB, partC, nchunk, n0, n1, N, vs, cs, m, tol, maxit);
+  k_fin_pc_fused<<<ncell, 32 * m, 0, st>>>(partA, partB, partC, nchunk, n0, n1, N, vs, cs, m, tol, maxit, ring,
+                                           etol);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
@@ -518,6 +648,46 @@ template int launch_px<float>(long, int, int, float*, float*, const float*, cons
                               cudaStream_t);
 template int launch_px<double>(long, int, int, double*, double*, const double*, const VecState*, const CellState*,
                                cudaStream_t);
+template <typename Tb, typename T>
+int launch_x0_scale(const LinearHandle& h, int nvec, int m, const Tb* b, T* x, T* Ax, const CellState* cs,
+                    double* partial, VecState* vs, cudaStream_t st) {
+  const long N = h.g.N;
+  ProfScope ps_(PK_OTHER, st);
+  k_x0_dots<Tb, T><<<dim3(kStatsBlocks, 3, nvec), 256, 0, st>>>(N, b, x, Ax, vs, cs, m, partial);
+  NLF_CHECK_LAUNCH();
+  k_x0_fin<<<(nvec + 7) / 8, 256, 0, st>>>(partial, kStatsBlocks, nvec, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  k_x0_apply<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, x, Ax, vs, cs, m);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+template int launch_x0_scale<double, double>(const LinearHandle&, int, int, const double*, double*, double*,
+                                             const CellState*, double*, VecState*, cudaStream_t);
+template int launch_x0_scale<float, float>(const LinearHandle&, int, int, const float*, float*, float*,
+                                           const CellState*, double*, VecState*, cudaStream_t);
+template <typename Tb, typename T>
+int launch_energy_init(const LinearHandle& h, int ncell, int m, const T* s, const Ede& ede, const Tb* b, const T* x,
+                       const T* Ax, bool x_given, const CellState* cs, double* partial, VecState* vs,
+                       cudaStream_t st) {
+  const long N = h.g.N;
+  const int nvec = ncell * m;
+  ProfScope ps_(PK_OTHER, st);
+  k_energy_base<T><<<ncell, 512, 0, st>>>(s, N, m, ede, vs, cs);
+  NLF_CHECK_LAUNCH();
+  if (x_given) {
+    k_x0_dots<Tb, T><<<dim3(kStatsBlocks, 3, nvec), 256, 0, st>>>(N, b, x, Ax, vs, cs, m, partial);
+    NLF_CHECK_LAUNCH();
+    k_energy_x0<<<(nvec + 7) / 8, 256, 0, st>>>(partial, kStatsBlocks, nvec, vs, cs, m);
+    NLF_CHECK_LAUNCH();
+  }
+  return NLF_OK;
+}
+template int launch_energy_init<double, double>(const LinearHandle&, int, int, const double*, const Ede&,
+                                                const double*, const double*, const double*, bool, const CellState*,
+                                                double*, VecState*, cudaStream_t);
+template int launch_energy_init<float, float>(const LinearHandle&, int, int, const float*, const Ede&, const float*,
+                                              const float*, const float*, bool, const CellState*, double*, VecState*,
+                                              cudaStream_t);
 int launch_mark(CellState* cs, int ncell, cudaStream_t st) {
   ProfScope ps_(PK_OTHER, st);
   k_mark<<<(ncell + 127) / 128, 128, 0, st>>>(cs, ncell);

@@ -31,10 +31,20 @@ int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, cons
 // fused iteration: (r, z), sums and the lock-step control from the FFT passes' partials; x and p updates together
 int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
                         const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
-                        cudaStream_t st);
+                        double* ring, double etol, cudaStream_t st);
+// energy stopping rule, at the start of a solve: ebase = ede[I] sum(s of the cell) (+ x0.K x0 - 2 (b, x0) when
+// x_given; Ax holds K x0 and its means), esum = 0
+template <typename Tb, typename T>
+int launch_energy_init(const LinearHandle& h, int ncell, int m, const T* s, const Ede& ede, const Tb* b, const T* x,
+                       const T* Ax, bool x_given, const CellState* cs, double* partial, VecState* vs,
+                       cudaStream_t st);
 template <typename T>
 int launch_px(long N, int nvec, int m, T* x, T* p, const T* z, const VecState* vs, const CellState* cs,
               cudaStream_t st);
+// x <- beta x, Ax <- beta Ax (and its means) with beta = (b, x) / (x, Ax - mean Ax) per vector (0 if not positive)
+template <typename Tb, typename T>
+int launch_x0_scale(const LinearHandle& h, int nvec, int m, const Tb* b, T* x, T* Ax, const CellState* cs,
+                    double* partial, VecState* vs, cudaStream_t st);
 int launch_mark(CellState* cs, int ncell, cudaStream_t st);
 int launch_cs_init(CellState* cs, int ncell, const int* mask, cudaStream_t st);
 int launch_count_active(const CellState* cs, int ncell, int* out, cudaStream_t st);

@@ -98,7 +98,7 @@ class LinearHomogenization:
 
     def __init__(self, shape, E=1.0, nu=0.3, emin=1e-3, p=3.0, dtype=np.float64, tol=1e-9, maxit=4000,
                  precision="fp64", precond="fft", inner_tol=1e-3, inner_maxit=200, max_sweeps=20, check_every=8,
-                 slots=0, use_graphs=False):
+                 slots=0, use_graphs=False, scale_x0=False, energy_tol=0.0):
         shape = tuple(int(n) for n in shape)
         self.plane = len(shape) == 2
         self.shape = shape + (1,) if self.plane else shape
@@ -107,7 +107,8 @@ class LinearHomogenization:
         self.precision, self.precond_kind = precision, precond
         self.inner_tol, self.inner_maxit, self.max_sweeps = inner_tol, inner_maxit, max_sweeps
         self.check_every = check_every
-        self.slots, self.use_graphs = int(slots), bool(use_graphs)
+        self.slots, self.use_graphs, self.scale_x0 = int(slots), bool(use_graphs), bool(scale_x0)
+        self.energy_tol = float(energy_tol)
         B = B_matrices()
         D = iso_D(E, nu)
         self.Dm = D
@@ -133,7 +134,8 @@ class LinearHomogenization:
             precision=_PREC[precision or self.precision], precond=_PC[precond or self.precond_kind],
             tol=self.tol if tol is None else float(tol), maxit=self.maxit if maxit is None else int(maxit),
             inner_tol=float(self.inner_tol), inner_maxit=int(self.inner_maxit), max_sweeps=int(self.max_sweeps),
-            check_every=int(self.check_every), slots=self.slots, use_graphs=int(self.use_graphs))
+            check_every=int(self.check_every), slots=self.slots, use_graphs=int(self.use_graphs),
+            scale_x0=int(self.scale_x0), energy_tol=self.energy_tol)
 
     def _cell(self, a, extra=()):
         """Coerce a per-cell field to (nx, ny, nz) + extra, adding the plane-strain axis where needed."""

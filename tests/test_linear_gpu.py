@@ -176,6 +176,25 @@ def test_slot_refill_and_graphs_equal_lock_step(L):
     assert short["status"] == 1 and np.all(short["it"] == a["it"].min() - 1)
 
 
+def test_energy_guard_and_warm_start_plumbing(L):
+    """The energy guard never stops a cell earlier than the residual rule and keeps C within 1e-8 of a long run;
+    a warm start from the converged correctors needs (almost) no iteration, and the energy-optimal scaling
+    recovers an exact multiple of them at once."""
+    cells = np.stack([OD.random_cell(i, n_o=8, beta=16.0)[0] for i in range(6)])
+    kw = dict(emin=1e-9, precond="scaled", maxit=4000, check_every=4)
+    star = L.LinearHomogenization(cells.shape[1:], tol=1e-14, **kw).C_full_batched(cells)["C"]
+    res = L.LinearHomogenization(cells.shape[1:], tol=1e-9, **kw).C_full_batched(cells, want_u=True)
+    grd = L.LinearHomogenization(cells.shape[1:], tol=1e-9, energy_tol=1e-10, **kw).C_full_batched(cells)
+    assert res["status"] == 0 and grd["status"] == 0
+    assert np.all(grd["it"] >= res["it"]), (grd["it"], res["it"])
+    assert max(rel(grd["C"][i], star[i]) for i in range(len(cells))) < 1e-8
+    ws = L.LinearHomogenization(cells.shape[1:], tol=1e-9, **kw)
+    assert np.all(ws.C_full_batched(cells, u0=res["u"])["it"] <= 4)
+    sc = L.LinearHomogenization(cells.shape[1:], tol=1e-9, scale_x0=True, **kw)
+    half = sc.C_full_batched(cells, u0=0.5 * res["u"])
+    assert np.all(half["it"] <= 4), half["it"]
+
+
 def test_high_contrast_variants_reach_the_fp64_C(L):
     """emin = 1e-9 Schwarz-P 16^3: the scaled preconditioner (FP64 and FP32-in-FP64 refinement) and the
     reference preconditioner (long run) reach the same C; every entry within 1e-8 of max |C|."""
