@@ -235,6 +235,94 @@ def calibrate_plain(L, rho_d, Cstar, n, stream, ncell=4, caps=(1000, 2000, 4000,
     return {"needed_iterations": need, "c_err_by_cap": table}
 
 
+def unet_flops(widths, n, nb):
+    """Algorithmic FLOPs (2 per multiply-add) of one U-Net forward over nb cells of n^3: every convolution's
+    voxels x taps x cin x cout (the 1-channel input counted as 1 channel, not the 8 the kernels pad it to)."""
+    w0, w1, w2 = widths
+    v0 = nb * n ** 3
+    v1, v2 = v0 // 8, v0 // 64
+    layers = [(v0, 1, w0, 27), (v0, w0, w0, 27), (v1, w0, w1, 27), (v1, w1, w1, 27), (v2, w1, w2, 27),
+              (v2, w2, w2, 27), (v1, w2 + w1, w1, 27), (v1, w1, w1, 27), (v0, w1 + w0, w0, 27), (v0, w0, w0, 27),
+              (v0, w0, 18, 1)]
+    return sum(2.0 * v * t * ci * co for v, ci, co, t in layers)
+
+
+def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
+    """The learned warm start: solver-generated training pairs (32^3 and n^3 cells of the same generator, other
+    seeds), Adam training of the U-Net on the GPU, then the measured workload solved cold and warm (u0 = the
+    network's prediction, scaled energy-optimally) with the same stopping rule."""
+    import torch
+    from nlfiber_b200 import _lib
+    from nlfiber_b200 import learned as LN
+    t0 = time.perf_counter()
+    c32 = gen_cells(list(range(10_000, 10_000 + args.train_cells32)), 16)
+    cbig = gen_cells(list(range(20_000, 20_000 + args.train_cells64)), n // 2)
+    sets = []
+    for cells in (c32, cbig):
+        m = cells.shape[1]
+        h = L.LinearHomogenization((m, m, m), **MATERIAL, **FAST)
+        h.stream = stream
+        rho = torch.from_numpy(cells).cuda()
+        r = h.C_full_batched(rho, want_u=True)
+        sets.append((rho.float(), LN.corrector_channels(torch.from_numpy(r["u"])).cuda(),
+                     LN.loss_weights(rho, MATERIAL["emin"], MATERIAL["p"]).cuda() + 0.05))
+        del r
+    t_data = time.perf_counter() - t0
+    widths = (16, 32, 64)
+    net = LN.UNet(widths, seed=0)
+    net.stream = stream
+    rng = np.random.default_rng(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    losses = []
+    e0.record()
+    for it in range(args.train_steps):
+        rho, tgt, w = sets[it % 2]
+        b = min(8, rho.shape[0]) if it % 2 == 0 else min(2, rho.shape[0])
+        idx = torch.as_tensor(rng.choice(rho.shape[0], size=b, replace=False), device="cuda")
+        ww = w[idx]
+        loss, _ = net.loss_grad(rho[idx], tgt[idx], ww / ww.sum())
+        net.adam_step(1e-4 + 0.5 * (2e-3 - 1e-4) * (1 + np.cos(np.pi * it / max(args.train_steps, 1))))
+        losses.append(loss)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    # convolution throughput: one profiled forward over the measured cells
+    rho32 = rho_d.float()
+    net.forward(rho32[:2])
+    _lib.profile(True)
+    net.forward(rho32)
+    torch.cuda.synchronize()
+    prof = _lib.profile_report()
+    _lib.profile(False)
+    conv_ms, conv_la = prof["unet_conv"][0], prof["unet_conv"][1]
+    flops = unet_flops(widths, n, rho_d.shape[0])
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    conv = {"kernel": "unet_conv (k_conv_tc)", "bound": "tensor", "achieved": round(flops / (conv_ms * 1e-3) / 1e12, 2),
+            "peak": peak, "unit": "TFLOP/s", "frac": round(flops / (conv_ms * 1e-3) / 1e12 / peak, 4),
+            "peak_kind": "of measured cuBLAS bf16 (burst)" if peak_kind == "measured" else "of fallback 1590",
+            "launches": conv_la, "ms": round(conv_ms, 3), "flops": flops}
+    out = {}
+    for name, kw in (("cold", {}), ("warm", {"scale_x0": True})):
+        h = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST, **kw)
+        h.stream = stream
+        C = torch.empty((rho_d.shape[0], 6, 6), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        e0.record()
+        u0 = LN.WarmStart(net).u0(rho_d) if name == "warm" else None
+        r = h.C_full_batched(rho_d, u0=u0, out_C=C)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"cells_per_s": round(rho_d.shape[0] / (ms / 1e3), 3), "it_mean": float(np.mean(r["it"])),
+                     "it_max": int(np.max(r["it"])), "c_err_max": float(rel_err(C.cpu().numpy(), Cstar).max()),
+                     "status": int(r["status"])}
+        del u0
+    return {"mode": "learned", "widths": widths, "train_pairs": [args.train_cells32, args.train_cells64],
+            "train_steps": args.train_steps, "train_s": round(train_ms / 1e3, 2), "data_s": round(t_data, 1),
+            "loss_first": float(np.mean(losses[:20])) if losses else None,
+            "loss_last": float(np.mean(losses[-20:])) if losses else None, "conv_roofline": conv, **out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,6 +339,12 @@ def main():
                     help="small fixed profiling case for ncu: one warm-up and one C_full of --cells cells with "
                          "--iters PCG iterations, no C*, no baselines")
     ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--learned", action="store_true",
+                    help="train the warm-start U-Net on solver-generated pairs and time the workload cold and warm "
+                         "(one step each) instead of the default measurement")
+    ap.add_argument("--train-cells32", type=int, default=256)
+    ap.add_argument("--train-cells64", type=int, default=32)
+    ap.add_argument("--train-steps", type=int, default=2000)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -301,6 +395,12 @@ def main():
     if args.calibrate_plain:
         if rank == 0:
             print(json.dumps({"calibrate_plain": calibrate_plain(L, rho_d, Cstar, n, stream)}), flush=True)
+        return
+    if args.learned:
+        peaks, peak_kind = measured_peaks()
+        res = learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind)
+        if rank == 0:
+            print(json.dumps(dict(res, workload=f"{B} seeded synthetic {n}^3 cells x 6 unit strains")), flush=True)
         return
 
     lh = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
