@@ -65,6 +65,8 @@ __host__ __device__ __forceinline__ int ilog2(int n) {
   return l;
 }
 
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
+
 // x / d with a shift when d is a power of two (the usual grid sides)
 __device__ __forceinline__ int fdiv(int x, int d) { return is_pow2(d) ? (x >> (31 - __clz(d))) : x / d; }
 

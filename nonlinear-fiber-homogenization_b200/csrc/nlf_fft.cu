@@ -13,6 +13,7 @@
 // sum over the 27 stencil blocks W_d cos(k.d); K(0) = I; Kinv = inv(K + 1e-12 |tr K| I); Kinv(0) = 0.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include "nlf_internal.h"
 #include "nlf_prof.cuh"
 
@@ -597,6 +598,501 @@ __global__ void __launch_bounds__(256, 3) k_fft_c(const cplx<T>* __restrict__ sp
   }
 }
 
+// ---- register-resident passes for cubic grids of 32 or 64 (FP64) ---------------------------------------------
+// A line of n = R L points (R = 4 or 8) lives in a group of L lanes with R registers each. Natural distribution:
+// lane l holds x[l + L r] in register r. Transposed distribution: lane l holds X[k1 + R brev(l)] in register k1 (brev over
+// log2 L bits). fft_nat_in maps natural -> transposed (register DFT, twiddle, cross-lane decimation in frequency
+// by warp shuffles); fft_tr_in maps transposed -> natural (cross-lane decimation in time, twiddle, register
+// DFT). Both compute the plain DFT (INV: conjugate twiddles, no scaling); tw[k] = e^{-2 pi i k / n}.
+__device__ __forceinline__ cplx<double> shfl_xor_c(cplx<double> v, int m) {
+  return {__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+__device__ __forceinline__ cplx<double> shfl_c(cplx<double> v, int src) {
+  return {__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+template <bool INV>
+__device__ __forceinline__ cplx<double> twid(const cplx<double>* __restrict__ tw, int e) {
+  const cplx<double> w = tw[e];
+  return INV ? cplx<double>{w.x, -w.y} : w;
+}
+template <int L>
+__device__ __forceinline__ int brevL(int l) {
+  return L == 1 ? 0 : (int)(__brev((unsigned)l) >> (32 - ilog2c(L)));
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(cplx<double> (&a)[R]) {
+  if constexpr (R == 8) {
+    dft_small<double, INV>(a, 8);
+  } else {
+    static_assert(R == 4, "register DFT of 4 or 8 points");
+    dft4<double, INV>(a[0], a[1], a[2], a[3]);
+  }
+}
+
+// The twiddles one lane needs for lines of n = R L points, read once from the table: W_n^{l k1} (k1 < R) and the
+// cross-lane stage factors W_{2s}^{l mod s} (stage s = 2^j in slot j).
+template <int L, int R>
+struct LaneTw {
+  static constexpr int NS = ilog2c(L) > 0 ? ilog2c(L) : 1;
+  cplx<double> r[R];
+  cplx<double> st[NS];
+  __device__ __forceinline__ void load(const cplx<double>* __restrict__ tw, int l) {
+    constexpr int n = R * L;
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) r[k1] = (l && k1) ? tw[l * k1] : cplx<double>{1.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+      const int s = 1 << j;
+      st[j] = (L > 1) ? tw[(l & (s - 1)) * (n / (2 * s))] : cplx<double>{1.0, 0.0};
+    }
+  }
+};
+template <bool INV>
+__device__ __forceinline__ cplx<double> cj(cplx<double> w) {
+  return INV ? cplx<double>{w.x, -w.y} : w;
+}
+
+template <int L, int R, bool INV>
+__device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const LaneTw<L, R>& T) {
+  dft_reg<R, INV>(a);
+  if (L == 1) return;
+#pragma unroll
+  for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.r[k1]));
+#pragma unroll
+  for (int j = ilog2c(L) - 1; j >= 0; --j) {
+    const int s = 1 << j;
+    const bool up = (l & s) != 0;
+    const cplx<double> w = cj<INV>(T.st[j]);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+      const cplx<double> pv = shfl_xor_c(a[k1], s);
+      a[k1] = up ? cmul(csub(pv, a[k1]), w) : cadd(a[k1], pv);
+    }
+  }
+}
+
+template <int L, int R, bool INV>
+__device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const LaneTw<L, R>& T) {
+  if (L > 1) {
+#pragma unroll
+    for (int j = 0; j < ilog2c(L); ++j) {
+      const int s = 1 << j;
+      const bool up = (l & s) != 0;
+      const cplx<double> w = cj<INV>(T.st[j]);
+#pragma unroll
+      for (int k1 = 0; k1 < R; ++k1) {
+        const cplx<double> pv = shfl_xor_c(a[k1], s);
+        a[k1] = up ? csub(pv, cmul(w, a[k1])) : cadd(a[k1], cmul(w, pv));
+      }
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.r[k1]));
+  }
+  dft_reg<R, INV>(a);
+}
+
+// shared plane index of bin kz in a row: within each run of 8 bins the low 3 bits are xor-ed with the run index
+// (the row-wise writes of pass A and the reads of pass C touch 8 bins that are 8 apart)
+template <int M>
+__device__ __forceinline__ int swz(int kz) {
+  return kz < M ? ((kz & ~7) | ((kz ^ (kz >> 3)) & 7)) : kz;
+}
+
+template <int N>
+struct Fast {
+  static constexpr int M = N / 2, H = M + 1;
+  static constexpr int Lz = M / 8, Ly = N / 8;
+  static constexpr int P = 256 / (N * Lz);  // x-planes per CTA of passes A and C
+  // pass B: lines of N = 4 Lb points in Lb lanes; a CTA takes KY ky rows, or half the kz range of one row (N = 64)
+  static constexpr int Lb = N / 4;
+  static constexpr int KY = (N == 64) ? 1 : 2;
+  static constexpr int KZC = (N == 64) ? 2 : 1;            // kz chunks per ky row (one CTA each)
+  static constexpr int KZN = (H + KZC - 1) / KZC;          // kz per chunk
+  static constexpr int NTB = ((KY * KZN * Lb) + 31) / 32 * 32;
+  static constexpr size_t smem_plane() { return (size_t)P * N * H * sizeof(cplx<double>); }
+};
+
+// deterministic block sum of K values: warp shuffles, per-warp slots, thread 0 adds the warps in order
+template <int K>
+__device__ __forceinline__ void block_sum_ordered(double (&v)[K], double* red /* [32][K] */) {
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[wid * K + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < nw; ++w)
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] += red[w * K + k];
+}
+
+// Pass A: (fused) r update and sums; w r; packed real z FFT + real post-processing per row; y FFT per column.
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_fa_fast(double* __restrict__ r, const double* __restrict__ w, cplx<double>* __restrict__ spec, int m,
+              const cplx<double>* __restrict__ tw_y, const cplx<double>* __restrict__ tw_z,
+              const cplx<double>* __restrict__ tw_n2, const CellState* __restrict__ cs,
+              unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
+  using F = Fast<N>;
+  constexpr int M = F::M, H = F::H, Lz = F::Lz, Ly = F::Ly, P = F::P;
+  constexpr long NN = (long)N * N * N;
+  extern __shared__ unsigned char smem_raw[];
+  cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);  // [P][N rows][H]
+  __shared__ double red[32 * 2 * P];
+  const int c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
+  const int t = threadIdx.x;
+  const int p = t / (N * Lz), rem = t - p * (N * Lz), y = rem / Lz, l = rem - y * Lz;
+  const int x = blockIdx.x * P + p;
+  const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;  // start of the row (x, y, :)
+  const double2* rp2 = reinterpret_cast<const double2*>(r + roff);
+  const double2* ap2 = fu.Ap ? reinterpret_cast<const double2*>(static_cast<const double*>(fu.Ap) + roff) : nullptr;
+  const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
+  cplx<double> a[8];
+  double sr = 0.0, srr = 0.0;
+  {
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = rp2[l + Lz * q];
+    if (ap2) {
+      const double al = fu.vs[vec].alpha, mu = fu.vs[vec].mean[c];
+      double2 u[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) u[q] = ap2[l + Lz * q];
+      double2* rw2 = reinterpret_cast<double2*>(r + roff);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        v[q].x -= al * (u[q].x - mu);
+        v[q].y -= al * (u[q].y - mu);
+        rw2[l + Lz * q] = v[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      sr += v[q].x + v[q].y;
+      srr += v[q].x * v[q].x + v[q].y * v[q].y;
+    }
+    if (wp2) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double2 ww = wp2[l + Lz * q];
+        v[q].x *= ww.x;
+        v[q].y *= ww.y;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = {v[q].x, v[q].y};
+  }
+  // packed z FFT: a[k1] = Z[k1 + 8 brev(l)]
+  {
+    LaneTw<Lz, 8> T;
+    T.load(tw_z, l);
+    fft_nat_in<Lz, 8, false>(a, l, T);
+  }
+  const int k2 = brevL<Lz>(l);
+  cplx<double>* row = sm + ((long)p * N + y) * H;
+  {
+    // k1 = 0 partner: bin M - 8 k2 = 8 ((Lz - k2) mod Lz)
+    const int lane0 = (t & 31) - l;
+    const cplx<double> b0 = shfl_c(a[0], lane0 + brevL<Lz>((Lz - k2) & (Lz - 1)));
+    cplx<double> bz[8];
+    bz[0] = b0;
+#pragma unroll
+    for (int k1 = 1; k1 < 8; ++k1) bz[k1] = shfl_xor_c(a[8 - k1], Lz - 1);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) {
+      const int k = k1 + 8 * k2;
+      cplx<double> R;
+      if (k == 0) {
+        R = {a[0].x + a[0].y, 0.0};
+        row[swz<M>(M)] = {a[0].x - a[0].y, 0.0};
+      } else {
+        const cplx<double> A = a[k1], B = bz[k1];  // X_k, X_{M-k}
+        const cplx<double> E{(A.x + B.x) * 0.5, (A.y - B.y) * 0.5};
+        const cplx<double> O{(A.y + B.y) * 0.5, -(A.x - B.x) * 0.5};
+        R = cadd(E, cmul(tw_n2[k], O));
+      }
+      row[swz<M>(k)] = R;
+    }
+  }
+  if (fu.partA) {
+    double v2[2] = {sr, srr};
+    // per-plane sums: the threads of a plane are contiguous and a multiple of 32
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v2[k] += __shfl_down_sync(0xffffffffu, v2[k], o);
+    if ((t & 31) == 0) {
+      red[(t >> 5) * 2] = v2[0];
+      red[(t >> 5) * 2 + 1] = v2[1];
+    }
+  }
+  __syncthreads();
+  if (fu.partA && t < P) {
+    constexpr int WPP = N * Lz / 32;  // warps per plane
+    double s0 = 0.0, s1 = 0.0;
+    for (int q = 0; q < WPP; ++q) {
+      s0 += red[(t * WPP + q) * 2];
+      s1 += red[(t * WPP + q) * 2 + 1];
+    }
+    double* o = fu.partA + (((long)vec * 3 + c) * N + blockIdx.x * P + t) * 2;
+    o[0] = s0;
+    o[1] = s1;
+  }
+  // y FFT per (plane, kz) column: groups of Ly lanes
+  constexpr int G = 256 / Ly, TASKS = P * H, IT = (TASKS + G - 1) / G;
+  const int g = t / Ly, ly = t - g * Ly;
+  cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
+  LaneTw<Ly, 8> Ty;
+  Ty.load(tw_y, ly);
+#pragma unroll 1
+  for (int it = 0; it < IT; ++it) {
+    const int task = g + it * G;
+    const bool ok = task < TASKS;
+    if (!__any_sync(0xffffffffu, ok)) break;  // whole warp past the last column
+    const int pp = ok ? task / H : 0, kz = ok ? task - pp * H : 0;
+    cplx<double> b[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) b[q] = sm[((long)pp * N + ly + Ly * q) * H + swz<M>(kz)];
+    fft_nat_in<Ly, 8, false>(b, ly, Ty);
+    if (ok) {
+      const int xx = blockIdx.x * P + pp, kb = 8 * brevL<Ly>(ly);
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
+    }
+  }
+}
+
+// Pass B: x FFT of the three components of each (ky, kz) column, 3x3 Kinv, Parseval (r, z) partial, inverse.
+template <int N>
+__global__ void __launch_bounds__(Fast<N>::NTB, 2)
+    k_fb_fast(cplx<double>* __restrict__ spec, const double* __restrict__ kinv, int m,
+              const cplx<double>* __restrict__ tw_x, const CellState* __restrict__ cs,
+              unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
+  using F = Fast<N>;
+  constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN;
+  __shared__ double red[32];
+  const int vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
+  const int t = threadIdx.x, task = t / L, l = t - task * L;
+  const int kyl = task / KZN, kzl = task - kyl * KZN;
+  const int kz = blockIdx.y * KZN + kzl;
+  const bool ok = kyl < KY && kz < H;
+  const int ky = blockIdx.x * KY + (ok ? kyl : 0);
+  const long NS = (long)N * N * H;
+  cplx<double> a[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
+  LaneTw<L, 4> T;
+  T.load(tw_x, l);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) fft_nat_in<L, 4, false>(a[c], l, T);
+  double dot[1] = {0.0};
+  const double wt = (kz == 0 || kz == M) ? 1.0 : 2.0;
+  const int kb = 4 * brevL<L>(l);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    const double* K = kinv + (((long)(k1 + kb) * N + ky) * H + (ok ? kz : 0)) * 6;
+    const double kxx = K[0], kyy = K[1], kzz = K[2], kyz = K[3], kxz = K[4], kxy = K[5];
+    const cplx<double> A = a[0][k1], B = a[1][k1], C = a[2][k1];
+    const cplx<double> ua{kxx * A.x + kxy * B.x + kxz * C.x, kxx * A.y + kxy * B.y + kxz * C.y};
+    const cplx<double> ub{kxy * A.x + kyy * B.x + kyz * C.x, kxy * A.y + kyy * B.y + kyz * C.y};
+    const cplx<double> uc{kxz * A.x + kyz * B.x + kzz * C.x, kxz * A.y + kyz * B.y + kzz * C.y};
+    dot[0] += wt * (A.x * ua.x + A.y * ua.y + B.x * ub.x + B.y * ub.y + C.x * uc.x + C.y * uc.y);
+    a[0][k1] = ua;
+    a[1][k1] = ub;
+    a[2][k1] = uc;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) fft_tr_in<L, 4, true>(a[c], l, T);
+  if (ok)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] = a[c][q];
+  if (fu.partB) {
+    if (!ok) dot[0] = 0.0;
+    block_sum_ordered<1>(dot, red);
+    // layout [vec][ky][KZC]: the CTA's sum in its first slot, zeros in the slots of its other ky rows
+    if (t < KY) fu.partB[((long)vec * N + blockIdx.x * KY + t) * KZC + blockIdx.y] = (t == 0) ? dot[0] : 0.0;
+  }
+}
+
+// Pass C: inverse y FFT per column; real pre-processing + inverse packed z FFT per row; scale, w; sums.
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_fc_fast(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
+              double* __restrict__ z, int m, const cplx<double>* __restrict__ tw_y,
+              const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2,
+              const CellState* __restrict__ cs, double* __restrict__ partial, unsigned long long* __restrict__ units,
+              int ukind, PcgFuse fu) {
+  using F = Fast<N>;
+  constexpr int M = F::M, H = F::H, Lz = F::Lz, Ly = F::Ly, P = F::P;
+  constexpr long NN = (long)N * N * N;
+  extern __shared__ unsigned char smem_raw[];
+  cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);
+  __shared__ double red[32 * 4];
+  const int c = blockIdx.y, vec = blockIdx.z;
+  if (cs && !cs[vec / m].active) return;
+  prof_count(units, ukind);
+  const int t = threadIdx.x;
+  const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
+  {
+    constexpr int G = 256 / Ly, TASKS = P * H, IT = (TASKS + G - 1) / G;
+    const int g = t / Ly, ly = t - g * Ly;
+    LaneTw<Ly, 8> Ty;
+    Ty.load(tw_y, ly);
+#pragma unroll 1
+    for (int it = 0; it < IT; ++it) {
+      const int task = g + it * G;
+      const bool ok = task < TASKS;
+      if (!__any_sync(0xffffffffu, ok)) break;  // whole warp past the last column
+      const int pp = ok ? task / H : 0, kz = ok ? task - pp * H : 0;
+      const int xx = blockIdx.x * P + pp;
+      cplx<double> b[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        b[q] = ok ? sp[((long)(ly + Ly * q) * N + xx) * H + kz] : cplx<double>{0.0, 0.0};
+      fft_nat_in<Ly, 8, true>(b, ly, Ty);
+      if (ok) {
+        const int yb = 8 * brevL<Ly>(ly);
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + yb) * H + swz<M>(kz)] = b[k1];
+      }
+    }
+  }
+  __syncthreads();
+  const int p = t / (N * Lz), rem = t - p * (N * Lz), y = rem / Lz, l = rem - y * Lz;
+  const int x = blockIdx.x * P + p;
+  const cplx<double>* row = sm + ((long)p * N + y) * H;
+  cplx<double> a[8];
+  const int k2 = brevL<Lz>(l);
+#pragma unroll
+  for (int k1 = 0; k1 < 8; ++k1) {
+    const int k = k1 + 8 * k2;
+    if (k == 0) {
+      // X_0 and X_M of a real signal are real: their imaginary parts are rounding and are dropped
+      const double A = row[swz<M>(0)].x, B = row[swz<M>(M)].x;
+      a[k1] = {(A + B) * 0.5, (A - B) * 0.5};
+    } else {
+      const cplx<double> A = row[swz<M>(k)], B = row[swz<M>(M - k)];
+      const cplx<double> E{(A.x + B.x) * 0.5, (A.y - B.y) * 0.5};
+      const cplx<double> D{(A.x - B.x) * 0.5, (A.y + B.y) * 0.5};
+      const cplx<double> O = cmul(D, cconj(tw_n2[k]));
+      a[k1] = {E.x - O.y, E.y + O.x};
+    }
+  }
+  {
+    LaneTw<Lz, 8> T;
+    T.load(tw_z, l);
+    fft_tr_in<Lz, 8, true>(a, l, T);
+  }
+  // the packed z transform has length N/2, so its unnormalised inverse carries N^3 / 2
+  constexpr double norm = 2.0 / (double)NN;
+  const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;
+  const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
+  double2* zp2 = reinterpret_cast<double2*>(z + roff);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double2 ww[8];
+  if (wp2)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) ww[q] = wp2[l + Lz * q];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    double2 v{a[q].x * norm, a[q].y * norm};
+    if (wp2) {
+      v.x *= ww[q].x;
+      v.y *= ww[q].y;
+    }
+    zp2[l + Lz * q] = v;
+    acc[0] += v.x + v.y;
+    if (partial) {
+      const double2 rv = reinterpret_cast<const double2*>(r + roff)[l + Lz * q];
+      acc[1] += rv.x * v.x + rv.y * v.y;
+      acc[2] += rv.x + rv.y;
+      acc[3] += rv.x * rv.x + rv.y * rv.y;
+    }
+  }
+  if (partial || fu.partC) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+    if ((t & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) red[(t >> 5) * 4 + k] = acc[k];
+    __syncthreads();
+    if (t < P) {
+      constexpr int WPP = N * Lz / 32;
+      double s[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int q = 0; q < WPP; ++q)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s[k] += red[(t * WPP + q) * 4 + k];
+      const long pl = ((long)vec * 3 + c) * N + blockIdx.x * P + t;
+      if (partial)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) partial[pl * 4 + k] = s[k];
+      if (fu.partC) fu.partC[pl] = s[0];
+    }
+  }
+}
+
+template <int N>
+static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double* z, cplx<double>* spec,
+                       const double* w, const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk,
+                       cudaStream_t st) {
+  using F = Fast<N>;
+  const cplx<double>* tw = h.t64.tw;
+  const size_t plane = F::smem_plane();
+  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fa_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fc_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  if (nchunk) *nchunk = F::KZC;
+  unsigned long long* units = prof_units();
+  const cplx<double>* twx = tw + h.tw.off0;
+  const cplx<double>* twy = tw + h.tw.off1;
+  const cplx<double>* twn2 = tw + h.tw.off2;
+  const cplx<double>* twz = tw + h.tw.off2h;
+  {
+    ProfScope ps(PK_FFTA64, st);
+    k_fa_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
+    NLF_CHECK_LAUNCH();
+  }
+  {
+    ProfScope ps(PK_FFTB64, st);
+    k_fb_fast<N><<<dim3(N / F::KY, F::KZC, nvec), F::NTB, 0, st>>>(spec, h.t64.kinv, m, twx, cs, units, PK_FFTB64,
+                                                                     fu);
+    NLF_CHECK_LAUNCH();
+  }
+  {
+    ProfScope ps(PK_FFTC64, st);
+    k_fc_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial, units,
+                                                             PK_FFTC64, fu);
+    NLF_CHECK_LAUNCH();
+  }
+  return NLF_OK;
+}
+
+// the register-resident passes apply to FP64 cubes of 32 or 64 (NLF_FFT_GENERIC=1 forces the generic passes)
+static int fast_n(const LinearHandle& h) {
+  static const bool generic = [] {
+    const char* e = std::getenv("NLF_FFT_GENERIC");
+    return e && e[0] == '1';
+  }();
+  const Geom& g = h.g;
+  if (generic || g.n0 != g.n1 || g.n1 != g.n2) return 0;
+  return (g.n0 == 32 || g.n0 == 64) ? g.n0 : 0;
+}
+
 static FftDims fft_dims(const LinearHandle& h) {
   FftDims d;
   d.n0 = h.g.n0;
@@ -642,6 +1138,11 @@ const float* kinv_table<float>(const LinearHandle& h) { return h.t32.kinv; }
 template <typename T>
 static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx<T>* spec, const T* w,
                         const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    const int nf = fast_n(h);
+    if (nf == 64) return launch_fast<64>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, st);
+    if (nf == 32) return launch_fast<32>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, st);
+  }
   FftDims d = fft_dims(h);
   const bool np2 = any_non_pow2(d);
   const int cap = (h.smem_optin > 0 ? h.smem_optin : 48 * 1024) - 2048;  // room for static shared memory

@@ -49,7 +49,7 @@ def _scaled_oracle(oh, s, r):
     return w * oh.precond(w * r)
 
 
-@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (6, 6, 6), (8, 8, 1)])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (64, 64, 64), (6, 6, 6), (8, 8, 1)])
 def test_fp32_and_scaled_operators(L, shape):
     """The FP32 operators of the mixed-precision solver agree with the FP64 oracle to FP32 rounding
     (rel 2e-6); the FP64 scaled preconditioner to FP64 rounding."""
