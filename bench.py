@@ -323,6 +323,70 @@ def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
             "loss_last": float(np.mean(losses[-20:])) if losses else None, "conv_roofline": conv, **out}
 
 
+def mech_arm(args, stream):
+    """Finite-strain compression (the reference's qoi.run_path "compression" driver, nlfiber/qoi.py:49-115):
+    compressible neo-Hookean cells (E 1, nu 0.3, void rho^3 with floor 1e-6, WLS (500, 0.01)), Fbar_xx = 1 - e
+    with the lateral stresses free (Mixed control of Fbar_yy, Fbar_zz), steps of 0.01 each warm-started from the
+    previous state, FP64 Newton-CG with EW forcing on the GPU. Cells of the same generator with seeds 0..."""
+    import torch
+    from nlfiber_b200 import _lib
+    from nlfiber_b200 import mech as MH
+    n = args.n
+    cells = gen_cells(list(range(args.mech_cells)), n // 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rows, newton, cg, steps = [], 0, 0, 0
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(len(cells)):
+        cell = MH.Cell(cells[i], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
+        mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond)
+        z = None
+        for k in range(1, args.mech_steps + 1):
+            e = -0.01 * k
+            Fb = np.eye(3)
+            if z is not None:
+                Fb = mix.unpack(z, Fb)[1]
+            Fb[0, 0] = 1.0 + e
+            w, F, log = mix.solve(Fb, z0=z)
+            P = np.asarray(cell.mean_stress(w, F))
+            rows.append({"cell": i, "e": e, "P_xx": float(P[0, 0]), "nu": [float(-(F[j, j] - 1) / e) for j in (1, 2)],
+                         "newton": int(log["newton"]), "cg": int(log["cg"]), "converged": bool(log["converged"])})
+            newton += int(log["newton"])
+            cg += int(log["cg"])
+            steps += 1
+            z = log["z"]
+            if not log["converged"]:
+                break
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # kernel classes from one more first step of cell 0 with per-launch events on (and no graph replay)
+    cell = MH.Cell(cells[0], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
+    mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond)
+    Fb = np.eye(3)
+    Fb[0, 0] = 0.99
+    _lib.profile(True)
+    _, _, plog = mix.solve(Fb)
+    torch.cuda.synchronize()
+    prof = _lib.profile_report()
+    _lib.profile(False)
+    N = n ** 3
+    el = prof.get("mech_elem", (0.0, 0, 0))
+    # tangent matvec bytes per voxel (FP64): v in and the element forces out (3 + 24 doubles: the forces of the
+    # 8 corners go to a per-element array that the gather sums), state w (3), s and gamma (2)
+    hvp_bytes = N * 8 * (3 + 24 + 3 + 2)
+    kernels = {k: {"ms": round(v[0], 2), "launches": v[1]} for k, v in prof.items() if v[1]}
+    kernels["profiled_step_cg_iterations"] = int(plog["cg"])
+    return {"mode": "mech", "workload": f"{len(cells)} seeded synthetic {n}^3 cells, compression to "
+            f"{0.01 * args.mech_steps:.2f} in steps of 0.01, lateral stresses free", "precond": args.mech_precond,
+            "steps": steps, "seconds": round(ms / 1e3, 2), "steps_per_s": round(steps / (ms / 1e3), 3),
+            "newton_per_step": round(newton / max(steps, 1), 2), "cg_per_step": round(cg / max(steps, 1), 1),
+            "ms_per_cg_iteration": round(ms / max(cg, 1), 3),
+            "mech_elem_ms_per_launch": round(el[0] / max(el[1], 1), 4),
+            "mech_elem_GBps_at_stated_bytes": round(hvp_bytes / (el[0] / max(el[1], 1) * 1e-3) / 1e9, 1) if el[1] else None,
+            "converged_all": all(r["converged"] for r in rows), "rows": rows, "kernels": kernels}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,12 +409,25 @@ def main():
     ap.add_argument("--train-cells32", type=int, default=256)
     ap.add_argument("--train-cells64", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--mech", action="store_true",
+                    help="finite-strain compression path (Newton-CG on the GPU) instead of the default measurement")
+    ap.add_argument("--mech-cells", type=int, default=2)
+    ap.add_argument("--mech-steps", type=int, default=3)
+    ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
+                    help="CG preconditioner of the Newton steps: the reference's (fft) or the node-scaled one")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.mech:
+        import torch
+        torch.cuda.set_device(local)
+        res = mech_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
 
     n_o = args.n // 2
     seeds = list(range(rank * args.cells, (rank + 1) * args.cells))

@@ -164,6 +164,11 @@ NLF_API int nlf_mech_hvp(nlf_mech* h, const double* w, const double* Fbar, const
                          double* hv, double* hP, void* stream);
 /* mech.py:172-189 precond_w: inverse of the homogeneous unit-stiffness operator (N x the linear symbol). */
 NLF_API int nlf_mech_precond_w(nlf_mech* h, const double* r, double* z, void* stream);
+/* Preconditioner of nlf_mech_cg and nlf_mech_precond_w: NLF_PC_FFT (default) is the reference's
+ * N K0^-1 / sws (mech.py:264-294); NLF_PC_FFT_SCALED is N w K0^-1 w with w the node stiffness scaling of
+ * nlf_precond_ex (sws then unused). Same Newton-CG solution to the same tolerances; far fewer CG iterations
+ * at high contrast. No counterpart in the reference. */
+NLF_API int nlf_mech_set_precond(nlf_mech* h, int precond);
 /* mech.py:127-129 grad_w: displacement gradient at the Gauss points, H (8, nx, ny, nz, 3, 3). */
 NLF_API int nlf_mech_grad_w(nlf_mech* h, const double* w, double* H, void* stream);
 /* mech.py:264-290 _cg_impl at the linearization point (w, Fbar) with k free macro components

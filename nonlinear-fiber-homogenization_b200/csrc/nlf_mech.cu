@@ -360,11 +360,13 @@ __global__ void k_cg_dot(long N, const double* __restrict__ a, const double* __r
   __shared__ double red[32 * 4];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (!st->done) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < 3 * N; i += (long)gridDim.x * blockDim.x) {
-      const double x = a[i];
-      acc[i / N] += x;
-      acc[3] += x * b[i];
-    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+        const double x = a[c * N + i];
+        acc[c] += x;
+        acc[3] += x * b[c * N + i];
+      }
   }
   block_sum<4>(acc, red);
   if (threadIdx.x == 0)
@@ -375,10 +377,16 @@ __global__ void k_cg_dot(long N, const double* __restrict__ a, const double* __r
 // after Ap = H p: mean of Ap's w part, pAp (tail included, p is mean-free), alpha and the negative-curvature flag
 __global__ void k_cg_fin_pap(long N, const double* __restrict__ partial, int nb, const double* __restrict__ p,
                              const double* __restrict__ Ap, MechCG* st) {
-  if (threadIdx.x != 0 || st->done) return;
+  if (st->done) return;
+  // one warp: lane-strided partial sums, then a shuffle reduction (fixed order)
   double s[4] = {0, 0, 0, 0};
-  for (int b = 0; b < nb; ++b)
+  for (int b = threadIdx.x; b < nb; b += 32)
     for (int q = 0; q < 4; ++q) s[q] += partial[b * 4 + q];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+  if (threadIdx.x != 0) return;
   double pap = s[3];
   for (int t = 0; t < st->k; ++t) pap += p[3 * N + t] * Ap[3 * N + t];
   for (int c = 0; c < 3; ++c) st->mAp[c] = s[c] / (double)N;
@@ -393,14 +401,20 @@ __global__ void k_cg_xr(long N, double* __restrict__ x, double* __restrict__ r, 
                         const double* __restrict__ Ap, const double* __restrict__ z0, const MechCG* __restrict__ st) {
   if (st->done) return;
   const double a = st->alpha;
-  const long L = 3 * N + st->k;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < L; i += (long)gridDim.x * blockDim.x) {
-    const double ap = i < 3 * N ? Ap[i] - st->mAp[i / N] : Ap[i];
-    r[i] -= a * ap;
-    if (st->neg) {
-      if (st->it == 0) x[i] = z0[i];
-    } else {
-      x[i] += a * p[i];
+  const bool neg = st->neg, first = st->it == 0;
+  const int k = st->k;
+  const long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x, step = (long)gridDim.x * blockDim.x;
+#pragma unroll
+  for (int c = 0; c <= 3; ++c) {  // c = 3: the macro tail (k entries)
+    const long off = c * N, len = c < 3 ? N : k;
+    const double mu = c < 3 ? st->mAp[c] : 0.0;
+    for (long i = i0; i < len; i += step) {
+      r[off + i] -= a * (Ap[off + i] - mu);
+      if (neg) {
+        if (first) x[off + i] = z0[off + i];
+      } else {
+        x[off + i] += a * p[off + i];
+      }
     }
   }
 }
@@ -408,14 +422,18 @@ __global__ void k_cg_xr(long N, double* __restrict__ x, double* __restrict__ r, 
 // after the preconditioner (w part unscaled in zf): mean of z, rz1, rr, convergence, beta, counters
 __global__ void k_cg_fin_pc(long N, int n0, const double* __restrict__ partial, const double* __restrict__ r,
                             MechCG* st, int init) {
-  if (threadIdx.x != 0 || st->done) return;
+  if (st->done) return;
+  // one warp: lane-strided partial sums over the x-planes, then a shuffle reduction (fixed order)
   double a[3][4];
   for (int c = 0; c < 3; ++c)
     for (int q = 0; q < 4; ++q) {
       double v = 0.0;
-      for (int x = 0; x < n0; ++x) v += partial[((long)c * n0 + x) * 4 + q];
+      for (int x = threadIdx.x; x < n0; x += 32) v += partial[((long)c * n0 + x) * 4 + q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       a[c][q] = v;
     }
+  if (threadIdx.x != 0) return;
   double rz1 = 0.0, rr = 0.0;
   for (int c = 0; c < 3; ++c) {
     st->mz[c] = a[c][0] / (double)N;
@@ -445,20 +463,49 @@ __global__ void k_cg_fin_pc(long N, int n0, const double* __restrict__ partial, 
 __global__ void k_cg_p(long N, double* __restrict__ p, const double* __restrict__ zf, const double* __restrict__ r,
                        double* __restrict__ z0, const MechCG* __restrict__ st, int init) {
   if (!init && !st->ran) return;
-  const double be = init ? 0.0 : st->beta;
-  const long L = 3 * N + st->k;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < L; i += (long)gridDim.x * blockDim.x) {
-    const double z = i < 3 * N ? st->scale * (zf[i] - st->mz[i / N]) : r[i] / st->dmac[i - 3 * N];
-    if (init) {
-      p[i] = z;
-      z0[i] = z;
-    } else {
-      p[i] = z + be * p[i];
+  const double be = init ? 0.0 : st->beta, sc = st->scale;
+  const int k = st->k;
+  const long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x, step = (long)gridDim.x * blockDim.x;
+#pragma unroll
+  for (int c = 0; c <= 3; ++c) {  // c = 3: the macro tail (k entries)
+    const long off = c * N, len = c < 3 ? N : k;
+    const double mu = c < 3 ? st->mz[c] : 0.0;
+    for (long i = i0; i < len; i += step) {
+      const double z = c < 3 ? sc * (zf[off + i] - mu) : r[off + i] / st->dmac[i];
+      if (init) {
+        p[off + i] = z;
+        z0[off + i] = z;
+      } else {
+        p[off + i] = z + be * p[off + i];
+      }
     }
   }
 }
 
 __global__ void k_cg_clear_ran(MechCG* st) { st->ran = 0; }
+
+// free macro index pairs (a, b) of the mixed control, packed as 3 a + b
+struct FreeIdx {
+  int k;
+  int ab[9];
+};
+
+// dFm (9, row-major) = sum_j p_tail[j] e_(a_j b_j): the macro part of the CG direction enters the element pass
+__global__ void k_cg_dfm(const double* __restrict__ ptail, FreeIdx f, double* __restrict__ dfm) {
+  const int q = threadIdx.x;
+  if (q < 9) {
+    double v = 0.0;
+    for (int j = 0; j < f.k; ++j)
+      if (f.ab[j] == q) v = ptail[j];
+    dfm[q] = v;
+  }
+}
+
+// Ap_tail[j] = the P-bar sensitivity sum9 at the free entry j
+__global__ void k_cg_aptail(const double* __restrict__ sum9, FreeIdx f, double* __restrict__ aptail) {
+  const int j = threadIdx.x;
+  if (j < f.k) aptail[j] = sum9[f.ab[j]];
+}
 
 // b = proj(b): subtract the mean of the w part (in place) using k_cg_dot partials of (b, b)
 __global__ void k_cg_mean_sub(long N, double* __restrict__ b, const double* __restrict__ partial, int nb) {
@@ -469,8 +516,9 @@ __global__ void k_cg_mean_sub(long N, double* __restrict__ b, const double* __re
     m[threadIdx.x] = a / (double)N;
   }
   __syncthreads();
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < 3 * N; i += (long)gridDim.x * blockDim.x)
-    b[i] -= m[i / N];
+  for (int c = 0; c < 3; ++c)
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+      b[c * N + i] -= m[c];
 }
 
 }  // namespace nlf
@@ -485,6 +533,12 @@ struct nlf_mech {
   DevBuf state;  // s, gamma, logs
   DevBuf ws;     // vectors and partials
   DevBuf io;     // staging
+  // CG iterations replayed from a CUDA graph on a handle-owned stream, ordered after and before the caller's
+  // stream by events (capture is not possible on the legacy default stream)
+  cudaStream_t gst = nullptr;
+  cudaEvent_t gev[2] = {nullptr, nullptr};
+  int pc_mode = NLF_PC_FFT;  // NLF_PC_FFT: the reference's N K0^-1 / sws; NLF_PC_FFT_SCALED: N w K0^-1 w
+  double* wnode = nullptr;   // w = (mean s of the 8 elements around a node)^-1/2, in `state`
 };
 
 namespace {
@@ -542,7 +596,7 @@ int mech_pass(nlf_mech* H, const double* w, const double* Fb, const double* v, c
   const long N = H->d.N;
   const int blocks = (int)std::min<long>((N + kMechThreads - 1) / kMechThreads, 4L * 148 * 4);
   *nb = blocks;
-  ProfScope ps(PK_OTHER, st);
+  ProfScope ps(PK_MECH_ELEM, st);
   k_mech_elem<MODE><<<blocks, kMechThreads, 0, st>>>(H->d, w, Fb, v, dFm, fe, partial);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -550,7 +604,7 @@ int mech_pass(nlf_mech* H, const double* w, const double* Fb, const double* v, c
 
 int gather(nlf_mech* H, const double* fe, double* out, cudaStream_t st) {
   const long N = H->d.N;
-  ProfScope ps(PK_OTHER, st);
+  ProfScope ps(PK_MECH_GATHER, st);
   k_mech_gather<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, H->d.n0, H->d.n1, H->d.n2, fe, out);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -621,6 +675,9 @@ NLF_API int nlf_mech_create(nlf_mech** out, int nx, int ny, int nz, double E, do
 
 NLF_API int nlf_mech_destroy(nlf_mech* H) {
   if (!H) return NLF_OK;
+  if (H->gst) cudaStreamDestroy(H->gst);
+  for (cudaEvent_t e : H->gev)
+    if (e) cudaEventDestroy(e);
   H->state.release();
   H->ws.release();
   H->io.release();
@@ -637,7 +694,7 @@ NLF_API int nlf_mech_set_rho(nlf_mech* H, const double* rho, double* s_out, doub
   }
   cudaStream_t st = (cudaStream_t)stream;
   const long N = H->d.N;
-  NLF_TRY(H->state.reserve(3 * al(N * 8)));
+  NLF_TRY(H->state.reserve(4 * al(N * 8)));
   NLF_TRY(H->io.reserve(al(N * 8)));
   const double* rd = nullptr;
   NLF_TRY(stage(rho, N, H->io, 0, &rd, st));
@@ -649,6 +706,8 @@ NLF_API int nlf_mech_set_rho(nlf_mech* H, const double* rho, double* s_out, doub
   NLF_CHECK_LAUNCH();
   H->d.s = s;
   H->d.gamma = gam;
+  H->wnode = reinterpret_cast<double*>((char*)H->state.ptr + 3 * al(N * 8));
+  NLF_TRY(launch_node_scaling(lin_of(H), 1, s, nullptr, H->wnode, nullptr, st));
   // sws = exp(mean log s) (mech.py:292-294), FP64 on the host from the device values
   std::vector<double> lg(N);
   NLF_CUDA_TRY(cudaMemcpyAsync(lg.data(), logs, N * 8, cudaMemcpyDeviceToHost, st));
@@ -762,7 +821,15 @@ NLF_API int nlf_mech_precond_w(nlf_mech* H, const double* r, double* z, void* st
     return NLF_EBADARG;
   }
   const LinearHandle& L = lin_of(H);
-  NLF_TRY(nlf_precond(H->lin, 1, r, z, stream));
+  if (H->pc_mode == NLF_PC_FFT_SCALED) {
+    if (!H->rho_set) {
+      set_error("nlf_mech_precond_w: the scaled preconditioner needs nlf_mech_set_rho first");
+      return NLF_EBADARG;
+    }
+    NLF_TRY(nlf_precond_ex(H->lin, 1, r, z, NLF_PREC_FP64, NLF_PC_FFT_SCALED, H->d.s, stream));
+  } else {
+    NLF_TRY(nlf_precond(H->lin, 1, r, z, stream));
+  }
   // scale in place (z is host or device)
   const long n = 3 * L.g.N;
   if (on_dev(z)) {
@@ -773,6 +840,15 @@ NLF_API int nlf_mech_precond_w(nlf_mech* H, const double* r, double* z, void* st
   } else {
     for (long i = 0; i < n; ++i) z[i] *= (double)L.g.N;
   }
+  return NLF_OK;
+}
+
+NLF_API int nlf_mech_set_precond(nlf_mech* H, int precond) {
+  if (!H || (precond != NLF_PC_FFT && precond != NLF_PC_FFT_SCALED)) {
+    set_error("nlf_mech_set_precond: bad arguments");
+    return NLF_EBADARG;
+  }
+  H->pc_mode = precond;
   return NLF_OK;
 }
 
@@ -854,7 +930,9 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
   hs.k = k;
   hs.maxit = maxit;
   hs.tol = tol;
-  hs.scale = (double)N / sws;
+  const bool scaled = H->pc_mode == NLF_PC_FFT_SCALED;
+  const double* wpc = scaled ? H->wnode : nullptr;
+  hs.scale = scaled ? (double)N : (double)N / sws;
   for (int j = 0; j < k; ++j) hs.dmac[j] = dmac[j];
   hs.done = maxit == 0 ? 1 : 0;
   NLF_CUDA_TRY(cudaMemcpyAsync(stt, &hs, sizeof(hs), cudaMemcpyHostToDevice, st));
@@ -865,40 +943,81 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
   k_cg_mean_sub<<<vb, vt, 0, st>>>(N, r, part, vb);
   NLF_CHECK_LAUNCH();
   // z0 = M b, p = z0, rz = (b, z0), bn = ||b||
-  NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, nullptr, nullptr, ppc, st));
+  NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, wpc, nullptr, ppc, st));
   k_cg_fin_pc<<<1, 32, 0, st>>>(N, L.g.n0, ppc, r, stt, 1);
   k_cg_p<<<vb, vt, 0, st>>>(N, p, zf, r, z0, stt, 1);
   NLF_CHECK_LAUNCH();
-  // the macro unknowns enter the element pass as dFm = sum_j p_tail[j] E_sel_j; build it on the device
-  int fidx[18] = {};
-  for (int j = 0; j < 2 * k; ++j) fidx[j] = free_idx[j];
+  // the macro unknowns enter the element pass as dFm = sum_j p_tail[j] E_sel_j; built on the device
+  FreeIdx fi{};
+  fi.k = k;
+  for (int j = 0; j < k; ++j) fi.ab[j] = 3 * free_idx[2 * j] + free_idx[2 * j + 1];
   const int every = check_every > 0 ? check_every : 8;
+  int nb = 0;
+  auto chunk = [&](cudaStream_t s) -> int {
+    for (int q = 0; q < every; ++q) {
+      k_cg_clear_ran<<<1, 1, 0, s>>>(stt);
+      // Ap = H p; the macro part of p enters as dFm (fbd[9..17])
+      k_cg_dfm<<<1, 32, 0, s>>>(p + 3 * N, fi, fbd + 9);
+      NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, s));
+      double* sum9 = part + 4096 * 9;
+      k_mech_sum<<<1, 32, 0, s>>>(part, nb, 9, sum9);
+      NLF_TRY(gather(H, fe, Ap, s));
+      if (k) k_cg_aptail<<<1, 32, 0, s>>>(sum9, fi, Ap + 3 * N);
+      // proj(Ap) and pAp
+      {
+        ProfScope ps(PK_OTHER, s);
+        k_cg_dot<<<vb, vt, 0, s>>>(N, Ap, p, stt, part + 4096 * 10 - 4 * vb);
+        k_cg_fin_pap<<<1, 32, 0, s>>>(N, part + 4096 * 10 - 4 * vb, vb, p, Ap, stt);
+        k_cg_xr<<<vb, vt, 0, s>>>(N, xs, r, p, Ap, z0, stt);
+      }
+      NLF_CHECK_LAUNCH();
+      NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, wpc, nullptr, ppc, s));
+      {
+        ProfScope ps(PK_OTHER, s);
+        k_cg_fin_pc<<<1, 32, 0, s>>>(N, L.g.n0, ppc, r, stt, 0);
+        k_cg_p<<<vb, vt, 0, s>>>(N, p, zf, r, z0, stt, 0);
+      }
+      NLF_CHECK_LAUNCH();
+    }
+    return NLF_OK;
+  };
+  // graph replay of the chunk unless the profiler (per-launch events) is on
+  cudaGraphExec_t gexec = nullptr;
+  if (!prof_on()) {
+    if (!H->gst) {
+      NLF_CUDA_TRY(cudaStreamCreateWithFlags(&H->gst, cudaStreamNonBlocking));
+      NLF_CUDA_TRY(cudaEventCreateWithFlags(&H->gev[0], cudaEventDisableTiming));
+      NLF_CUDA_TRY(cudaEventCreateWithFlags(&H->gev[1], cudaEventDisableTiming));
+    }
+    cudaGraph_t graph = nullptr;
+    NLF_CUDA_TRY(cudaStreamBeginCapture(H->gst, cudaStreamCaptureModeThreadLocal));
+    const int rc = chunk(H->gst);
+    const cudaError_t e = cudaStreamEndCapture(H->gst, &graph);
+    if (rc != NLF_OK || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != NLF_OK) return rc;
+      NLF_CUDA_TRY(e);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    NLF_CUDA_TRY(ei);
+  }
+  struct ExecGuard {
+    cudaGraphExec_t g;
+    ~ExecGuard() {
+      if (g) cudaGraphExecDestroy(g);
+    }
+  } guard{gexec};
   int host_done = hs.done, iters = 0;
   while (!host_done) {
-    for (int q = 0; q < every; ++q) {
-      k_cg_clear_ran<<<1, 1, 0, st>>>(stt);
-      // Ap = H p; the macro part of p enters as dFm[a][b] = p_tail[j] for (a, b) = free[j] (fbd[9..17])
-      NLF_CUDA_TRY(cudaMemsetAsync(fbd + 9, 0, 72, st));
-      for (int j = 0; j < k; ++j)
-        NLF_CUDA_TRY(cudaMemcpyAsync(fbd + 9 + fidx[2 * j] * 3 + fidx[2 * j + 1], p + 3 * N + j, 8,
-                                     cudaMemcpyDeviceToDevice, st));
-      int nb = 0;
-      NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, st));
-      double* sum9 = part + 4096 * 9;
-      k_mech_sum<<<1, 32, 0, st>>>(part, nb, 9, sum9);
-      NLF_TRY(gather(H, fe, Ap, st));
-      for (int j = 0; j < k; ++j)
-        NLF_CUDA_TRY(cudaMemcpyAsync(Ap + 3 * N + j, sum9 + fidx[2 * j] * 3 + fidx[2 * j + 1], 8,
-                                     cudaMemcpyDeviceToDevice, st));
-      // proj(Ap) and pAp
-      k_cg_dot<<<vb, vt, 0, st>>>(N, Ap, p, stt, part + 4096 * 10 - 4 * vb);
-      k_cg_fin_pap<<<1, 32, 0, st>>>(N, part + 4096 * 10 - 4 * vb, vb, p, Ap, stt);
-      k_cg_xr<<<vb, vt, 0, st>>>(N, xs, r, p, Ap, z0, stt);
-      NLF_CHECK_LAUNCH();
-      NLF_TRY(launch_precond<double>(L, 1, 1, r, zf, spec, nullptr, nullptr, ppc, st));
-      k_cg_fin_pc<<<1, 32, 0, st>>>(N, L.g.n0, ppc, r, stt, 0);
-      k_cg_p<<<vb, vt, 0, st>>>(N, p, zf, r, z0, stt, 0);
-      NLF_CHECK_LAUNCH();
+    if (gexec) {
+      NLF_CUDA_TRY(cudaEventRecord(H->gev[0], st));
+      NLF_CUDA_TRY(cudaStreamWaitEvent(H->gst, H->gev[0], 0));
+      NLF_CUDA_TRY(cudaGraphLaunch(gexec, H->gst));
+      NLF_CUDA_TRY(cudaEventRecord(H->gev[1], H->gst));
+      NLF_CUDA_TRY(cudaStreamWaitEvent(st, H->gev[1], 0));
+    } else {
+      NLF_TRY(chunk(st));
     }
     iters += every;
     NLF_CUDA_TRY(cudaMemcpyAsync(&hs, stt, sizeof(hs), cudaMemcpyDeviceToHost, st));

@@ -23,7 +23,7 @@ EXPORTS = (
     "nlf_bilinear", "nlf_dC_drho", "nlf_C_full", "nlf_precond_symbol", "nlf_apply_K_ex", "nlf_precond_ex",
     "nlf_profile", "nlf_profile_report", "nlf_profile_name", "nlf_bilinear_noalloc",
     "nlf_mech_create", "nlf_mech_destroy", "nlf_mech_set_rho", "nlf_mech_energy", "nlf_mech_hvp",
-    "nlf_mech_precond_w", "nlf_mech_grad_w", "nlf_mech_cg",
+    "nlf_mech_precond_w", "nlf_mech_grad_w", "nlf_mech_cg", "nlf_mech_set_precond",
     "nlf_unet_create", "nlf_unet_destroy", "nlf_unet_param_count", "nlf_unet_get_params", "nlf_unet_set_params",
     "nlf_unet_forward", "nlf_unet_backward", "nlf_unet_adam_step",
 )
@@ -81,6 +81,7 @@ def _load():
         "nlf_mech_precond_w": (I, [P, P, P, P]),
         "nlf_mech_grad_w": (I, [P, P, P, P]),
         "nlf_mech_cg": (I, [P, P, P, I, P, P, P, D, D, I, P, P, P, P, I, P]),
+        "nlf_mech_set_precond": (I, [P, I]),
         "nlf_unet_create": (I, [ctypes.POINTER(P), I, I, I, ctypes.c_ulonglong]),
         "nlf_unet_destroy": (I, [P]),
         "nlf_unet_param_count": (ctypes.c_longlong, [P]),

@@ -156,10 +156,17 @@ class Mixed:
     """mech.py:195-346: Fbar components in `free` are unknowns with zero conjugate stress, the rest prescribed.
     Unknown z = (w, Fbar_free); minimizes W(z) by Newton-CG."""
 
-    def __init__(self, cell, free=((1, 1), (2, 2)), forcing="ew"):
+    def __init__(self, cell, free=((1, 1), (2, 2)), forcing="ew", precond="fft"):
+        """precond "fft" is the reference's preconditioner (homogeneous inverse / sws); "scaled" wraps the same
+        inverse in the node stiffness scaling (same solution, fewer CG iterations at high contrast). The choice
+        is kept by the cell's device handle."""
         self.c = cell
         self.free = [tuple(f) for f in free]
         self.forcing = forcing
+        if precond not in ("fft", "scaled"):
+            raise ValueError(f"precond must be 'fft' or 'scaled', got {precond!r}")
+        self.precond_kind = precond
+        check(lib.nlf_mech_set_precond(cell._h, 1 if precond == "scaled" else 0))
         self.shape = cell.shape
         self.nw = 3 * cell.N
         self.k = len(self.free)
@@ -226,8 +233,8 @@ class Mixed:
         return np.concatenate([w.ravel(), r[self.nw:] / dmac])
 
     def _sws(self):
-        """mech.py:292-294."""
-        return self.c.sws
+        """mech.py:292-294 (1 for the scaled preconditioner, which carries the stiffness itself)."""
+        return 1.0 if self.precond_kind == "scaled" else self.c.sws
 
     def _cgA(self, A, b, dmac, sws, tol, maxit):
         """mech.py:264-290 on the device: (x, iterations, converged, negative curvature)."""
