@@ -7,10 +7,11 @@
 //
 // The apply kernel marches a CTA along x (the slowest axis) over a TY x TZ tile of the (y, z) plane. Each
 // thread owns one element of the (TY+1) x (TZ+1) element layer that touches the tile (one element row and
-// column of halo). Per layer it reads the 4 new corner nodes from a shared node plane (the other 4 are the
-// previous layer's, kept in registers), computes the 24 element forces with the mode form of Ke, adds the
+// column of halo). Per layer it reads its 8 corner nodes from the two shared node planes of the layer, computes
+// the 24 element forces with the mode form of Ke, adds the
 // forces on the finished plane to the top-corner forces carried from the previous layer, and publishes them
-// to shared memory; each output node then sums its 4 in-plane element contributions. Every output node is
+// to shared memory; each output node then sums its 4 in-plane element contributions. Node planes are
+// prefetched three layers ahead into a three-slot ring, so one barrier per layer suffices. Every output node is
 // written once, with a fixed summation order (deterministic), and the whole 27-point stencil stays on chip.
 #include "nlf_internal.h"
 #include "nlf_prof.cuh"
@@ -27,9 +28,11 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   constexpr int NT = (NE + 31) / 32 * 32;
   constexpr int NP = HY * HZ;
   constexpr int PF = (3 * NP + NT - 1) / NT;  // plane values each thread prefetches per layer
-  __shared__ T pl[2][3][NP];                  // node plane j lives in pl[j & 1]
-  __shared__ T sl[NE];
-  __shared__ T g[4][3][NE];
+  // One barrier per layer: node plane j lives in pl[j % 3] (written three layers ahead, after the barrier of
+  // the layer that last read the slot), element forces and scales alternate between two buffers.
+  __shared__ T pl[3][3][NP];
+  __shared__ T sl[2][NE];
+  __shared__ T g[2][4][3][NE];
   __shared__ int gys[HY], gzs[HZ];
   __shared__ double red[32 * 4];
   (void)EY;
@@ -72,19 +75,20 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   const bool outp = tid < TY * TZ;
   const int ty = tid / TZ, tz = tid - (tid / TZ) * TZ;
   const int own = (ty + 1) * HZ + tz + 1;  // the output node in node-plane coordinates
+  auto slot = [](int j) { return ((j % 3) + 3) % 3; };
 
-  // prologue: node planes xb - 1 and xb, element scales of layer xb - 1
+  // prologue: node planes xb - 1, xb, xb + 1 and the element scales of layer xb - 1
 #pragma unroll
   for (int i = 0; i < PF; ++i)
     if (poff[i] >= 0) {
       const int idx = tid + i * NT;
-      pl[(xb - 1) & 1][0][idx] = __ldg(xv + (long)wrap(xb - 1, n0) * P + poff[i]);
-      pl[xb & 1][0][idx] = __ldg(xv + (long)wrap(xb, n0) * P + poff[i]);
+#pragma unroll
+      for (int j = -1; j <= 1; ++j) pl[slot(xb + j)][0][idx] = __ldg(xv + (long)wrap(xb + j, n0) * P + poff[i]);
     }
-  if (ev) sl[tid] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
+  if (ev) sl[(xb - 1) & 1][tid] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
   __syncthreads();
 
-  T ft[3][4];
+  T ft[3][4];  // top-corner forces carried to the next layer
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -92,21 +96,22 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
   for (int k = xb - 1; k < xe; ++k) {
-    // prefetch node plane k + 2 and the scales of layer k + 1 into registers; they land while this layer's
-    // elements are computed and are stored after the first barrier
+    // prefetch node plane k + 3 and the scales of layer k + 1 into registers
     T pre[PF];
     T pres = T(0);
-    const bool more = k + 1 < xe;
-    if (more) {
-      const long base = (long)wrap(k + 2, n0) * P;
+    const bool pnext = k + 3 <= xe, snext = k + 1 < xe;
+    if (pnext) {
+      const long base = (long)wrap(k + 3, n0) * P;
 #pragma unroll
       for (int i = 0; i < PF; ++i) pre[i] = poff[i] >= 0 ? __ldg(xv + base + poff[i]) : T(0);
-      if (ev) pres = __ldg(sv + (long)wrap(k + 1, n0) * P + soff);
     }
-    const T(*lo)[NP] = pl[k & 1];
-    const T(*hi)[NP] = pl[(k + 1) & 1];
+    if (snext && ev) pres = __ldg(sv + (long)wrap(k + 1, n0) * P + soff);
+    const T(*lo)[NP] = pl[slot(k)];
+    const T(*hi)[NP] = pl[slot(k + 1)];
+    T(*gk)[3][NE] = g[k & 1];
     T xo[3] = {T(0), T(0), T(0)};
     if (ev) {
+      // (carrying the lower corners in registers instead of re-reading them measured slower: register pressure)
       T v[3][8], f[3][8];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -115,24 +120,25 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
           v[c][2 * q] = lo[c][cidx[q]];
           v[c][2 * q + 1] = hi[c][cidx[q]];
         }
-      const ModeC<T> ks = scale_modec(kc, sl[tid]);
+      const ModeC<T> ks = scale_modec(kc, sl[k & 1][tid]);
       element_force(v, ks, f);
       if (k >= xb) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) g[q][c][tid] = ft[c][q] + f[c][2 * q];
+          for (int q = 0; q < 4; ++q) gk[q][c][tid] = ft[c][q] + f[c][2 * q];
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) ft[c][q] = f[c][2 * q + 1];
+      if (snext) sl[(k + 1) & 1][tid] = pres;  // layer k + 1's scales; sl[(k+1)&1] was last read by layer k - 1
     }
     if (partial && outp && k >= xb) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) xo[c] = lo[c][own];
     }
-    __syncthreads();  // g complete; every read of pl[k & 1] and sl is done
+    __syncthreads();  // gk complete; every read of plane k is done
     if (k >= xb && outp) {
       const int yy = y0 + ty, zz = z0 + tz;
       if (yy < n1 && zz < n2) {
@@ -141,7 +147,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
         const long idx = (long)k * P + (long)yy * n2 + zz;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const T o = (g[0][c][e00] + g[1][c][e00 - EZ]) + (g[2][c][e00 - 1] + g[3][c][e00 - EZ - 1]);
+          const T o = (gk[0][c][e00] + gk[1][c][e00 - EZ]) + (gk[2][c][e00 - 1] + gk[3][c][e00 - EZ - 1]);
           yv[c * N + idx] = o;
           if (partial) {
             acc[c] += (double)o;
@@ -150,13 +156,11 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
         }
       }
     }
-    if (more) {
+    if (pnext) {
 #pragma unroll
       for (int i = 0; i < PF; ++i)
-        if (poff[i] >= 0) pl[k & 1][0][tid + i * NT] = pre[i];  // plane k + 2 replaces plane k
-      if (ev) sl[tid] = pres;
+        if (poff[i] >= 0) pl[slot(k + 3)][0][tid + i * NT] = pre[i];  // plane k + 3 replaces plane k
     }
-    __syncthreads();  // next layer's planes and scales are in place; g is free again
   }
   if (partial) {
     block_sum<4>(acc, red);
