@@ -44,7 +44,7 @@ def test_apply_load_precond_symbol(L, shape):
 
 
 def _scaled_oracle(oh, s, r):
-    sn = sum(np.roll(s, shift=tuple(off), axis=(0, 1, 2)) for off in OL.NODES) / 8.0
+    sn = np.sqrt(sum(np.roll(s, shift=tuple(off), axis=(0, 1, 2)) ** 2 for off in OL.NODES) / 8.0)
     w = (1.0 / np.sqrt(sn))[..., None]
     return w * oh.precond(w * r)
 
