@@ -387,6 +387,45 @@ def mech_arm(args, stream):
             "converged_all": all(r["converged"] for r in rows), "rows": rows, "kernels": kernels}
 
 
+def _gen3(i, n_o):
+    """Uneven-batch generator: the benchmark generator with beta drawn from {4, 8, 16} by default_rng(20000 + i)."""
+    from nlfiber_b200 import density as D
+    beta = float(np.random.default_rng(20_000 + i).choice([4.0, 8.0, 16.0]))
+    return D.random_cell(i, n_o=n_o, r=1.5, beta=beta, kmax=2)[0]
+
+
+def uneven_arm(args, stream):
+    """Uneven batch: cells of several grid sizes (default 128 at 32^3, 64 at 64^3, 16 at 128^3), one handle and
+    one slot-refilled batched solve per size, the sizes running concurrently on their own streams. Reports the
+    per-size iterations and C error against C* (same solver to residual 1e-14) and the whole batch's cells/s."""
+    import torch
+    from nlfiber_b200 import linear as L
+    sizes = [int(v) for v in args.uneven.split(",")]
+    cells = []
+    for n, cnt in zip(sizes[0::2], sizes[1::2]):
+        with mp.get_context("spawn").Pool(8) as pool:
+            arr = pool.starmap(_gen3, [(i, n // 2) for i in range(cnt)])
+        cells += [torch.from_numpy(a).cuda() for a in arr]
+    handles = {}
+    ref = L.C_full_uneven(cells, concurrent=True, **MATERIAL, **CSTAR)
+    L.C_full_uneven(cells[:1], handles=handles, **MATERIAL, **FAST)  # warm-up of one handle
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = L.C_full_uneven(cells, handles=handles, concurrent=True, **MATERIAL, **FAST)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    err = rel_err(res["C"], ref["C"])
+    per = {}
+    for shape, idx in res["groups"].items():
+        per[f"{shape[0]}^3"] = {"cells": len(idx), "it_mean": float(np.mean(res["it"][idx])),
+                                "it_max": int(np.max(res["it"][idx])), "c_err_max": float(err[idx].max())}
+    return {"mode": "uneven", "workload": "seeded synthetic cells, beta in {4, 8, 16}: " +
+            ", ".join(f"{v['cells']} at {k}" for k, v in per.items()), "cells": len(cells),
+            "seconds": round(dt, 3), "cells_per_s": round(len(cells) / dt, 3), "status": int(res["status"]),
+            "c_err_max": float(err.max()), "per_size": per,
+            "timing": "host wall clock around the concurrent per-size solves (device-resident rho, C to host)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,6 +452,8 @@ def main():
                     help="finite-strain compression path (Newton-CG on the GPU) instead of the default measurement")
     ap.add_argument("--mech-cells", type=int, default=2)
     ap.add_argument("--mech-steps", type=int, default=3)
+    ap.add_argument("--uneven", default=None,
+                    help="uneven batch 'n1,count1,n2,count2,...' (e.g. 32,128,64,64,128,16) instead of the default")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
                     help="CG preconditioner of the Newton steps: the reference's (fft) or the node-scaled one")
     args = ap.parse_args()
@@ -421,6 +462,13 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.uneven:
+        import torch
+        torch.cuda.set_device(local)
+        res = uneven_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
     if args.mech:
         import torch
         torch.cuda.set_device(local)

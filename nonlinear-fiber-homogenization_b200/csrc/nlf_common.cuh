@@ -19,6 +19,15 @@ namespace nlf {
 
 void set_error(const char* fmt, ...);
 
+// Raises the dynamic shared memory limit of a kernel to at least `bytes` and never lowers it: handles of
+// different grid sizes may launch the same kernel from several host threads at once, and a lowered limit would
+// fail another thread's launch. Thread-safe.
+cudaError_t raise_dyn_smem(const void* func, int bytes);
+template <typename F>
+cudaError_t raise_dyn_smem(F* func, int bytes) {
+  return raise_dyn_smem(reinterpret_cast<const void*>(func), bytes);
+}
+
 #define NLF_CUDA_TRY(expr)                                                                     \
   do {                                                                                         \
     cudaError_t _e = (expr);                                                                   \

@@ -1054,8 +1054,8 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   using F = Fast<N>;
   const cplx<double>* tw = h.t64.tw;
   const size_t plane = F::smem_plane();
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fa_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fc_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N>, (int)plane));
   if (nchunk) *nchunk = F::KZC;
   unsigned long long* units = prof_units();
   const cplx<double>* twx = tw + h.tw.off0;
@@ -1159,9 +1159,9 @@ static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx
   const size_t smemb = (size_t)3 * d.n0 * kc * sizeof(cplx<T>) * mult;
   if (nchunk) *nchunk = (d.n2h + kc - 1) / kc;
   const cplx<T>* tw = twiddles<T>(h);
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_a<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_fft_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemb));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fft_a<T>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fft_c<T>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fft_b<T>, (int)smemb));
   const int nt = 256;
   const bool f32 = sizeof(T) == 4;
   unsigned long long* units = prof_units();

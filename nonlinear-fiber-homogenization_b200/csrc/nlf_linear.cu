@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 #include "nlf_vec.cuh"
 #include "nlf_prof.cuh"
@@ -18,6 +20,17 @@ void set_error(const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+}
+
+cudaError_t raise_dyn_smem(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cur;
+  std::lock_guard<std::mutex> lock(mu);
+  int& c = cur[func];
+  if (bytes <= c) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) c = bytes;
+  return e;
 }
 
 int DevBuf::reserve(size_t n) {

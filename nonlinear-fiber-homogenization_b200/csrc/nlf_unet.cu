@@ -502,7 +502,7 @@ template <int NPAD>
 int conv_npad(const ConvArgs& a, cudaStream_t st) {
   const long total = (long)a.nb * a.n0 * a.n1 * a.n2;
   const size_t smem = 1024 + kStages * (kStageA + NPAD * 128);
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_conv_tc<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  NLF_CUDA_TRY(raise_dyn_smem(k_conv_tc<NPAD>, (int)smem));
   k_conv_tc<NPAD><<<(unsigned)((total + 127) / 128), 128, smem, st>>>(a);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
@@ -510,7 +510,7 @@ int conv_npad(const ConvArgs& a, cudaStream_t st) {
 template <int NPAD>
 int dw_npad(const DwArgs& a, int mtiles, int nchunk, cudaStream_t st) {
   const size_t smem = 1024 + kStages * (kStageA + NPAD * 128);
-  NLF_CUDA_TRY(cudaFuncSetAttribute(k_dw_tc<NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  NLF_CUDA_TRY(raise_dyn_smem(k_dw_tc<NPAD>, (int)smem));
   k_dw_tc<NPAD><<<dim3(mtiles, nchunk), 128, smem, st>>>(a);
   NLF_CHECK_LAUNCH();
   return NLF_OK;

@@ -312,6 +312,51 @@ class LinearHomogenization:
         return self.invariants_from(s, u2), u2, it
 
 
+def C_full_uneven(cells, handles=None, concurrent=False, **kw):
+    """C (6x6), iterations and status of cells of different grid sizes: one handle (and one batched, slot-refilled
+    solve) per grid shape, results in the input order. `cells` is a sequence of rho arrays (NumPy or CUDA float64
+    torch tensors); `kw` are LinearHomogenization keywords (E, nu, emin, p, tol, maxit, precond, slots, ...).
+    With concurrent=True (CUDA torch available) the shapes run at once on their own streams from host threads (the
+    library is reentrant per handle). `handles` (dict shape -> LinearHomogenization) reuses handles across calls.
+    Returns dict(C=(ncell, 6, 6), it=(ncell,), status=worst status, groups={shape: indices})."""
+    groups = {}
+    for i, r in enumerate(cells):
+        groups.setdefault(tuple(int(n) for n in r.shape), []).append(i)
+    handles = {} if handles is None else handles
+    C = np.empty((len(cells), 6, 6))
+    it = np.zeros(len(cells), dtype=np.int32)
+    status = [0]
+
+    def run(shape, idx):
+        lh = handles.get(shape)
+        if lh is None:
+            lh = handles[shape] = LinearHomogenization(shape, **kw)
+        if concurrent:
+            import torch
+            st = torch.cuda.Stream()
+            lh.stream = st.cuda_stream
+        rho = cells[idx[0]]
+        if hasattr(rho, "data_ptr") and not isinstance(rho, np.ndarray):
+            import torch
+            batch = torch.stack([cells[i] for i in idx])
+        else:
+            batch = np.stack([np.asarray(cells[i], dtype=np.float64) for i in idx])
+        r = lh.C_full_batched(batch)
+        C[idx] = r["C"]
+        it[idx] = r["it"]
+        status[0] = max(status[0], r["status"])
+
+    if concurrent and len(groups) > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(len(groups)) as ex:
+            for f in [ex.submit(run, sh, ix) for sh, ix in groups.items()]:
+                f.result()
+    else:
+        for sh, ix in groups.items():
+            run(sh, ix)
+    return dict(C=C, it=it, status=status[0], groups=groups)
+
+
 # nlfiber/linear.py:267-291
 def cubic_invariants(C):
     C = np.asarray(C)

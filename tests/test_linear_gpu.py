@@ -195,6 +195,22 @@ def test_energy_guard_and_warm_start_plumbing(L):
     assert np.all(half["it"] <= 4), half["it"]
 
 
+def test_uneven_batch_equals_per_size_batches(L):
+    """Cells of two grid sizes in one call (one handle per size, run concurrently on their own streams) give the
+    per-size batches' C and iterations bit for bit, in the input order."""
+    import torch
+    a = [OD.random_cell(i, n_o=4, beta=8.0)[0] for i in range(3)]
+    b = [OD.random_cell(10 + i, n_o=8, beta=8.0)[0] for i in range(2)]
+    cells = [torch.tensor(c, device="cuda") for c in (a[0], b[0], a[1], b[1], a[2])]
+    kw = dict(precond="scaled", tol=1e-9, maxit=2000, check_every=4)
+    r = L.C_full_uneven(cells, concurrent=True, **kw)
+    ra = L.LinearHomogenization(a[0].shape, **kw).C_full_batched(np.stack(a))
+    rb = L.LinearHomogenization(b[0].shape, **kw).C_full_batched(np.stack(b))
+    assert r["status"] == 0
+    assert np.array_equal(r["C"][[0, 2, 4]], ra["C"]) and np.array_equal(r["C"][[1, 3]], rb["C"])
+    assert np.array_equal(r["it"][[0, 2, 4]], ra["it"]) and np.array_equal(r["it"][[1, 3]], rb["it"])
+
+
 def test_high_contrast_variants_reach_the_fp64_C(L):
     """emin = 1e-9 Schwarz-P 16^3: the scaled preconditioner (FP64 and FP32-in-FP64 refinement) and the
     reference preconditioner (long run) reach the same C; every entry within 1e-8 of max |C|."""
