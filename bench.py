@@ -175,6 +175,13 @@ def cpu_reference(cells, sample_iters=2):
     return 1.0 / cell_s, sample, t4 - t0
 
 
+def workload_config(n, cells, world):
+    """The `config` of both arms' JSON lines: the workload, not the solver."""
+    return {"workload": f"{cells} seeded synthetic {n}^3 cells per GPU x 6 unit strains, C_full, emin 1e-9",
+            "grid": n, "cells_per_gpu": cells, "cases": 6,
+            "l2": "working set > L2 (126 MB) every step; no flush needed", "parallelism": f"dp{world}"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -190,8 +197,10 @@ def run_reference(args, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"seeded synthetic {args.n}^3 cells x 6 unit strains, C_full, emin 1e-9",
-                       "grid": args.n, "cases": 6},
+            "config": dict(workload_config(args.n, args.cells, args.gpus),
+                           solver="the reference algorithm: FP64 PCG with the unit-stiffness FFT preconditioner "
+                                  "(the oracle port on the host cores; each step one cell sampled, scaled to the "
+                                  "calibrated iteration count)"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -607,11 +616,10 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{B} seeded synthetic {n}^3 cells per GPU x 6 unit strains, C_full, emin 1e-9",
-                   "grid": n, "cells_per_gpu": B, "cases": 6, "solver": "FP64 PCG, node-scaled FFT "
-                   f"preconditioner, {FAST['slots']} cells in flight, a converged cell's slot refilled from the "
-                   "queue", "tol": FAST["tol"],
-                   "l2": "working set > L2 (126 MB) every step; no flush needed", "parallelism": f"dp{world}"},
+        "config": dict(workload_config(n, B, world),
+                       solver="FP64 PCG, node-scaled FFT preconditioner, "
+                              f"{FAST['slots']} cells in flight, a converged cell's slot refilled from the queue, "
+                              f"stop at residual {FAST['tol']} and energy guard {FAST['energy_tol']}"),
         "c_err_max": float(err.max()), "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
         "roofline": roof, "kernels": kernels, "gpu_launches": launches, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "plain_fp64_gpu": plain,
