@@ -1047,6 +1047,156 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, L2 only)
+__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Pass C, persistent and pipelined (cubes of 64): each CTA walks the planes (vec, comp, x) blockIdx.x,
+// blockIdx.x + gridDim.x, ... of active cells; while it transforms one plane, the spectrum rows of its next
+// plane stream into the other of two shared staging buffers by cp.async. Same arithmetic as k_fc_fast.
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_fc_pipe(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
+              double* __restrict__ z, int m, int nvec, const cplx<double>* __restrict__ tw_y,
+              const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2,
+              const CellState* __restrict__ cs, double* __restrict__ partial, unsigned long long* __restrict__ units,
+              int ukind, PcgFuse fu) {
+  using F = Fast<N>;
+  constexpr int M = F::M, H = F::H, Lz = F::Lz, Ly = F::Ly;
+  static_assert(F::P == 1, "one plane per step");
+  constexpr long NN = (long)N * N * N;
+  extern __shared__ unsigned char smem_raw[];
+  cplx<double>* stage = reinterpret_cast<cplx<double>*>(smem_raw);  // [2][N ky][H kz]
+  cplx<double>* T = stage + 2 * N * H;                               // [N y][H kz] (swizzled kz)
+  __shared__ double red[8 * 4];
+  const int t = threadIdx.x;
+  const long nplanes = (long)nvec * 3 * N;
+  auto active = [&](long j) { return !cs || cs[(int)(j / (3 * N)) / m].active; };
+  auto next_active = [&](long j) {
+    while (j < nplanes && !active(j)) j += gridDim.x;
+    return j;
+  };
+  auto issue = [&](long j, int b) {
+    const int vec = (int)(j / (3 * N)), c = (int)((j / N) % 3), x = (int)(j % N);
+    const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H) + (long)x * H;
+    cplx<double>* dst = stage + b * N * H;
+    for (int i = t; i < N * H; i += 256) {
+      const int ky = i / H, kz = i - ky * H;
+      cp16_async(dst + i, sp + (long)ky * N * H + kz);
+    }
+  };
+  long j = next_active(blockIdx.x);
+  if (j < nplanes) issue(j, 0);
+  cp_async_commit();
+  for (int it = 0; j < nplanes; ++it) {
+    const long jn = next_active(j + gridDim.x);
+    if (jn < nplanes) issue(jn, (it + 1) & 1);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();  // plane j staged
+    const int vec = (int)(j / (3 * N)), c = (int)((j / N) % 3), x = (int)(j % N);
+    if (units && c == 0 && x == 0 && t == 0) atomicAdd(units + ukind, 1ull);
+    const cplx<double>* S = stage + (it & 1) * N * H;
+    {
+      constexpr int G = 256 / Ly, IT = (H + G - 1) / G;
+      const int g = t / Ly, ly = t - g * Ly;
+      LaneTw<Ly, 8> Ty;
+      Ty.load(tw_y, ly);
+#pragma unroll 1
+      for (int q2 = 0; q2 < IT; ++q2) {
+        const int kz = g + q2 * G;
+        const bool ok = kz < H;
+        if (!__any_sync(0xffffffffu, ok)) break;
+        cplx<double> b[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) b[q] = ok ? S[(ly + Ly * q) * H + kz] : cplx<double>{0.0, 0.0};
+        fft_nat_in<Ly, 8, true>(b, ly, Ty);
+        if (ok) {
+          const int yb = 8 * brevL<Ly>(ly);
+#pragma unroll
+          for (int k1 = 0; k1 < 8; ++k1) T[(k1 + yb) * H + swz<M>(kz)] = b[k1];
+        }
+      }
+    }
+    __syncthreads();  // T complete; S free
+    const int y = t / Lz, l = t - y * Lz;
+    const cplx<double>* row = T + y * H;
+    cplx<double> a[8];
+    const int k2 = brevL<Lz>(l);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) {
+      const int k = k1 + 8 * k2;
+      if (k == 0) {
+        const double A = row[swz<M>(0)].x, B = row[swz<M>(M)].x;
+        a[k1] = {(A + B) * 0.5, (A - B) * 0.5};
+      } else {
+        const cplx<double> A = row[swz<M>(k)], B = row[swz<M>(M - k)];
+        const cplx<double> E{(A.x + B.x) * 0.5, (A.y - B.y) * 0.5};
+        const cplx<double> D{(A.x - B.x) * 0.5, (A.y + B.y) * 0.5};
+        const cplx<double> O = cmul(D, cconj(tw_n2[k]));
+        a[k1] = {E.x - O.y, E.y + O.x};
+      }
+    }
+    {
+      LaneTw<Lz, 8> Tz;
+      Tz.load(tw_z, l);
+      fft_tr_in<Lz, 8, true>(a, l, Tz);
+    }
+    constexpr double norm = 2.0 / (double)NN;
+    const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;
+    const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
+    double2* zp2 = reinterpret_cast<double2*>(z + roff);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double2 ww[8];
+    if (wp2)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) ww[q] = wp2[l + Lz * q];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      double2 v{a[q].x * norm, a[q].y * norm};
+      if (wp2) {
+        v.x *= ww[q].x;
+        v.y *= ww[q].y;
+      }
+      zp2[l + Lz * q] = v;
+      acc[0] += v.x + v.y;
+      if (partial) {
+        const double2 rv = reinterpret_cast<const double2*>(r + roff)[l + Lz * q];
+        acc[1] += rv.x * v.x + rv.y * v.y;
+        acc[2] += rv.x + rv.y;
+        acc[3] += rv.x * rv.x + rv.y * rv.y;
+      }
+    }
+    if (partial || fu.partC) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+      if ((t & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) red[(t >> 5) * 4 + k] = acc[k];
+    }
+    __syncthreads();  // T reads done (next plane rewrites it); warp sums in red
+    if ((partial || fu.partC) && t == 0) {
+      double s4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s4[k] += red[q * 4 + k];
+      const long pl = ((long)vec * 3 + c) * N + x;
+      if (partial)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) partial[pl * 4 + k] = s4[k];
+      if (fu.partC) fu.partC[pl] = s4[0];
+    }
+    j = jn;
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 template <int N>
 static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double* z, cplx<double>* spec,
                        const double* w, const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk,
@@ -1075,8 +1225,16 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   }
   {
     ProfScope ps(PK_FFTC64, st);
-    k_fc_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial, units,
-                                                             PK_FFTC64, fu);
+    if constexpr (N == 64) {
+      const size_t pipe = (size_t)3 * N * F::H * sizeof(cplx<double>);  // two staging planes and the transpose
+      NLF_CUDA_TRY(raise_dyn_smem(k_fc_pipe<N>, (int)pipe));
+      const long planes = (long)nvec * 3 * N;
+      const int grid = (int)std::min<long>(planes, 2L * h.nsm);
+      k_fc_pipe<N><<<grid, 256, pipe, st>>>(spec, w, r, z, m, nvec, twy, twz, twn2, cs, partial, units, PK_FFTC64, fu);
+    } else {
+      k_fc_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial,
+                                                               units, PK_FFTC64, fu);
+    }
     NLF_CHECK_LAUNCH();
   }
   return NLF_OK;
