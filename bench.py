@@ -487,7 +487,8 @@ def main():
         return
 
     n_o = args.n // 2
-    seeds = list(range(rank * args.cells, (rank + 1) * args.cells))
+    from nlfiber_b200 import shard
+    seeds = shard.cell_seeds(rank, args.cells)
     t_gen = time.perf_counter()
     cells = gen_cells(seeds, n_o)
     t_gen = time.perf_counter() - t_gen
@@ -564,13 +565,11 @@ def main():
     torch.cuda.synchronize()
     prof = _lib.profile_report()
     _lib.profile(False)
+    ms = shard.max_over_ranks(ms, dist, device="cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     err = rel_err(C_d.cpu().numpy(), Cstar)
-    value = world * B * args.steps / (ms / 1e3)
+    value = shard.whole_job_rate(B * args.steps, world, ms / 1e3)
 
     # end to end through the same API with pinned host buffers (H2D of rho and D2H of C inside the region)
     rho_h = torch.from_numpy(cells).pin_memory()
@@ -585,11 +584,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * B * e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * N * 8,
+    e2e_ms = shard.max_over_ranks(e2e_ms, dist, device="cuda")
+    e2e = {"value": shard.whole_job_rate(B * e2e_steps, world, e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * N * 8,
            "d2h_bytes_per_step": B * 36 * 8, "c_err_max": float(rel_err(C_h.numpy(), Cstar).max())}
 
     peaks, peak_kind = measured_peaks()
