@@ -336,7 +336,8 @@ def mech_arm(args, stream):
     """Finite-strain compression (the reference's qoi.run_path "compression" driver, nlfiber/qoi.py:49-115):
     compressible neo-Hookean cells (E 1, nu 0.3, void rho^3 with floor 1e-6, WLS (500, 0.01)), Fbar_xx = 1 - e
     with the lateral stresses free (Mixed control of Fbar_yy, Fbar_zz), steps of 0.01 each warm-started from the
-    previous state, FP64 Newton-CG with EW forcing on the GPU. Cells of the same generator with seeds 0..."""
+    previous state, FP64 Newton-CG with EW forcing on the GPU (state and Newton vectors device-resident). Cells of
+    the same generator with seeds 0..."""
     import torch
     from nlfiber_b200 import _lib
     from nlfiber_b200 import mech as MH
@@ -348,7 +349,7 @@ def mech_arm(args, stream):
     e0.record()
     for i in range(len(cells)):
         cell = MH.Cell(cells[i], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
-        mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond)
+        mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
         z = None
         for k in range(1, args.mech_steps + 1):
             e = -0.01 * k
@@ -371,7 +372,7 @@ def mech_arm(args, stream):
     ms = e0.elapsed_time(e1)
     # kernel classes from one more first step of cell 0 with per-launch events on (and no graph replay)
     cell = MH.Cell(cells[0], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
-    mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond)
+    mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
     Fb = np.eye(3)
     Fb[0, 0] = 0.99
     _lib.profile(True)

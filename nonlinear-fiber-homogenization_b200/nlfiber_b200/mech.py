@@ -38,6 +38,32 @@ def to_voigt(M):
     return np.array([S[0, 0], S[1, 1], S[2, 2], 2 * S[1, 2], 2 * S[0, 2], 2 * S[0, 1]])
 
 
+def _is_dev(a):
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def _empty_like_kind(ref, shape):
+    """An output buffer on the device of `ref` (a CUDA torch tensor) or on the host."""
+    if _is_dev(ref):
+        import torch
+        return torch.empty(shape, dtype=torch.float64, device=ref.device)
+    return np.empty(shape)
+
+
+def _norm(v):
+    if _is_dev(v):
+        import torch
+        return float(torch.linalg.vector_norm(v))
+    return float(np.linalg.norm(v))
+
+
+def _dot(a, b):
+    if _is_dev(a):
+        import torch
+        return float(torch.dot(a, b))
+    return float(a @ b)
+
+
 def _linesearch(E, gnorm, x, dx, E0, slope, gn):
     """mech.py:73-85: halve from t = 1 until Armijo (1e-4) holds, or the energy is flat to rounding and the
     gradient norm drops; None below t = 1e-6."""
@@ -118,9 +144,10 @@ class Cell:
         return W.value
 
     def grad(self, w, Fbar):
-        """(dW/dw (nx, ny, nz, 3), dW/dFbar (3, 3)): the reference's jax.grad of `energy` (mech.py:168-169)."""
+        """(dW/dw (nx, ny, nz, 3), dW/dFbar (3, 3)): the reference's jax.grad of `energy` (mech.py:168-169).
+        dW/dw is a CUDA tensor when w is one."""
         W = ctypes.c_double()
-        gw = np.empty(self.shape + (3,))
+        gw = _empty_like_kind(w, self.shape + (3,))
         P = np.empty((3, 3))
         check(lib.nlf_mech_energy(self._h, ptr(as_f64(w)), ptr(as_f64(Fbar)), ctypes.byref(W), ptr(gw), ptr(P),
                                   self.stream))
@@ -132,7 +159,7 @@ class Cell:
 
     def hvp(self, w, Fbar, v, dFbar):
         """Second derivative of W at (w, Fbar) applied to (v, dFbar): (dw part, dFbar part)."""
-        hv = np.empty(self.shape + (3,))
+        hv = _empty_like_kind(v, self.shape + (3,))
         hP = np.empty((3, 3))
         check(lib.nlf_mech_hvp(self._h, ptr(as_f64(w)), ptr(as_f64(Fbar)), ptr(as_f64(v)), ptr(as_f64(dFbar)),
                                ptr(hv), ptr(hP), self.stream))
@@ -140,7 +167,7 @@ class Cell:
 
     def precond_w(self, r):
         """mech.py:187-189."""
-        z = np.empty(self.shape + (3,))
+        z = _empty_like_kind(r, self.shape + (3,))
         check(lib.nlf_mech_precond_w(self._h, ptr(as_f64(r)), ptr(z), self.stream))
         return z
 
@@ -156,10 +183,13 @@ class Mixed:
     """mech.py:195-346: Fbar components in `free` are unknowns with zero conjugate stress, the rest prescribed.
     Unknown z = (w, Fbar_free); minimizes W(z) by Newton-CG."""
 
-    def __init__(self, cell, free=((1, 1), (2, 2)), forcing="ew", precond="fft"):
+    def __init__(self, cell, free=((1, 1), (2, 2)), forcing="ew", precond="fft", device=None):
         """precond "fft" is the reference's preconditioner (homogeneous inverse / sws); "scaled" wraps the same
         inverse in the node stiffness scaling (same solution, fewer CG iterations at high contrast). The choice
-        is kept by the cell's device handle."""
+        is kept by the cell's device handle. device="cuda" keeps the Newton state z and every Newton vector in
+        CUDA tensors that the library reads and writes in place (only scalars and the macro values go to the
+        host); None keeps them in NumPy, as the reference's host loop does."""
+        self.device = device
         self.c = cell
         self.free = [tuple(f) for f in free]
         self.forcing = forcing
@@ -176,21 +206,40 @@ class Mixed:
 
     def unpack(self, z, Fb):
         """mech.py:209-211."""
-        z = np.asarray(z)
+        if not _is_dev(z):
+            z = np.asarray(z)
         w = z[: self.nw].reshape(self.shape + (3,))
         F = np.array(Fb, dtype=np.float64)
         if self.k:
-            F[self.idx] = z[self.nw:]
+            F[self.idx] = z[self.nw:].cpu().numpy() if _is_dev(z) else z[self.nw:]
         return w, F
+
+    def _as_state(self, v):
+        """v in the state's kind: a CUDA float64 tensor with device="cuda", else a NumPy array."""
+        if self.device is None:
+            return v.cpu().numpy() if _is_dev(v) else np.asarray(v, dtype=np.float64)
+        import torch
+        return torch.as_tensor(v, dtype=torch.float64, device=self.device)
+
+    def _cat(self, w, tail):
+        """(w part, macro tail) -> one vector of the state's kind."""
+        if _is_dev(w):
+            import torch
+            return torch.cat([w.reshape(-1), torch.as_tensor(np.asarray(tail, dtype=np.float64), device=w.device)])
+        return np.concatenate([np.asarray(w).ravel(), np.asarray(tail, dtype=np.float64)])
 
     def z0(self, Fb):
         """mech.py:243-245."""
         Fb = np.asarray(Fb, dtype=np.float64)
-        return np.concatenate([np.zeros(self.nw), Fb[self.idx] if self.k else np.zeros(0)])
+        return self._as_state(np.concatenate([np.zeros(self.nw), Fb[self.idx] if self.k else np.zeros(0)]))
 
     def proj(self, v):
         """mech.py:247-250."""
         w = v[: self.nw].reshape(self.shape + (3,))
+        if _is_dev(v):
+            import torch
+            w = w - w.mean(dim=(0, 1, 2))
+            return torch.cat([w.reshape(-1), v[self.nw:]])
         w = w - w.mean(axis=(0, 1, 2))
         return np.concatenate([w.ravel(), v[self.nw:]])
 
@@ -204,33 +253,40 @@ class Mixed:
     def _g(self, z, Fb):
         """Gradient of Ez in z (mech.py:221)."""
         gw, P = self.c.grad(*self.unpack(z, Fb))
-        return np.concatenate([gw.ravel(), P[self.idx] if self.k else np.zeros(0)])
+        return self._cat(gw, P[self.idx] if self.k else np.zeros(0))
 
     def tangent(self, z, Fb):
         return Tangent(*self.unpack(z, Fb))
 
     def hvp_A(self, A, v):
         """mech.py:233-236 with the tangent applied matrix-free at A's linearization point."""
-        v = np.asarray(v, dtype=np.float64)
+        v = self._as_state(v)
         dF = np.zeros((3, 3))
         if self.k:
-            dF[self.idx] = v[self.nw:]
-        hv, hP = self.c.hvp(A.w, A.F, np.ascontiguousarray(v[: self.nw]).reshape(self.shape + (3,)), dF)
-        return np.concatenate([hv.ravel(), hP[self.idx] if self.k else np.zeros(0)])
+            dF[self.idx] = v[self.nw:].cpu().numpy() if _is_dev(v) else v[self.nw:]
+        vw = v[: self.nw].reshape(self.shape + (3,))
+        hv, hP = self.c.hvp(A.w, A.F, vw.contiguous() if _is_dev(vw) else np.ascontiguousarray(vw), dF)
+        return self._cat(hv, hP[self.idx] if self.k else np.zeros(0))
 
     def macro_diag(self, A, Fb=None):
         """mech.py:252-258."""
         d = []
         for j in range(self.k):
-            e = np.zeros(self.nw + self.k)
+            if self.device is None:
+                e = np.zeros(self.nw + self.k)
+            else:
+                import torch
+                e = torch.zeros(self.nw + self.k, dtype=torch.float64, device=self.device)
             e[self.nw + j] = 1.0
-            d.append(self.hvp_A(A, e)[self.nw + j])
+            d.append(float(self.hvp_A(A, e)[self.nw + j]))
         return np.abs(np.array(d)) + 1e-12
 
     def precond(self, r, dmac, swscale):
         """mech.py:260-262."""
-        w = self.c.precond_w(np.ascontiguousarray(r[: self.nw]).reshape(self.shape + (3,))) / swscale
-        return np.concatenate([w.ravel(), r[self.nw:] / dmac])
+        rw = r[: self.nw].reshape(self.shape + (3,))
+        w = self.c.precond_w(rw.contiguous() if _is_dev(rw) else np.ascontiguousarray(rw)) / swscale
+        tail = (r[self.nw:].cpu().numpy() if _is_dev(r) else r[self.nw:]) / dmac
+        return self._cat(w, tail)
 
     def _sws(self):
         """mech.py:292-294 (1 for the scaled preconditioner, which carries the stiffness itself)."""
@@ -238,7 +294,7 @@ class Mixed:
 
     def _cgA(self, A, b, dmac, sws, tol, maxit):
         """mech.py:264-290 on the device: (x, iterations, converged, negative curvature)."""
-        x = np.empty(self.nw + self.k)
+        x = _empty_like_kind(b, self.nw + self.k)
         it, conv, neg = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         dm = np.ascontiguousarray(np.asarray(dmac, dtype=np.float64) if self.k else np.ones(1))
         check(lib.nlf_mech_cg(self.c._h, ptr(as_f64(A.w)), ptr(as_f64(A.F)), self.k, ptr(self._free_idx),
@@ -255,13 +311,13 @@ class Mixed:
     def solve(self, Fbar, z0=None, rtol=1e-9, maxnewton=30, cg_tol=1e-6, cg_maxit=20000, g_ref=None):
         """mech.py:302-346: Newton-CG. Returns (w, Fbar_full, log) with log['z'] the state."""
         Fb = np.asarray(Fbar, dtype=np.float64)
-        z = self.z0(Fb) if z0 is None else np.asarray(z0, dtype=np.float64)
+        z = self.z0(Fb) if z0 is None else self._as_state(z0)
         g0, log = g_ref, dict(newton=0, cg=0, converged=False, gnorm=[], negative_curvature=False)
         eta, gprev = None, None
         sws = self._sws()
         for k in range(maxnewton):
             g = self.proj(self._g(z, Fb))
-            gn = float(np.linalg.norm(g))
+            gn = _norm(g)
             g0 = gn if g0 is None else g0
             log["gnorm"].append(gn)
             if gn <= rtol * max(g0, 1e-300) or gn < 1e-14:
@@ -280,11 +336,11 @@ class Mixed:
             dz, its, ok, neg = self._cgA(A, -g, dmac, sws, tol, int(cg_maxit))
             log["cg"] += int(its)
             log["negative_curvature"] |= bool(neg)
-            E0, slope = float(self._E(z, Fb)), float(g @ dz)
+            E0, slope = float(self._E(z, Fb)), _dot(g, dz)
             if slope >= 0:
                 dz = -self.proj(self.precond(g, dmac, sws))
-                slope = float(g @ dz)
-            t = _linesearch(lambda x: self._E(x, Fb), lambda x: float(np.linalg.norm(self.proj(self._g(x, Fb)))),
+                slope = _dot(g, dz)
+            t = _linesearch(lambda x: self._E(x, Fb), lambda x: _norm(self.proj(self._g(x, Fb))),
                             z, dz, E0, slope, gn)
             log["newton"] = k + 1
             if t is None:

@@ -95,6 +95,25 @@ def test_scaled_mech_preconditioner_same_solution_fewer_cg(M):
     assert res["scaled"][2] < res["fft"][2], (res["scaled"][2], res["fft"][2])
 
 
+def test_device_resident_newton_matches_host_loop(M):
+    """Mixed(device="cuda") keeps z and the Newton vectors on the GPU: the same converged state as the host loop,
+    to the rounding of the mean removals (done by the device instead of NumPy) within the Newton tolerance."""
+    rho = OD.random_cell(5, n_o=8, beta=8.0)[0]
+    Fb = np.diag([0.98, 1.0, 1.0])
+    out = {}
+    for dev in (None, "cuda"):
+        c = M.Cell(rho, emin=1e-3)
+        w, F, log = M.Mixed(c, [(1, 1), (2, 2)], precond="scaled", device=dev).solve(Fb, rtol=1e-10, cg_tol=1e-8)
+        assert log["converged"]
+        w = w.cpu().numpy() if hasattr(w, "cpu") else w
+        out[dev] = (w, F, log["newton"], c.mean_stress(w, F))
+    # the stop at rtol 1e-10 sits near the rounding floor, so the two may stop one Newton step apart
+    assert abs(out[None][2] - out["cuda"][2]) <= 1
+    np.testing.assert_allclose(out["cuda"][1], out[None][1], atol=1e-10)
+    assert rel(out["cuda"][3], out[None][3]) < 1e-6
+    assert rel(out["cuda"][0], out[None][0]) < 1e-4
+
+
 def test_small_strain_limit_is_linear_C(M):
     from nlfiber_b200 import linear as L
     rho = OD.grey_cell(3, beta=3.0)
