@@ -113,13 +113,6 @@ int launch_precond_pcg(const LinearHandle& h, int nvec, int m, T* r, const T* Ap
                        int* nchunk, cudaStream_t st);
 int build_tables(LinearHandle& h);
 
-// vector kernels
-template <typename T>
-int launch_sum3(const LinearHandle& h, int nvec, const T* x, double* partial /*[nvec][3][nb]*/, int* nb,
-                cudaStream_t st);
-int launch_scale_fields(const LinearHandle& h, int ncell, const double* rho, double* s64, float* s32,
-                        double* w64, float* w32, int want_rho_is_s, cudaStream_t st);
-
 // stiffness scale only (s = emin + (1 - emin) clip01(rho)^p)
 int launch_stiffness_scale(const LinearHandle& h, long count, const double* rho, double* s, cudaStream_t st);
 

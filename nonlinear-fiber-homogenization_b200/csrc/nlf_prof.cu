@@ -35,7 +35,7 @@ void recycle() {
 }
 
 const char* kNames[PK_COUNT] = {"apply_f32", "apply_f64", "fft_a_f32", "fft_b_f32", "fft_c_f32",
-                                "fft_a_f64", "fft_b_f64", "fft_c_f64", "xr_update", "p_update",
+                                "fft_a_f64", "fft_b_f64", "fft_c_f64", "p_update",
                                 "stats",     "finalize",  "bilinear",  "load",      "other",
                                 "unet_conv", "unet_wgrad", "unet_misc", "mech_elem", "mech_gather"};
 }  // namespace

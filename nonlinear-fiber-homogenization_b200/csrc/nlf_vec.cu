@@ -238,19 +238,6 @@ __global__ void k_fin_apply(const double* __restrict__ partial, int nblk, long N
   }
 }
 
-// x += alpha p; r -= alpha (Ap - mean)
-template <typename T>
-__global__ void k_xr(long N, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ Ap,
-                     const VecState* __restrict__ vs, const CellState* __restrict__ cs, int m) {
-  const int vec = blockIdx.z, c = blockIdx.y;
-  if (cs && !cs[vec / m].active) return;
-  const T al = (T)vs[vec].alpha, mu = (T)vs[vec].mean[c];
-  const long off = ((long)vec * 3 + c) * N;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
-    x[off + i] += al * p[off + i];
-    r[off + i] -= al * (Ap[off + i] - mu);
-  }
-}
 
 // r = b - (Ax - mean)
 template <typename Tb, typename T>
@@ -600,14 +587,6 @@ int launch_fin_apply(int nvec, int m, const double* partial, int nblk, long N, V
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
-template <typename T>
-int launch_xr(long N, int nvec, int m, T* x, T* r, const T* p, const T* Ap, const VecState* vs, const CellState* cs,
-              cudaStream_t st) {
-  ProfScope ps_(PK_XR, st);
-  k_xr<T><<<vec_grid(N, nvec), 256, 0, st>>>(N, x, r, p, Ap, vs, cs, m);
-  NLF_CHECK_LAUNCH();
-  return NLF_OK;
-}
 template <typename Tb, typename T>
 int launch_r_init(long N, int nvec, int m, T* r, const Tb* b, const T* Ax, const VecState* vs, const CellState* cs,
                   cudaStream_t st) {
@@ -725,10 +704,6 @@ int launch_x_update(long N, int nvec, int m, double* x64, const float* x32, cons
   return NLF_OK;
 }
 
-template int launch_xr<float>(long, int, int, float*, float*, const float*, const float*, const VecState*,
-                              const CellState*, cudaStream_t);
-template int launch_xr<double>(long, int, int, double*, double*, const double*, const double*, const VecState*,
-                               const CellState*, cudaStream_t);
 template int launch_r_init<double, double>(long, int, int, double*, const double*, const double*, const VecState*,
                                            const CellState*, cudaStream_t);
 template int launch_r_init<float, float>(long, int, int, float*, const float*, const float*, const VecState*,

@@ -17,9 +17,6 @@ int launch_sub_mean(const LinearHandle& h, int nvec, int m, T* x, const VecState
                     cudaStream_t st);
 int launch_fin_apply(int nvec, int m, const double* partial, int nblk, long N, VecState* vs, const CellState* cs,
                      int init, cudaStream_t st);
-template <typename T>
-int launch_xr(long N, int nvec, int m, T* x, T* r, const T* p, const T* Ap, const VecState* vs, const CellState* cs,
-              cudaStream_t st);
 template <typename Tb, typename T>
 int launch_r_init(long N, int nvec, int m, T* r, const Tb* b, const T* Ax, const VecState* vs, const CellState* cs,
                   cudaStream_t st);
