@@ -37,8 +37,8 @@ typedef struct nlf_mech nlf_mech;
 
 /* Preconditioner. */
 #define NLF_PC_FFT 0        /* the reference's unit-stiffness FFT inverse (nlfiber/linear.py:154-170) */
-#define NLF_PC_FFT_SCALED 1 /* S^-1/2 K0^-1 S^-1/2 with S the root mean square of the stiffness scales of
-                               the 8 elements around each node (same converged solution, far fewer
+#define NLF_PC_FFT_SCALED 1 /* S^-a K0^-1 S^-a, a = 0.47, with S the root mean square of the stiffness scales
+                               of the 8 elements around each node (same converged solution, far fewer
                                iterations at high contrast) */
 
 typedef struct nlf_solve_opts {
@@ -97,7 +97,7 @@ NLF_API int nlf_precond(nlf_linear* h, int nvec, const double* r, double* z, voi
 
 /* precond in a chosen arithmetic and preconditioner: precond NLF_PC_FFT (s ignored, may be NULL) or
  * NLF_PC_FFT_SCALED (s: the cell's stiffness scale (nx, ny, nz); z = w irfftn(Kinv rfftn(w r)) with
- * w = (root mean square of s over the 8 elements around each node)^-1/2). */
+ * w = (root mean square of s over the 8 elements around each node)^-0.47). */
 NLF_API int nlf_precond_ex(nlf_linear* h, int nvec, const double* r, double* z, int precision, int precond,
                            const double* s, void* stream);
 

@@ -1,5 +1,5 @@
 // FFT preconditioner of the periodic corrector solve: z = irfftn(Kinv(k) rfftn(r)) (nlfiber/linear.py:154-170),
-// optionally with node scaling w = S^-1/2 on both sides (z = w .* irfftn(Kinv rfftn(w .* r))).
+// optionally with node scaling w = S^-0.47 on both sides (z = w .* irfftn(Kinv rfftn(w .* r))).
 //
 // Three passes over a half spectrum stored [vec][comp][ky][x][kz], kz in [0, nz/2]:
 //   A  one CTA per (vec, comp, x-plane): real plane -> 2D transform along z (real, packed as a half-length

@@ -34,6 +34,9 @@ struct Ede {
 };
 constexpr int kEnergyWindow = 32;
 
+// exponent of the node scaling of the scaled preconditioner, w = S^-kNodeScaleExp
+constexpr double kNodeScaleExp = 0.47;
+
 // Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188).
 struct CellState {
   int it;

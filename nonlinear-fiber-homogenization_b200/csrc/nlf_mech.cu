@@ -538,7 +538,7 @@ struct nlf_mech {
   cudaStream_t gst = nullptr;
   cudaEvent_t gev[2] = {nullptr, nullptr};
   int pc_mode = NLF_PC_FFT;  // NLF_PC_FFT: the reference's N K0^-1 / sws; NLF_PC_FFT_SCALED: N w K0^-1 w
-  double* wnode = nullptr;   // w = (root mean square of s over the 8 elements around a node)^-1/2, in `state`
+  double* wnode = nullptr;   // w = (root mean square of s over the 8 elements around a node)^-0.47, in `state`
 };
 
 namespace {

@@ -45,7 +45,7 @@ def test_apply_load_precond_symbol(L, shape):
 
 def _scaled_oracle(oh, s, r):
     sn = np.sqrt(sum(np.roll(s, shift=tuple(off), axis=(0, 1, 2)) ** 2 for off in OL.NODES) / 8.0)
-    w = (1.0 / np.sqrt(sn))[..., None]
+    w = (sn ** -0.47)[..., None]
     return w * oh.precond(w * r)
 
 
