@@ -118,13 +118,16 @@ def unit_bytes(kind, N, NS, m):
     the kernel must read and write at least once. Half spectrum: NS = nx ny (nz/2+1) complex per component."""
     w = 8 if kind.endswith("f64") else 4
     cw = 2 * w
-    # PCG iterations run the fused forms: pass A also updates r from Ap, pass C no longer reads r, and the p
-    # update also does x += alpha p (the first residual of a solve takes the unfused passes once)
+    # PCG iterations run the fused forms: pass A also updates r from Ap; on FP64 cubes of 32 and 64 pass C
+    # updates x and p (x += alpha p, p = z + beta p) in place of writing z, elsewhere it writes z and the p update
+    # does x += alpha p (the first residual of a solve takes the unfused passes once)
+    px = w == 8 and round(N ** (1 / 3)) in (32, 64)
     return {
         "apply": N * (6 * w + w / m),                      # x in, y out (3 components each), s shared by m cases
         "fft_a": 3 * N * 3 * w + NS * 3 * cw + N * w / m,   # r, Ap in, r out, half spectrum out, node scaling
         "fft_b": 2 * NS * 3 * cw,                           # half spectrum in and out (Kinv table is shared)
-        "fft_c": NS * 3 * cw + N * 3 * w + N * w / m,       # spectrum in, z out, node scaling
+        # spectrum in, node scaling, and x, p in and out (fused) or z out
+        "fft_c": NS * 3 * cw + (4 if px else 1) * N * 3 * w + N * w / m,
     }.get(kind.rsplit("_", 1)[0])
 
 

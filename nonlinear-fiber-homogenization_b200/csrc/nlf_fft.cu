@@ -288,12 +288,16 @@ struct FftDims {
 //   A: r <- r - alpha (Ap - mean Ap) before the transform (written back), partials (sum r, sum r^2) per plane
 //   B: Parseval partial of (w r, K0^-1 w r) = (r, z) per CTA (the half spectrum weighted 1 or 2 per kz)
 //   C: partial sum z per plane (mean removal), without reading r
+//   C (register-resident FP64 passes, x and p set): x <- x + alpha p, p <- z + beta p in place of writing z, for
+//      the cells that ran this iteration (status bit 1), alpha and beta from vs
 struct PcgFuse {
   const void* Ap;         // A: Ap of this iteration (T, same layout as r)
-  const VecState* vs;     // A: alpha and mean Ap per vector
+  const VecState* vs;     // A: alpha and mean Ap per vector; C with x/p: alpha and beta
   double* partA;          // [vec][comp][x-plane][2]
   double* partB;          // [vec][ky][chunk]
   double* partC;          // [vec][comp][x-plane]
+  double* x;              // C: PCG iterate and search direction ([vec][comp][N]), FP64
+  double* p;
 };
 
 // global loads issued together before their first use: enough bytes in flight per thread for HBM latency while
@@ -928,7 +932,35 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   }
 }
 
-// Pass C: inverse y FFT per column; real pre-processing + inverse packed z FFT per row; scale, w; sums.
+// Epilogue of the fused pass C for one thread's 8 double pairs of a z row (pair i = l + Lz q, q < 8):
+// z = norm a w (w = 1 unscaled), x += alpha p, p = z + beta p. Two halves of 4 pairs keep the loads of w, p and
+// x in flight together without holding all 24 pairs.
+template <int Lz>
+__device__ __forceinline__ void px_row(const cplx<double> (&a)[8], double norm, const double2* __restrict__ wp2,
+                                       double2* __restrict__ xp2, double2* __restrict__ pp2, int l, double al,
+                                       double be) {
+#pragma unroll
+  for (int hf = 0; hf < 2; ++hf) {
+    double2 ww[4], po[4], xo[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = l + Lz * (4 * hf + q);
+      ww[q] = wp2 ? wp2[i] : make_double2(1.0, 1.0);
+      po[q] = pp2[i];
+      xo[q] = xp2[i];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = l + Lz * (4 * hf + q);
+      const cplx<double> v = a[4 * hf + q];
+      xp2[i] = make_double2(xo[q].x + al * po[q].x, xo[q].y + al * po[q].y);
+      pp2[i] = make_double2((v.x * norm) * ww[q].x + be * po[q].x, (v.y * norm) * ww[q].y + be * po[q].y);
+    }
+  }
+}
+
+// Pass C: inverse y FFT per column; real pre-processing + inverse packed z FFT per row; scale, w; sums (or the
+// fused x/p update, fu.p set).
 template <int N>
 __global__ void __launch_bounds__(256, 2)
     k_fc_fast(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
@@ -943,7 +975,7 @@ __global__ void __launch_bounds__(256, 2)
   cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);
   __shared__ double red[32 * 4];
   const int c = blockIdx.y, vec = blockIdx.z;
-  if (cs && !cs[vec / m].active) return;
+  if (cs && !(fu.p ? (cs[vec / m].status & 2) : cs[vec / m].active)) return;
   prof_count(units, ukind);
   const int t = threadIdx.x;
   const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
@@ -1001,6 +1033,11 @@ __global__ void __launch_bounds__(256, 2)
   constexpr double norm = 2.0 / (double)NN;
   const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;
   const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
+  if (fu.p) {  // partial and partC are null here, so no thread reaches the barrier below
+    px_row<Lz>(a, norm, wp2, reinterpret_cast<double2*>(fu.x + roff), reinterpret_cast<double2*>(fu.p + roff), l,
+               fu.vs[vec].alpha, fu.vs[vec].beta);
+    return;
+  }
   double2* zp2 = reinterpret_cast<double2*>(z + roff);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   double2 ww[8];
@@ -1075,7 +1112,11 @@ __global__ void __launch_bounds__(256, 2)
   __shared__ double red[8 * 4];
   const int t = threadIdx.x;
   const long nplanes = (long)nvec * 3 * N;
-  auto active = [&](long j) { return !cs || cs[(int)(j / (3 * N)) / m].active; };
+  auto active = [&](long j) {
+    if (!cs) return true;
+    const CellState& s = cs[(int)(j / (3 * N)) / m];
+    return fu.p ? (s.status & 2) != 0 : s.active != 0;
+  };
   auto next_active = [&](long j) {
     while (j < nplanes && !active(j)) j += gridDim.x;
     return j;
@@ -1149,26 +1190,31 @@ __global__ void __launch_bounds__(256, 2)
     constexpr double norm = 2.0 / (double)NN;
     const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;
     const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
-    double2* zp2 = reinterpret_cast<double2*>(z + roff);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    double2 ww[8];
-    if (wp2)
+    if (fu.p) {
+      px_row<Lz>(a, norm, wp2, reinterpret_cast<double2*>(fu.x + roff), reinterpret_cast<double2*>(fu.p + roff), l,
+                 fu.vs[vec].alpha, fu.vs[vec].beta);
+    } else {
+      double2* zp2 = reinterpret_cast<double2*>(z + roff);
+      double2 ww[8];
+      if (wp2)
 #pragma unroll
-      for (int q = 0; q < 8; ++q) ww[q] = wp2[l + Lz * q];
+        for (int q = 0; q < 8; ++q) ww[q] = wp2[l + Lz * q];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      double2 v{a[q].x * norm, a[q].y * norm};
-      if (wp2) {
-        v.x *= ww[q].x;
-        v.y *= ww[q].y;
-      }
-      zp2[l + Lz * q] = v;
-      acc[0] += v.x + v.y;
-      if (partial) {
-        const double2 rv = reinterpret_cast<const double2*>(r + roff)[l + Lz * q];
-        acc[1] += rv.x * v.x + rv.y * v.y;
-        acc[2] += rv.x + rv.y;
-        acc[3] += rv.x * rv.x + rv.y * rv.y;
+      for (int q = 0; q < 8; ++q) {
+        double2 v{a[q].x * norm, a[q].y * norm};
+        if (wp2) {
+          v.x *= ww[q].x;
+          v.y *= ww[q].y;
+        }
+        zp2[l + Lz * q] = v;
+        acc[0] += v.x + v.y;
+        if (partial) {
+          const double2 rv = reinterpret_cast<const double2*>(r + roff)[l + Lz * q];
+          acc[1] += rv.x * v.x + rv.y * v.y;
+          acc[2] += rv.x + rv.y;
+          acc[3] += rv.x * rv.x + rv.y * rv.y;
+        }
       }
     }
     if (partial || fu.partC) {
@@ -1197,10 +1243,11 @@ __global__ void __launch_bounds__(256, 2)
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// stages: bit 0 pass A, bit 1 pass B, bit 2 pass C
 template <int N>
 static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double* z, cplx<double>* spec,
                        const double* w, const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk,
-                       cudaStream_t st) {
+                       int stages, cudaStream_t st) {
   using F = Fast<N>;
   const cplx<double>* tw = h.t64.tw;
   const size_t plane = F::smem_plane();
@@ -1212,18 +1259,18 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   const cplx<double>* twy = tw + h.tw.off1;
   const cplx<double>* twn2 = tw + h.tw.off2;
   const cplx<double>* twz = tw + h.tw.off2h;
-  {
+  if (stages & 1) {
     ProfScope ps(PK_FFTA64, st);
     k_fa_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
     NLF_CHECK_LAUNCH();
   }
-  {
+  if (stages & 2) {
     ProfScope ps(PK_FFTB64, st);
     k_fb_fast<N><<<dim3(N / F::KY, F::KZC, nvec), F::NTB, 0, st>>>(spec, h.t64.kinv, m, twx, cs, units, PK_FFTB64,
                                                                      fu);
     NLF_CHECK_LAUNCH();
   }
-  {
+  if (stages & 4) {
     ProfScope ps(PK_FFTC64, st);
     if constexpr (N == 64) {
       const size_t pipe = (size_t)3 * N * F::H * sizeof(cplx<double>);  // two staging planes and the transpose
@@ -1298,8 +1345,8 @@ static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx
                         const CellState* cs, double* partial, const PcgFuse& fu, int* nchunk, cudaStream_t st) {
   if constexpr (sizeof(T) == 8) {
     const int nf = fast_n(h);
-    if (nf == 64) return launch_fast<64>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, st);
-    if (nf == 32) return launch_fast<32>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, st);
+    if (nf == 64) return launch_fast<64>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, 7, st);
+    if (nf == 32) return launch_fast<32>(h, nvec, m, r, z, spec, w, cs, partial, fu, nchunk, 7, st);
   }
   FftDims d = fft_dims(h);
   const bool np2 = any_non_pow2(d);
@@ -1348,7 +1395,7 @@ static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx
 template <typename T>
 int launch_precond(const LinearHandle& h, int nvec, int m, const T* r, T* z, cplx<T>* spec, const T* w,
                    const CellState* cs, double* partial, cudaStream_t st) {
-  PcgFuse fu{nullptr, nullptr, nullptr, nullptr, nullptr};
+  PcgFuse fu{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   return precond_impl<T>(h, nvec, m, const_cast<T*>(r), z, spec, w, cs, partial, fu, nullptr, st);
 }
 
@@ -1356,8 +1403,32 @@ template <typename T>
 int launch_precond_pcg(const LinearHandle& h, int nvec, int m, T* r, const T* Ap, const VecState* vs, T* z,
                        cplx<T>* spec, const T* w, const CellState* cs, double* partA, double* partB, double* partC,
                        int* nchunk, cudaStream_t st) {
-  PcgFuse fu{Ap, vs, partA, partB, partC};
+  PcgFuse fu{Ap, vs, partA, partB, partC, nullptr, nullptr};
   return precond_impl<T>(h, nvec, m, r, z, spec, w, cs, nullptr, fu, nchunk, st);
+}
+
+bool precond_fuses_px(const LinearHandle& h) { return fast_n(h) != 0; }
+
+static int launch_fast_stages(const LinearHandle& h, int nvec, int m, double* r, cplx<double>* spec, const double* w,
+                              const CellState* cs, const PcgFuse& fu, int* nchunk, int stages, cudaStream_t st) {
+  const int nf = fast_n(h);
+  if (nf == 64) return launch_fast<64>(h, nvec, m, r, nullptr, spec, w, cs, nullptr, fu, nchunk, stages, st);
+  if (nf == 32) return launch_fast<32>(h, nvec, m, r, nullptr, spec, w, cs, nullptr, fu, nchunk, stages, st);
+  set_error("fused pass C: no register-resident passes for a %d x %d x %d grid", h.g.n0, h.g.n1, h.g.n2);
+  return NLF_EBADARG;
+}
+
+int launch_precond_pcg_ab(const LinearHandle& h, int nvec, int m, double* r, const double* Ap, const VecState* vs,
+                          cplx<double>* spec, const double* w, const CellState* cs, double* partA, double* partB,
+                          int* nchunk, cudaStream_t st) {
+  PcgFuse fu{Ap, vs, partA, partB, nullptr, nullptr, nullptr};
+  return launch_fast_stages(h, nvec, m, r, spec, w, cs, fu, nchunk, 3, st);
+}
+
+int launch_precond_pcg_cpx(const LinearHandle& h, int nvec, int m, cplx<double>* spec, const double* w,
+                           const VecState* vs, const CellState* cs, double* x, double* p, cudaStream_t st) {
+  PcgFuse fu{nullptr, vs, nullptr, nullptr, nullptr, x, p};
+  return launch_fast_stages(h, nvec, m, nullptr, spec, w, cs, fu, nullptr, 4, st);
 }
 
 template int launch_precond_pcg<float>(const LinearHandle&, int, int, float*, const float*, const VecState*, float*,

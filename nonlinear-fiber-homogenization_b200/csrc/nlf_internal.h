@@ -114,6 +114,17 @@ template <typename T>
 int launch_precond_pcg(const LinearHandle& h, int nvec, int m, T* r, const T* Ap, const VecState* vs, T* z,
                        cplx<T>* spec, const T* w, const CellState* cs, double* partA, double* partB, double* partC,
                        int* nchunk, cudaStream_t st);
+// FP64 grids with register-resident passes (cubes of 32 and 64) split the fused iteration around the control:
+// passes A and B as in launch_precond_pcg; then, once beta is known, pass C transforms back and, instead of
+// writing z, updates x <- x + alpha p and p <- z + beta p for the cells that ran this iteration. z is not
+// projected, so p and x pick up per-component constants; K annihilates constants, so alpha, beta and r are
+// those of the projected iteration, and the caller projects x when the solve ends.
+bool precond_fuses_px(const LinearHandle& h);
+int launch_precond_pcg_ab(const LinearHandle& h, int nvec, int m, double* r, const double* Ap, const VecState* vs,
+                          cplx<double>* spec, const double* w, const CellState* cs, double* partA, double* partB,
+                          int* nchunk, cudaStream_t st);
+int launch_precond_pcg_cpx(const LinearHandle& h, int nvec, int m, cplx<double>* spec, const double* w,
+                           const VecState* vs, const CellState* cs, double* x, double* p, cudaStream_t st);
 int build_tables(LinearHandle& h);
 
 // stiffness scale only (s = emin + (1 - emin) clip01(rho)^p)

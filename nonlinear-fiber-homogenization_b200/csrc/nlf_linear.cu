@@ -205,10 +205,19 @@ static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl,
   NLF_TRY(launch_mark(P.cs, P.ncell, st));
   NLF_TRY(launch_apply<T>(h, P.s, P.m, P.nvec, P.p, P.Ap, P.cs, P.part_ap, &nblk, st));
   NLF_TRY(launch_fin_apply(P.nvec, P.m, P.part_ap, nblk, N, P.vs, P.cs, 0, st));
-  // r update, (r, r), (r, z) and the sums ride on the FFT passes; x += alpha p rides on the p update
   double* partA = P.part_pc;
-  double* partC = P.part_pc + (size_t)P.nvec * 3 * h.g.n0 * 2;
   int nchunk = 0;
+  if constexpr (sizeof(T) == 8) {
+    if (precond_fuses_px(h)) {
+      // r update, (r, r) and (r, z) ride on passes A and B; the control sets beta; pass C updates x and p
+      NLF_TRY(launch_precond_pcg_ab(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.spec, P.w, P.cs, partA, P.part_b, &nchunk, st));
+      NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, nullptr, nchunk, P.vs, P.cs,
+                                  ctl.tol, ctl.maxit, P.ring, ctl.energy_tol, st));
+      return launch_precond_pcg_cpx(h, P.nvec, P.m, P.spec, P.w, P.vs, P.cs, P.x, P.p, st);
+    }
+  }
+  // r update, (r, r), (r, z) and the sums ride on the FFT passes; x += alpha p rides on the p update
+  double* partC = P.part_pc + (size_t)P.nvec * 3 * h.g.n0 * 2;
   NLF_TRY(launch_precond_pcg<T>(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.z, P.spec, P.w, P.cs, partA, P.part_b, partC,
                                 &nchunk, st));
   NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, partC, nchunk, P.vs, P.cs, ctl.tol,
@@ -328,6 +337,18 @@ static int run_iterations(LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl, int 
   return NLF_OK;
 }
 
+// x <- proj(x) for the vectors of a set whose iterations ran the fused pass C (which leaves z unprojected)
+template <typename T>
+static int project_x(const LinearHandle& h, PcgSet<T>& P, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    if (precond_fuses_px(h)) {
+      NLF_TRY(launch_stats<T>(h, P.nvec, P.m, P.x, nullptr, P.part_st, P.vs, 0, st));
+      NLF_TRY(launch_sub_mean<T>(h, P.nvec, P.m, P.x, P.vs, nullptr, st));
+    }
+  }
+  return NLF_OK;
+}
+
 // Lock-step PCG for K x = b on the mean-free subspace (nlfiber/linear.py:173-203), batched over cells.
 // b: [nvec][3][N] in Tb, already mean-free. x: initial guess if x_given (projected here), else zero.
 // mask: device per-cell flags of the cells to solve (nullptr: all).
@@ -346,7 +367,7 @@ static int pcg(LinearHandle& h, PcgSet<T>& P, const Tb* b, bool x_given, const P
     act = count_active(P.cs, P.ncell, P.d_count, h_count, st);
     if (act < 0) return act;
   }
-  return NLF_OK;
+  return project_x<T>(h, P, st);
 }
 
 static bool poison_workspace() {
@@ -478,6 +499,8 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
       }
       iters_h[c] = cs_h[sl].it;
       status = worse(status, cell_status(vs_h + (size_t)sl * m, m, o.tol));
+      PcgSet<double> v = pcg_view(P, h, sl, 1);
+      NLF_TRY(project_x<double>(h, v, st));
       NLF_CUDA_TRY(cudaMemcpyAsync(xout + (size_t)c * Vc, P.x + (size_t)sl * Vc, Vc * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
       slot_cell[sl] = -1;

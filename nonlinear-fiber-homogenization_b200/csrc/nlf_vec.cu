@@ -327,8 +327,10 @@ __global__ void k_p(long N, T* __restrict__ p, const T* __restrict__ z, const Ve
 // Fused form of k_fin_pc for an iteration whose preconditioner passes also updated r:
 //   partA [vec][3][n0][2]: sum r, (r, r) of the updated residual (FFT pass A)
 //   partB [vec][n1][nchunk]: Parseval partials of (r, z) on the half spectrum, unnormalised (pass B)
-//   partC [vec][3][n0]: sum z (pass C)
-// rz1 = (r, z - mean z) = (r, z) - sum_c mean z_c sum r_c; the control is that of k_fin_pc.
+//   partC [vec][3][n0]: sum z (pass C), or null when pass C runs after this kernel (fused x/p update, z not
+//   projected)
+// rz1 = (r, z - mean z) = (r, z) - sum_c mean z_c sum r_c (partC null: rz1 = (r, z)); the control is that of
+// k_fin_pc.
 __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* __restrict__ partB,
                                const double* __restrict__ partC, int nchunk, int n0, int n1, long N,
                                VecState* __restrict__ vs, CellState* __restrict__ cs, int m, double tol, int maxit,
@@ -349,7 +351,7 @@ __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* _
         const long i = ((long)vec * 3 + c) * n0 + x;
         sr[c] += partA[2 * i];
         rr += partA[2 * i + 1];
-        sz[c] += partC[i];
+        if (partC) sz[c] += partC[i];
       }
     for (int i = lane; i < n1 * nchunk; i += 32) dot += partB[(long)vec * n1 * nchunk + i];
 #pragma unroll
@@ -382,11 +384,12 @@ __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* _
     if (lane == 0) {
       VecState& v = vs[vec];
       double rz1 = dot / (double)N;
-      for (int c = 0; c < 3; ++c) {
-        const double mz = sz[c] / (double)N;
-        v.mean[c] = mz;
-        rz1 -= mz * sr[c];
-      }
+      if (partC)
+        for (int c = 0; c < 3; ++c) {
+          const double mz = sz[c] / (double)N;
+          v.mean[c] = mz;
+          rz1 -= mz * sr[c];
+        }
       v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
       v.rz = rz1;
       v.rr = rr;
