@@ -439,6 +439,104 @@ def uneven_arm(args, stream):
             "timing": "host wall clock around the concurrent per-size solves (device-resident rho, C to host)"}
 
 
+def density_bytes(kind, n_o):
+    """Algorithmic bytes per cell of a density-map kernel class (FP64): what it must read or write once.
+    dens_filter: phi in, the filtered field u out; dens_var: u read for its standard deviation; dens_fold: u read,
+    the folded octant out, one value per orbit out; dens_eta: the orbit values in, rho per orbit out; dens_rho:
+    rho out (the orbit values it gathers are cached)."""
+    n = 2 * n_o
+    N, NO = n ** 3, n_o ** 3
+    R = (n_o + 2) * (n_o + 1) * n_o // 6
+    return {"dens_filter": 8 * (NO + N), "dens_var": 8 * N, "dens_fold": 8 * (N + NO + R), "dens_eta": 16 * R,
+            "dens_rho": 8 * N}.get(kind)
+
+
+def density_arm(args, stream, peaks, peak_kind):
+    """The density map phi -> rho (exact volume) of the benchmark cells on the GPU: device-resident phi and rho
+    for the timed steps, a host round trip for e2e, the NumPy host map as the CPU baseline."""
+    import ctypes
+
+    import torch
+    from nlfiber_b200 import _lib
+    from nlfiber_b200 import density as D
+    n_o, nc = args.n // 2, args.cells
+    phi_h = np.stack([D.random_start(n_o, 3, seed=i, kmax=2) for i in range(nc)])
+    vols = np.array([float(np.random.default_rng(10_000 + i).uniform(0.2, 0.5)) for i in range(nc)])
+    g = D.GpuDensityMap(n_o, 3, r=1.5)
+    g.stream = stream
+    phi = torch.as_tensor(phi_h, device="cuda")
+    v = torch.as_tensor(vols, device="cuda")
+    n = 2 * n_o
+    rho = torch.empty((nc, n, n, n), dtype=torch.float64, device="cuda")
+    eta = torch.empty(nc, dtype=torch.float64, device="cuda")
+
+    def step(ph, vv, ro, et):
+        _lib.check(_lib.lib.nlf_density_rho(g._h, nc, _lib.ptr(ph), _lib.ptr(vv), ctypes.c_double(16.0),
+                                            _lib.ptr(ro), None, _lib.ptr(et), stream))
+
+    for _ in range(args.warmup):
+        step(phi, v, rho, eta)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step(phi, v, rho, eta)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # accuracy against the host map (the NumPy mirror of nlfiber/density.py) on two cells
+    err = max(float(np.abs(rho[i].cpu().numpy() - D.DensityMap(n_o, 3, r=1.5, v=vols[i]).rho(phi_h[i], 16.0)).max())
+              for i in range(2))
+    vol_err = float((rho.mean(dim=(1, 2, 3)) - v).abs().max())
+    # end to end: pinned host phi in, rho and eta back to pinned host memory, inside the timed region
+    phi_p = torch.as_tensor(phi_h).pin_memory()
+    v_p = torch.as_tensor(vols).pin_memory()
+    rho_p = torch.empty((nc, n, n, n), dtype=torch.float64).pin_memory()
+    eta_p = torch.empty(nc, dtype=torch.float64).pin_memory()
+    step(phi_p, v_p, rho_p, eta_p)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(phi_p, v_p, rho_p, eta_p)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    # kernel classes over one extra profiled step
+    _lib.profile(True)
+    step(phi, v, rho, eta)
+    prof = {k: x for k, x in _lib.profile_report().items() if k.startswith("dens_") and x[1]}
+    _lib.profile(False)
+    best = max(prof, key=lambda k: prof[k][0])
+    tot = sum(x[0] for x in prof.values())
+    kernels = {k: {"ms": round(x[0], 4), "launches": x[1], "share": round(x[0] / tot, 4),
+                   "gbs": round(density_bytes(k, n_o) * nc / (x[0] * 1e-3) / 1e9, 1)} for k, x in prof.items()}
+    bms, bla, _ = prof[best]
+    achieved = density_bytes(best, n_o) * nc / (bms * 1e-3) / 1e9
+    peak = float(peaks["hbm_gbs"])
+    # CPU baseline: the host NumPy map on a sample of cells
+    ns = min(nc, 8)
+    t0 = time.perf_counter()
+    for i in range(ns):
+        D.DensityMap(n_o, 3, r=1.5, v=vols[i]).rho(phi_h[i], 16.0)
+    cpu_s = (time.perf_counter() - t0) / ns
+    return {"metric": f"density maps/s at {n}^3 (phi -> rho, exact volume)", "value": round(nc / (ms * 1e-3), 1),
+            "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{nc} seeded pre-densities random_start({n_o}, seed=i, kmax=2), v_i ~ U[0.2, "
+                                   f"0.5], cone filter r = 1.5, beta = 16", "cells": nc, "grid": n},
+            "rho_err_max_vs_host": err, "volume_err_max": vol_err,
+            "roofline": {"kernel": best, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "peak_kind": "of measured copy bandwidth" if peak_kind == "measured"
+                         else "of fallback 6650 GB/s",
+                         "avg_launch_ms": round(bms / max(bla, 1), 4),
+                         "algorithmic_bytes_per_launch": density_bytes(best, n_o) * nc, "traffic": None},
+            "kernels": kernels,
+            "e2e": {"value": round(nc / e2e_s, 1), "unit": "cells/s", "h2d_bytes_per_step": int(phi_h.nbytes + vols.nbytes),
+                    "d2h_bytes_per_step": int(rho_p.numel() * 8 + nc * 8)},
+            "cpu_baseline": {"value": round(1.0 / cpu_s, 2), "unit": "cells/s", "cores": 1, "kind": "port",
+                             "sample": f"{ns} cells through the host NumPy map (FFT filter, full-cell bisection)"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,6 +565,8 @@ def main():
     ap.add_argument("--mech-steps", type=int, default=3)
     ap.add_argument("--uneven", default=None,
                     help="uneven batch 'n1,count1,n2,count2,...' (e.g. 32,128,64,64,128,16) instead of the default")
+    ap.add_argument("--density", action="store_true",
+                    help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
                     help="CG preconditioner of the Newton steps: the reference's (fft) or the node-scaled one")
     args = ap.parse_args()
@@ -479,6 +579,14 @@ def main():
         import torch
         torch.cuda.set_device(local)
         res = uneven_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+    if args.density:
+        import torch
+        torch.cuda.set_device(local)
+        peaks, peak_kind = measured_peaks()
+        res = density_arm(args, torch.cuda.current_stream().cuda_stream, peaks, peak_kind)
         if rank == 0:
             print(json.dumps(res), flush=True)
         return

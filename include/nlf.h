@@ -206,6 +206,27 @@ NLF_API int nlf_unet_backward(nlf_unet* net, int nb, int nx, int ny, int nz, con
 /* One Adam step (Kingma & Ba 2015, bias-corrected) with the gradient of the last nlf_unet_backward. */
 NLF_API int nlf_unet_adam_step(nlf_unet* net, double lr, double beta1, double beta2, double eps, void* stream);
 
+/* ---- density map (nlfiber/density.py, nlfiber/symmetry.py) ------------------------------------------------
+ * The input side of the solve: a pre-density phi on the symmetric octant (n_o)^3 becomes the physical density
+ * rho of the full periodic cell (2 n_o)^3 with mean(rho) = v exactly. Cubes (d = 3) only. */
+typedef struct nlf_density nlf_density;
+
+/* nlfiber/density.py:75-82 DensityMap.__init__(n_o, d=3, r, v) without v: the periodic cone filter of radius r
+ * voxels (density.py:23-31; at most 8192 nonzero taps) and the symmetry orbits of the octant
+ * (symmetry.py:74-96). */
+NLF_API int nlf_density_create(nlf_density** out, int n_o, double r);
+NLF_API int nlf_density_destroy(nlf_density* dm);
+/* Number of symmetry orbits of the octant (sorted index triples, symmetry.py:20-22 n_free); -1 for NULL. */
+NLF_API int nlf_density_orbits(const nlf_density* dm);
+/* nlfiber/density.py:84-94 DensityMap.smooth and rho (threshold / solve_eta, density.py:43-72) for ncell cells:
+ * phi (ncell, n_o, n_o, n_o) octant pre-densities (symmetrized here, as sym_perm does in smooth); v (ncell,) the
+ * volume fraction of each cell; beta > 0 the sharpness. Outputs, each NULL when not wanted (at least one):
+ * rho (ncell, n, n, n); u (ncell, n, n, n) the smoothed, exactly symmetric field of DensityMap.smooth;
+ * eta (ncell,) the threshold with mean(sigmoid(beta (u - eta))) = v. The filter is applied as a direct periodic
+ * sum over its taps (the reference multiplies FFTs: equal to rounding). */
+NLF_API int nlf_density_rho(nlf_density* dm, int ncell, const double* phi, const double* v, double beta,
+                            double* rho, double* u, double* eta, void* stream);
+
 /* ---- kernel profiler ------------------------------------------------------------------------------------- */
 
 /* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library

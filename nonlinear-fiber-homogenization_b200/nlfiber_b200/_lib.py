@@ -26,6 +26,7 @@ EXPORTS = (
     "nlf_mech_precond_w", "nlf_mech_grad_w", "nlf_mech_cg", "nlf_mech_set_precond",
     "nlf_unet_create", "nlf_unet_destroy", "nlf_unet_param_count", "nlf_unet_get_params", "nlf_unet_set_params",
     "nlf_unet_forward", "nlf_unet_backward", "nlf_unet_adam_step",
+    "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho",
 )
 
 
@@ -90,6 +91,10 @@ def _load():
         "nlf_unet_forward": (I, [P, I, I, I, I, P, P, P]),
         "nlf_unet_backward": (I, [P, I, I, I, I, P, P, P, P, P, P]),
         "nlf_unet_adam_step": (I, [P, D, D, D, D, P]),
+        "nlf_density_create": (I, [ctypes.POINTER(P), I, D]),
+        "nlf_density_destroy": (I, [P]),
+        "nlf_density_orbits": (I, [P]),
+        "nlf_density_rho": (I, [P, I, P, P, D, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

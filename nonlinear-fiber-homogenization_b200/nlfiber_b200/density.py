@@ -1,7 +1,8 @@
-"""Pre-density phi -> physical density rho with exact volume (host side, NumPy).
+"""Pre-density phi -> physical density rho with exact volume.
 
 Mirror of nlfiber/density.py and nlfiber/symmetry.py (and nlfiber/fiber.py:103-121 `random_start`): the input
-side of the homogenization solve. It produces rho on the host; the solve itself runs on the GPU.
+side of the homogenization solve. `DensityMap` runs on the host (NumPy, bit-identical to the test oracle);
+`GpuDensityMap` is the same map for batches of cubic cells in libnlf.so (nlf_density_*), on CUDA tensors.
 
     u   = F mirror(sym_perm(phi)) / std    periodic hat filter on the full cell, unit standard deviation
     rho = sigmoid(beta (u - eta)),         eta such that mean(rho) = v (bisection, then Newton)
@@ -9,6 +10,7 @@ side of the homogenization solve. It produces rho on the host; the solve itself 
 `exact_symmetrize` copies one value per symmetry orbit, so symmetric voxels are bit-identical and a threshold
 never splits an orbit (nlfiber/symmetry.py:60-65).
 """
+import ctypes
 import itertools
 
 import numpy as np
@@ -122,6 +124,72 @@ class DensityMap:
 
     def eta(self, phi, beta):
         return float(solve_eta(self.smooth(phi), self.v, beta))
+
+
+class GpuDensityMap:
+    """DensityMap on the GPU (nlfiber/density.py:75-94 smooth / rho / eta) for cubic cells, batched.
+
+    phi is an octant (n_o)^3 pre-density (or a batch (ncell, n_o, n_o, n_o)); NumPy arrays are copied in, CUDA
+    float64 tensors are used in place. Results are CUDA float64 tensors. The filter runs as a direct periodic sum
+    over its taps and the volume bisection over the symmetry orbits, so values agree with `DensityMap` to
+    rounding (not bitwise); symmetric voxels are bit-identical and mean(rho) = v to rounding."""
+
+    def __init__(self, n_o, d=3, r=1.5, v=0.3):
+        if d != 3:
+            raise ValueError("GpuDensityMap takes cubic cells (d = 3)")
+        from ._lib import check, lib
+        self.n_o, self.d, self.r, self.v = int(n_o), d, float(r), float(v)
+        self.n = 2 * self.n_o
+        self.shape = (self.n,) * 3
+        h = ctypes.c_void_p()
+        check(lib.nlf_density_create(ctypes.byref(h), self.n_o, self.r))
+        self._h = h
+        self.orbits = int(lib.nlf_density_orbits(h))
+        self.stream = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            from ._lib import lib
+            lib.nlf_density_destroy(h)
+            self._h = None
+
+    def _phi(self, phi):
+        import torch
+        if torch.is_tensor(phi):
+            phi = phi.to(device="cuda", dtype=torch.float64).contiguous()
+        else:
+            phi = torch.as_tensor(np.ascontiguousarray(np.asarray(phi, dtype=np.float64)), device="cuda")
+        if phi.dim() == 3:
+            phi = phi.unsqueeze(0)
+        if tuple(phi.shape[1:]) != (self.n_o,) * 3:
+            raise ValueError(f"phi must be (ncell, {self.n_o}, {self.n_o}, {self.n_o}), got {tuple(phi.shape)}")
+        return phi
+
+    def run(self, phi, beta, v=None, rho=True, smooth=False, eta=True):
+        """The map for a batch: {"rho": (ncell, n, n, n), "u": smoothed field or None, "eta": (ncell,)};
+        v is a scalar or one volume fraction per cell (default: the map's v)."""
+        import torch
+        from ._lib import check, lib, ptr
+        phi = self._phi(phi)
+        nc = phi.shape[0]
+        vv = torch.as_tensor(np.broadcast_to(np.asarray(self.v if v is None else v, dtype=np.float64), (nc,)).copy(),
+                             device="cuda")
+        out = {k: (torch.empty((nc,) + self.shape, dtype=torch.float64, device="cuda") if want else None)
+               for k, want in (("rho", rho), ("u", smooth))}
+        out["eta"] = torch.empty(nc, dtype=torch.float64, device="cuda") if eta else None
+        check(lib.nlf_density_rho(self._h, nc, ptr(phi), ptr(vv), float(beta), ptr(out["rho"]), ptr(out["u"]),
+                                  ptr(out["eta"]), self.stream))
+        return out
+
+    def smooth(self, phi):
+        return self.run(phi, 1.0, rho=False, smooth=True, eta=False)["u"][0]
+
+    def rho(self, phi, beta):
+        return self.run(phi, beta, eta=False)["rho"][0]
+
+    def eta(self, phi, beta):
+        return float(self.run(phi, beta, rho=False)["eta"][0])
 
 
 def random_start(n_o, d=3, seed=0, kmax=3, nterms=40):
