@@ -448,7 +448,7 @@ def density_bytes(kind, n_o):
     N, NO = n ** 3, n_o ** 3
     R = (n_o + 2) * (n_o + 1) * n_o // 6
     return {"dens_filter": 8 * (NO + N), "dens_var": 8 * N, "dens_fold": 8 * (N + NO + R), "dens_eta": 16 * R,
-            "dens_rho": 8 * N}.get(kind)
+            "dens_rho": 8 * N}.get(kind, 0)
 
 
 def density_arm(args, stream, peaks, peak_kind):
@@ -500,10 +500,30 @@ def density_arm(args, stream, peaks, peak_kind):
         step(phi_p, v_p, rho_p, eta_p)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / args.steps
-    # kernel classes over one extra profiled step
+    # the reverse mode (3 cotangent rows per cell, as Fiber.value_jac pulls back dc_k/drho): forward recomputed
+    gbar = torch.randn((nc, 3, n, n, n), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    phib = torch.empty((nc, 3, n_o, n_o, n_o), dtype=torch.float64, device="cuda")
+
+    def vjp_step():
+        _lib.check(_lib.lib.nlf_density_vjp(g._h, nc, 3, _lib.ptr(phi), _lib.ptr(v), ctypes.c_double(16.0),
+                                            _lib.ptr(gbar), _lib.ptr(phib), stream))
+
+    for _ in range(args.warmup):
+        vjp_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        vjp_step()
+    e1.record()
+    torch.cuda.synchronize()
+    vjp_ms = e0.elapsed_time(e1) / args.steps
+    # kernel classes over one extra profiled step, then over one reverse-mode call
     _lib.profile(True)
     step(phi, v, rho, eta)
     prof = {k: x for k, x in _lib.profile_report().items() if k.startswith("dens_") and x[1]}
+    _lib.profile(True)
+    vjp_step()
+    vprof = _lib.profile_report()
     _lib.profile(False)
     best = max(prof, key=lambda k: prof[k][0])
     tot = sum(x[0] for x in prof.values())
@@ -531,6 +551,9 @@ def density_arm(args, stream, peaks, peak_kind):
                          "avg_launch_ms": round(bms / max(bla, 1), 4),
                          "algorithmic_bytes_per_launch": density_bytes(best, n_o) * nc, "traffic": None},
             "kernels": kernels,
+            "vjp": {"ms_per_call": round(vjp_ms, 4), "cells": nc, "rows_per_cell": 3,
+                    "cells_per_s": round(nc / (vjp_ms * 1e-3), 1), "reverse_kernels_ms": round(vprof["dens_vjp"][0], 4),
+                    "note": "forward recomputed inside each call"},
             "e2e": {"value": round(nc / e2e_s, 1), "unit": "cells/s", "h2d_bytes_per_step": int(phi_h.nbytes + vols.nbytes),
                     "d2h_bytes_per_step": int(rho_p.numel() * 8 + nc * 8)},
             "cpu_baseline": {"value": round(1.0 / cpu_s, 2), "unit": "cells/s", "cores": 1, "kind": "port",

@@ -227,6 +227,13 @@ NLF_API int nlf_density_orbits(const nlf_density* dm);
 NLF_API int nlf_density_rho(nlf_density* dm, int ncell, const double* phi, const double* v, double beta,
                             double* rho, double* u, double* eta, void* stream);
 
+/* Vector-Jacobian product of nlf_density_rho (what JAX's reverse mode gives for DensityMap.rho,
+ * nlfiber/density.py:66-94, with the implicit d eta of `threshold`): for nrow cotangents rho_bar (ncell, nrow,
+ * n, n, n) of rho, phi_bar (ncell, nrow, n_o, n_o, n_o) = (d rho / d phi)^T rho_bar. Recomputes the forward map.
+ * nlfiber/fiber.py:34-39 (Fiber.value_and_jac) pulls the 3 rows of dc/drho back through this map. */
+NLF_API int nlf_density_vjp(nlf_density* dm, int ncell, int nrow, const double* phi, const double* v, double beta,
+                            const double* rho_bar, double* phi_bar, void* stream);
+
 /* ---- kernel profiler ------------------------------------------------------------------------------------- */
 
 /* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library

@@ -42,7 +42,15 @@ struct DensityHandle {
   int* orbit_of = nullptr;    // [n_o^3] orbit of each octant point (its sorted index triple)
   int* orbit_abc = nullptr;   // [R][3] the sorted triple a <= b <= c of each orbit, lexicographic order
   double* orbit_mult = nullptr;  // [R] number of octant points in the orbit
-  DevBuf ws;
+  DevBuf ws;   // forward intermediates
+  DevBuf wsb;  // vector-Jacobian product
+};
+
+// Forward intermediates of one density_run, kept in the handle's workspace
+struct DensWs {
+  double *F = nullptr, *u = nullptr, *psum = nullptr, *pvar = nullptr, *orb = nullptr, *ro = nullptr,
+         *eta = nullptr;
+  int nsum = 0, nvar = 0;
 };
 
 namespace {
@@ -383,6 +391,174 @@ __global__ void k_dens_rho(int n_o, int R, const int* __restrict__ orbit_of, con
   if (u_out) u_out[(long)cell * N + t] = o[(long)cell * R + q];
 }
 
+// ---- vector-Jacobian product of the map (the cotangent of phi for a cotangent of rho) -------------------------
+// Transposes, in reverse order of the forward map: threshold with the implicit d eta (d eta / du_j =
+// d_j / sum d, d = s (1 - s)); exact_symmetrize^T = the mean over each symmetry orbit of the full cell; the
+// unit-std scaling (d std / du_j = (u_j - mean u) / (N std)); the cone filter (its own transpose, k(g) = k(-g));
+// mirror^T (the octant sum of the 8 mirror images); sym_perm^T = sym_perm.
+
+// go[p] = sum of g over the 8 mirror images of octant point p, axis by axis (x, then y, then z)
+__global__ void k_dv_mirror_t(int n_o, const double* __restrict__ g, double* __restrict__ go) {
+  const int n = 2 * n_o;
+  const long NO = (long)n_o * n_o * n_o, N = (long)n * n * n;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= NO) return;
+  const int vec = blockIdx.y;
+  const int c = (int)(t % n_o), b = (int)((t / n_o) % n_o), a = (int)(t / ((long)n_o * n_o));
+  const double* x = g + (long)vec * N;
+  auto x1 = [&](int j, int k) { return x[((long)a * n + j) * n + k] + x[((long)(n - 1 - a) * n + j) * n + k]; };
+  const int b1 = n - 1 - b, c1 = n - 1 - c;
+  go[(long)vec * NO + t] = (x1(b, c) + x1(b1, c)) + (x1(b, c1) + x1(b1, c1));
+}
+
+// Per orbit r of vector vec (cell vec / nrow): W_r = beta d_r gs_r, gs_r the sum of go over the orbit's distinct
+// permutations (the orbit's sum of the rho cotangent), d_r = s_r (1 - s_r); then the orbit mean of the threshold's
+// transpose, ubs_r = W_r / (8 mult_r) - d_r (sum_r W_r) / (8 sum_r mult_r d_r). One CTA per vector.
+__global__ void __launch_bounds__(1024) k_dv_orbits(int n_o, int R, int nrow, const int* __restrict__ orbit_abc,
+                                                    const double* __restrict__ mult, const double* __restrict__ ro,
+                                                    const double* __restrict__ go, double beta,
+                                                    double* __restrict__ ubs) {
+  __shared__ double red[32 * 2];  // block_sum<2> scratch
+  __shared__ double s_w, s_d;
+  const int vec = blockIdx.x, cell = vec / nrow;
+  const long NO = (long)n_o * n_o * n_o;
+  const double* G = go + (long)vec * NO;
+  const double* sr = ro + (long)cell * R;
+  double* out = ubs + (long)vec * R;
+  auto at = [&](int i, int j, int k) { return G[((long)i * n_o + j) * n_o + k]; };
+  double acc[2] = {0.0, 0.0};
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const int a = orbit_abc[3 * r], b = orbit_abc[3 * r + 1], c = orbit_abc[3 * r + 2];
+    double gs = at(a, b, c);
+    if (a == b && b == c) {
+    } else if (a == b) {
+      gs = gs + at(a, c, a);
+      gs = gs + at(c, a, a);
+    } else if (b == c) {
+      gs = gs + at(b, a, b);
+      gs = gs + at(b, b, a);
+    } else {
+      gs = gs + at(a, c, b);
+      gs = gs + at(b, a, c);
+      gs = gs + at(b, c, a);
+      gs = gs + at(c, a, b);
+      gs = gs + at(c, b, a);
+    }
+    const double d = sr[r] * (1.0 - sr[r]);
+    const double W = beta * d * gs;
+    out[r] = W;
+    acc[0] += W;
+    acc[1] += mult[r] * d;
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) {
+    s_w = acc[0];
+    s_d = 8.0 * acc[1];
+  }
+  __syncthreads();
+  const double k = s_w / s_d;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const double d = sr[r] * (1.0 - sr[r]);
+    out[r] = out[r] / (8.0 * mult[r]) - d * k;
+  }
+}
+
+// pdot[vec][blk] = partial sum over the cell of ubs[orbit(x)] u(x)
+__global__ void k_dv_dot(int n_o, int R, int nrow, const int* __restrict__ orbit_of, const double* __restrict__ ubs,
+                         const double* __restrict__ u, double* __restrict__ pdot) {
+  __shared__ double red[32];
+  const int n = 2 * n_o, vec = blockIdx.y, cell = vec / nrow;
+  const long N = (long)n * n * n;
+  const double* uc = u + (long)cell * N;
+  const double* ub = ubs + (long)vec * R;
+  double a[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % n), j = (int)((i / n) % n), x = (int)(i / ((long)n * n));
+    a[0] += ub[orbit_of[((long)fold_idx(x, n_o) * n_o + fold_idx(j, n_o)) * n_o + fold_idx(k, n_o)]] * uc[i];
+  }
+  block_sum<1>(a, red);
+  if (threadIdx.x == 0) pdot[(long)vec * gridDim.x + blockIdx.x] = a[0];
+}
+
+// uf[vec] = the cone filter of ubar(x) = ubs[orbit(x)] / D - cc (u(x) - mean) / (N sd), the transpose of the
+// unit-std scaling applied to the orbit-mean cotangent (D = sd + 1e-12, cc = sum ubs u / D^2; mean and sd from
+// the forward's partials). Tiled as k_dens_filter_tile, the staged values computed from that expression.
+__global__ void k_dv_filter_tile(int n_o, int H, int ntap, int nrow, int R, const int* __restrict__ tap_off,
+                                 const double* __restrict__ tap_w, const int* __restrict__ orbit_of,
+                                 const double* __restrict__ ubs, const double* __restrict__ u, int nsum,
+                                 const double* __restrict__ psum, int nvar, const double* __restrict__ pvar,
+                                 int ndot, const double* __restrict__ pdot, double* __restrict__ uf) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double sc[4];
+  const int n = 2 * n_o;
+  const int SX = kTX + 2 * H, SY = kTY + 2 * H, SZ = n + 2 * H;
+  double* S = reinterpret_cast<double*>(smem_raw);
+  double* sw = S + (size_t)SX * SY * SZ;
+  int* soff = reinterpret_cast<int*>(sw + ntap);
+  for (int i = threadIdx.x; i < ntap; i += blockDim.x) {
+    sw[i] = tap_w[i];
+    soff[i] = -((tap_off[3 * i] * SY + tap_off[3 * i + 1]) * SZ + tap_off[3 * i + 2]);
+  }
+  const int vec = blockIdx.y, cell = vec / nrow;
+  const long N = (long)n * n * n;
+  {
+    const double t0 = warp0_sum(psum + (long)cell * nsum, nsum);
+    const double t1 = warp0_sum(pvar + (long)cell * nvar, nvar);
+    const double t2 = warp0_sum(pdot + (long)vec * ndot, ndot);
+    if (threadIdx.x == 0) {
+      const double sd = sqrt(t1 / (double)N), D = sd + 1e-12;
+      sc[0] = t0 / (double)N;       // mean u
+      sc[1] = D;
+      sc[2] = t2 / (D * D);         // cc
+      sc[3] = (double)N * sd;
+    }
+  }
+  __syncthreads();
+  const double mean = sc[0], D = sc[1], cc = sc[2], Nsd = sc[3];
+  const int tiles_y = (n + kTY - 1) / kTY;
+  const int x0 = (blockIdx.x / tiles_y) * kTX, y0 = (blockIdx.x % tiles_y) * kTY;
+  const double* uc = u + (long)cell * N;
+  const double* ub = ubs + (long)vec * R;
+  const int lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  for (int row = threadIdx.x >> 5; row < SX * SY; row += nwarp) {
+    const int sx = row / SY, sy = row - sx * SY;
+    const int X = wrap(x0 + sx - H, n), Y = wrap(y0 + sy - H, n);
+    const int* orow = orbit_of + ((long)fold_idx(X, n_o) * n_o + fold_idx(Y, n_o)) * n_o;
+    const double* urow = uc + ((long)X * n + Y) * n;
+    for (int sz = lane; sz < SZ; sz += 32) {
+      int Z = sz - H;
+      Z = Z < 0 ? Z + n : (Z >= n ? Z - n : Z);
+      S[row * SZ + sz] = ub[orow[fold_idx(Z, n_o)]] / D - cc * (urow[Z] - mean) / Nsd;
+    }
+  }
+  __syncthreads();
+  constexpr int kVox = 4;
+  const int total = kTX * kTY * n;
+  for (int q0 = 0; q0 < total; q0 += kVox * blockDim.x) {
+    int base[kVox];
+    long dst[kVox];
+    double acc[kVox];
+#pragma unroll
+    for (int v = 0; v < kVox; ++v) {
+      const int q = q0 + threadIdx.x + v * blockDim.x;
+      const int qn = fdiv(q, n), z = q - qn * n, y = qn % kTY, x = qn / kTY;
+      const bool ok = q < total && x0 + x < n && y0 + y < n;
+      base[v] = ok ? ((x + H) * SY + (y + H)) * SZ + (z + H) : (H * SY + H) * SZ + H;
+      dst[v] = ok ? (long)vec * N + ((long)(x0 + x) * n + (y0 + y)) * n + z : -1;
+      acc[v] = 0.0;
+    }
+    for (int t = 0; t < ntap; ++t) {
+      const double w = sw[t];
+      const int o = soff[t];
+#pragma unroll
+      for (int v = 0; v < kVox; ++v) acc[v] += w * S[base[v] + o];
+    }
+#pragma unroll
+    for (int v = 0; v < kVox; ++v)
+      if (dst[v] >= 0) uf[dst[v]] = acc[v];
+  }
+}
+
 bool dens_on_dev(const void* p) {
   if (!p) return false;
   cudaPointerAttributes at;
@@ -462,11 +638,12 @@ static void density_free(DensityHandle& h) {
   cudaFree(h.orbit_abc);
   cudaFree(h.orbit_mult);
   h.ws.release();
+  h.wsb.release();
 }
 
 // the whole map for ncell cells on device arrays; rho, u_out, eta_out may each be null
 static int density_run(DensityHandle& h, int ncell, const double* phi, const double* vol, double beta, double* rho,
-                       double* u_out, double* eta_out, cudaStream_t st) {
+                       double* u_out, double* eta_out, cudaStream_t st, DensWs* keep = nullptr) {
   const int n_o = h.n_o, n = h.n;
   const long NO = (long)n_o * n_o * n_o, N = (long)n * n * n;
   // the tiled filter when its staged region fits in shared memory (cone radii up to ~6 at 64^3), else the gather
@@ -492,6 +669,17 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
   double* orb = reinterpret_cast<double*>(b + o_orb);
   double* ro = reinterpret_cast<double*>(b + o_ro);
   double* eta = eta_out ? eta_out : reinterpret_cast<double*>(b + o_eta);
+  if (keep) {
+    keep->F = phis;
+    keep->u = u;
+    keep->psum = psum;
+    keep->pvar = pvar;
+    keep->orb = orb;
+    keep->ro = ro;
+    keep->eta = eta;
+    keep->nsum = nsum;
+    keep->nvar = nvar;
+  }
   {
     ProfScope ps(PK_DENS_FILTER, st);
     k_dens_symphi<<<dim3((unsigned)((NO + 255) / 256), ncell), 256, 0, st>>>(n_o, phi, phis);
@@ -531,6 +719,52 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
                                                                           u_out);
     NLF_CHECK_LAUNCH();
   }
+  return NLF_OK;
+}
+
+// phi_bar (ncell, nrow, n_o^3) = the cotangents of phi for the rho cotangents gbar (ncell, nrow, n^3): the
+// forward map again (its intermediates stay in the handle's workspace), then the transposes
+static int density_vjp_run(DensityHandle& h, int ncell, int nrow, const double* phi, const double* vol, double beta,
+                           const double* gbar, double* phibar, cudaStream_t st) {
+  const int n_o = h.n_o, n = h.n, nvec = ncell * nrow;
+  const long NO = (long)n_o * n_o * n_o, N = (long)n * n * n;
+  const size_t tsm = tile_smem(n, h.halo, h.ntap);
+  if (tsm > 200 * 1024) {
+    set_error("nlf_density_vjp: the filter radius %g needs %zu B of shared memory per tile (at most 200 KiB)", h.r,
+              tsm);
+    return NLF_EBADARG;
+  }
+  DensWs f;
+  NLF_TRY(density_run(h, ncell, phi, vol, beta, nullptr, nullptr, nullptr, st, &f));
+  const int ndot = (int)std::min<long>(128, (N + 2047) / 2048);
+  const int ntile = ((n + kTX - 1) / kTX) * ((n + kTY - 1) / kTY);
+  const size_t o_go = 0, o_ubs = al256(o_go + (size_t)nvec * NO * 8), o_dot = al256(o_ubs + (size_t)nvec * h.R * 8),
+               o_uf = al256(o_dot + (size_t)nvec * ndot * 8), o_mt = al256(o_uf + (size_t)nvec * N * 8),
+               total = al256(o_mt + (size_t)nvec * NO * 8);
+  NLF_TRY(h.wsb.reserve(total));
+  char* b = (char*)h.wsb.ptr;
+  double* go = reinterpret_cast<double*>(b + o_go);
+  double* ubs = reinterpret_cast<double*>(b + o_ubs);
+  double* pdot = reinterpret_cast<double*>(b + o_dot);
+  double* uf = reinterpret_cast<double*>(b + o_uf);
+  double* mt = reinterpret_cast<double*>(b + o_mt);
+  ProfScope ps(PK_DENS_VJP, st);
+  const dim3 goct((unsigned)((NO + 255) / 256), nvec);
+  k_dv_mirror_t<<<goct, 256, 0, st>>>(n_o, gbar, go);
+  NLF_CHECK_LAUNCH();
+  k_dv_orbits<<<nvec, 1024, 0, st>>>(n_o, h.R, nrow, h.orbit_abc, h.orbit_mult, f.ro, go, beta, ubs);
+  NLF_CHECK_LAUNCH();
+  k_dv_dot<<<dim3((unsigned)ndot, nvec), 256, 0, st>>>(n_o, h.R, nrow, h.orbit_of, ubs, f.u, pdot);
+  NLF_CHECK_LAUNCH();
+  if (tsm > 48 * 1024) NLF_CUDA_TRY(raise_dyn_smem(k_dv_filter_tile, (int)tsm));
+  k_dv_filter_tile<<<dim3((unsigned)ntile, nvec), 256, tsm, st>>>(n_o, h.halo, h.ntap, nrow, h.R, h.tap_off, h.tap_w,
+                                                                  h.orbit_of, ubs, f.u, f.nsum, f.psum, f.nvar,
+                                                                  f.pvar, ndot, pdot, uf);
+  NLF_CHECK_LAUNCH();
+  k_dv_mirror_t<<<goct, 256, 0, st>>>(n_o, uf, mt);
+  NLF_CHECK_LAUNCH();
+  k_dens_symphi<<<goct, 256, 0, st>>>(n_o, mt, phibar);
+  NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
 
@@ -610,6 +844,44 @@ NLF_API int nlf_density_rho(nlf_density* H, int ncell, const double* phi, const 
   if (rho && !drho) NLF_CUDA_TRY(cudaMemcpyAsync(rho, rhod, (size_t)ncell * N * 8, cudaMemcpyDeviceToHost, st));
   if (u && !du) NLF_CUDA_TRY(cudaMemcpyAsync(u, ud, (size_t)ncell * N * 8, cudaMemcpyDeviceToHost, st));
   if (eta && !deta) NLF_CUDA_TRY(cudaMemcpyAsync(eta, etad, (size_t)ncell * 8, cudaMemcpyDeviceToHost, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_density_vjp(nlf_density* H, int ncell, int nrow, const double* phi, const double* v, double beta,
+                            const double* rho_bar, double* phi_bar, void* stream) {
+  if (!H || ncell < 1 || nrow < 1 || !phi || !v || !rho_bar || !phi_bar || !(beta > 0.0) || !std::isfinite(beta)) {
+    set_error("nlf_density_vjp: bad arguments (ncell, nrow >= 1, phi, v, rho_bar, phi_bar, beta > 0)");
+    return NLF_EBADARG;
+  }
+  DensityHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long NO = (long)h.n_o * h.n_o * h.n_o, N = (long)h.n * h.n * h.n;
+  const size_t nvec = (size_t)ncell * nrow;
+  const bool dphi = dens_on_dev(phi), dv = dens_on_dev(v), dg = dens_on_dev(rho_bar), dout = dens_on_dev(phi_bar);
+  const size_t o_phi = 0, o_v = al256(o_phi + (dphi ? 0 : (size_t)ncell * NO * 8)),
+               o_g = al256(o_v + (dv ? 0 : (size_t)ncell * 8)), o_out = al256(o_g + (dg ? 0 : nvec * N * 8)),
+               total = al256(o_out + (dout ? 0 : nvec * NO * 8));
+  NLF_TRY(H->io.reserve(total));
+  char* b = (char*)H->io.ptr;
+  const double* phid = phi;
+  const double* vd = v;
+  const double* gd = rho_bar;
+  if (!dphi) {
+    NLF_CUDA_TRY(cudaMemcpyAsync(b + o_phi, phi, (size_t)ncell * NO * 8, cudaMemcpyHostToDevice, st));
+    phid = reinterpret_cast<const double*>(b + o_phi);
+  }
+  if (!dv) {
+    NLF_CUDA_TRY(cudaMemcpyAsync(b + o_v, v, (size_t)ncell * 8, cudaMemcpyHostToDevice, st));
+    vd = reinterpret_cast<const double*>(b + o_v);
+  }
+  if (!dg) {
+    NLF_CUDA_TRY(cudaMemcpyAsync(b + o_g, rho_bar, nvec * N * 8, cudaMemcpyHostToDevice, st));
+    gd = reinterpret_cast<const double*>(b + o_g);
+  }
+  double* outd = dout ? phi_bar : reinterpret_cast<double*>(b + o_out);
+  NLF_TRY(density_vjp_run(h, ncell, nrow, phid, vd, beta, gd, outd, st));
+  if (!dout) NLF_CUDA_TRY(cudaMemcpyAsync(phi_bar, outd, nvec * NO * 8, cudaMemcpyDeviceToHost, st));
   NLF_CUDA_TRY(cudaStreamSynchronize(st));
   return NLF_OK;
 }

@@ -182,6 +182,30 @@ class GpuDensityMap:
                                   ptr(out["eta"]), self.stream))
         return out
 
+    def vjp(self, phi, beta, rho_bar, v=None):
+        """Cotangents of phi for cotangents of rho (the reverse mode of `rho`, with the implicit d eta of
+        nlfiber/density.py:66-72). phi (n_o,)*3 with rho_bar (nrow, n, n, n), or a batch (ncell, n_o, n_o, n_o)
+        with rho_bar (ncell, nrow, n, n, n). Returns (nrow, n_o, n_o, n_o) or (ncell, nrow, n_o, n_o, n_o)."""
+        import torch
+        from ._lib import check, lib, ptr
+        single = np.ndim(phi) == 3
+        phi = self._phi(phi)
+        nc = phi.shape[0]
+        if torch.is_tensor(rho_bar):
+            g = rho_bar.to(device="cuda", dtype=torch.float64).contiguous()
+        else:
+            g = torch.as_tensor(np.ascontiguousarray(np.asarray(rho_bar, dtype=np.float64)), device="cuda")
+        if single:
+            g = g.reshape((1, -1) + self.shape)
+        if g.dim() != 5 or g.shape[0] != nc or tuple(g.shape[2:]) != self.shape:
+            raise ValueError(f"rho_bar must be (ncell, nrow) + {self.shape}, got {tuple(g.shape)}")
+        nrow = g.shape[1]
+        vv = torch.as_tensor(np.broadcast_to(np.asarray(self.v if v is None else v, dtype=np.float64), (nc,)).copy(),
+                             device="cuda")
+        out = torch.empty((nc, nrow) + (self.n_o,) * 3, dtype=torch.float64, device="cuda")
+        check(lib.nlf_density_vjp(self._h, nc, nrow, ptr(phi), ptr(vv), float(beta), ptr(g), ptr(out), self.stream))
+        return out[0] if single else out
+
     def smooth(self, phi):
         return self.run(phi, 1.0, rho=False, smooth=True, eta=False)["u"][0]
 

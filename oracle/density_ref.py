@@ -178,6 +178,55 @@ class DensityMap:
         return b
 
 
+def rho_vjp(dm, phi, beta, gbar):
+    """Cotangent of phi for the cotangent gbar of rho = dm.rho(phi, beta): the linear map that JAX's reverse mode
+    gives for nlfiber/density.py:66-72 (threshold, with the implicit d eta = d.du / 1.d, d = s (1 - s)) composed
+    with DensityMap.smooth (density.py:84-88) and the symmetry maps (symmetry.py:25-65).
+
+    Transposes used: exact_symmetrize^T averages a field over each symmetry orbit of the full cell (mirror^T sums
+    the 8 mirror images, from_free^T sums an orbit's octant points, to_free^T puts the sum at the sorted triple,
+    sym_perm^T = sym_perm spreads it back with 1/6 per permutation, fold^T = mirror / 8); the cone filter is
+    symmetric (k(g) = k(-g)), so filt^T = filt; sym_perm^T = sym_perm; u / (std(u) + 1e-12) has
+    d(std)/du_j = (u_j - mean u) / (N std)."""
+    phi = np.asarray(phi, dtype=np.float64)
+    gbar = np.asarray(gbar, dtype=np.float64)
+    x = mirror(sym_perm(phi))
+    u_raw = filt(x, dm.kfft)
+    sd = np.std(u_raw)
+    D = sd + 1e-12
+    u_sym = exact_symmetrize(u_raw / D)
+    eta = solve_eta(u_sym, dm.v, beta)
+    s = _sigmoid(beta * (u_sym - eta))
+    d = s * (1.0 - s)
+    w = gbar * beta * d
+    ubar = w - d * (w.sum() / d.sum())                      # threshold
+    ubar = _orbit_mean(ubar)                                # exact_symmetrize^T
+    N = ubar.size
+    ubar = ubar / D - (np.sum(ubar * u_raw) / D ** 2) * (u_raw - u_raw.mean()) / (N * sd)   # unit-std scaling
+    ubar = filt(ubar, dm.kfft)                              # filter (symmetric kernel)
+    return sym_perm(_mirror_T(ubar))                        # mirror^T, sym_perm^T
+
+
+def _mirror_T(full):
+    """Transpose of mirror: the octant sum of the 8 mirror images."""
+    x = np.asarray(full)
+    for ax in range(x.ndim):
+        n = x.shape[ax] // 2
+        x = np.take(x, np.arange(n), axis=ax) + np.flip(np.take(x, np.arange(n, 2 * n), axis=ax), ax)
+    return x
+
+
+def _orbit_mean(full):
+    """Mean of a full-cell field over each orbit of the 48 mirror / permutation symmetries (= exact_symmetrize^T,
+    and the orthogonal projection onto symmetric fields)."""
+    oct_sum = _mirror_T(full)
+    n_o, d = oct_sum.shape[0], oct_sum.ndim
+    rep = representative_index(n_o, d)
+    tot = np.bincount(rep.ravel(), weights=oct_sum.ravel())
+    cnt = np.bincount(rep.ravel()) * 2 ** d
+    return mirror((tot / cnt)[rep])
+
+
 def _dilate_periodic(b):
     """nlfiber/density.py:125-130."""
     out = b.copy()

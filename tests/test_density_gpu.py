@@ -150,3 +150,49 @@ def test_gather_filter_path_agrees(tmp_path):
     out = _gpu(n_o, r, v).run(phi, beta, smooth=True)
     assert np.abs(np.load(tmp_path / "u.npy") - out["u"][0].cpu().numpy()).max() < 1e-14
     assert np.abs(np.load(tmp_path / "rho.npy") - out["rho"][0].cpu().numpy()).max() < 1e-13
+
+
+@pytest.mark.parametrize("n_o,r,v,beta", [(4, 1.5, 0.27, 4.0), (3, 2.5, 0.3, 16.0), (5, 1.0, 0.4, 8.0),
+                                          (8, 1.5, 0.3, 16.0), (16, 1.5, 0.25, 32.0)])
+def test_vjp_matches_oracle(n_o, r, v, beta):
+    """nlf_density_vjp against the oracle's reverse mode (pinned by finite differences on the CPU), for a batch of
+    2 cells with per-cell volumes and 3 cotangent rows each. Tolerance 1e-10 of the largest entry: the filter and
+    the reductions round differently."""
+    rng = np.random.default_rng(n_o)
+    phis = rng.standard_normal((2,) + (n_o,) * 3)
+    vols = np.array([v, v + 0.05])
+    g = rng.standard_normal((2, 3) + (2 * n_o,) * 3)
+    out = _gpu(n_o, r, v).vjp(phis, beta, g, v=vols).cpu().numpy()
+    for i in range(2):
+        dm = OD.DensityMap(n_o, 3, r=r, v=float(vols[i]))
+        for k in range(3):
+            ref = OD.rho_vjp(dm, phis[i], beta, g[i, k])
+            assert np.abs(out[i, k] - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+
+
+def test_fiber_value_jac_matches_oracle_chain_and_finite_differences():
+    """nlfiber/fiber.py:34-39,53-57 on the GPU: c = (C11, C12, C44) / E of the two-case solve and its Jacobian
+    rows dc_k/dphi (dC/drho with the correctors held fixed, pulled back through the density map). Checked against
+    the oracle's chain (oracle solve, dC_drho, rho_vjp) and against central differences of the GPU value."""
+    from nlfiber_b200.fiber import Fiber
+    from oracle import linear_ref as OL
+    n_o, beta, v = 4, 8.0, 0.35
+    phi = OD.sym_perm(np.random.default_rng(5).standard_normal((n_o,) * 3))
+    fib = Fiber(n_o, v=v, r=1.5, emin=1e-3, tol=1e-13, maxit=20000)
+    c, J = fib.value_jac(phi, beta, warm=False)
+    dm = OD.DensityMap(n_o, 3, r=1.5, v=v)
+    rho = dm.rho(phi, beta)
+    lh = OL.LinearHomogenization(rho.shape, emin=1e-3, tol=1e-13, maxit=20000)
+    c_o, u2, _ = lh.invariants(rho)
+    np.testing.assert_allclose(c, c_o, rtol=1e-10)
+    u3 = np.stack([u2[0], lh.swap_xy(u2[0]), u2[1]])
+    Es = np.stack([OL.unit_strain(0), OL.unit_strain(1), OL.unit_strain(3)])
+    dC = lh.dC_drho(rho, Es, u3)
+    for k, (I, Jx) in enumerate(((0, 0), (1, 0), (2, 2))):
+        ref = OD.rho_vjp(dm, phi, beta, dC[I, Jx] / lh.E)
+        assert np.abs(J[k] - ref).max() <= 1e-8 * np.abs(ref).max()
+    d = OD.sym_perm(np.random.default_rng(6).standard_normal((n_o,) * 3))
+    h = 1e-5
+    fd = (fib.value(phi + h * d, beta, warm=False) - fib.value(phi - h * d, beta, warm=False)) / (2 * h)
+    jd = np.tensordot(J, d, axes=3)
+    np.testing.assert_allclose(jd, fd, rtol=1e-6, atol=1e-9)
