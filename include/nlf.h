@@ -134,6 +134,16 @@ NLF_API int nlf_dC_drho(nlf_linear* h, int ncell, const double* rho, const doubl
 NLF_API int nlf_bilinear_noalloc(int nx, int ny, int nz, double E, double nu, int ncell, const double* s,
                                  const double* Es, int m, const double* u, double* C, void* stream);
 
+/* nlfiber/linear.py:118-134 the backward of `correctors`' custom VJP: for the cotangent ubar (ncell, m, nx, ny, nz,
+ * 3) of the correctors u of (s, Es), lam solves K(s) lam = -proj(ubar) (PCG from zero with `opts`, as _solve_rhs)
+ * and sbar_e = sum_I lam_I,e . (Ke u_I,e + G^T E_I), the VJP of residual(s, Es, u) in s. Give s (ncell, nx, ny,
+ * nz), or rho instead of s: then s = stiffness_scale(rho) and sbar is the cotangent of rho (times ds/drho,
+ * nlfiber/linear.py:137-141). Es (m, 6), m <= 6; lam (the shape of u) and iters (ncell) may be NULL. Returns the
+ * solve's status. */
+NLF_API int nlf_correctors_vjp(nlf_linear* h, int ncell, const double* s, const double* rho, const double* Es, int m,
+                               const double* u, const double* ubar, double* sbar, double* lam, int* iters,
+                               const nlf_solve_opts* opts, void* stream);
+
 /* nlfiber/linear.py:231-236 C_full(rho, u0) for a batch: rho -> s -> 6 unit strains -> PCG -> C.
  * u0, u, dC may be NULL (cold start / corrector not returned / no sensitivities).
  * C: (ncell, 6, 6); u: (ncell, 6, nx, ny, nz, 3); dC: (ncell, 6, 6, nx, ny, nz); iters: (ncell,). */

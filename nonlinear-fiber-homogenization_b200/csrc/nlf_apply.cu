@@ -375,6 +375,60 @@ __global__ void k_reduce_C(const double* __restrict__ Cpart, int nblk, int m, do
   }
 }
 
+// sbar_e = sum_I lam_I,e . (Ke u_I,e + G^T E_I) = sum_I (c'_lam,I . M c'_u,I + E_I . D eps(lam_I)): the VJP in s
+// of <lam, residual(s, Es, u)>, the backward of the reference's corrector custom VJP (nlfiber/linear.py:124-131).
+// With rho, the same times ds/drho (rhobar). u, lam: SoA [cell][I][comp][N]; one thread per element.
+__global__ void __launch_bounds__(128) k_adjoint_sbar(const double* __restrict__ Es, int m, int n0, int n1, int n2,
+                                                      double lam, double mu, const double* __restrict__ u,
+                                                      const double* __restrict__ lamv, const double* __restrict__ rho,
+                                                      double emin, double pexp, double* __restrict__ out) {
+  const long N = (long)n0 * n1 * n2;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int cell = blockIdx.y;
+  if (e >= N) return;
+  const int k = (int)(e % n2), j = (int)((e / n2) % n1), i = (int)(e / ((long)n1 * n2));
+  long nid[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int ii = wrap(i + (a & 1), n0), jj = wrap(j + ((a >> 1) & 1), n1), kk = wrap(k + (a >> 2), n2);
+    nid[a] = ((long)ii * n1 + jj) * n2 + kk;
+  }
+  const ModeC<double> unit = make_modec<double>(lam, mu);
+  double acc = 0.0;
+  for (int I = 0; I < m; ++I) {
+    const long off = ((long)cell * m + I) * 3 * N;
+    double cu[3][8], fu[3][8], cl[3][8], sl[6];
+    gather_modes(u + off, N, nid, cu);
+    mode_force(cu, unit, fu);
+    gather_modes(lamv + off, N, nid, cl);
+    mean_stress(cl, lam, mu, sl);
+    double b = 0.0;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) b += Es[I * 6 + v] * sl[v];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+      for (int a = 1; a < 8; ++a) b += cl[cc][a] * fu[cc][a];
+    acc += b;
+  }
+  if (rho) {
+    const double r = rho[(long)cell * N + e];
+    const double rc = r > 1.0 ? 1.0 : (r < 0.0 ? 0.0 : r);
+    acc *= (r > 1.0 || r < 0.0) ? 0.0 : (1.0 - emin) * pexp * pow(rc, pexp - 1.0);
+  }
+  out[(long)cell * N + e] = acc;
+}
+
+int launch_adjoint_sbar(const LinearHandle& h, const double* Es, int m, int ncell, const double* u,
+                        const double* lamv, const double* rho, double* out, cudaStream_t st) {
+  const long N = h.g.N;
+  ProfScope ps(PK_BILINEAR, st);
+  k_adjoint_sbar<<<dim3((unsigned)((N + 127) / 128), ncell), 128, 0, st>>>(Es, m, h.g.n0, h.g.n1, h.g.n2, h.lam,
+                                                                           h.mu, u, lamv, rho, h.emin, h.p, out);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
 int launch_bilinear(const LinearHandle& h, const double* s, const double* EsEDE, int m, int ncell,
                     const double* u, double* Cpart, int* nblk, const double* rho, double* dC, cudaStream_t st) {
   if (m > kMaxM) {

@@ -99,6 +99,9 @@ int launch_load(const LinearHandle& h, const double* s, const double* fe /*(m,24
 int launch_bilinear(const LinearHandle& h, const double* s, const double* Es /*device (m,6)*/, int m,
                     int ncell, const double* u, double* Cpart, int* nblk, const double* rho, double* dC,
                     cudaStream_t st);
+// sbar_e = sum_I lam_I,e . (Ke u_I,e + G^T E_I) (times ds/drho when rho is given); Es device (m, 6); u, lam SoA
+int launch_adjoint_sbar(const LinearHandle& h, const double* Es, int m, int ncell, const double* u,
+                        const double* lamv, const double* rho, double* out, cudaStream_t st);
 int launch_reduce_C(const LinearHandle& h, const double* Cpart, int nblk, int m, int ncell, double* C,
                     cudaStream_t st);
 

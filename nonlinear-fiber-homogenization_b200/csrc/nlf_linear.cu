@@ -1107,6 +1107,66 @@ NLF_API int nlf_dC_drho(nlf_linear* H, int ncell, const double* rho, const doubl
   return bilinear_entry(H, ncell, nullptr, rho, Es, m, u, nullptr, dC, stream);
 }
 
+NLF_API int nlf_correctors_vjp(nlf_linear* H, int ncell, const double* s, const double* rho, const double* Es, int m,
+                               const double* u, const double* ubar, double* sbar, double* lam, int* iters,
+                               const nlf_solve_opts* opts, void* stream) {
+  if (bad_handle(H) || ncell < 1 || m < 1 || m > 6 || (!s && !rho) || !Es || !u || !ubar || !sbar) {
+    set_error("nlf_correctors_vjp: bad arguments (s or rho, Es, u, ubar, sbar; 1 <= m <= 6)");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const int nvec = ncell * m;
+  const size_t V = (size_t)nvec * 3 * N;
+  // io2 (the solve stages through io): s | rho | ubar -> b = -ubar (AoS) | lam (AoS) | u, lam (SoA) | Es | out
+  const size_t o_s = 0, o_r = al((size_t)ncell * N * 8), o_b = o_r + al((size_t)ncell * N * 8),
+               o_l = o_b + al(V * 8), o_us = o_l + al(V * 8), o_ls = o_us + al(V * 8), o_e = o_ls + al(V * 8),
+               o_o = o_e + al((size_t)m * 6 * 8), total = o_o + al((size_t)ncell * N * 8);
+  NLF_TRY(h.io2.reserve(total));
+  char* b = (char*)h.io2.ptr;
+  InView rv;
+  double* sd = reinterpret_cast<double*>(b + o_s);
+  if (rho) {
+    NLF_TRY(stage_in(rho, (size_t)ncell * N, h.io2, o_r, rv, st));
+    NLF_TRY(launch_stiffness_scale(h, (long)ncell * N, rv.d, sd, st));
+  } else if (is_device_ptr(s)) {
+    NLF_CUDA_TRY(cudaMemcpyAsync(sd, s, (size_t)ncell * N * 8, cudaMemcpyDeviceToDevice, st));
+  } else {
+    NLF_CUDA_TRY(cudaMemcpyAsync(sd, s, (size_t)ncell * N * 8, cudaMemcpyHostToDevice, st));
+  }
+  // b = -ubar (the solve projects it: K lam = -proj(ubar), nlfiber/linear.py:127)
+  double* bd = reinterpret_cast<double*>(b + o_b);
+  NLF_CUDA_TRY(cudaMemcpyAsync(bd, ubar, V * 8, is_device_ptr(ubar) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               st));
+  NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, bd, reinterpret_cast<double*>(b + o_us), -1.0, st)));
+  NLF_TRY((launch_soa_to_aos<double, double>(N, nvec, reinterpret_cast<double*>(b + o_us), bd, st)));
+  double* ld = reinterpret_cast<double*>(b + o_l);
+  int status = solve_entry(H, ncell, sd, nullptr, bd, m, nullptr, ld, iters, opts, stream);
+  if (status < 0) return status;
+  // u and lam to SoA, then sbar (or rhobar)
+  InView uv;
+  double* us = reinterpret_cast<double*>(b + o_us);
+  double* ls = reinterpret_cast<double*>(b + o_ls);
+  if (is_device_ptr(u)) {
+    NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, u, us, 1.0, st)));
+  } else {
+    NLF_CUDA_TRY(cudaMemcpyAsync(ls, u, V * 8, cudaMemcpyHostToDevice, st));  // staged through the lam slot
+    NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, ls, us, 1.0, st)));
+  }
+  NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, ld, ls, 1.0, st)));
+  std::vector<double> Esh;
+  NLF_TRY(host_copy_small(Es, (size_t)m * 6, Esh));
+  double* ed = reinterpret_cast<double*>(b + o_e);
+  NLF_CUDA_TRY(cudaMemcpyAsync(ed, Esh.data(), Esh.size() * 8, cudaMemcpyHostToDevice, st));
+  double* od = is_device_ptr(sbar) ? sbar : reinterpret_cast<double*>(b + o_o);
+  NLF_TRY(launch_adjoint_sbar(h, ed, m, ncell, us, ls, rho ? rv.d : nullptr, od, st));
+  if (od != sbar) NLF_TRY(copy_out(sbar, od, (size_t)ncell * N, st));
+  if (lam) NLF_TRY(copy_out(lam, ld, V, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return status;
+}
+
 NLF_API int nlf_C_full(nlf_linear* H, int ncell, const double* rho, const double* u0, double* C, double* u,
                        double* dC, int* iters, const nlf_solve_opts* opts, void* stream) {
   if (bad_handle(H) || ncell < 1 || !rho || !C) {

@@ -236,8 +236,26 @@ class LinearHomogenization:
         return u, int(it[0])
 
     def correctors(self, s, Es, u0):
-        """nlfiber/linear.py:118-121 (value; the adjoint of the reference's custom VJP is `_solve_rhs`)."""
+        """nlfiber/linear.py:118-121 (the value; its custom VJP's backward is `correctors_vjp`)."""
         return self.solve(s, Es, u0)[0]
+
+    def correctors_vjp(self, s, Es, u, ubar, rho=None, **opt):
+        """nlfiber/linear.py:124-131, the backward of `correctors`: lam solves K(s) lam = -proj(ubar) and
+        sbar = d<lam, residual(s, Es, u)>/ds. With rho (s=None), s = stiffness_scale(rho) and the result is the
+        cotangent of rho. Returns (sbar (nx, ny, nz), lam (m, nx, ny, nz, 3), iterations)."""
+        Es = as_f64(np.atleast_2d(Es))
+        m = Es.shape[0]
+        u = as_f64(u)
+        ubar = as_f64(ubar)
+        sv = None if s is None else self._cell(s)
+        rv = None if rho is None else self._cell(rho)
+        sbar = np.empty(self.shape)
+        lam = np.empty((m,) + self.shape + (3,))
+        it = np.zeros(1, dtype=np.int32)
+        o = self.opts(**opt)
+        check(lib.nlf_correctors_vjp(self._h, 1, ptr(sv), ptr(rv), ptr(Es), m, ptr(u), ptr(ubar), ptr(sbar),
+                                     ptr(lam), ptr(it), ctypes.byref(o), self.stream))
+        return sbar, lam, int(it[0])
 
     # --- homogenized stiffness -----------------------------------------------------------------------------
     def bilinear(self, s, Es, u):

@@ -227,6 +227,15 @@ class LinearHomogenization:
         b = self.element_bracket(np.asarray(Es, dtype=np.float64), u)
         return b * self.dscale_drho(rho)[None, None] / float(np.prod(self.shape))
 
+    def correctors_vjp(self, s, Es, u, ubar, maxit=None):
+        """nlfiber/linear.py:124-131 (the backward of `correctors`' custom VJP): lam = _solve_rhs(s, -proj(ubar)),
+        sbar_e = sum_I lam_I,e . (Ke u_I,e + G^T E_I), the VJP of residual(s, Es, u) in s. Returns (sbar, lam)."""
+        lam, _ = self._solve_rhs(s, -proj(np.asarray(ubar, dtype=np.float64)), maxit)
+        le, ue = gather(lam), gather(u)
+        Es = np.asarray(Es, dtype=np.float64)
+        sbar = np.einsum("ixyze,ixyze->xyz", le, ue @ self.Ke) + np.einsum("ie,ixyze->xyz", Es, le @ self.G.T)
+        return sbar, lam
+
     # nlfiber/linear.py:231-236
     def C_full(self, rho, u0=None, maxit=None, history=None):
         s = self.stiffness_scale(rho)

@@ -232,3 +232,29 @@ def test_not_converged_is_silent_and_bad_args_raise(L):
     from nlfiber_b200 import _lib
     with pytest.raises(_lib.NlfError):
         L.LinearHomogenization((0, 4, 4))
+
+
+@pytest.mark.parametrize("shape", [(6, 6, 6), (32, 32, 32)])
+def test_correctors_vjp_matches_oracle(L, shape):
+    """nlf_correctors_vjp (the backward of nlfiber/linear.py:118-134's custom VJP: K lam = -proj(ubar), then the VJP
+    of the residual in s) against the oracle's restatement (pinned by finite differences in test_oracle.py), on a
+    grid with the generic FFT passes and one with the register-resident ones; with s, and with rho (cotangent of
+    rho through the stiffness scale). Both solves to a 1e-12 relative residual; tolerance 1e-8 of the largest
+    entry."""
+    rng = np.random.default_rng(shape[0])
+    n = shape[0]
+    rho = OD.random_cell(2, n_o=n // 2)[0]
+    lh = L.LinearHomogenization(shape, emin=1e-3, tol=1e-12, maxit=20000)
+    oh = OL.LinearHomogenization(shape, emin=1e-3, tol=1e-12, maxit=20000)
+    s = oh.stiffness_scale(rho)
+    Es = np.stack([OL.unit_strain(0), OL.unit_strain(3), OL.unit_strain(5)])
+    u, _ = oh.solve(s, Es)
+    ubar = rng.standard_normal(u.shape)
+    sb_o, lam_o = oh.correctors_vjp(s, Es, u, ubar)
+    sb, lam, it = lh.correctors_vjp(s, Es, u, ubar)
+    assert it > 0
+    assert np.abs(sb - sb_o).max() <= 1e-8 * np.abs(sb_o).max()
+    assert np.abs(lam - lam_o).max() <= 1e-8 * np.abs(lam_o).max()
+    rb, _, _ = lh.correctors_vjp(None, Es, u, ubar, rho=rho)
+    rb_o = sb_o * oh.dscale_drho(rho)
+    assert np.abs(rb - rb_o).max() <= 1e-8 * np.abs(rb_o).max()

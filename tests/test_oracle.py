@@ -109,3 +109,22 @@ def test_element_mode_form_equals_dense_Ke():
             ue = rng.standard_normal((8, 3))
             ref = (ue.reshape(24) @ Ke).reshape(8, 3)
             np.testing.assert_allclose(_elem_force_modes(ue, lam, mu), ref, atol=1e-14 * np.abs(Ke).max() * 10)
+
+
+def test_oracle_correctors_vjp_matches_finite_differences():
+    """The backward of `correctors`' custom VJP (nlfiber/linear.py:118-134): <sbar, ds> equals the directional
+    derivative of <ubar, u(s)> with u(s) the converged correctors, by central differences of the oracle's solve."""
+    rng = np.random.default_rng(3)
+    shape = (4, 4, 4)
+    lh = OL.LinearHomogenization(shape, emin=1e-3, tol=1e-14, maxit=5000)
+    s = 0.1 + 0.9 * rng.random(shape)
+    Es = np.stack([OL.unit_strain(0), OL.unit_strain(3)])
+    ubar = rng.standard_normal((2,) + shape + (3,))
+    ds = rng.standard_normal(shape)
+    u, _ = lh.solve(s, Es)
+    sbar, lam = lh.correctors_vjp(s, Es, u, ubar)
+    h = 1e-6
+    fp = np.sum(ubar * lh.solve(s + h * ds, Es)[0])
+    fm = np.sum(ubar * lh.solve(s - h * ds, Es)[0])
+    fd = (fp - fm) / (2 * h)
+    assert abs(np.sum(sbar * ds) - fd) <= 1e-7 * abs(fd)
