@@ -560,6 +560,41 @@ def density_arm(args, stream, peaks, peak_kind):
                              "sample": f"{ns} cells through the host NumPy map (FFT filter, full-cell bisection)"}}
 
 
+def toec_arm(args, stream):
+    """Third-order elastic constants (nlfiber/mech.py:458-493) of benchmark cells at --n^3: linear correctors
+    from the batched solve, then nlf_mech_toec timed with CUDA events (correctors resident on the device)."""
+    import torch
+    from nlfiber_b200 import linear as L
+    from nlfiber_b200 import mech as MH
+    n, nc = args.n, 2
+    cells = gen_cells(list(range(nc)), n // 2)
+    lh = L.LinearHomogenization((n, n, n), emin=1e-3, precond="scaled", tol=1e-10, maxit=8000, check_every=16)
+    res = lh.C_full_batched(np.stack(cells), want_u=True)
+    rows = []
+    for i in range(nc):
+        cell = MH.Cell(cells[i], emin=1e-3)
+        chi = torch.as_tensor(res["u"][i], device="cuda")
+        for _ in range(args.warmup):
+            MH.toec(cell, chi)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            C, T = MH.toec(cell, chi)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        N = n ** 3
+        # FP64 operations per element and Gauss point: 21 pairs (~40 flops) and 56 triples (~140 flops)
+        flops = N * 8 * (21 * 40 + 56 * 140)
+        rows.append({"cell": i, "ms": round(ms, 4), "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                     "C_rel_diff_vs_linear": float(np.abs(C - res["C"][i]).max() / np.abs(res["C"][i]).max()),
+                     "cubic": MH.cubic_toec(T)})
+    return {"mode": "toec", "workload": f"{nc} benchmark cells at {n}^3, emin 1e-3, neo-Hookean with WLS (500, 0.01)",
+            "rows": rows, "timing": "CUDA events around nlf_mech_toec (6 correctors on the device, C and T to host)",
+            "fp64_peak_note": "nominal FP64 vector peak 37.2 TFLOP/s (148 SMs x 64 FMA/clk x 1.965 GHz)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -588,6 +623,8 @@ def main():
     ap.add_argument("--mech-steps", type=int, default=3)
     ap.add_argument("--uneven", default=None,
                     help="uneven batch 'n1,count1,n2,count2,...' (e.g. 32,128,64,64,128,16) instead of the default")
+    ap.add_argument("--toec", action="store_true",
+                    help="time the third-order elastic constants of two benchmark cells instead of the default")
     ap.add_argument("--density", action="store_true",
                     help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
@@ -602,6 +639,13 @@ def main():
         import torch
         torch.cuda.set_device(local)
         res = uneven_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+    if args.toec:
+        import torch
+        torch.cuda.set_device(local)
+        res = toec_arm(args, torch.cuda.current_stream().cuda_stream)
         if rank == 0:
             print(json.dumps(res), flush=True)
         return

@@ -188,6 +188,14 @@ NLF_API int nlf_mech_cg(nlf_mech* h, const double* w, const double* Fbar, int k,
                         const double* dmac, double sws, double tol, int maxit, double* x, int* it, int* conv, int* neg,
                         int check_every, void* stream);
 
+/* nlfiber/mech.py:458-493 toec(cell, chi): C (6, 6) and the Lagrangian-strain third-order elastic constants
+ * T (6, 6, 6) of the cell (its s and gamma from nlf_mech_set_rho, its material) from the linear correctors chi
+ * (6, nx, ny, nz, 3) of the 6 unit Voigt strains (same stiffness scale, E and nu): C = f''(0),
+ * T = f'''(0) - 3 Sym C(e_I, voigt(e_J e_K)) with f(s) = wq sum_{g,e} s_e psi_eff(I + sum_I s_I H_I),
+ * H_I = voigt(I) + grad chi_I. The reference differentiates f by autodiff; here f'' and f''' at F = I are
+ * closed forms (the neo-Hookean energy's; zero third derivative for the linear material). C, T host or device. */
+NLF_API int nlf_mech_toec(nlf_mech* cell, const double* chi, double* C, double* T, void* stream);
+
 /* ---- learned warm start ----------------------------------------------------------------------------------
  * A 3-level U-Net (widths w0, w1, w2; periodic 3x3x3 convolutions, ReLU, 2x average pooling, nearest
  * upsampling with skip concatenation, a final 1x1 convolution to 18 channels) maps a density cell to the 6

@@ -11,6 +11,7 @@
 //   neo-Hookean: P = mu (F - F^-T) + lam lnJ F^-T,
 //                dP = mu dF + (mu - lam lnJ) F^-T dF^T F^-T + lam (F^-T : dF) F^-T.
 // Element forces go to a [24][N] buffer; a gather kernel sums the 8 contributions of each node in a fixed order.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -341,6 +342,132 @@ __global__ void k_mech_gradw(long N, int n0, int n1, int n2, const double* __res
         for (int q = 0; q < 8; ++q) h += wn[c][q] * cDN[g][q][d];
         H[(((long)g * N + e) * 3 + c) * 3 + d] = h;
       }
+}
+
+// ---- third-order elastic constants (mech.py:458-493) ------------------------------------------------------------
+// f(s) = wq sum_{g,e} s_e psi_eff(I + sum_I s_I H_I), H_I = voigt(I) + grad chi_I. At s = 0 (F = I) the
+// derivatives have closed forms: f''_IJ = wq sum s (lam trH_I trH_J + mu (H_I : H_J + tr H_I H_J)) for either
+// material (the WLS factor gamma cancels: psi_NH''(I) = psi_lin''), and for the neo-Hookean material
+// f'''_IJK = wq sum s gamma^3 [-mu tr((H_I H_J + H_J H_I) H_K) - lam (trH_I tr H_J H_K + trH_J tr H_K H_I +
+// trH_K tr H_I H_J)] (psi_NH'''(I); the quadratic parts drop out). Outputs per CTA: the 21 distinct f''_IJ
+// (I <= J) then the 56 distinct f'''_IJK (I <= J <= K), without wq; accumulators in shared memory, one column
+// per thread, reduced in a fixed order.
+constexpr int kToecOut = 77, kToecThreads = 256, kToecWarps = kToecThreads / 32;
+
+__host__ __device__ __forceinline__ double voigt_entry(int I, int c, int d) {
+  // the symmetric tensor of Voigt unit strain I (engineering shear: off-diagonals 1/2), Voigt xx yy zz yz xz xy
+  const int a = I < 3 ? I : (I == 3 ? 1 : 0), b = I < 3 ? I : (I == 5 ? 1 : 2);
+  if (I < 3) return (c == a && d == a) ? 1.0 : 0.0;
+  return ((c == a && d == b) || (c == b && d == a)) ? 0.5 : 0.0;
+}
+
+// output q -> (I, J) for q < 21 (I <= J), (I, J, K) for q >= 21 (I <= J <= K), lexicographic
+__constant__ signed char cToecIdx[kToecOut][3];
+
+// One warp per element: lanes 0..17 form grad chi_I (row c of I = lane / 3, c = lane % 3) at the 8 Gauss points
+// into the warp's shared H[g][I][3][3] (plus voigt(I)); then lane l accumulates outputs l, l + 32, l + 64 over
+// the 8 Gauss points in registers. At the end the CTA's partial sums are reduced in a fixed order.
+__global__ void __launch_bounds__(kToecThreads) k_mech_toec(MechDev d, const double* __restrict__ chi,
+                                                            double* __restrict__ part) {
+  __shared__ double Hs[kToecWarps][8][6][9];
+  __shared__ double red[kToecWarps][kToecOut];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long N = d.N;
+  const bool nh = d.material == 1;
+  double acc[3] = {0.0, 0.0, 0.0};
+  int oi[3][3];
+  int nout = 0;
+  for (int r = 0; r < 3; ++r) {
+    const int q = lane + 32 * r;
+    if (q < kToecOut) {
+      oi[r][0] = cToecIdx[q][0];
+      oi[r][1] = cToecIdx[q][1];
+      oi[r][2] = cToecIdx[q][2];
+      nout = r + 1;
+    }
+  }
+  double (*H)[6][9] = Hs[wid];
+  for (long e = (long)blockIdx.x * kToecWarps + wid; e < N; e += (long)gridDim.x * kToecWarps) {
+    const int k = (int)(e % d.n2), j = (int)((e / d.n2) % d.n1), i = (int)(e / ((long)d.n1 * d.n2));
+    if (lane < 18) {
+      const int I = lane / 3, c = lane - 3 * (lane / 3);
+      double nv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const long nd = ((long)wrap(i + (q & 1), d.n0) * d.n1 + wrap(j + ((q >> 1) & 1), d.n1)) * d.n2 +
+                        wrap(k + (q >> 2), d.n2);
+        nv[q] = chi[((long)I * 3 + c) * N + nd];
+      }
+#pragma unroll
+      for (int g = 0; g < 8; ++g)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          double h = 0.0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h += nv[q] * cDN[g][q][dd];
+          H[g][I][c * 3 + dd] = h + voigt_entry(I, c, dd);
+        }
+    }
+    __syncwarp();
+    const double se = d.s[e];
+    const double ga = d.use_gamma ? d.gamma[e] : 1.0;
+    const double w3 = nh ? se * ga * ga * ga : 0.0;
+    for (int r = 0; r < nout; ++r) {
+      const int I = oi[r][0], J = oi[r][1], K = oi[r][2];
+      const int q = lane + 32 * r;
+      double sum = 0.0;
+      for (int g = 0; g < 8; ++g) {
+        const double* A = H[g][I];
+        const double* B = H[g][J];
+        const double trA = A[0] + A[4] + A[8], trB = B[0] + B[4] + B[8];
+        if (q < 21) {
+          double dd = 0.0, qq = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b2 = 0; b2 < 3; ++b2) {
+              dd += A[a * 3 + b2] * B[a * 3 + b2];
+              qq += A[a * 3 + b2] * B[b2 * 3 + a];
+            }
+          sum += se * (d.lam * trA * trB + d.mu * (dd + qq));
+        } else if (nh) {
+          const double* Cc = H[g][K];
+          const double trC = Cc[0] + Cc[4] + Cc[8];
+          double t1 = 0.0, qAB = 0.0, qBC = 0.0, qCA = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double pac = 0.0;  // (AB + BA)[a][c]
+#pragma unroll
+              for (int b2 = 0; b2 < 3; ++b2) pac += A[a * 3 + b2] * B[b2 * 3 + c] + B[a * 3 + b2] * A[b2 * 3 + c];
+              t1 += pac * Cc[c * 3 + a];
+              qAB += A[a * 3 + c] * B[c * 3 + a];
+              qBC += B[a * 3 + c] * Cc[c * 3 + a];
+              qCA += Cc[a * 3 + c] * A[c * 3 + a];
+            }
+          sum += w3 * (-d.mu * t1 - d.lam * (trA * qBC + trB * qCA + trC * qAB));
+        }
+      }
+      acc[r] += sum;
+    }
+    __syncwarp();  // H is rewritten for the next element
+  }
+  for (int r = 0; r < nout; ++r) red[wid][lane + 32 * r] = acc[r];
+  __syncthreads();
+  for (int q = threadIdx.x; q < kToecOut; q += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < kToecWarps; ++w) s += red[w][q];
+    part[(long)blockIdx.x * kToecOut + q] = s;
+  }
+}
+
+__global__ void k_mech_toec_reduce(const double* __restrict__ part, int nblk, double wq, double* __restrict__ out) {
+  const int q = threadIdx.x;
+  if (q >= kToecOut) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(long)b * kToecOut + q];
+  out[q] = wq * s;
 }
 
 // ---- CG (mech.py:264-290) on z = (w [3][N], macro tail [k]) ------------------------------------------------------
@@ -872,6 +999,129 @@ NLF_API int nlf_mech_grad_w(nlf_mech* H, const double* w, double* Hout, void* st
   NLF_CHECK_LAUNCH();
   if (hd != Hout) NLF_TRY(copy_back(Hout, hd, 72 * N, st));
   NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+NLF_API int nlf_mech_toec(nlf_mech* H, const double* chi, double* C, double* T, void* stream) {
+  if (bad(H) || !chi || !C || !T) {
+    if (H && H->rho_set) set_error("nlf_mech_toec: bad arguments");
+    return NLF_EBADARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = H->d.N;
+  const int nblk = (int)std::min<long>(4 * 148, (N + kToecWarps - 1) / kToecWarps);
+  const size_t o_soa = 0, o_part = al(18 * N * 8), o_out = o_part + al((size_t)nblk * kToecOut * 8);
+  NLF_TRY(H->ws.reserve(o_out + al(kToecOut * 8)));
+  NLF_TRY(H->io.reserve(al(18 * N * 8)));
+  const double* cd = nullptr;
+  NLF_TRY(stage(chi, 18 * N, H->io, 0, &cd, st));
+  char* b = (char*)H->ws.ptr;
+  double* soa = reinterpret_cast<double*>(b + o_soa);
+  double* part = reinterpret_cast<double*>(b + o_part);
+  double* out = reinterpret_cast<double*>(b + o_out);
+  NLF_TRY((launch_aos_to_soa<double, double>(N, 6, cd, soa, 1.0, st)));
+  static bool idx_ready[64] = {};  // the output -> index table, uploaded once per device
+  int dev = 0;
+  NLF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("nlf_mech_toec: device index %d out of range", dev);
+    return NLF_EBADARG;
+  }
+  if (!idx_ready[dev]) {
+    signed char idx[kToecOut][3];
+    int q = 0;
+    for (int I = 0; I < 6; ++I)
+      for (int J = I; J < 6; ++J, ++q) {
+        idx[q][0] = (signed char)I;
+        idx[q][1] = (signed char)J;
+        idx[q][2] = 0;
+      }
+    for (int I = 0; I < 6; ++I)
+      for (int J = I; J < 6; ++J)
+        for (int K = J; K < 6; ++K, ++q) {
+          idx[q][0] = (signed char)I;
+          idx[q][1] = (signed char)J;
+          idx[q][2] = (signed char)K;
+        }
+    NLF_CUDA_TRY(cudaMemcpyToSymbol(cToecIdx, idx, sizeof(idx)));
+    idx_ready[dev] = true;
+  }
+  {
+    ProfScope ps(PK_MECH_ELEM, st);
+    k_mech_toec<<<nblk, kToecThreads, 0, st>>>(H->d, soa, part);
+    NLF_CHECK_LAUNCH();
+    k_mech_toec_reduce<<<1, 128, 0, st>>>(part, nblk, H->d.wq, out);
+    NLF_CHECK_LAUNCH();
+  }
+  double o[kToecOut];
+  NLF_CUDA_TRY(cudaMemcpyAsync(o, out, sizeof(o), cudaMemcpyDeviceToHost, st));
+  NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  // C, f''' as full symmetric arrays, then T = f''' - 3 Sym_IJK C(e_I, voigt(e_J e_K)) (mech.py:482-492)
+  double Cm[6][6], T3[6][6][6];
+  int q = 0;
+  for (int I = 0; I < 6; ++I)
+    for (int J = I; J < 6; ++J, ++q) Cm[I][J] = Cm[J][I] = o[q];
+  for (int I = 0; I < 6; ++I)
+    for (int J = I; J < 6; ++J)
+      for (int K = J; K < 6; ++K, ++q) {
+        const int p[6][3] = {{I, J, K}, {I, K, J}, {J, I, K}, {J, K, I}, {K, I, J}, {K, J, I}};
+        for (auto& x : p) T3[x[0]][x[1]][x[2]] = o[q];
+      }
+  // X[:, J, K] = Voigt vector of the symmetric part of voigt(J) voigt(K)
+  auto vt = [](int I, double (&M)[3][3]) {
+    for (auto& r : M)
+      for (double& x : r) x = 0.0;
+    const int a = I < 3 ? I : (I == 3 ? 1 : 0), bb = I < 3 ? I : (I == 5 ? 1 : 2);
+    if (I < 3) {
+      M[a][a] = 1.0;
+    } else {
+      M[a][bb] = M[bb][a] = 0.5;
+    }
+  };
+  double X[6][6][6];
+  for (int J = 0; J < 6; ++J)
+    for (int K = 0; K < 6; ++K) {
+      double A[3][3], Bm[3][3], P[3][3];
+      vt(J, A);
+      vt(K, Bm);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          P[r][c] = 0.0;
+          for (int m = 0; m < 3; ++m) P[r][c] += A[r][m] * Bm[m][c];
+        }
+      double S[3][3];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) S[r][c] = 0.5 * (P[r][c] + P[c][r]);
+      const double v[6] = {S[0][0], S[1][1], S[2][2], 2 * S[1][2], 2 * S[0][2], 2 * S[0][1]};
+      for (int i = 0; i < 6; ++i) X[i][J][K] = v[i];
+    }
+  double CX[6][6][6];
+  for (int i = 0; i < 6; ++i)
+    for (int J = 0; J < 6; ++J)
+      for (int K = 0; K < 6; ++K) {
+        double a = 0.0;
+        for (int m = 0; m < 6; ++m) a += Cm[i][m] * X[m][J][K];
+        CX[i][J][K] = a;
+      }
+  double Ch[36], Th[216];
+  for (int I = 0; I < 6; ++I)
+    for (int J = 0; J < 6; ++J) {
+      Ch[I * 6 + J] = Cm[I][J];
+      for (int K = 0; K < 6; ++K) {
+        const double sym = (CX[I][J][K] + CX[I][K][J] + CX[J][I][K] + CX[J][K][I] + CX[K][I][J] + CX[K][J][I]) / 6.0;
+        Th[(I * 6 + J) * 6 + K] = T3[I][J][K] - 3.0 * sym;
+      }
+    }
+  if (on_dev(C)) {
+    NLF_CUDA_TRY(cudaMemcpy(C, Ch, sizeof(Ch), cudaMemcpyHostToDevice));
+  } else {
+    std::memcpy(C, Ch, sizeof(Ch));
+  }
+  if (on_dev(T)) {
+    NLF_CUDA_TRY(cudaMemcpy(T, Th, sizeof(Th), cudaMemcpyHostToDevice));
+  } else {
+    std::memcpy(T, Th, sizeof(Th));
+  }
   return NLF_OK;
 }
 

@@ -27,7 +27,7 @@ EXPORTS = (
     "nlf_unet_create", "nlf_unet_destroy", "nlf_unet_param_count", "nlf_unet_get_params", "nlf_unet_set_params",
     "nlf_unet_forward", "nlf_unet_backward", "nlf_unet_adam_step",
     "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
-    "nlf_correctors_vjp",
+    "nlf_correctors_vjp", "nlf_mech_toec",
 )
 
 
@@ -98,6 +98,7 @@ def _load():
         "nlf_density_rho": (I, [P, I, P, P, D, P, P, P, P]),
         "nlf_density_vjp": (I, [P, I, I, P, P, D, P, P, P]),
         "nlf_correctors_vjp": (I, [P, I, P, P, P, I, P, P, P, P, P, P, P]),
+        "nlf_mech_toec": (I, [P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -352,3 +352,28 @@ class Mixed:
         w, F = self.unpack(z, Fb)
         log["z"], log["g0"] = z, g0
         return w, F, log
+
+
+# --- third-order elastic constants (mech.py:458-515) --------------------------------------------------------------
+def toec(cell, chi):
+    """mech.py:458-493: C (6x6) and the Lagrangian-strain third-order constants T (6x6x6) of `cell` from the linear
+    correctors chi (6, nx, ny, nz, 3) of the unit Voigt strains (nlf_mech_toec; f'' and f''' in closed form)."""
+    C = np.empty((6, 6))
+    T = np.empty((6, 6, 6))
+    check(lib.nlf_mech_toec(cell._h, ptr(as_f64(chi)), ptr(C), ptr(T), cell.stream))
+    return C, T
+
+
+CUBIC_TOEC = {  # mech.py:496-503: index triples averaged into each cubic constant
+    "C111": [(0, 0, 0), (1, 1, 1), (2, 2, 2)],
+    "C112": [(0, 0, 1), (0, 0, 2), (1, 1, 0), (1, 1, 2), (2, 2, 0), (2, 2, 1)],
+    "C123": [(0, 1, 2)],
+    "C144": [(0, 3, 3), (1, 4, 4), (2, 5, 5)],
+    "C155": [(0, 4, 4), (0, 5, 5), (1, 3, 3), (1, 5, 5), (2, 3, 3), (2, 4, 4)],
+    "C456": [(3, 4, 5)],
+}
+
+
+def cubic_toec(T):
+    """mech.py:511-515: the six cubic TOECs as means over their index triples."""
+    return {k: float(np.mean([T[i] for i in v])) for k, v in CUBIC_TOEC.items()}

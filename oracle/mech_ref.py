@@ -169,6 +169,70 @@ class Cell:
         return np.fft.irfftn(np.einsum("...ac,...c->...a", Kinv, rh), s=self.shape, axes=(0, 1, 2))
 
 
+# --- third-order elastic constants (nlfiber/mech.py:56-70,458-493) ----------------------------------------------
+VOIGT_PAIRS = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))
+PERMS3 = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+
+
+def voigt_tensor(I):
+    """nlfiber/mech.py:56-64: symmetric 3x3 tensor of the Voigt unit strain I (engineering shear)."""
+    H = np.zeros((3, 3))
+    i, j = VOIGT_PAIRS[I]
+    if i == j:
+        H[i, i] = 1.0
+    else:
+        H[i, j] = H[j, i] = 0.5
+    return H
+
+
+def to_voigt(M):
+    """nlfiber/mech.py:67-70."""
+    S = 0.5 * (M + M.T)
+    return np.array([S[0, 0], S[1, 1], S[2, 2], 2 * S[1, 2], 2 * S[0, 2], 2 * S[0, 1]])
+
+
+def toec_geometric(C):
+    """The geometric correction 3 Sym_IJK C(e_I, voigt(e_J e_K)) of nlfiber/mech.py:482-492."""
+    X = np.zeros((6, 6, 6))
+    for J in range(6):
+        for K in range(6):
+            X[:, J, K] = to_voigt(voigt_tensor(J) @ voigt_tensor(K))
+    CX = np.einsum("ia,ajk->ijk", C, X)
+    return 3.0 * sum(np.transpose(CX, p) for p in PERMS3) / 6.0
+
+
+def toec(cell, chi):
+    """nlfiber/mech.py:458-493: C (6x6) and the Lagrangian-strain third-order constants T (6x6x6) from the linear
+    correctors chi (6, nx, ny, nz, 3): f(s) = wq sum_{g,e} s_e psi_eff(I + sum_I s_I H_I), H_I = voigt(I) +
+    grad chi_I, C = f''(0), T = f'''(0) - 3 Sym(C X). The reference takes f'' and f''' by autodiff; here they are
+    the closed forms at F = I. psi_eff''(I) = psi_lin'' for either material: the WLS factor gamma cancels and the
+    neo-Hookean energy linearises to psi_lin. psi_eff'''(I)[A, B, C] = gamma^3 psi_NH'''(I)[A, B, C], where
+    psi_NH'''(I)[A, B, C] = -mu (tr ABC + tr ACB) - lam (trA tr BC + trB tr CA + trC tr AB); it is zero for the
+    linear material."""
+    lam, mu = cell.lam, cell.mu
+    H = np.stack([voigt_tensor(I) + cell.grad_w(np.asarray(chi[I])) for I in range(6)])  # (6, 8, nx, ny, nz, 3, 3)
+    w = cell.wq * cell.s[None]
+    tr = np.trace(H, axis1=-2, axis2=-1)
+    Ht = np.swapaxes(H, -1, -2)
+    C = np.zeros((6, 6))
+    for I in range(6):
+        for J in range(6):
+            dd = np.sum(H[I] * H[J], axis=(-2, -1)) + np.sum(H[I] * Ht[J], axis=(-2, -1))
+            C[I, J] = np.sum(w * (lam * tr[I] * tr[J] + mu * dd))
+    T3 = np.zeros((6, 6, 6))
+    if cell.material == "neohooke":
+        g3 = w * cell._gam()[None] ** 3
+        mm = lambda A, B: np.einsum("...ab,...bc->...ac", A, B)  # noqa: E731
+        trm = lambda A: np.trace(A, axis1=-2, axis2=-1)  # noqa: E731
+        for I in range(6):
+            for J in range(6):
+                for K in range(6):
+                    t1 = trm(mm(mm(H[I], H[J]), H[K])) + trm(mm(mm(H[I], H[K]), H[J]))
+                    t2 = tr[I] * trm(mm(H[J], H[K])) + tr[J] * trm(mm(H[K], H[I])) + tr[K] * trm(mm(H[I], H[J]))
+                    T3[I, J, K] = np.sum(g3 * (-mu * t1 - lam * t2))
+    return C, T3 - toec_geometric(C)
+
+
 class Mixed:
     """nlfiber/mech.py:195-346: mixed macroscopic control, Newton-CG on z = (w, Fbar_free)."""
 

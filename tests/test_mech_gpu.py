@@ -124,3 +124,27 @@ def test_small_strain_limit_is_linear_C(M):
     assert log["converged"]
     P = c.mean_stress(w, F)
     np.testing.assert_allclose([P[0, 0], P[1, 1], P[2, 2]], C[:3, 0] * e, rtol=2e-3)
+
+
+@pytest.mark.parametrize("material,wls", [("neohooke", (500.0, 0.01)), ("neohooke", None), ("linear", None)])
+def test_toec_matches_oracle(M, material, wls):
+    """nlf_mech_toec (nlfiber/mech.py:458-493) against the oracle's closed forms (pinned by finite differences in
+    test_mech_oracle.py), with the linear correctors of the cell; C from the TOEC path equals the linear C^H of the
+    same cell (the small-strain limit the reference builds in). Tolerance 1e-11: summation order only."""
+    from oracle import linear_ref as OL
+    rho = OD.random_cell(3, n_o=4)[0]
+    cell, ocell = M.Cell(rho, material=material, wls=wls, emin=1e-3), OM.Cell(rho, material=material, wls=wls,
+                                                                              emin=1e-3)
+    lh = OL.LinearHomogenization(rho.shape, emin=1e-3, tol=1e-12, maxit=20000)
+    Clin, u, _ = lh.C_full(rho)
+    C, T = M.toec(cell, u)
+    Co, To = OM.toec(ocell, u)
+    assert rel(C, Co) < 1e-11
+    assert rel(T, To) < 1e-11
+    assert rel(C, Clin) < 1e-9
+    chi = 0.05 * np.random.default_rng(1).standard_normal(u.shape)
+    C2, T2 = M.toec(cell, chi)
+    C2o, T2o = OM.toec(ocell, chi)
+    assert rel(C2, C2o) < 1e-11 and rel(T2, T2o) < 1e-11
+    cub = M.cubic_toec(T)
+    assert set(cub) == {"C111", "C112", "C123", "C144", "C155", "C456"}

@@ -61,3 +61,33 @@ def test_small_strain_solve_matches_linear_C(cell):
     S = np.linalg.inv(C)
     nu0 = -S[1, 0] / S[0, 0]
     assert abs(-(F[1, 1] - 1) / e - nu0) < 1e-3
+
+
+@pytest.mark.parametrize("material,wls", [("neohooke", (500.0, 0.01)), ("neohooke", None), ("linear", None)])
+def test_toec_closed_forms_match_finite_differences(material, wls):
+    """nlfiber/mech.py:458-493 takes C = f''(0) and f'''(0) of f(s) = wq sum s psi_eff(I + sum_I s_I H_I) by
+    autodiff; the oracle's closed forms are checked by central differences of that f (built from the oracle's
+    psi_eff), whose truncation error is O(h^2)."""
+    rng = np.random.default_rng(0)
+    rho = OD.random_cell(1, n_o=2)[0]
+    cell = OM.Cell(rho, material=material, wls=wls, emin=1e-3)
+    chi = 0.05 * rng.standard_normal((6,) + rho.shape + (3,))
+    C, T = OM.toec(cell, chi)
+    T3 = T + OM.toec_geometric(C)
+    H = np.stack([OM.voigt_tensor(I) + cell.grad_w(chi[I]) for I in range(6)])
+
+    def f(sv):
+        F = np.eye(3) + np.tensordot(sv, H, axes=1)
+        return cell.wq * np.sum(cell.s[None] * cell.psi_eff(F, None if cell.gamma is None else cell.gamma[None]))
+
+    e, h = np.eye(6), 1e-3
+    for I in range(6):
+        for J in range(6):
+            fd = (f(h * (e[I] + e[J])) - f(h * (e[I] - e[J])) - f(h * (e[J] - e[I])) + f(-h * (e[I] + e[J]))) / (4 * h * h)
+            assert abs(fd - C[I, J]) <= 1e-5 * np.abs(C).max()
+    h = 2e-3
+    for I, J, K in [(0, 0, 0), (0, 1, 2), (3, 3, 0), (1, 4, 4), (2, 5, 3), (3, 4, 5), (5, 5, 5)]:
+        a, b, c = e[I] * h, e[J] * h, e[K] * h
+        fd = (f(a + b + c) - f(a + b - c) - f(a - b + c) + f(a - b - c) - f(-a + b + c) + f(-a + b - c)
+              + f(-a - b + c) - f(-a - b - c)) / (8 * h ** 3)
+        assert abs(fd - T3[I, J, K]) <= 1e-4 * max(np.abs(T3).max(), 1.0)
