@@ -390,7 +390,34 @@ def mech_arm(args, stream):
     hvp_bytes = N * 8 * (3 + 24 + 3 + 2)
     kernels = {k: {"ms": round(v[0], 2), "launches": v[1]} for k, v in prof.items() if v[1]}
     kernels["profiled_step_cg_iterations"] = int(plog["cg"])
-    return {"mode": "mech", "workload": f"{len(cells)} seeded synthetic {n}^3 cells, compression to "
+    stab = None
+    if args.mech_stability:
+        # stability at the last state of cell 0 (mech.py:363-455): effective tangent (9 CG solves on the GPU)
+        # and its rank-one minimum, then the 4 lowest eigenvalues of the scaled Hessian by LOBPCG
+        import warnings
+        cell = MH.Cell(cells[0], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
+        mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
+        z = None
+        for k in range(1, args.mech_steps + 1):
+            Fb = np.eye(3) if z is None else mix.unpack(z, np.eye(3))[1]
+            Fb[0, 0] = 1.0 - 0.01 * k
+            w, F, log = mix.solve(Fb, z0=z)
+            z = log["z"]
+        t0 = time.perf_counter()
+        A = MH.effective_tangent(cell, w, F, cg_tol=1e-10)
+        torch.cuda.synchronize()
+        t_at = time.perf_counter() - t0
+        rmin, _ = MH.rank_one_min(A)
+        mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
+        t0 = time.perf_counter()
+        vals, _, its = mix.lowest_eigs(z, F, k=4, tol=1e-5, maxiter=2000)
+        torch.cuda.synchronize()
+        t_eig = time.perf_counter() - t0
+        stab = {"effective_tangent_s": round(t_at, 3), "rank_one_min": rmin, "lowest_eigs_s": round(t_eig, 2),
+                "lobpcg_iterations": int(its), "lowest_eigs": [float(x) for x in vals],
+                "timing": "host wall clock; the CG solves, the matvecs and the LOBPCG blocks run on the GPU "
+                          "(the 3m x 3m projected eigenproblems too, through torch)"}
+    return {"mode": "mech", "stability": stab, "workload": f"{len(cells)} seeded synthetic {n}^3 cells, compression to "
             f"{0.01 * args.mech_steps:.2f} in steps of 0.01, lateral stresses free", "precond": args.mech_precond,
             "steps": steps, "seconds": round(ms / 1e3, 2), "steps_per_s": round(steps / (ms / 1e3), 3),
             "newton_per_step": round(newton / max(steps, 1), 2), "cg_per_step": round(cg / max(steps, 1), 1),
@@ -620,6 +647,8 @@ def main():
     ap.add_argument("--mech", action="store_true",
                     help="finite-strain compression path (Newton-CG on the GPU) instead of the default measurement")
     ap.add_argument("--mech-cells", type=int, default=2)
+    ap.add_argument("--mech-stability", action="store_true",
+                    help="with --mech: also time the effective tangent and the lowest eigenvalues of cell 0")
     ap.add_argument("--mech-steps", type=int, default=3)
     ap.add_argument("--uneven", default=None,
                     help="uneven batch 'n1,count1,n2,count2,...' (e.g. 32,128,64,64,128,16) instead of the default")

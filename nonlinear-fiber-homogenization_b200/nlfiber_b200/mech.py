@@ -308,6 +308,86 @@ class Mixed:
         x, it, conv, neg = self._cgA(A, b, dmac, self._sws(), tol, int(maxit))
         return x, it, conv
 
+    # --- stability (mech.py:363-416): the Hessian applied on the GPU (nlf_mech_hvp), LOBPCG on the host --------
+    def _diag_scale(self):
+        """mech.py:395-416: 1 / sqrt(|D| + 1e-30), D the Hessian diagonal at the undeformed state, probed per
+        component with the 8 node colours of the 2x2x2 colouring (24 tangent matvecs) and per macro unknown."""
+        if getattr(self, "_dsc", None) is None:
+            A = self.tangent(self.z0(np.eye(3)), np.eye(3))
+            d = np.zeros(self.nw + self.k)
+            par = np.indices(self.shape) % 2
+            col = par[0] + 2 * par[1] + 4 * par[2]
+            dw = d[: self.nw].reshape(self.shape + (3,))
+            for cc in range(8):
+                for comp in range(3):
+                    e = np.zeros(self.shape + (3,))
+                    e[..., comp] = col == cc
+                    hv = self.hvp_A(A, np.concatenate([e.ravel(), np.zeros(self.k)]))
+                    hv = (hv.cpu().numpy() if _is_dev(hv) else np.asarray(hv))[: self.nw].reshape(self.shape + (3,))
+                    dw[..., comp][col == cc] = hv[..., comp][col == cc]
+            for j in range(self.k):
+                e = np.zeros(self.nw + self.k)
+                e[self.nw + j] = 1.0
+                hv = self.hvp_A(A, e)
+                d[self.nw + j] = float(hv[self.nw + j])
+            self._dsc = 1.0 / np.sqrt(np.abs(d) + 1e-30)
+        return self._dsc
+
+    def lowest_eigs(self, z, Fb, k=4, X=None, tol=1e-5, maxiter=2000):
+        """mech.py:363-393: lowest eigenvalues of D^-1/2 H D^-1/2 (rigid translations excluded). With
+        device="cuda" the LOBPCG iteration runs on the device (`lobpcg_device`); otherwise scipy's LOBPCG as in the
+        reference, each block applied column by column as tangent matvecs on the GPU. Returns (values, vectors
+        in z coordinates, iterations)."""
+        if self.device is not None:
+            return self._lowest_eigs_device(z, Fb, k, X, tol, maxiter)
+        from scipy.sparse.linalg import LinearOperator, lobpcg
+        A = self.tangent(z, np.asarray(Fb, dtype=np.float64))
+        dsc = self._diag_scale()
+        nz = self.nw + self.k
+        T = np.zeros((nz, 3))
+        for i in range(3):
+            T[i:self.nw:3, i] = 1.0
+        Y, _ = np.linalg.qr(T / dsc[:, None])
+
+        def mm(v):
+            V = np.asarray(v, dtype=np.float64).reshape(nz, -1) * dsc[:, None]
+            cols = []
+            for j in range(V.shape[1]):
+                h = self.hvp_A(A, np.ascontiguousarray(V[:, j]))
+                cols.append(h.cpu().numpy() if _is_dev(h) else np.asarray(h))
+            return (np.stack(cols, axis=1) * dsc[:, None]).reshape(np.shape(v))
+
+        op = LinearOperator((nz, nz), matvec=mm, matmat=mm, dtype=np.float64)
+        if X is None:
+            X = np.random.default_rng(0).standard_normal((nz, k))
+        vals, vecs, hist = lobpcg(op, X, Y=Y, largest=False, tol=tol, maxiter=maxiter, retLambdaHistory=True)
+        o = np.argsort(vals)
+        return vals[o], vecs[:, o] * dsc[:, None], len(hist)
+
+    def _lowest_eigs_device(self, z, Fb, k, X, tol, maxiter):
+        import torch
+        dev = self.device
+        A = self.tangent(self._as_state(z), np.asarray(Fb, dtype=np.float64))
+        dsc = torch.as_tensor(self._diag_scale(), device=dev)
+        nz = self.nw + self.k
+        T = torch.zeros((nz, 3), dtype=torch.float64, device=dev)
+        for i in range(3):
+            T[i:self.nw:3, i] = 1.0
+        Y, _ = torch.linalg.qr(T / dsc[:, None])
+
+        def op(V):
+            out = torch.empty_like(V)
+            Vs = V * dsc[:, None]
+            for j in range(V.shape[1]):
+                out[:, j] = self.hvp_A(A, Vs[:, j].contiguous())
+            return out * dsc[:, None]
+
+        if X is None:
+            X = np.random.default_rng(0).standard_normal((nz, k))
+        vals, vecs, its = lobpcg_device(op, torch.as_tensor(np.asarray(X), dtype=torch.float64, device=dev), Y, tol,
+                                        maxiter)
+        return vals, (vecs * dsc[:, None]).cpu().numpy(), its
+
     def solve(self, Fbar, z0=None, rtol=1e-9, maxnewton=30, cg_tol=1e-6, cg_maxit=20000, g_ref=None):
         """mech.py:302-346: Newton-CG. Returns (w, Fbar_full, log) with log['z'] the state."""
         Fb = np.asarray(Fbar, dtype=np.float64)
@@ -352,6 +432,113 @@ class Mixed:
         w, F = self.unpack(z, Fb)
         log["z"], log["g0"] = z, g0
         return w, F, log
+
+
+def effective_tangent(cell, w, Fbar, cg_tol=1e-10, precond="scaled"):
+    """mech.py:419-436: A_abcd = d Pbar_ab / d Fbar_cd at the equilibrium (w, Fbar) under full control. For each
+    unit E_cd: the tangent matvec at (0, E) gives (d grad_w/dF) E and dP/dF E; one CG solve H dz = -(d grad_w/dF)
+    E; then A = dP/dF E + dP/dw dz (all on the GPU). precond "scaled" (node-scaled FFT inverse) or "fft" (the
+    reference's) only changes the CG iteration count; it is left set on the cell afterwards."""
+    full = Mixed(cell, free=[], precond=precond)
+    Fb = np.asarray(Fbar, dtype=np.float64)
+    z = w.reshape(-1) if _is_dev(w) else np.asarray(w, dtype=np.float64).ravel()
+    At = full.tangent(z, Fb)
+    wz = At.w
+    zero = _empty_like_kind(wz, cell.shape + (3,))
+    zero[...] = 0.0
+    A = np.zeros((3, 3, 3, 3))
+    for c in range(3):
+        for d in range(3):
+            E = np.zeros((3, 3))
+            E[c, d] = 1.0
+            hw, dPF = cell.hvp(wz, Fb, zero, E)
+            dz, _, _ = full.solve_linear(At, -hw.reshape(-1), cg_tol)
+            dzw = dz.reshape(cell.shape + (3,))
+            _, dPz = cell.hvp(wz, Fb, dzw.contiguous() if _is_dev(dzw) else np.ascontiguousarray(dzw), np.zeros((3, 3)))
+            A[:, :, c, d] = dPF + dPz
+    return A
+
+
+def lobpcg_device(op, X, Y=None, tol=1e-5, maxiter=2000):
+    """The smallest eigenpairs of a symmetric operator by LOBPCG (Knyazev, SIAM J. Sci. Comput. 23 (2001)), with
+    every block on the device: op maps an (n, m) CUDA tensor to A times it; X (n, m) starts the iteration; Y
+    (n, c), orthonormal, spans a constraint space the iterates stay orthogonal to. Each iteration forms
+    W = A X - X diag(theta) (columns of converged pairs are dropped), orthonormalises [X, W, P] by QR (columns
+    scaled to unit norm first; P is dropped for the step if the block is numerically rank deficient), and solves
+    the projected 3m x 3m eigenproblem; A applied to the new basis is recombined from A X, A W and A P, so one
+    block application (of W) per iteration; the operator is applied as P A P, P the projector onto the complement
+    of Y (as scipy's constrained LOBPCG). Stops when every residual norm is at most tol. Returns (eigenvalues
+    ascending as a NumPy array, eigenvectors (n, m), iterations)."""
+    import torch
+
+    def cons(V):
+        return V if Y is None else V - Y @ (Y.T @ V)
+
+    def opc(V):  # the operator restricted to the complement of Y (P A P)
+        return cons(op(cons(V))) if Y is not None else op(V)
+
+    m = X.shape[1]
+    X = cons(X)
+    X, _ = torch.linalg.qr(X)
+    AX = opc(X)
+    G = X.T @ AX
+    th, C = torch.linalg.eigh(0.5 * (G + G.T))
+    X, AX = X @ C, AX @ C
+    P = AP = None
+    it = 0
+    for it in range(1, maxiter + 1):
+        R = AX - X * th[None, :]
+        rn = torch.linalg.vector_norm(R, dim=0)
+        active = rn > tol
+        if not bool(active.any()):
+            break
+        W = cons(R[:, active])
+        W = W / torch.linalg.vector_norm(W, dim=0).clamp_min(1e-300)[None, :]
+        AW = opc(W)
+        blocks, ablocks = [X, W], [AX, AW]
+        if P is not None:
+            pn = torch.linalg.vector_norm(P, dim=0).clamp_min(1e-300)[None, :]
+            blocks.append(P / pn)
+            ablocks.append(AP / pn)
+        S, AS = torch.cat(blocks, dim=1), torch.cat(ablocks, dim=1)
+        Q, Rq = torch.linalg.qr(S)
+        d = torch.abs(torch.diagonal(Rq))
+        if P is not None and bool((d < 1e-10 * d.max()).any()):
+            S, AS = torch.cat(blocks[:2], dim=1), torch.cat(ablocks[:2], dim=1)
+            Q, Rq = torch.linalg.qr(S)
+        AQ = torch.linalg.solve_triangular(Rq, AS, upper=True, left=False)
+        G = Q.T @ AQ
+        w, V = torch.linalg.eigh(0.5 * (G + G.T))
+        th, C = w[:m], V[:, :m]
+        Xn, AXn = Q @ C, AQ @ C
+        P, AP = Q[:, m:] @ C[m:, :], AQ[:, m:] @ C[m:, :]
+        X, AX = Xn, AXn
+    o = torch.argsort(th)
+    return th[o].cpu().numpy(), X[:, o], it
+
+
+def fibonacci_sphere(m):
+    """mech.py:439-443."""
+    i = np.arange(m) + 0.5
+    polar = np.arccos(1.0 - 2.0 * i / m)
+    az = np.pi * (1.0 + 5.0 ** 0.5) * i
+    return np.stack([np.cos(az) * np.sin(polar), np.sin(az) * np.sin(polar), np.cos(polar)], axis=1)
+
+
+def rank_one_min(A, m=1000, plane=False):
+    """mech.py:446-455: min over unit n of the smallest eigenvalue of Q_ik = A_ijkl n_j n_l (host, 3x3 work)."""
+    if plane:
+        th = np.linspace(0.0, np.pi, m, endpoint=False)
+        ns = np.stack([np.cos(th), np.sin(th), np.zeros_like(th)], axis=1)
+    else:
+        ns = fibonacci_sphere(m)
+    Q = np.einsum("ijkl,nj,nl->nik", A, ns, ns)
+    Q = 0.5 * (Q + np.swapaxes(Q, 1, 2))
+    if plane:
+        Q = Q[:, :2, :2]
+    ev = np.linalg.eigvalsh(Q)[:, 0]
+    i = int(np.argmin(ev))
+    return float(ev[i]), ns[i]
 
 
 # --- third-order elastic constants (mech.py:458-515) --------------------------------------------------------------

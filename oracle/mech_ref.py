@@ -359,6 +359,98 @@ class Mixed:
         return w, F, log
 
 
+# --- stability (nlfiber/mech.py:363-455) ---------------------------------------------------------------------------
+def diag_scale(mix):
+    """nlfiber/mech.py:395-416: 1 / sqrt(|D| + 1e-30), D the Hessian diagonal at the undeformed state (Fbar = I,
+    z = z0), probed per component with the 8 node colours of the 2x2x2 colouring (nodes of one colour do not
+    share an element on an even grid) and per macro unknown with its unit vector."""
+    Fb = I3
+    z = mix.z0(Fb)
+    d = np.zeros(mix.nw + mix.k)
+    par = np.indices(mix.shape) % 2
+    col = par[0] + 2 * par[1] + 4 * par[2]
+    dw = d[: mix.nw].reshape(mix.shape + (3,))
+    for cc in range(8):
+        for comp in range(3):
+            e = np.zeros(mix.shape + (3,))
+            e[..., comp] = col == cc
+            hv = mix.hvp(z, Fb, np.concatenate([e.ravel(), np.zeros(mix.k)]))[: mix.nw].reshape(mix.shape + (3,))
+            dw[..., comp][col == cc] = hv[..., comp][col == cc]
+    for j in range(mix.k):
+        e = np.zeros(mix.nw + mix.k)
+        e[mix.nw + j] = 1.0
+        d[mix.nw + j] = mix.hvp(z, Fb, e)[mix.nw + j]
+    return 1.0 / np.sqrt(np.abs(d) + 1e-30)
+
+
+def lowest_eigs(mix, z, Fb, k=4, X=None, tol=1e-5, maxiter=2000):
+    """nlfiber/mech.py:363-393: the lowest eigenvalues of D^-1/2 H D^-1/2 by LOBPCG (scipy), the 3 rigid
+    translations excluded as constraints. Returns (values, vectors in z coordinates, iterations)."""
+    from scipy.sparse.linalg import LinearOperator, lobpcg
+    dsc = diag_scale(mix)
+    nz = mix.nw + mix.k
+    T = np.zeros((nz, 3))
+    for i in range(3):
+        T[i:mix.nw:3, i] = 1.0
+    Y, _ = np.linalg.qr(T / dsc[:, None])
+
+    def mm(v):
+        V = np.asarray(v, dtype=np.float64).reshape(nz, -1) * dsc[:, None]
+        out = np.stack([mix.hvp(z, Fb, V[:, j]) for j in range(V.shape[1])], axis=1) * dsc[:, None]
+        return out.reshape(np.shape(v))
+
+    op = LinearOperator((nz, nz), matvec=mm, matmat=mm, dtype=np.float64)
+    if X is None:
+        X = np.random.default_rng(0).standard_normal((nz, k))
+    vals, vecs, hist = lobpcg(op, X, Y=Y, largest=False, tol=tol, maxiter=maxiter, retLambdaHistory=True)
+    o = np.argsort(vals)
+    return vals[o], vecs[:, o] * dsc[:, None], len(hist)
+
+
+def effective_tangent(cell, w, Fbar, cg_tol=1e-10, cg_maxit=20000):
+    """nlfiber/mech.py:419-436: A_abcd = d Pbar_ab / d Fbar_cd at the equilibrium (w, Fbar) under full control:
+    for each unit E_cd, H dz = -(d grad_w / dF) E (one CG solve), A = dP/dF E + dP/dw dz."""
+    full = Mixed(cell, free=[])
+    Fb = np.asarray(Fbar, dtype=np.float64)
+    z = np.asarray(w, dtype=np.float64).ravel()
+    zero = np.zeros(cell.shape + (3,))
+    A = np.zeros((3, 3, 3, 3))
+    for c in range(3):
+        for d in range(3):
+            E = np.zeros((3, 3))
+            E[c, d] = 1.0
+            hw, dPF = cell.hvp(w, Fb, zero, E)
+            dz, _, _, _ = full.cg(z, Fb, -hw.ravel(), np.zeros(0), full._sws(), cg_tol, cg_maxit)
+            _, dPz = cell.hvp(w, Fb, dz.reshape(cell.shape + (3,)), np.zeros((3, 3)))
+            A[:, :, c, d] = dPF + dPz
+    return A
+
+
+def fibonacci_sphere(m):
+    """nlfiber/mech.py:439-443: m nearly uniform unit vectors."""
+    i = np.arange(m) + 0.5
+    polar = np.arccos(1.0 - 2.0 * i / m)
+    az = np.pi * (1.0 + 5.0 ** 0.5) * i
+    return np.stack([np.cos(az) * np.sin(polar), np.sin(az) * np.sin(polar), np.cos(polar)], axis=1)
+
+
+def rank_one_min(A, m=1000, plane=False):
+    """nlfiber/mech.py:446-455: min over unit n of the smallest eigenvalue of the acoustic tensor
+    Q_ik = A_ijkl n_j n_l (n in the x-y plane for 2D cells). Returns (value, n)."""
+    if plane:
+        th = np.linspace(0.0, np.pi, m, endpoint=False)
+        ns = np.stack([np.cos(th), np.sin(th), np.zeros_like(th)], axis=1)
+    else:
+        ns = fibonacci_sphere(m)
+    Q = np.einsum("ijkl,nj,nl->nik", A, ns, ns)
+    Q = 0.5 * (Q + np.swapaxes(Q, 1, 2))
+    if plane:
+        Q = Q[:, :2, :2]
+    ev = np.linalg.eigvalsh(Q)[:, 0]
+    i = int(np.argmin(ev))
+    return float(ev[i]), ns[i]
+
+
 def linesearch(E, gnorm, x, dx, E0, slope, gn):
     """mech.py:73-85."""
     tol = 64 * np.finfo(np.float64).eps * max(abs(E0), 1e-300)

@@ -148,3 +148,40 @@ def test_toec_matches_oracle(M, material, wls):
     assert rel(C2, C2o) < 1e-11 and rel(T2, T2o) < 1e-11
     cub = M.cubic_toec(T)
     assert set(cub) == {"C111", "C112", "C123", "C144", "C155", "C456"}
+
+
+@pytest.mark.parametrize("n_o", [2, 4])
+def test_stability_matches_oracle(M, n_o):
+    """nlfiber/mech.py:363-455 on the GPU matvec: the probed Hessian diagonal, LOBPCG's lowest eigenvalues of the
+    scaled Hessian at a deformed equilibrium, the effective tangent (9 CG solves) and its rank-one minimum,
+    against the oracle's restatements (pinned in test_mech_oracle.py) at the same state."""
+    import warnings
+    rho = OD.random_cell(4, n_o=n_o)[0]
+    cell, ocell = M.Cell(rho, emin=1e-3), OM.Cell(rho, emin=1e-3)
+    ofull = OM.Mixed(ocell, free=[])
+    w, F, log = ofull.solve(np.diag([1.03, 1.0, 1.0]), rtol=1e-12, cg_tol=1e-12)
+    assert log["converged"]
+    A = M.effective_tangent(cell, w, F, cg_tol=1e-13)
+    Ao = OM.effective_tangent(ocell, w, F, cg_tol=1e-13)
+    assert rel(A, Ao) < 1e-9
+    v, n = M.rank_one_min(A)
+    vo, no = OM.rank_one_min(Ao)
+    assert abs(v - vo) <= 1e-9 * abs(vo)
+    mix, omix = M.Mixed(cell), OM.Mixed(ocell)
+    assert rel(mix._diag_scale(), OM.diag_scale(omix)) < 1e-12
+    z = omix.z0(F)
+    z[: omix.nw] = w.ravel()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        vals, vecs, it = mix.lowest_eigs(z, F, k=4, tol=1e-8)
+        ovals, _, _ = OM.lowest_eigs(omix, z, F, k=4, tol=1e-8)
+    np.testing.assert_allclose(vals, ovals, rtol=1e-6)
+    assert vecs.shape == (omix.nw + omix.k, 4)
+    # the device-resident LOBPCG (state, blocks and matvecs on the GPU)
+    import torch
+    dmix = M.Mixed(cell, device="cuda")
+    # (a residual of 1e-8 is below this operator's rounding floor, where scipy's LOBPCG stops at maxiter too; at
+    # 1e-6 the triply degenerate lowest cluster of these cubic cells is pinned to ~1e-6 relative)
+    dvals, dvecs, dit = dmix.lowest_eigs(torch.as_tensor(z, device="cuda"), F, k=4, tol=1e-6)
+    np.testing.assert_allclose(dvals, ovals, rtol=1e-5)
+    assert dit < 2000 and dvecs.shape == (omix.nw + omix.k, 4)

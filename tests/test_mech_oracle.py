@@ -91,3 +91,56 @@ def test_toec_closed_forms_match_finite_differences(material, wls):
         fd = (f(a + b + c) - f(a + b - c) - f(a - b + c) + f(a - b - c) - f(-a + b + c) + f(-a + b - c)
               + f(-a - b + c) - f(-a - b - c)) / (8 * h ** 3)
         assert abs(fd - T3[I, J, K]) <= 1e-4 * max(np.abs(T3).max(), 1.0)
+
+
+def _stab_cell():
+    return OM.Cell(OD.random_cell(4, n_o=2)[0], emin=1e-3)
+
+
+def test_effective_tangent_matches_finite_differences():
+    """nlfiber/mech.py:419-436: A = dPbar/dFbar of the re-equilibrated cell (full control), against central
+    differences of the mean stress of Newton solves at Fbar +- h E (h = 1e-4: the error is O(h^2), 2.6e-9 here;
+    at h = 1e-5 the perturbed Newton solve stalls on its relative tolerance)."""
+    cell = _stab_cell()
+    full = OM.Mixed(cell, free=[])
+    w, F, log = full.solve(np.diag([1.03, 1.0, 1.0]), rtol=1e-12, cg_tol=1e-12)
+    assert log["converged"]
+    A = OM.effective_tangent(cell, w, F, cg_tol=1e-13)
+    h = 1e-4
+    for c, d in ((0, 0), (1, 2), (2, 1), (0, 1)):
+        E = np.zeros((3, 3))
+        E[c, d] = 1.0
+        wp, Fp, _ = full.solve(F + h * E, z0=w.ravel(), rtol=1e-13, cg_tol=1e-13)
+        wm, Fm, _ = full.solve(F - h * E, z0=w.ravel(), rtol=1e-13, cg_tol=1e-13)
+        fd = (cell.mean_stress(wp, Fp) - cell.mean_stress(wm, Fm)) / (2 * h)
+        assert np.abs(fd - A[:, :, c, d]).max() <= 2e-8
+
+
+def test_lowest_eigs_match_dense_spectrum():
+    """nlfiber/mech.py:363-416: the probed diagonal is the Hessian's diagonal, and LOBPCG's lowest eigenvalues of
+    D^-1/2 H D^-1/2 (translations excluded) are those of the dense operator restricted to the complement."""
+    cell = _stab_cell()
+    mix = OM.Mixed(cell)
+    z, Fb = mix.z0(np.eye(3)), np.eye(3)
+    vals, _, _ = OM.lowest_eigs(mix, z, Fb, k=4, tol=1e-8, maxiter=2000)
+    dsc = OM.diag_scale(mix)
+    nz = mix.nw + mix.k
+    Hd = np.stack([mix.hvp(z, Fb, np.eye(nz)[:, j]) for j in range(nz)], axis=1)
+    assert np.abs(1.0 / np.sqrt(np.abs(np.diag(Hd)) + 1e-30) - dsc).max() <= 1e-14 * dsc.max()
+    S = dsc[:, None] * Hd * dsc[None, :]
+    T = np.zeros((nz, 3))
+    for i in range(3):
+        T[i:mix.nw:3, i] = 1.0
+    Y, _ = np.linalg.qr(T / dsc[:, None])
+    Qf, _ = np.linalg.qr(np.concatenate([Y, np.random.default_rng(1).standard_normal((nz, nz - 3))], axis=1))
+    ev = np.linalg.eigvalsh(Qf[:, 3:].T @ (0.5 * (S + S.T)) @ Qf[:, 3:])[:4]
+    np.testing.assert_allclose(vals, ev, rtol=1e-7)
+
+
+def test_rank_one_min_isotropic():
+    """The acoustic tensor of isotropic linear elasticity has smallest eigenvalue mu for every direction."""
+    lam, mu = OL.lame(1.0, 0.3)
+    d = np.eye(3)
+    A = (lam * np.einsum("ij,kl->ijkl", d, d) + mu * (np.einsum("ik,jl->ijkl", d, d) + np.einsum("il,jk->ijkl", d, d)))
+    v, n = OM.rank_one_min(A, m=200)
+    assert abs(v - mu) < 1e-12 and abs(np.linalg.norm(n) - 1.0) < 1e-12
