@@ -131,6 +131,13 @@ def unit_bytes(kind, N, NS, m):
     }.get(kind.rsplit("_", 1)[0])
 
 
+# DRAM bytes per vector of a kernel class at 64^3, from one ncu --set full capture on the small profiling case
+# (`bench.py --ncu --cells 4 --iters 8`, one launch of 24 vectors; the full workload is too large to capture),
+# scaled to a launch by the vectors it processes: k_fc_pipe<64> (fused pass C) read 466.1 MB and wrote
+# 247.3 MB for 24 vectors.
+NCU_TRAFFIC_PER_VECTOR_64 = {"fft_c_f64": (466.139904e6 + 247.341312e6) / 24}
+
+
 def roofline(prof, N, NS, m, peaks, peak_kind):
     tot = sum(v[0] for v in prof.values())
     best, best_ms = None, -1.0
@@ -145,11 +152,14 @@ def roofline(prof, N, NS, m, peaks, peak_kind):
     bytes_total = un * unit_bytes(best, N, NS, m)
     achieved = bytes_total / (ms * 1e-3) / 1e9
     peak = float(peaks["hbm_gbs"])
+    tv = NCU_TRAFFIC_PER_VECTOR_64.get(best) if N == 64 ** 3 else None
     return {"kernel": best, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "peak_kind": "of measured copy bandwidth" if peak_kind == "measured" else "of fallback 6650 GB/s",
             "avg_launch_ms": round(ms / max(la, 1), 4),
-            "algorithmic_bytes_per_launch": round(bytes_total / max(la, 1)), "traffic": None}, kernels
+            "algorithmic_bytes_per_launch": round(bytes_total / max(la, 1)),
+            "traffic": round(tv * un / max(la, 1)) if tv else None,
+            "traffic_source": "ncu capture of the small profiling case, scaled by vectors per launch" if tv else None}, kernels
 
 
 def cpu_reference(cells, sample_iters=2):
