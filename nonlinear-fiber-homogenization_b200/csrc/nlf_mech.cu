@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include "nlf_vec.cuh"
 #include "nlf_prof.cuh"
@@ -1021,30 +1022,34 @@ NLF_API int nlf_mech_toec(nlf_mech* H, const double* chi, double* C, double* T, 
   double* out = reinterpret_cast<double*>(b + o_out);
   NLF_TRY((launch_aos_to_soa<double, double>(N, 6, cd, soa, 1.0, st)));
   static bool idx_ready[64] = {};  // the output -> index table, uploaded once per device
+  static std::mutex idx_mu;
   int dev = 0;
   NLF_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) {
     set_error("nlf_mech_toec: device index %d out of range", dev);
     return NLF_EBADARG;
   }
-  if (!idx_ready[dev]) {
-    signed char idx[kToecOut][3];
-    int q = 0;
-    for (int I = 0; I < 6; ++I)
-      for (int J = I; J < 6; ++J, ++q) {
-        idx[q][0] = (signed char)I;
-        idx[q][1] = (signed char)J;
-        idx[q][2] = 0;
-      }
-    for (int I = 0; I < 6; ++I)
-      for (int J = I; J < 6; ++J)
-        for (int K = J; K < 6; ++K, ++q) {
+  {
+    std::lock_guard<std::mutex> lock(idx_mu);
+    if (!idx_ready[dev]) {
+      signed char idx[kToecOut][3];
+      int q = 0;
+      for (int I = 0; I < 6; ++I)
+        for (int J = I; J < 6; ++J, ++q) {
           idx[q][0] = (signed char)I;
           idx[q][1] = (signed char)J;
-          idx[q][2] = (signed char)K;
+          idx[q][2] = 0;
         }
-    NLF_CUDA_TRY(cudaMemcpyToSymbol(cToecIdx, idx, sizeof(idx)));
-    idx_ready[dev] = true;
+      for (int I = 0; I < 6; ++I)
+        for (int J = I; J < 6; ++J)
+          for (int K = J; K < 6; ++K, ++q) {
+            idx[q][0] = (signed char)I;
+            idx[q][1] = (signed char)J;
+            idx[q][2] = (signed char)K;
+          }
+      NLF_CUDA_TRY(cudaMemcpyToSymbol(cToecIdx, idx, sizeof(idx)));
+      idx_ready[dev] = true;
+    }
   }
   {
     ProfScope ps(PK_MECH_ELEM, st);

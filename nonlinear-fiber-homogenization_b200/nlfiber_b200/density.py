@@ -144,13 +144,14 @@ class GpuDensityMap:
         h = ctypes.c_void_p()
         check(lib.nlf_density_create(ctypes.byref(h), self.n_o, self.r))
         self._h = h
+        self._lib = lib  # kept for __del__, which may run while the interpreter shuts down
         self.orbits = int(lib.nlf_density_orbits(h))
         self.stream = None
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            from ._lib import lib
+        lib = getattr(self, "_lib", None)
+        if h is not None and h.value and lib is not None:
             lib.nlf_density_destroy(h)
             self._h = None
 
