@@ -38,8 +38,9 @@ typedef struct nlf_mech nlf_mech;
 /* Preconditioner. */
 #define NLF_PC_FFT 0        /* the reference's unit-stiffness FFT inverse (nlfiber/linear.py:154-170) */
 #define NLF_PC_FFT_SCALED 1 /* S^-a K0^-1 S^-a, a = 0.47, with S the root mean square of the stiffness scales
-                               of the 8 elements around each node (same converged solution, far fewer
-                               iterations at high contrast) */
+                               of the 8 elements around each node and K0 the unit operator of a reference
+                               medium with Poisson ratio 0 (same converged solution, far fewer iterations at
+                               high contrast) */
 
 typedef struct nlf_solve_opts {
   int precision;     /* NLF_PREC_* */
@@ -96,8 +97,9 @@ NLF_API int nlf_load(nlf_linear* h, const double* s, const double* Es, int m, do
 NLF_API int nlf_precond(nlf_linear* h, int nvec, const double* r, double* z, void* stream);
 
 /* precond in a chosen arithmetic and preconditioner: precond NLF_PC_FFT (s ignored, may be NULL) or
- * NLF_PC_FFT_SCALED (s: the cell's stiffness scale (nx, ny, nz); z = w irfftn(Kinv rfftn(w r)) with
- * w = (root mean square of s over the 8 elements around each node)^-0.47). */
+ * NLF_PC_FFT_SCALED (s: the cell's stiffness scale (nx, ny, nz); z = w irfftn(Kinv0 rfftn(w r)) with
+ * w = (root mean square of s over the 8 elements around each node)^-0.47 and Kinv0 the symbol inverse of the
+ * same element with Poisson ratio 0). */
 NLF_API int nlf_precond_ex(nlf_linear* h, int nvec, const double* r, double* z, int precision, int precond,
                            const double* s, void* stream);
 
@@ -175,8 +177,8 @@ NLF_API int nlf_mech_hvp(nlf_mech* h, const double* w, const double* Fbar, const
 /* mech.py:172-189 precond_w: inverse of the homogeneous unit-stiffness operator (N x the linear symbol). */
 NLF_API int nlf_mech_precond_w(nlf_mech* h, const double* r, double* z, void* stream);
 /* Preconditioner of nlf_mech_cg and nlf_mech_precond_w: NLF_PC_FFT (default) is the reference's
- * N K0^-1 / sws (mech.py:264-294); NLF_PC_FFT_SCALED is N w K0^-1 w with w the node stiffness scaling of
- * nlf_precond_ex (sws then unused). Same Newton-CG solution to the same tolerances; far fewer CG iterations
+ * N K0^-1 / sws (mech.py:264-294); NLF_PC_FFT_SCALED is N w K0'^-1 w with w the node stiffness scaling and K0'
+ * the Poisson-ratio-0 reference medium of nlf_precond_ex (sws then unused). Same Newton-CG solution to the same tolerances; far fewer CG iterations
  * at high contrast. No counterpart in the reference. */
 NLF_API int nlf_mech_set_precond(nlf_mech* h, int precond);
 /* mech.py:127-129 grad_w: displacement gradient at the Gauss points, H (8, nx, ny, nz, 3, 3). */

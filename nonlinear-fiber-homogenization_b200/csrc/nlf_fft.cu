@@ -1266,7 +1266,9 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   }
   if (stages & 2) {
     ProfScope ps(PK_FFTB64, st);
-    k_fb_fast<N><<<dim3(N / F::KY, F::KZC, nvec), F::NTB, 0, st>>>(spec, h.t64.kinv, m, twx, cs, units, PK_FFTB64,
+    // the scaled preconditioner (w given) inverts its own reference medium
+    k_fb_fast<N><<<dim3(N / F::KY, F::KZC, nvec), F::NTB, 0, st>>>(spec, w ? h.t64s.kinv : h.t64.kinv, m, twx, cs,
+                                                                     units, PK_FFTB64,
                                                                      fu);
     NLF_CHECK_LAUNCH();
   }
@@ -1333,12 +1335,13 @@ template <>
 cplx<double>* twiddles<double>(const LinearHandle& h) { return h.t64.tw; }
 template <>
 cplx<float>* twiddles<float>(const LinearHandle& h) { return h.t32.tw; }
+// Kinv of the material (the reference's preconditioner) or of the scaled preconditioner's reference medium
 template <typename T>
-static const T* kinv_table(const LinearHandle& h);
+static const T* kinv_table(const LinearHandle& h, bool scaled);
 template <>
-const double* kinv_table<double>(const LinearHandle& h) { return h.t64.kinv; }
+const double* kinv_table<double>(const LinearHandle& h, bool scaled) { return scaled ? h.t64s.kinv : h.t64.kinv; }
 template <>
-const float* kinv_table<float>(const LinearHandle& h) { return h.t32.kinv; }
+const float* kinv_table<float>(const LinearHandle& h, bool scaled) { return scaled ? h.t32s.kinv : h.t32.kinv; }
 
 template <typename T>
 static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx<T>* spec, const T* w,
@@ -1379,7 +1382,7 @@ static int precond_impl(const LinearHandle& h, int nvec, int m, T* r, T* z, cplx
   {
     const int kind = f32 ? PK_FFTB32 : PK_FFTB64;
     ProfScope ps(kind, st);
-    k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h), d, kc, m, tw,
+    k_fft_b<T><<<dim3(d.n1, (d.n2h + kc - 1) / kc, nvec), nt, smemb, st>>>(spec, kinv_table<T>(h, w != nullptr), d, kc, m, tw,
                                                                           cs, units, kind, fu);
     NLF_CHECK_LAUNCH();
   }
@@ -1522,10 +1525,14 @@ int build_tables(LinearHandle& h) {
   NLF_CUDA_TRY(cudaMemcpy(h.t32.tw, t32.data(), t32.size() * sizeof(cplx<float>), cudaMemcpyHostToDevice));
   NLF_CUDA_TRY(cudaMalloc(&h.t64.kinv, g.NS * 6 * sizeof(double)));
   NLF_CUDA_TRY(cudaMalloc(&h.t32.kinv, g.NS * 6 * sizeof(float)));
+  NLF_CUDA_TRY(cudaMalloc(&h.t64s.kinv, g.NS * 6 * sizeof(double)));
+  NLF_CUDA_TRY(cudaMalloc(&h.t32s.kinv, g.NS * 6 * sizeof(float)));
   double* dW = nullptr;
-  NLF_CUDA_TRY(cudaMalloc(&dW, sizeof(h.W27)));
+  NLF_CUDA_TRY(cudaMalloc(&dW, 2 * sizeof(h.W27)));
   NLF_CUDA_TRY(cudaMemcpy(dW, h.W27, sizeof(h.W27), cudaMemcpyHostToDevice));
+  NLF_CUDA_TRY(cudaMemcpy(dW + 27 * 9, h.W27s, sizeof(h.W27s), cudaMemcpyHostToDevice));
   k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW, g.n0, g.n1, g.n2, g.n2h, h.t64.kinv, h.t32.kinv);
+  k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW + 27 * 9, g.n0, g.n1, g.n2, g.n2h, h.t64s.kinv, h.t32s.kinv);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   cudaFree(dW);

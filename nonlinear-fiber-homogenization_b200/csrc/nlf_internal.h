@@ -37,6 +37,11 @@ constexpr int kEnergyWindow = 32;
 // exponent of the node scaling of the scaled preconditioner, w = S^-kNodeScaleExp
 constexpr double kNodeScaleExp = 0.47;
 
+// Poisson ratio of the reference medium whose FFT inverse the scaled preconditioner wraps (its Young's modulus
+// does not matter: PCG is invariant to scaling the preconditioner). The unscaled preconditioner keeps the
+// material's own (E, nu), as the reference does.
+constexpr double kScaledRefNu = 0.0;
+
 // Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188).
 struct CellState {
   int it;
@@ -72,9 +77,12 @@ struct LinearHandle {
   double Gm[6][24];
   double Dm[6][6];
   double W27[27][9];  // unit-stiffness stencil blocks W_d, d = (dx+1)*9 + (dy+1)*3 + (dz+1)
+  double W27s[27][9];  // the same for the scaled preconditioner's reference medium (Poisson ratio kScaledRefNu)
   Twiddle tw;
   Tables<double> t64;
   Tables<float> t32;
+  Tables<double> t64s;  // Kinv of the scaled preconditioner's reference medium (twiddles shared with t64)
+  Tables<float> t32s;
   DevBuf ws;          // solver workspace
   DevBuf io;          // staging for host <-> device copies
   DevBuf io2;

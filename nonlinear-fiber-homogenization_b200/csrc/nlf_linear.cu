@@ -133,14 +133,48 @@ static void element_matrices(LinearHandle& h) {
       for (int j = 0; j < 24; ++j) h.Gm[i][j] += DB[i][j] / 8.0;
   }
   // 27-point stencil blocks of the unit-stiffness operator: W_d = sum_{a,b: off_a - off_b = d} Ke_ab
-  std::memset(h.W27, 0, sizeof(h.W27));
-  for (int a = 0; a < 8; ++a)
-    for (int b = 0; b < 8; ++b) {
-      const int dx = (a & 1) - (b & 1), dy = ((a >> 1) & 1) - ((b >> 1) & 1), dz = (a >> 2) - (b >> 2);
-      double* W = h.W27[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) W[r * 3 + c] += h.Ke[3 * a + r][3 * b + c];
+  auto stencil = [](const double (&K)[24][24], double (&W27)[27][9]) {
+    std::memset(W27, 0, sizeof(W27));
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        const int dx = (a & 1) - (b & 1), dy = ((a >> 1) & 1) - ((b >> 1) & 1), dz = (a >> 2) - (b >> 2);
+        double* W = W27[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)];
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) W[r * 3 + c] += K[3 * a + r][3 * b + c];
+      }
+  };
+  stencil(h.Ke, h.W27);
+  // the scaled preconditioner's reference medium: the same element with Poisson ratio kScaledRefNu
+  {
+    const double nu0 = kScaledRefNu, lam0 = h.E * nu0 / ((1.0 + nu0) * (1.0 - 2.0 * nu0)),
+                 mu0 = h.E / (2.0 * (1.0 + nu0));
+    double D0[6][6] = {}, K0[24][24] = {};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) D0[i][j] = lam0;
+    for (int i = 0; i < 3; ++i) D0[i][i] = lam0 + 2 * mu0;
+    for (int i = 3; i < 6; ++i) D0[i][i] = mu0;
+    for (int g = 0; g < 8; ++g) {
+      double B[6][24] = {};
+      for (int a = 0; a < 8; ++a) {
+        const double dx = dN[g][a][0], dy = dN[g][a][1], dz = dN[g][a][2];
+        const int c = 3 * a;
+        B[0][c] = dx;
+        B[1][c + 1] = dy;
+        B[2][c + 2] = dz;
+        B[3][c + 1] = dz;
+        B[3][c + 2] = dy;
+        B[4][c + 0] = dz;
+        B[4][c + 2] = dx;
+        B[5][c + 0] = dy;
+        B[5][c + 1] = dx;
+      }
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j)
+          for (int k = 0; k < 6; ++k)
+            for (int l = 0; l < 6; ++l) K0[i][j] += B[k][i] * D0[k][l] * B[l][j] / 8.0;
     }
+    stencil(K0, h.W27s);
+  }
 }
 
 // ---- PCG ---------------------------------------------------------------------------------------------------------
@@ -809,6 +843,8 @@ NLF_API int nlf_linear_destroy(nlf_linear* H) {
     if (e) cudaEventDestroy(e);
   cudaFree(h.t64.kinv);
   cudaFree(h.t32.kinv);
+  cudaFree(h.t64s.kinv);
+  cudaFree(h.t32s.kinv);
   cudaFree(h.t64.tw);
   cudaFree(h.t32.tw);
   h.ws.release();

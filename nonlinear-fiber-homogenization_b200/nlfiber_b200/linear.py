@@ -10,8 +10,8 @@ xy, engineering shear. For a macroscopic strain E_I the periodic corrector u_I s
 C_IJ = (1/N_e) sum_e s_e b_e(E_I + u_I, E_J + u_J) (nlfiber/linear.py:1-13).
 
 Beyond the reference: `precision="mixed"` (FP32 operator and PCG inside FP64 iterative refinement),
-`precond="scaled"` (the FFT preconditioner wrapped in the node stiffness scaling S^-0.47, same converged
-solution), batched calls over many cells of one shape, and `dC_drho`, the sensitivity of C that the reference
+`precond="scaled"` (the FFT inverse of a Poisson-ratio-0 reference medium wrapped in the node stiffness
+scaling S^-0.47, same converged solution), batched calls over many cells of one shape, and `dC_drho`, the sensitivity of C that the reference
 gets by autodiff with the correctors held fixed.
 """
 import ctypes
@@ -192,7 +192,8 @@ class LinearHomogenization:
 
     def precond(self, r, precision="fp64", precond="fft", s=None):
         """nlfiber/linear.py:167-170: irfftn(Kinv rfftn(r)) for r (..., nx, ny, nz, 3). precond="scaled" (needs
-        the stiffness scale s) wraps it in the node scaling w = (root mean square of s around the node)^-0.47;
+        the stiffness scale s) wraps the inverse of a Poisson-ratio-0 reference medium in the node scaling
+        w = (root mean square of s around the node)^-0.47;
         precision="mixed" runs it in FP32."""
         r = as_f64(r)
         nvec = int(np.prod(r.shape)) // (3 * self.N)
