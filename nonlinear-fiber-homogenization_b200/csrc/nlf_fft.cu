@@ -1495,6 +1495,25 @@ __global__ void k_kinv(const double* __restrict__ W27, int n0, int n1, int n2, i
   }
 }
 
+// Kinv (FP64 and FP32) of the unit-stiffness operator with stencil W, into k64 and k32 (NS x 6 each)
+int kinv_tables(const LinearHandle& h, const double (&W)[27][9], double* k64, float* k32) {
+  const Geom& g = h.g;
+  double* dW = nullptr;
+  NLF_CUDA_TRY(cudaMalloc(&dW, sizeof(W)));
+  cudaError_t e = cudaMemcpy(dW, W, sizeof(W), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW, g.n0, g.n1, g.n2, g.n2h, k64, k32);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(dW);
+  if (e != cudaSuccess) {
+    set_error("kinv table: %s", cudaGetErrorString(e));
+    return NLF_ECUDA;
+  }
+  return NLF_OK;
+}
+
 int build_tables(LinearHandle& h) {
   const Geom& g = h.g;
   // twiddles: lengths n0, n1, n2, n2/2 (full circles, e^{-2 pi i k / L}, k < L)
@@ -1527,20 +1546,8 @@ int build_tables(LinearHandle& h) {
   NLF_CUDA_TRY(cudaMalloc(&h.t32.kinv, g.NS * 6 * sizeof(float)));
   NLF_CUDA_TRY(cudaMalloc(&h.t64s.kinv, g.NS * 6 * sizeof(double)));
   NLF_CUDA_TRY(cudaMalloc(&h.t32s.kinv, g.NS * 6 * sizeof(float)));
-  double* dW = nullptr;
-  NLF_CUDA_TRY(cudaMalloc(&dW, 2 * sizeof(h.W27)));
-  NLF_CUDA_TRY(cudaMemcpy(dW, h.W27, sizeof(h.W27), cudaMemcpyHostToDevice));
-  NLF_CUDA_TRY(cudaMemcpy(dW + 27 * 9, h.W27s, sizeof(h.W27s), cudaMemcpyHostToDevice));
-  k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW, g.n0, g.n1, g.n2, g.n2h, h.t64.kinv, h.t32.kinv);
-  k_kinv<<<(unsigned)((g.NS + 255) / 256), 256>>>(dW + 27 * 9, g.n0, g.n1, g.n2, g.n2h, h.t64s.kinv, h.t32s.kinv);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  cudaFree(dW);
-  if (e != cudaSuccess) {
-    set_error("kinv table: %s", cudaGetErrorString(e));
-    return NLF_ECUDA;
-  }
-  return NLF_OK;
+  NLF_TRY(kinv_tables(h, h.W27, h.t64.kinv, h.t32.kinv));
+  return kinv_tables(h, h.W27s, h.t64s.kinv, h.t32s.kinv);
 }
 
 }  // namespace nlf

@@ -77,7 +77,8 @@ struct LinearHandle {
   double Gm[6][24];
   double Dm[6][6];
   double W27[27][9];  // unit-stiffness stencil blocks W_d, d = (dx+1)*9 + (dy+1)*3 + (dz+1)
-  double W27s[27][9];  // the same for the scaled preconditioner's reference medium (Poisson ratio kScaledRefNu)
+  double W27s[27][9];  // the same for the scaled preconditioner's reference medium (Poisson ratio scaled_ref_nu)
+  double scaled_ref_nu = kScaledRefNu;
   Twiddle tw;
   Tables<double> t64;
   Tables<float> t32;
@@ -137,6 +138,10 @@ int launch_precond_pcg_ab(const LinearHandle& h, int nvec, int m, double* r, con
 int launch_precond_pcg_cpx(const LinearHandle& h, int nvec, int m, cplx<double>* spec, const double* w,
                            const VecState* vs, const CellState* cs, double* x, double* p, cudaStream_t st);
 int build_tables(LinearHandle& h);
+int kinv_tables(const LinearHandle& h, const double (&W)[27][9], double* k64, float* k32);
+// Rebuild the scaled preconditioner's Kinv tables for a reference medium of Poisson ratio nu (the handle's
+// element, unit stiffness). The finite-strain solver uses the material's own nu there.
+int rebuild_scaled_kinv(LinearHandle& h, double nu);
 
 // stiffness scale only (s = emin + (1 - emin) clip01(rho)^p)
 int launch_stiffness_scale(const LinearHandle& h, long count, const double* rho, double* s, cudaStream_t st);

@@ -144,9 +144,9 @@ static void element_matrices(LinearHandle& h) {
       }
   };
   stencil(h.Ke, h.W27);
-  // the scaled preconditioner's reference medium: the same element with Poisson ratio kScaledRefNu
+  // the scaled preconditioner's reference medium: the same element with Poisson ratio h.scaled_ref_nu
   {
-    const double nu0 = kScaledRefNu, lam0 = h.E * nu0 / ((1.0 + nu0) * (1.0 - 2.0 * nu0)),
+    const double nu0 = h.scaled_ref_nu, lam0 = h.E * nu0 / ((1.0 + nu0) * (1.0 - 2.0 * nu0)),
                  mu0 = h.E / (2.0 * (1.0 + nu0));
     double D0[6][6] = {}, K0[24][24] = {};
     for (int i = 0; i < 3; ++i)
@@ -175,6 +175,16 @@ static void element_matrices(LinearHandle& h) {
     }
     stencil(K0, h.W27s);
   }
+}
+
+int rebuild_scaled_kinv(LinearHandle& h, double nu) {
+  if (!(nu > -1.0) || !(nu < 0.5)) {
+    set_error("scaled preconditioner: reference Poisson ratio %g outside (-1, 0.5)", nu);
+    return NLF_EBADARG;
+  }
+  h.scaled_ref_nu = nu;
+  element_matrices(h);
+  return kinv_tables(h, h.W27s, h.t64s.kinv, h.t32s.kinv);
 }
 
 // ---- PCG ---------------------------------------------------------------------------------------------------------
