@@ -17,6 +17,7 @@ import multiprocessing as mp
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -84,8 +85,9 @@ class ClockSampler:
 
     def start(self):
         try:
-            self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            out_dir = os.environ.get("NLF_CLOCKS_DIR", tempfile.gettempdir())
+            self.path = os.path.join(out_dir, f"nlf_clocks_{os.getpid()}.csv")
+            os.makedirs(out_dir, exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.index)], stdout=self.f,
