@@ -17,8 +17,8 @@ import multiprocessing as mp
 import os
 import statistics
 import subprocess
-import tempfile
 import sys
+import tempfile
 import time
 
 import numpy as np
