@@ -1,0 +1,75 @@
+"""CPU tests of the package's device-agnostic host logic (no GPU, no compute call into libnlf.so): the LOBPCG of
+`Mixed.lowest_eigs` on the device (`lobpcg_device`, torch code that runs on any device), the rank-one
+ellipticity minimum and the cubic TOEC map, each against an independent computation."""
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def M():
+    from nlfiber_b200 import mech
+    return mech
+
+
+def _dense_spd(n, seed):
+    rng = np.random.default_rng(seed)
+    B = rng.standard_normal((n, n))
+    return B @ B.T / n + np.diag(np.linspace(0.01, 5.0, n))
+
+
+@pytest.mark.parametrize("constrained", [False, True])
+def test_lobpcg_device_matches_dense_eigensolve(M, constrained):
+    """Knyazev's LOBPCG restated in torch: the lowest 4 eigenvalues of a dense SPD operator (on CPU tensors), with
+    and without a 3-column constraint space, against numpy's eigh of the operator restricted to the complement."""
+    import torch
+    n = 240
+    A = _dense_spd(n, 0)
+    At = torch.as_tensor(A)
+    rng = np.random.default_rng(1)
+    Y = None
+    Q = np.eye(n)
+    if constrained:
+        Yn, _ = np.linalg.qr(rng.standard_normal((n, 3)))
+        Y = torch.as_tensor(Yn)
+        Qf, _ = np.linalg.qr(np.concatenate([Yn, rng.standard_normal((n, n - 3))], axis=1))
+        Q = Qf[:, 3:]
+    vals, vecs, it = M.lobpcg_device(lambda V: At @ V, torch.as_tensor(rng.standard_normal((n, 4))), Y, 1e-9, 1000)
+    ref = np.linalg.eigvalsh(Q.T @ A @ Q)[:4]
+    np.testing.assert_allclose(vals, ref, rtol=1e-10)
+    assert it < 1000
+    V = vecs.numpy()
+    AV = A @ V
+    if constrained:  # eigenpairs of the operator restricted to the complement of Y: P A V = V diag(vals)
+        Yn = Y.numpy()
+        AV = AV - Yn @ (Yn.T @ AV)
+        assert np.abs(Yn.T @ V).max() < 1e-12
+    np.testing.assert_allclose(AV, V * vals[None, :], atol=1e-8)
+
+
+def test_rank_one_min_isotropic_and_plane(M):
+    """For isotropic linear elasticity every direction's acoustic tensor has smallest eigenvalue mu; the 2D
+    variant searches the x-y plane only."""
+    from nlfiber_b200.linear import lame
+    lam, mu = lame(1.0, 0.3)
+    d = np.eye(3)
+    A = lam * np.einsum("ij,kl->ijkl", d, d) + mu * (np.einsum("ik,jl->ijkl", d, d) + np.einsum("il,jk->ijkl", d, d))
+    for plane in (False, True):
+        v, n = M.rank_one_min(A, m=300, plane=plane)
+        assert abs(v - mu) < 1e-12 and abs(np.linalg.norm(n) - 1.0) < 1e-12
+        if plane:
+            assert n[2] == 0.0
+    pts = M.fibonacci_sphere(500)
+    np.testing.assert_allclose(np.linalg.norm(pts, axis=1), 1.0, atol=1e-14)
+    assert np.abs(pts.mean(axis=0)).max() < 1e-2
+
+
+def test_cubic_toec_means_over_equivalent_entries(M):
+    """cubic_toec averages each cubic constant over its equivalent Voigt index triples (nlfiber/mech.py:496-515);
+    a T built from known cubic values returns them."""
+    vals = {"C111": -3.0, "C112": -1.0, "C123": 0.2, "C144": -0.1, "C155": -0.5, "C456": 0.05}
+    T = np.zeros((6, 6, 6))
+    for k, idx in M.CUBIC_TOEC.items():
+        for t in idx:
+            T[t] = vals[k]
+    out = M.cubic_toec(T)
+    assert out == pytest.approx(vals, abs=1e-15)
