@@ -66,6 +66,14 @@ def rel_err(C, Cs):
     return np.abs(C - Cs).reshape(len(C), -1).max(1) / np.abs(Cs).reshape(len(Cs), -1).max(1)
 
 
+def entry_errors(C, Cs):
+    """Every entry's error: for each (I, J), the max over cells of |C_IJ - C*_IJ| / max |C*| of that cell (the
+    metric's C error is the max of these). Returns a 6x6 nested list."""
+    C, Cs = np.asarray(C), np.asarray(Cs)
+    scale = np.abs(Cs).reshape(len(Cs), -1).max(1)[:, None, None]
+    return (np.abs(C - Cs) / scale).max(0).tolist()
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -849,6 +857,7 @@ def main():
     if dist:
         dist.barrier()
     err = rel_err(C_d.cpu().numpy(), Cstar)
+    ent = entry_errors(C_d.cpu().numpy(), Cstar)
     value = shard.whole_job_rate(B * args.steps, world, ms / 1e3)
 
     # end to end through the same API with pinned host buffers (H2D of rho and D2H of C inside the region)
@@ -896,7 +905,8 @@ def main():
                        solver="FP64 PCG, node-scaled FFT preconditioner, "
                               f"{FAST['slots']} cells in flight, a converged cell's slot refilled from the queue, "
                               f"stop at residual {FAST['tol']} and energy guard {FAST['energy_tol']}"),
-        "c_err_max": float(err.max()), "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
+        "c_err_max": float(err.max()), "c_err_entries": ent,
+        "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
         "roofline": roof, "kernels": kernels, "gpu_launches": launches, "clocks": clk, "e2e": e2e,
         "cpu_baseline": cpu, "plain_fp64_gpu": plain,
         "speedup_vs_plain_fp64": (value / world / plain["cells_per_s"]) if plain else None,

@@ -73,3 +73,17 @@ def test_cubic_toec_means_over_equivalent_entries(M):
             T[t] = vals[k]
     out = M.cubic_toec(T)
     assert out == pytest.approx(vals, abs=1e-15)
+
+
+def test_bench_entry_errors_are_per_cell_normalised_maxima():
+    """bench.entry_errors: each (I, J) error is the max over cells of |dC_IJ| / max |C*| of the cell, so its max
+    over entries is the metric's C error (bench.rel_err)."""
+    import bench
+    rng = np.random.default_rng(0)
+    Cs = rng.standard_normal((5, 6, 6)) * np.array([1.0, 10.0, 0.1, 2.0, 5.0])[:, None, None]
+    C = Cs + 1e-9 * rng.standard_normal(Cs.shape)
+    ent = np.array(bench.entry_errors(C, Cs))
+    assert ent.shape == (6, 6)
+    ref = np.max(np.abs(C - Cs) / np.abs(Cs).reshape(5, -1).max(1)[:, None, None], axis=0)
+    np.testing.assert_allclose(ent, ref, rtol=0, atol=0)
+    assert ent.max() == pytest.approx(bench.rel_err(C, Cs).max(), rel=1e-15)
