@@ -198,6 +198,69 @@ def cpu_reference(cells, sample_iters=2):
     return 1.0 / cell_s, sample, t4 - t0
 
 
+def cpu_processes(n):
+    """Processes for the CPU arm: one per host core this process may run on, capped by the available host memory
+    (one 64^3 sample peaks near 1 GB; 1.5 GB is reserved per process, scaled by (n / 64)^3)."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        per = max(256 << 20, int(1.5 * (1 << 30) * (n / 64) ** 3))
+        cores = min(cores, int(psutil.virtual_memory().available // per))
+    except ImportError:
+        pass
+    return max(1, cores)
+
+
+def _cpu_worker(idx, n_o, rounds, barrier, out):
+    """One CPU-arm process: its own cell (seed idx), BLAS held to one thread (the FFTs are single-threaded
+    already), one `cpu_reference` sample per entry of `rounds` (its PCG iteration count), each started together
+    with the other processes' samples at the barrier."""
+    from threadpoolctl import threadpool_limits
+    cells = _gen(idx, n_o)[None]
+    with threadpool_limits(1):
+        for k, iters in enumerate(rounds):
+            barrier.wait(timeout=1800)
+            v, sample, wall = cpu_reference(cells, sample_iters=iters)
+            out.put((k, idx, v, wall, sample))
+
+
+def cpu_reference_parallel(n_o, rounds, procs=None):
+    """The CPU arm on all host cores: `procs` spawned single-threaded processes, one cell each (seeds
+    0..procs-1), run `cpu_reference` together, one sample per entry of `rounds`. The cells are independent, so
+    the host's throughput is the sum of the processes' cells/s; running them together charges each with the
+    memory-bandwidth contention of the others. Returns per round (sum of cells/s, slowest wall seconds, one
+    process's sample text) and the process count."""
+    import queue
+    procs = procs or cpu_processes(2 * n_o)
+    ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(procs), ctx.Queue()
+    ps = [ctx.Process(target=_cpu_worker, args=(i, n_o, list(rounds), barrier, out), daemon=True)
+          for i in range(procs)]
+    for p in ps:
+        p.start()
+    res = [[] for _ in rounds]
+    try:
+        for _ in range(procs * len(rounds)):
+            try:
+                k, _i, v, wall, sample = out.get(timeout=3600)
+            except queue.Empty:
+                raise RuntimeError("a CPU-arm process returned no sample within an hour") from None
+            res[k].append((v, wall, sample))
+    finally:
+        for p in ps:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.terminate()
+    return [(sum(r[0] for r in rk), max(r[1] for r in rk), rk[0][2]) for rk in res], procs
+
+
+def cpu_sample_text(procs, n, wall, sample):
+    return (f"{procs} cells, one per single-threaded process on {procs} host cores, run together (slowest "
+            f"{wall:.1f} s); each: {sample.split(': ', 1)[1].split(' (', 1)[0]}, iterations scaled to "
+            f"{REF_ITERS_64} (the reference algorithm's count to C err 1e-8 on this workload); value = sum of "
+            f"the processes' cells/s")
+
+
 def workload_config(n, cells, world):
     """The `config` of both arms' JSON lines: the workload, not the solver."""
     return {"workload": f"{cells} seeded synthetic {n}^3 cells per GPU x 6 unit strains, C_full, emin 1e-9",
@@ -208,24 +271,20 @@ def workload_config(n, cells, world):
 def run_reference(args, rank):
     if rank != 0:
         return
-    cells = gen_cells([0], args.n // 2, procs=1)
     t_all = time.perf_counter()
-    for _ in range(args.warmup):
-        cpu_reference(cells, sample_iters=1)
-    vals, sample = [], ""
-    for _ in range(max(1, args.steps)):
-        v, sample, _ = cpu_reference(cells)
-        vals.append(v)
-    value = statistics.median(vals)
+    steps = max(1, args.steps)
+    res, procs = cpu_reference_parallel(args.n // 2, [1] * args.warmup + [2] * steps)
+    timed = res[args.warmup:]
+    value = statistics.median(r[0] for r in timed)
+    sample = cpu_sample_text(procs, args.n, max(r[1] for r in timed), timed[0][2])
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(args.n, args.cells, args.gpus),
                            solver="the reference algorithm: FP64 PCG with the unit-stiffness FFT preconditioner "
-                                  "(the oracle port on the host cores; each step one cell sampled, scaled to the "
-                                  "calibrated iteration count)"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                             "sample": sample},
+                                  "(the oracle port on all host cores, one cell per process; each step a sample "
+                                  "of every process's cell, scaled to the calibrated iteration count)"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": round(time.perf_counter() - t_all, 1)}
     print(json.dumps(line), flush=True)
@@ -890,8 +949,10 @@ def main():
                  "cells_per_s": 1.0 / (t_it * REF_ITERS_64),
                  "note": "time per iteration measured here; iteration count from --calibrate-plain"}
     if rank == 0 and world == 1 and not args.skip_cpu:
-        v, sample, _ = cpu_reference(cells)
-        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample}
+        res, procs = cpu_reference_parallel(n // 2, [2])
+        v, wall, sample = res[0]
+        cpu ={"value": v, "unit": UNIT, "cores": procs, "kind": "port",
+               "sample": cpu_sample_text(procs, n, wall, sample)}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

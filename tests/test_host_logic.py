@@ -87,3 +87,33 @@ def test_bench_entry_errors_are_per_cell_normalised_maxima():
     ref = np.max(np.abs(C - Cs) / np.abs(Cs).reshape(5, -1).max(1)[:, None, None], axis=0)
     np.testing.assert_allclose(ent, ref, rtol=0, atol=0)
     assert ent.max() == pytest.approx(bench.rel_err(C, Cs).max(), rel=1e-15)
+
+
+def test_bench_reference_arm_line_on_all_cores():
+    """`bench.py --impl reference` (a 16^3 grid here, to keep it short): one JSON line in the driver's contract,
+    its CPU sample run as one single-threaded process per host core, `cores` the process count."""
+    import json
+    import subprocess
+    import sys
+
+    import bench
+    out = subprocess.run([sys.executable, bench.__file__, "--impl", "reference", "--steps", "1", "--warmup", "1",
+                          "--n", "16"], capture_output=True, text=True, timeout=600, check=True)
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "cells/s" and line["higher_is_better"] is True
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    cpu = line["cpu_baseline"]
+    assert cpu["kind"] == "port" and cpu["value"] == line["value"]
+    assert cpu["cores"] == bench.cpu_processes(16)
+    assert cpu["sample"].startswith(f"{cpu['cores']} cells, one per single-threaded process")
+
+
+def test_cpu_reference_parallel_sums_the_processes():
+    """Two processes, one 16^3 cell each, two rounds of a one-iteration sample: one positive summed rate per
+    round, with the slowest process's wall time and its sample text."""
+    import bench
+    res, procs = bench.cpu_reference_parallel(8, [1, 1], procs=2)
+    assert procs == 2 and len(res) == 2
+    for v, wall, sample in res:
+        assert v > 0 and wall > 0 and "1 FP64 PCG iterations" in sample

@@ -122,7 +122,9 @@ def test_lowest_eigs_match_dense_spectrum():
     cell = _stab_cell()
     mix = OM.Mixed(cell)
     z, Fb = mix.z0(np.eye(3)), np.eye(3)
-    vals, _, _ = OM.lowest_eigs(mix, z, Fb, k=4, tol=1e-8, maxiter=2000)
+    # residual tolerance 1e-7: the residuals' rounding floor here is near 1e-8, where scipy stops with a warning;
+    # the eigenvalues' error is second order in the residual
+    vals, _, _ = OM.lowest_eigs(mix, z, Fb, k=4, tol=1e-7, maxiter=2000)
     dsc = OM.diag_scale(mix)
     nz = mix.nw + mix.k
     Hd = np.stack([mix.hvp(z, Fb, np.eye(nz)[:, j]) for j in range(nz)], axis=1)

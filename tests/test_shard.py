@@ -34,7 +34,7 @@ def _rank(rank, world, port, out):
 
 def test_two_gloo_ranks_shard_cells_and_reduce_timing():
     world, port = 2, _free_port()
-    with tmp.Manager() as mgr:
+    with tmp.get_context("spawn").Manager() as mgr:  # no fork of this (threaded) test process
         out = mgr.dict()
         tmp.start_processes(_rank, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
         res = dict(out)
