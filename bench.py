@@ -254,11 +254,22 @@ def cpu_reference_parallel(n_o, rounds, procs=None):
     return [(sum(r[0] for r in rk), max(r[1] for r in rk), rk[0][2]) for rk in res], procs
 
 
+def host_math_libs():
+    """The BLAS NumPy loaded (name and version, from threadpoolctl) and its FFT: what the CPU arm runs on."""
+    try:
+        from threadpoolctl import threadpool_info
+        blas = sorted({f"{i['internal_api']} {i.get('version') or ''}".strip() for i in threadpool_info()
+                       if i.get("user_api") == "blas"})
+    except ImportError:
+        blas = []
+    return f"NumPy {np.__version__}, BLAS {', '.join(blas) or 'unknown'} (1 thread per process), FFT pocketfft"
+
+
 def cpu_sample_text(procs, n, wall, sample):
     return (f"{procs} cells, one per single-threaded process on {procs} host cores, run together (slowest "
             f"{wall:.1f} s); each: {sample.split(': ', 1)[1].split(' (', 1)[0]}, iterations scaled to "
             f"{REF_ITERS_64} (the reference algorithm's count to C err 1e-8 on this workload); value = sum of "
-            f"the processes' cells/s")
+            f"the processes' cells/s; {host_math_libs()}")
 
 
 def workload_config(n, cells, world):
