@@ -962,7 +962,7 @@ def main():
     if rank == 0 and world == 1 and not args.skip_cpu:
         res, procs = cpu_reference_parallel(n // 2, [2])
         v, wall, sample = res[0]
-        cpu ={"value": v, "unit": UNIT, "cores": procs, "kind": "port",
+        cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "port",
                "sample": cpu_sample_text(procs, n, wall, sample)}
     if dist:
         dist.barrier()
