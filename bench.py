@@ -200,7 +200,8 @@ def cpu_reference(cells, sample_iters=2):
 
 def cpu_processes(n):
     """Processes for the CPU arm: one per host core this process may run on, capped by the available host memory
-    (one 64^3 sample peaks near 1 GB; 1.5 GB is reserved per process, scaled by (n / 64)^3)."""
+    (one 64^3 sample peaks near 1 GB; 1.5 GB is reserved per process, scaled by (n / 64)^3). The callers also cap
+    it at the workload's cell count."""
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     try:
         import psutil
@@ -284,7 +285,8 @@ def run_reference(args, rank):
         return
     t_all = time.perf_counter()
     steps = max(1, args.steps)
-    res, procs = cpu_reference_parallel(args.n // 2, [1] * args.warmup + [2] * steps)
+    res, procs = cpu_reference_parallel(args.n // 2, [1] * args.warmup + [2] * steps,
+                                        procs=min(cpu_processes(args.n), args.cells))
     timed = res[args.warmup:]
     value = statistics.median(r[0] for r in timed)
     sample = cpu_sample_text(procs, args.n, max(r[1] for r in timed), timed[0][2])
@@ -960,7 +962,7 @@ def main():
                  "cells_per_s": 1.0 / (t_it * REF_ITERS_64),
                  "note": "time per iteration measured here; iteration count from --calibrate-plain"}
     if rank == 0 and world == 1 and not args.skip_cpu:
-        res, procs = cpu_reference_parallel(n // 2, [2])
+        res, procs = cpu_reference_parallel(n // 2, [2], procs=min(cpu_processes(n), B))
         v, wall, sample = res[0]
         cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "port",
                "sample": cpu_sample_text(procs, n, wall, sample)}

@@ -105,7 +105,7 @@ def test_bench_reference_arm_line_on_all_cores():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "port" and cpu["value"] == line["value"]
-    assert cpu["cores"] == bench.cpu_processes(16)
+    assert cpu["cores"] == min(bench.cpu_processes(16), 64)  # one per core, at most one per cell
     assert cpu["sample"].startswith(f"{cpu['cores']} cells, one per single-threaded process")
 
 
