@@ -1,6 +1,7 @@
 """CPU tests of the package's device-agnostic host logic (no GPU, no compute call into libnlf.so): the LOBPCG of
 `Mixed.lowest_eigs` on the device (`lobpcg_device`, torch code that runs on any device), the rank-one
-ellipticity minimum and the cubic TOEC map, each against an independent computation."""
+ellipticity minimum and the cubic TOEC map, each against an independent computation; and the bench's host-side
+pieces: the per-entry C errors and the CPU arm (the oracle on all host cores)."""
 import numpy as np
 import pytest
 
