@@ -9,9 +9,12 @@ void floor 1e-9); no dataset is involved.
   python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--calibrate-plain]
 
 --impl reference times the reference's algorithm on the host cores (the NumPy FP64 restatement in oracle/;
-the reference itself needs JAX, which is not installed) on a bounded sample of the same workload.
+the reference itself needs JAX, which is not installed) on a bounded sample of the same workload: one cell per
+process, the per-cell setup once and one PCG iteration per step, scaled to the calibrated iteration count.
+The GPU arms generate their cells with the library's own density map; only the CPU legs run the oracle.
 """
 import argparse
+import itertools
 import json
 import multiprocessing as mp
 import os
@@ -48,17 +51,73 @@ CSTAR = dict(precision="fp64", precond="scaled", tol=1e-14, maxit=10000, check_e
 REF_ITERS_64 = 21000
 
 
-def _gen(i, n_o):
-    from nlfiber_b200 import density as D
-    return D.random_cell(i, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0]
+def synth_phi(seed, n_o, kmax=2, nterms=40):
+    """The seeded pre-density of the workloads on the symmetric (n_o)^3 octant, drawn as the reference generator
+    draws it (nlfiber/fiber.py:103-121 random_start): `nterms` integer wavevectors k in [0, kmax]^3 (k = 0
+    skipped, no amplitude drawn for it), each with amplitude N(0, 1) / |k| on prod_d cos(2 pi k_d x_d) at
+    x = (i + 1/2) / (2 n_o); then the mean over the 6 axis permutations, standardised to zero mean and unit
+    standard deviation."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n_o) + 0.5) / (2 * n_o)
+    cos_k = [np.cos(2 * np.pi * k * x) for k in range(kmax + 1)]
+    field = np.zeros((n_o, n_o, n_o))
+    for _ in range(nterms):
+        k = rng.integers(0, kmax + 1, size=3)
+        if k.any():
+            amp = rng.standard_normal() / np.sqrt(float(k @ k))
+            field += amp * (cos_k[k[0]][:, None, None] * cos_k[k[1]][None, :, None] * cos_k[k[2]][None, None, :])
+    field = sum(field.transpose(q) for q in itertools.permutations(range(3))) / 6.0
+    return (field - field.mean()) / (field.std() + 1e-12)
 
 
-def gen_cells(seeds, n_o, procs=8):
-    """Seeded synthetic cells (host NumPy), generated in spawned workers before any CUDA call."""
-    if len(seeds) == 1 or procs <= 1:
-        return np.stack([_gen(i, n_o) for i in seeds])
-    with mp.get_context("spawn").Pool(min(procs, len(seeds))) as pool:
-        return np.stack(pool.starmap(_gen, [(i, n_o) for i in seeds]))
+def synth_volume(i, base=10_000):
+    """Volume fraction of cell i: U[0.2, 0.5] from default_rng(base + i)."""
+    return float(np.random.default_rng(base + i).uniform(0.2, 0.5))
+
+
+def gpu_cells(seeds, n_o, beta=16.0, betas=None, stream=None):
+    """rho of the seeded cells, (len(seeds), 2 n_o, 2 n_o, 2 n_o) CUDA float64: pre-densities `synth_phi` on the
+    host, then the library's density map on the GPU (periodic cone filter r = 1.5, exact volume `synth_volume`,
+    sharpness `beta`, or betas[i] per cell)."""
+    import torch
+    from nlfiber_b200.density import GpuDensityMap
+    dm = GpuDensityMap(n_o, 3, r=1.5)
+    dm.stream = stream
+    phi = np.stack([synth_phi(i, n_o) for i in seeds])
+    vols = np.array([synth_volume(i) for i in seeds])
+    bs = np.full(len(seeds), float(beta)) if betas is None else np.asarray(betas, dtype=np.float64)
+    n = 2 * n_o
+    rho = torch.empty((len(seeds), n, n, n), dtype=torch.float64, device="cuda")
+    for b in np.unique(bs):
+        idx = np.nonzero(bs == b)[0]
+        part = dm.run(phi[idx], float(b), v=vols[idx], eta=False)["rho"]
+        rho[torch.as_tensor(idx, device="cuda")] = part
+    torch.cuda.synchronize()
+    return rho
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_golden.npz")
+
+
+def oracle_c_errors(C, seeds, n):
+    """C error (max_IJ |C - C_o| / max |C_o|) of the cells whose oracle C is in the committed fixture
+    (tests/golden/bench_golden.npz: the NumPy oracle solved to a relative residual of 1e-12 on the host, made by
+    tests/golden/make_bench_golden.py), by seed; None when the fixture has none of these cells."""
+    if not os.path.exists(GOLDEN):
+        return None
+    g = np.load(GOLDEN)
+    key = {64: "b64", 32: "b32"}.get(n)
+    if key is None:
+        return None
+    out = {}
+    for j, sd in enumerate(g[f"{key}_seeds"]):
+        if int(sd) in seeds:
+            i = seeds.index(int(sd))
+            out[str(int(sd))] = float(rel_err(C[i:i + 1], g[f"{key}_C"][j:j + 1])[0])
+    if not out:
+        return None
+    return {"per_seed": out, "max": max(out.values()),
+            "reference": "oracle C from tests/golden/bench_golden.npz (NumPy FP64 PCG to residual 1e-12)"}
 
 
 def rel_err(C, Cs):
@@ -172,67 +231,62 @@ def roofline(prof, N, NS, m, peaks, peak_kind):
             "traffic_source": "ncu capture of the small profiling case, scaled by vectors per launch" if tv else None}, kernels
 
 
-def cpu_reference(cells, sample_iters=2):
-    """The reference algorithm (FP64 PCG with the unit-stiffness FFT preconditioner; the NumPy restatement in
-    oracle/) on one cell, all host threads. Times the setup (stiffness scale, load, first residual and
-    preconditioner, C assembly) and `sample_iters` PCG iterations, and scales to REF_ITERS_64 iterations."""
+def _cpu_worker(idx, n_o, rounds, barrier, out):
+    """One process of the CPU arm: the oracle (the NumPy restatement of nlfiber/linear.py) on its own seeded cell
+    (cell idx of the workload), BLAS held to one thread (the FFTs are single-threaded already). It times the
+    per-cell setup once (stiffness scale, load, first residual and preconditioner, C assembly), then, for each
+    round, started together with the other processes at the barrier, `k` PCG iterations of the reference
+    algorithm (unit-stiffness FFT preconditioner) and, in rounds marked so, `k` iterations of the same PCG with
+    the node-scaled preconditioner. Puts (round, idx, setup s, s per reference iteration, s per scaled
+    iteration or None) per round."""
+    from threadpoolctl import threadpool_limits
+    from oracle import density_ref as OD
     from oracle import linear_ref as OL
-    rho = cells[0]
-    lh = OL.LinearHomogenization(rho.shape, **MATERIAL, tol=0.0)
-    t0 = time.perf_counter()
-    s = lh.stiffness_scale(rho)
-    b = -lh.load(s, np.eye(6))
-    t1 = time.perf_counter()
-    x, _ = lh._cg(s, b, np.zeros_like(b), maxit=0)
-    t2 = time.perf_counter()
-    lh._cg(s, b, np.zeros_like(b), maxit=sample_iters)
-    t3 = time.perf_counter()
-    lh.bilinear(s, np.eye(6), x)
-    t4 = time.perf_counter()
-    setup = (t1 - t0) + (t2 - t1) + (t4 - t3)
-    per_it = max((t3 - t2) - (t2 - t1), 1e-9) / sample_iters
-    cell_s = setup + REF_ITERS_64 * per_it
-    sample = (f"1 cell {rho.shape[0]}^3 x 6 cases: setup, C assembly and {sample_iters} FP64 PCG iterations timed "
-              f"({t4 - t0:.1f} s), iterations scaled to {REF_ITERS_64} (the reference algorithm's count to C "
-              f"err 1e-8 on this workload)")
-    return 1.0 / cell_s, sample, t4 - t0
+    with threadpool_limits(1):
+        rho = OD.random_cell(idx, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0]
+        lh = OL.LinearHomogenization(rho.shape, **MATERIAL, tol=0.0)
+        t0 = time.perf_counter()
+        s = lh.stiffness_scale(rho)
+        b = -lh.load(s, np.eye(6))
+        ref = OL.PCGState(lh, s, b, np.zeros_like(b))
+        lh.bilinear(s, np.eye(6), ref.x)
+        setup = time.perf_counter() - t0
+        scaled = OL.PCGState(lh, s, b, np.zeros_like(b), OL.ScaledPrecond(lh, s))
+        for k, (iters, with_scaled) in enumerate(rounds):
+            barrier.wait(timeout=1800)
+            t0 = time.perf_counter()
+            for _ in range(iters):
+                ref.step()
+            t_ref = (time.perf_counter() - t0) / iters
+            t_sc = None
+            if with_scaled:
+                t0 = time.perf_counter()
+                for _ in range(iters):
+                    scaled.step()
+                t_sc = (time.perf_counter() - t0) / iters
+            out.put((k, idx, setup, t_ref, t_sc))
 
 
 def cpu_processes(n):
     """Processes for the CPU arm: one per host core this process may run on, capped by the available host memory
-    (one 64^3 sample peaks near 1 GB; 1.5 GB is reserved per process, scaled by (n / 64)^3). The callers also cap
-    it at the workload's cell count."""
+    (one 64^3 process with both PCG states peaks near 2 GB; 2.5 GB is reserved per process, scaled by (n / 64)^3).
+    The callers also cap it at the workload's cell count."""
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     try:
         import psutil
-        per = max(256 << 20, int(1.5 * (1 << 30) * (n / 64) ** 3))
+        per = max(256 << 20, int(2.5 * (1 << 30) * (n / 64) ** 3))
         cores = min(cores, int(psutil.virtual_memory().available // per))
     except ImportError:
         pass
     return max(1, cores)
 
 
-def _cpu_worker(idx, n_o, rounds, barrier, out):
-    """One CPU-arm process: its own cell (seed idx), BLAS held to one thread (the FFTs are single-threaded
-    already), one `cpu_reference` sample per entry of `rounds` (its PCG iteration count), each started together
-    with the other processes' samples at the barrier."""
-    from threadpoolctl import threadpool_limits
-    cells = _gen(idx, n_o)[None]
-    with threadpool_limits(1):
-        for k, iters in enumerate(rounds):
-            barrier.wait(timeout=1800)
-            v, sample, wall = cpu_reference(cells, sample_iters=iters)
-            out.put((k, idx, v, wall, sample))
-
-
-def cpu_reference_parallel(n_o, rounds, procs=None):
-    """The CPU arm on all host cores: `procs` spawned single-threaded processes, one cell each (seeds
-    0..procs-1), run `cpu_reference` together, one sample per entry of `rounds`. The cells are independent, so
-    the host's throughput is the sum of the processes' cells/s; running them together charges each with the
-    memory-bandwidth contention of the others. Returns per round (sum of cells/s, slowest wall seconds, one
-    process's sample text) and the process count."""
+def cpu_reference_parallel(n_o, rounds, procs):
+    """The CPU arm on all host cores: `procs` spawned single-threaded processes, one seeded cell each (cells
+    0..procs-1 of the workload), running their rounds together (each round starts at a barrier, so every process
+    is timed under the others' memory traffic). Returns per round the list of (setup, s per reference
+    iteration, s per scaled iteration or None) over the processes."""
     import queue
-    procs = procs or cpu_processes(2 * n_o)
     ctx = mp.get_context("spawn")
     barrier, out = ctx.Barrier(procs), ctx.Queue()
     ps = [ctx.Process(target=_cpu_worker, args=(i, n_o, list(rounds), barrier, out), daemon=True)
@@ -243,16 +297,22 @@ def cpu_reference_parallel(n_o, rounds, procs=None):
     try:
         for _ in range(procs * len(rounds)):
             try:
-                k, _i, v, wall, sample = out.get(timeout=3600)
+                k, _i, setup, t_ref, t_sc = out.get(timeout=3600)
             except queue.Empty:
                 raise RuntimeError("a CPU-arm process returned no sample within an hour") from None
-            res[k].append((v, wall, sample))
+            res[k].append((setup, t_ref, t_sc))
     finally:
         for p in ps:
             p.join(timeout=60)
             if p.is_alive():
                 p.terminate()
-    return [(sum(r[0] for r in rk), max(r[1] for r in rk), rk[0][2]) for rk in res], procs
+    return res
+
+
+def cpu_rate(rows, iters, which=1):
+    """Cells/s of the host: the sum over the processes (independent cells) of 1 / (setup + iters x s per
+    iteration), with column `which` of `cpu_reference_parallel`'s rows (1: reference, 2: scaled)."""
+    return sum(1.0 / (r[0] + iters * r[which]) for r in rows)
 
 
 def host_math_libs():
@@ -266,11 +326,36 @@ def host_math_libs():
     return f"NumPy {np.__version__}, BLAS {', '.join(blas) or 'unknown'} (1 thread per process), FFT pocketfft"
 
 
-def cpu_sample_text(procs, n, wall, sample):
-    return (f"{procs} cells, one per single-threaded process on {procs} host cores, run together (slowest "
-            f"{wall:.1f} s); each: {sample.split(': ', 1)[1].split(' (', 1)[0]}, iterations scaled to "
-            f"{REF_ITERS_64} (the reference algorithm's count to C err 1e-8 on this workload); value = sum of "
-            f"the processes' cells/s; {host_math_libs()}")
+# The reference algorithm's iteration count per 64^3 cell of this workload, and where it comes from.
+REF_ITERS_SOURCE = ("--calibrate-plain on B200: the plain FP64 GPU PCG (the reference algorithm's iterates) on cells "
+                    "0-3 needed > 32000, 4000, 32000 and 16000 iterations to C err 1e-8; mean 21000 with the first "
+                    "counted at its 32000 lower bound")
+# Mean PCG iterations per 64^3 cell of the measured GPU path (node-scaled preconditioner, residual 1e-9 with the
+# energy guard) on this workload's 64 cells; the CPU arm's same-algorithm figure scales its per-iteration time by it.
+SCALED_ITERS_64 = 188
+
+
+def cpu_summary(res, procs, n, timed_rounds):
+    """The CPU figures of a `cpu_reference_parallel` run: the reference algorithm's cells/s per timed round, the
+    node-scaled algorithm's cells/s (from the rounds that ran it) and the sample text."""
+    vals = [cpu_rate(res[k], REF_ITERS_64) for k in timed_rounds]
+    sc_rounds = [k for k in range(len(res)) if res[k][0][2] is not None]
+    sc_vals = [sum(1.0 / (r[0] + SCALED_ITERS_64 * r[2]) for r in res[k]) for k in sc_rounds]
+    it_ref = statistics.median(r[1] for k in timed_rounds for r in res[k])
+    setup = statistics.median(r[0] for r in res[0])
+    n_it = len(timed_rounds)
+    sample = (f"{procs} cells of {n}^3 x 6 cases, one per single-threaded process on {procs} host cores, run "
+              f"together: per process the cell's setup and C assembly timed once ({setup:.1f} s) and {n_it} PCG "
+              f"iterations of the reference algorithm (median {it_ref:.2f} s per iteration of 6 cases), scaled to "
+              f"{REF_ITERS_64} iterations per cell; value = sum of the processes' cells/s; {host_math_libs()}")
+    same = None
+    if sc_vals:
+        it_sc = statistics.median(r[2] for k in sc_rounds for r in res[k])
+        same = {"value": statistics.median(sc_vals), "unit": UNIT, "cores": procs, "kind": "port",
+                "sample": f"the same processes running the node-scaled preconditioner ({len(sc_rounds)} rounds, "
+                          f"median {it_sc:.2f} s per iteration) scaled to {SCALED_ITERS_64} iterations per cell, the "
+                          f"GPU path's mean on this workload"}
+    return vals, same, sample
 
 
 def workload_config(n, cells, world):
@@ -281,23 +366,29 @@ def workload_config(n, cells, world):
 
 
 def run_reference(args, rank):
+    """--impl reference: the reference algorithm on the host cores (the oracle port; the reference needs JAX,
+    which is not installed). Warm-up rounds run one iteration of each preconditioner, timed rounds one iteration
+    of the reference algorithm; the value of a round is the host's cells/s at the calibrated iteration count, and
+    the line's value the median over the timed rounds."""
     if rank != 0:
         return
     t_all = time.perf_counter()
     steps = max(1, args.steps)
-    res, procs = cpu_reference_parallel(args.n // 2, [1] * args.warmup + [2] * steps,
-                                        procs=min(cpu_processes(args.n), args.cells))
-    timed = res[args.warmup:]
-    value = statistics.median(r[0] for r in timed)
-    sample = cpu_sample_text(procs, args.n, max(r[1] for r in timed), timed[0][2])
+    procs = min(cpu_processes(args.n), args.cells)
+    rounds = [(1, True)] * args.warmup + [(1, False)] * steps
+    res = cpu_reference_parallel(args.n // 2, rounds, procs)
+    vals, same, sample = cpu_summary(res, procs, args.n, list(range(args.warmup, args.warmup + steps)))
+    value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload_config(args.n, args.cells, args.gpus),
-                           solver="the reference algorithm: FP64 PCG with the unit-stiffness FFT preconditioner "
-                                  "(the oracle port on all host cores, one cell per process; each step a sample "
-                                  "of every process's cell, scaled to the calibrated iteration count)"),
+            "config": workload_config(args.n, args.cells, args.gpus),
+            "solver": "the reference algorithm: FP64 PCG with the unit-stiffness FFT preconditioner (the oracle port "
+                      "on all host cores, one cell per process)",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+            "extrapolation": {"iterations_timed_per_process": steps, "iterations_per_cell": REF_ITERS_64,
+                              "source": REF_ITERS_SOURCE},
+            "cpu_same_algorithm": same,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": round(time.perf_counter() - t_all, 1)}
     print(json.dumps(line), flush=True)
@@ -359,14 +450,13 @@ def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
     from nlfiber_b200 import _lib
     from nlfiber_b200 import learned as LN
     t0 = time.perf_counter()
-    c32 = gen_cells(list(range(10_000, 10_000 + args.train_cells32)), 16)
-    cbig = gen_cells(list(range(20_000, 20_000 + args.train_cells64)), n // 2)
+    c32 = gpu_cells(range(10_000, 10_000 + args.train_cells32), 16, stream=stream)
+    cbig = gpu_cells(range(20_000, 20_000 + args.train_cells64), n // 2, stream=stream)
     sets = []
-    for cells in (c32, cbig):
-        m = cells.shape[1]
+    for rho in (c32, cbig):
+        m = rho.shape[1]
         h = L.LinearHomogenization((m, m, m), **MATERIAL, **FAST)
         h.stream = stream
-        rho = torch.from_numpy(cells).cuda()
         r = h.C_full_batched(rho, want_u=True)
         sets.append((rho.float(), LN.corrector_channels(torch.from_numpy(r["u"])).cuda(),
                      LN.loss_weights(rho, MATERIAL["emin"], MATERIAL["p"]).cuda() + 0.05))
@@ -437,7 +527,7 @@ def mech_arm(args, stream):
     from nlfiber_b200 import _lib
     from nlfiber_b200 import mech as MH
     n = args.n
-    cells = gen_cells(list(range(args.mech_cells)), n // 2)
+    cells = gpu_cells(range(args.mech_cells), n // 2, stream=stream).cpu().numpy()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     rows, newton, cg, steps = [], 0, 0, 0
     torch.cuda.synchronize()
@@ -519,11 +609,9 @@ def mech_arm(args, stream):
             "converged_all": all(r["converged"] for r in rows), "rows": rows, "kernels": kernels}
 
 
-def _gen3(i, n_o):
-    """Uneven-batch generator: the benchmark generator with beta drawn from {4, 8, 16} by default_rng(20000 + i)."""
-    from nlfiber_b200 import density as D
-    beta = float(np.random.default_rng(20_000 + i).choice([4.0, 8.0, 16.0]))
-    return D.random_cell(i, n_o=n_o, r=1.5, beta=beta, kmax=2)[0]
+def uneven_beta(i):
+    """Sharpness of cell i of the uneven batch: drawn from {4, 8, 16} by default_rng(20000 + i)."""
+    return float(np.random.default_rng(20_000 + i).choice([4.0, 8.0, 16.0]))
 
 
 def uneven_arm(args, stream):
@@ -535,9 +623,8 @@ def uneven_arm(args, stream):
     sizes = [int(v) for v in args.uneven.split(",")]
     cells = []
     for n, cnt in zip(sizes[0::2], sizes[1::2]):
-        with mp.get_context("spawn").Pool(8) as pool:
-            arr = pool.starmap(_gen3, [(i, n // 2) for i in range(cnt)])
-        cells += [torch.from_numpy(a).cuda() for a in arr]
+        rho = gpu_cells(range(cnt), n // 2, betas=[uneven_beta(i) for i in range(cnt)], stream=stream)
+        cells += [rho[i] for i in range(cnt)]
     handles = {}
     ref = L.C_full_uneven(cells, concurrent=True, **MATERIAL, **CSTAR)
     L.C_full_uneven(cells[:1], handles=handles, **MATERIAL, **FAST)  # warm-up of one handle
@@ -572,15 +659,16 @@ def density_bytes(kind, n_o):
 
 def density_arm(args, stream, peaks, peak_kind):
     """The density map phi -> rho (exact volume) of the benchmark cells on the GPU: device-resident phi and rho
-    for the timed steps, a host round trip for e2e, the NumPy host map as the CPU baseline."""
+    for the timed steps, a host round trip for e2e, the oracle's NumPy map (the restatement of
+    nlfiber/density.py) as the accuracy check and the CPU baseline."""
     import ctypes
 
     import torch
     from nlfiber_b200 import _lib
     from nlfiber_b200 import density as D
     n_o, nc = args.n // 2, args.cells
-    phi_h = np.stack([D.random_start(n_o, 3, seed=i, kmax=2) for i in range(nc)])
-    vols = np.array([float(np.random.default_rng(10_000 + i).uniform(0.2, 0.5)) for i in range(nc)])
+    phi_h = np.stack([synth_phi(i, n_o) for i in range(nc)])
+    vols = np.array([synth_volume(i) for i in range(nc)])
     g = D.GpuDensityMap(n_o, 3, r=1.5)
     g.stream = stream
     phi = torch.as_tensor(phi_h, device="cuda")
@@ -603,9 +691,6 @@ def density_arm(args, stream, peaks, peak_kind):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    # accuracy against the host map (the NumPy mirror of nlfiber/density.py) on two cells
-    err = max(float(np.abs(rho[i].cpu().numpy() - D.DensityMap(n_o, 3, r=1.5, v=vols[i]).rho(phi_h[i], 16.0)).max())
-              for i in range(2))
     vol_err = float((rho.mean(dim=(1, 2, 3)) - v).abs().max())
     # end to end: pinned host phi in, rho and eta back to pinned host memory, inside the timed region
     phi_p = torch.as_tensor(phi_h).pin_memory()
@@ -651,18 +736,20 @@ def density_arm(args, stream, peaks, peak_kind):
     bms, bla, _ = prof[best]
     achieved = density_bytes(best, n_o) * nc / (bms * 1e-3) / 1e9
     peak = float(peaks["hbm_gbs"])
-    # CPU baseline: the host NumPy map on a sample of cells
+    # CPU baseline: the oracle's NumPy map (the restatement of nlfiber/density.py) on a sample of cells; its
+    # values also check the GPU map's
+    from oracle import density_ref as OD
     ns = min(nc, 8)
     t0 = time.perf_counter()
-    for i in range(ns):
-        D.DensityMap(n_o, 3, r=1.5, v=vols[i]).rho(phi_h[i], 16.0)
+    host = [OD.DensityMap(n_o, 3, r=1.5, v=vols[i]).rho(phi_h[i], 16.0) for i in range(ns)]
     cpu_s = (time.perf_counter() - t0) / ns
+    err = max(float(np.abs(rho[i].cpu().numpy() - host[i]).max()) for i in range(ns))
     return {"metric": f"density maps/s at {n}^3 (phi -> rho, exact volume)", "value": round(nc / (ms * 1e-3), 1),
             "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{nc} seeded pre-densities random_start({n_o}, seed=i, kmax=2), v_i ~ U[0.2, "
                                    f"0.5], cone filter r = 1.5, beta = 16", "cells": nc, "grid": n},
-            "rho_err_max_vs_host": err, "volume_err_max": vol_err,
+            "rho_err_max_vs_oracle": err, "volume_err_max": vol_err,
             "roofline": {"kernel": best, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "peak_kind": "of measured copy bandwidth" if peak_kind == "measured"
@@ -676,7 +763,7 @@ def density_arm(args, stream, peaks, peak_kind):
             "e2e": {"value": round(nc / e2e_s, 1), "unit": "cells/s", "h2d_bytes_per_step": int(phi_h.nbytes + vols.nbytes),
                     "d2h_bytes_per_step": int(rho_p.numel() * 8 + nc * 8)},
             "cpu_baseline": {"value": round(1.0 / cpu_s, 2), "unit": "cells/s", "cores": 1, "kind": "port",
-                             "sample": f"{ns} cells through the host NumPy map (FFT filter, full-cell bisection)"}}
+                             "sample": f"{ns} cells through the oracle's NumPy map (FFT filter, full-cell bisection)"}}
 
 
 def toec_arm(args, stream):
@@ -686,7 +773,7 @@ def toec_arm(args, stream):
     from nlfiber_b200 import linear as L
     from nlfiber_b200 import mech as MH
     n, nc = args.n, 2
-    cells = gen_cells(list(range(nc)), n // 2)
+    cells = gpu_cells(range(nc), n // 2, stream=stream).cpu().numpy()
     lh = L.LinearHomogenization((n, n, n), emin=1e-3, precond="scaled", tol=1e-10, maxit=8000, check_every=16)
     res = lh.C_full_batched(np.stack(cells), want_u=True)
     rows = []
@@ -849,9 +936,6 @@ def main():
     n_o = args.n // 2
     from nlfiber_b200 import shard
     seeds = shard.cell_seeds(rank, args.cells)
-    t_gen = time.perf_counter()
-    cells = gen_cells(seeds, n_o)
-    t_gen = time.perf_counter() - t_gen
 
     import torch
     torch.cuda.set_device(local)
@@ -867,7 +951,9 @@ def main():
     N = n ** 3
     NS = n * n * (n // 2 + 1)
     stream = torch.cuda.current_stream().cuda_stream
-    rho_d = torch.from_numpy(cells).cuda()
+    t_gen = time.perf_counter()
+    rho_d = gpu_cells(seeds, n_o, stream=stream)
+    t_gen = time.perf_counter() - t_gen
     C_d = torch.empty((B, 6, 6), dtype=torch.float64, device="cuda")
 
     if args.ncu:
@@ -930,10 +1016,11 @@ def main():
         dist.barrier()
     err = rel_err(C_d.cpu().numpy(), Cstar)
     ent = entry_errors(C_d.cpu().numpy(), Cstar)
+    vs_oracle = oracle_c_errors(C_d.cpu().numpy(), seeds, n)
     value = shard.whole_job_rate(B * args.steps, world, ms / 1e3)
 
     # end to end through the same API with pinned host buffers (H2D of rho and D2H of C inside the region)
-    rho_h = torch.from_numpy(cells).pin_memory()
+    rho_h = rho_d.cpu().pin_memory()
     C_h = torch.empty((B, 6, 6), dtype=torch.float64).pin_memory()
     e2e_steps = max(1, args.steps // 2)
     torch.cuda.synchronize()
@@ -955,17 +1042,17 @@ def main():
         roof["measured_on"] = "CUDA events around every launch of one extra step of the same workload"
     launches = sum(v[1] for v in prof.values()) * args.steps  # per step alike: the same cells every step
 
-    plain, cpu = None, None
+    plain, cpu, cpu_same = None, None, None
     if rank == 0 and not args.skip_plain:
         t_it = plain_fp64_time(L, rho_d, n, stream)
         plain = {"sec_per_iteration_per_cell": t_it, "iterations_to_1e-8": REF_ITERS_64,
                  "cells_per_s": 1.0 / (t_it * REF_ITERS_64),
                  "note": "time per iteration measured here; iteration count from --calibrate-plain"}
     if rank == 0 and world == 1 and not args.skip_cpu:
-        res, procs = cpu_reference_parallel(n // 2, [2], procs=min(cpu_processes(n), B))
-        v, wall, sample = res[0]
-        cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "port",
-               "sample": cpu_sample_text(procs, n, wall, sample)}
+        procs = min(cpu_processes(n), B)
+        res = cpu_reference_parallel(n // 2, [(1, True)] + [(1, False)] * 3, procs)
+        vals, cpu_same, sample = cpu_summary(res, procs, n, [1, 2, 3])
+        cpu = {"value": statistics.median(vals), "unit": UNIT, "cores": procs, "kind": "port", "sample": sample}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -975,14 +1062,15 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(workload_config(n, B, world),
-                       solver="FP64 PCG, node-scaled FFT preconditioner, "
-                              f"{FAST['slots']} cells in flight, a converged cell's slot refilled from the queue, "
-                              f"stop at residual {FAST['tol']} and energy guard {FAST['energy_tol']}"),
+        "config": workload_config(n, B, world),
+        "solver": "FP64 PCG, node-scaled FFT preconditioner, "
+                  f"{FAST['slots']} cells in flight, a converged cell's slot refilled from the queue, "
+                  f"stop at residual {FAST['tol']} and energy guard {FAST['energy_tol']}",
         "c_err_max": float(err.max()), "c_err_entries": ent,
+        "c_err_vs_oracle": vs_oracle,
         "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
         "roofline": roof, "kernels": kernels, "gpu_launches": launches, "clocks": clk, "e2e": e2e,
-        "cpu_baseline": cpu, "plain_fp64_gpu": plain,
+        "cpu_baseline": cpu, "cpu_same_algorithm": cpu_same, "plain_fp64_gpu": plain,
         "speedup_vs_plain_fp64": (value / world / plain["cells_per_s"]) if plain else None,
         "input_gen_s": round(t_gen, 1),
     }

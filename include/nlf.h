@@ -131,8 +131,10 @@ NLF_API int nlf_dC_drho(nlf_linear* h, int ncell, const double* rho, const doubl
  * host array. Same values as nlf_bilinear. No handle: the grid shape and material are arguments. At most 64
  * cells and 6 load cases per call (-1 with a message beyond). The partial sums live in a fixed 672 KiB device
  * array held by every GPU that loads the library; calls that overlap on the GPU race on it, so serialise them.
- * The first call on a device looks up that array's address; make it before any stream capture. Asynchronous on
- * `stream`: C is ready when the stream reaches it. */
+ * The first call on a device looks up that array's address; make it before any stream capture. That address
+ * belongs to the device's context: after cudaDeviceReset of a device, do not call this entry point on it again.
+ * Pointers into another GPU's memory are rejected (-1). Asynchronous on `stream`: C is ready when the stream
+ * reaches it. */
 NLF_API int nlf_bilinear_noalloc(int nx, int ny, int nz, double E, double nu, int ncell, const double* s,
                                  const double* Es, int m, const double* u, double* C, void* stream);
 

@@ -15,7 +15,10 @@
 // calls, and the array keeps the last call's partials.
 //
 // Set-up: the first call on a device (with that device current) looks up the array's device address with
-// cudaGetSymbolAddress and remembers it per device. Make that first call before any stream capture.
+// cudaGetSymbolAddress and remembers it per device. Make that first call before any stream capture. The
+// remembered address belongs to the device's current context: after cudaDeviceReset on that device it is stale,
+// so a process that resets a device must not call this entry point on it again.
+#include <atomic>
 #include <cstring>
 #include "nlf_internal.h"
 
@@ -32,7 +35,8 @@ constexpr int kNaMaxDevices = 64;
 // 64 cells x 64 CTAs x 21 pairs x 8 B = 672 KiB, held by every GPU that loads the library until exit.
 static __device__ __align__(256) double g_na_scratch[kNaCells * kNaBlocks * kNaPairs];
 
-double* g_na_addr[kNaMaxDevices] = {};
+// per device ordinal: the scratch array's device address (every writer stores the same value)
+std::atomic<double*> g_na_addr[kNaMaxDevices] = {};
 
 struct NaArgs {
   double Es[kNaCases * 6];
@@ -138,6 +142,7 @@ __global__ void k_na_reduce(const double* __restrict__ scratch, int nblk, int m,
   }
 }
 
+// Device (or managed) memory at all, whichever device it belongs to.
 bool on_device(const void* p) {
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
@@ -145,6 +150,17 @@ bool on_device(const void* p) {
     return false;
   }
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// Device memory of device `dev`: a pointer into another GPU's memory would make the kernels read and write
+// that GPU over the interconnect (or fault without peer access). Managed memory is reachable from every device.
+bool on_device_of(const void* p, int dev) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == dev);
 }
 
 }  // namespace
@@ -168,21 +184,23 @@ extern "C" NLF_API int nlf_bilinear_noalloc(int nx, int ny, int nz, double E, do
     set_error("nlf_bilinear_noalloc: Es is read on the host and must be a host array (m, 6)");
     return NLF_EBADARG;
   }
-  if (!on_device(s) || !on_device(u) || !on_device(C)) {
-    set_error("nlf_bilinear_noalloc: s, u and C must be device pointers of the current device "
-              "(it copies nothing; use nlf_bilinear for host arrays)");
-    return NLF_EBADARG;
-  }
   int dev = 0;
   NLF_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNaMaxDevices) {
     set_error("nlf_bilinear_noalloc: device ordinal %d out of range", dev);
     return NLF_EBADARG;
   }
-  if (!g_na_addr[dev]) {  // first call on this device: look up the scratch array's device address
+  if (!on_device_of(s, dev) || !on_device_of(u, dev) || !on_device_of(C, dev)) {
+    set_error("nlf_bilinear_noalloc: s, u and C must be device pointers of the current device %d "
+              "(it copies nothing; use nlf_bilinear for host arrays)", dev);
+    return NLF_EBADARG;
+  }
+  double* scratch = g_na_addr[dev].load(std::memory_order_acquire);
+  if (!scratch) {  // first call on this device: look up the scratch array's device address
     void* p = nullptr;
     NLF_CUDA_TRY(cudaGetSymbolAddress(&p, g_na_scratch));
-    g_na_addr[dev] = static_cast<double*>(p);
+    scratch = static_cast<double*>(p);
+    g_na_addr[dev].store(scratch, std::memory_order_release);
   }
   NaArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -208,9 +226,9 @@ extern "C" NLF_API int nlf_bilinear_noalloc(int nx, int ny, int nz, double E, do
     }
   cudaStream_t st = (cudaStream_t)stream;
   const long N = (long)nx * ny * nz;
-  k_na_partials<<<dim3(kNaBlocks, ncell), kNaThreads, 0, st>>>(a, s, u, g_na_addr[dev]);
+  k_na_partials<<<dim3(kNaBlocks, ncell), kNaThreads, 0, st>>>(a, s, u, scratch);
   NLF_CHECK_LAUNCH();
-  k_na_reduce<<<ncell, 32, 0, st>>>(g_na_addr[dev], kNaBlocks, m, 1.0 / (double)N, C);
+  k_na_reduce<<<ncell, 32, 0, st>>>(scratch, kNaBlocks, m, 1.0 / (double)N, C);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }

@@ -167,39 +167,24 @@ class LinearHomogenization:
     def _A(self, s, x):
         return np.stack([self.apply_K(s, xi) for xi in x])
 
-    # nlfiber/linear.py:173-203 (lock-step batched PCG, same guards and stopping rule)
-    def _cg(self, s, b, x0, maxit=None, history=None):
+    # nlfiber/linear.py:173-203 (lock-step batched PCG, same guards and stopping rule). M: the preconditioner
+    # r -> z (default: the reference's `precond`; `ScaledPrecond` checks the library's node-scaled variant).
+    def _cg(self, s, b, x0, maxit=None, history=None, M=None):
         maxit = self.maxit if maxit is None else maxit
-        b = proj(b)
-        bn = np.sqrt(np.sum(b * b, axis=(1, 2, 3, 4))) + 1e-300
-        x = proj(x0)
-        r = b - proj(self._A(s, x))
-        z = proj(self.precond(r))
-        p = z
-        rz = np.sum(r * z, axis=(1, 2, 3, 4))
-        it = 0
-        while it < maxit and np.any(np.sqrt(np.sum(r * r, axis=(1, 2, 3, 4))) > self.tol * bn):
-            Ap = proj(self._A(s, p))
-            pAp = np.sum(p * Ap, axis=(1, 2, 3, 4))
-            a = rz / np.where(pAp == 0, 1.0, pAp)
-            x = x + a[:, None, None, None, None] * p
-            r = r - a[:, None, None, None, None] * Ap
-            z = proj(self.precond(r))
-            rz1 = np.sum(r * z, axis=(1, 2, 3, 4))
-            p = z + (rz1 / np.where(rz == 0, 1.0, rz))[:, None, None, None, None] * p
-            rz = rz1
-            it += 1
+        st = PCGState(self, s, b, x0, M)
+        while st.it < maxit and st.active():
+            st.step()
             if history is not None:
-                history(it, x, r)
-        return x, it
+                history(st.it, st.x, st.r)
+        return st.x, st.it
 
     # nlfiber/linear.py:205-217
-    def solve(self, s, Es, u0=None, maxit=None, history=None):
+    def solve(self, s, Es, u0=None, maxit=None, history=None, M=None):
         Es = np.asarray(Es, dtype=np.float64)
         s = np.asarray(s, dtype=np.float64)
         if u0 is None:
             u0 = np.zeros((Es.shape[0],) + self.shape + (3,))
-        return self._cg(s, -self.load(s, Es), np.asarray(u0, dtype=np.float64), maxit, history)
+        return self._cg(s, -self.load(s, Es), np.asarray(u0, dtype=np.float64), maxit, history, M)
 
     def _solve_rhs(self, s, b, maxit=None):
         """nlfiber/linear.py:208-210."""
@@ -237,10 +222,13 @@ class LinearHomogenization:
         return sbar, lam
 
     # nlfiber/linear.py:231-236
-    def C_full(self, rho, u0=None, maxit=None, history=None):
+    def C_full(self, rho, u0=None, maxit=None, history=None, precond="fft"):
+        """precond "scaled" runs the library's node-scaled preconditioner (`ScaledPrecond`) instead of the
+        reference's: the same C at convergence, in far fewer iterations at high contrast."""
         s = self.stiffness_scale(rho)
         Es = np.eye(6)
-        u, it = self.solve(s, Es, u0, maxit, history)
+        M = ScaledPrecond(self, s) if precond == "scaled" else None
+        u, it = self.solve(s, Es, u0, maxit, history, M)
         return self.bilinear(s, Es, u), u, it
 
     # nlfiber/linear.py:239-264
@@ -265,6 +253,67 @@ class LinearHomogenization:
         s = self.stiffness_scale(rho)
         u2, it = self.solve(s, self.sym_cases(), u0, maxit)
         return self.invariants_from(s, u2), u2, it
+
+
+class PCGState:
+    """The state of the lock-step PCG of nlfiber/linear.py:173-203, advanced one iteration per `step` (the loop
+    of `LinearHomogenization._cg`; also lets a caller time single iterations). Same guards as the reference:
+    pAp == 0 -> 1, rz == 0 -> 1; x, r and z stay projected onto the mean-free subspace."""
+
+    def __init__(self, lh, s, b, x0, M=None):
+        self.lh, self.s = lh, s
+        self.M = lh.precond if M is None else M
+        b = proj(b)
+        self.bn = np.sqrt(np.sum(b * b, axis=(1, 2, 3, 4))) + 1e-300
+        self.x = proj(x0)
+        self.r = b - proj(lh._A(s, self.x))
+        z = proj(self.M(self.r))
+        self.p = z
+        self.rz = np.sum(self.r * z, axis=(1, 2, 3, 4))
+        self.it = 0
+
+    def rnorm(self):
+        return np.sqrt(np.sum(self.r * self.r, axis=(1, 2, 3, 4)))
+
+    def active(self):
+        """The reference's loop condition: some case has ||r|| > tol ||b||."""
+        return bool(np.any(self.rnorm() > self.lh.tol * self.bn))
+
+    def step(self):
+        col = (slice(None), None, None, None, None)
+        Ap = proj(self.lh._A(self.s, self.p))
+        pAp = np.sum(self.p * Ap, axis=(1, 2, 3, 4))
+        a = self.rz / np.where(pAp == 0, 1.0, pAp)
+        self.x = self.x + a[col] * self.p
+        self.r = self.r - a[col] * Ap
+        z = proj(self.M(self.r))
+        rz1 = np.sum(self.r * z, axis=(1, 2, 3, 4))
+        self.p = z + (rz1 / np.where(self.rz == 0, 1.0, self.rz))[col] * self.p
+        self.rz = rz1
+        self.it += 1
+
+
+def node_scaling(s, expo=0.47):
+    """Node scaling of the library's scaled preconditioner (NLF_PC_FFT_SCALED; no counterpart in the reference):
+    w_n = S_n^-expo with S_n the root mean square of the stiffness scales of the 8 elements around node n (element
+    e owns the nodes e + NODES[a], so they are the elements n - NODES[a])."""
+    s = np.asarray(s, dtype=np.float64)
+    acc = sum(np.roll(s * s, shift=tuple(int(o) for o in off), axis=(0, 1, 2)) for off in NODES)
+    return (acc / 8.0) ** (-0.5 * expo)
+
+
+class ScaledPrecond:
+    """The library's node-scaled FFT preconditioner restated for the tests (no counterpart in the reference):
+    z = w irfftn(Kinv0 rfftn(w r)), with w = node_scaling(s) and Kinv0 the reference's symbol inverse
+    (nlfiber/linear.py:154-165) of the same element with Poisson ratio nu0 = 0. The converged solution is the
+    reference's; only the iterates differ."""
+
+    def __init__(self, lh, s, nu0=0.0, expo=0.47):
+        self.ref = LinearHomogenization(lh.shape, E=lh.E, nu=nu0, emin=lh.emin, p=lh.p)
+        self.w = node_scaling(s, expo)[..., None]
+
+    def __call__(self, r):
+        return self.w * self.ref.precond(self.w * r)
 
 
 # nlfiber/linear.py:267-291

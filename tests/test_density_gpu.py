@@ -98,18 +98,15 @@ def test_host_and_device_pointers_agree():
     np.testing.assert_array_equal(eta_h, out["eta"].cpu().numpy())
 
 
-def test_benchmark_cells_match_host_generator():
-    """The 64^3 cells of the benchmark generator (random_start(32, seed=i, kmax=2), v ~ U[0.2, 0.5] from
-    default_rng(10000 + i), r = 1.5, beta = 16) from the GPU map agree with the host generator."""
-    from nlfiber_b200 import density as D
+def test_benchmark_cells_match_oracle_generator():
+    """The 64^3 cells of the benchmark (bench.gpu_cells: bench.synth_phi(seed, 32) on the host, v ~ U[0.2, 0.5]
+    from default_rng(10000 + i), then the GPU map with r = 1.5, beta = 16) agree with the oracle's generator."""
+    import bench
     seeds = [0, 1]
-    phis = np.stack([D.random_start(32, 3, seed=i, kmax=2) for i in seeds])
-    vols = np.array([float(np.random.default_rng(10_000 + i).uniform(0.2, 0.5)) for i in seeds])
-    out = _gpu(32, 1.5, 0.3).run(phis, 16.0, v=vols)
+    rho_d = bench.gpu_cells(seeds, 32)
     for k, i in enumerate(seeds):
-        rho_h, v = D.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)
-        assert v == vols[k]
-        rho = out["rho"][k].cpu().numpy()
+        rho_h, v = OD.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)
+        rho = rho_d[k].cpu().numpy()
         assert np.abs(rho - rho_h).max() < TOL
         assert abs(rho.mean() - v) < 1e-12
 

@@ -92,29 +92,61 @@ def test_bench_entry_errors_are_per_cell_normalised_maxima():
 
 def test_bench_reference_arm_line_on_all_cores():
     """`bench.py --impl reference` (a 16^3 grid here, to keep it short): one JSON line in the driver's contract,
-    its CPU sample run as one single-threaded process per host core, `cores` the process count."""
+    its CPU sample run as one single-threaded process per host core, `cores` the process count; the solver
+    description sits outside `config` (so both arms carry the same config), and the iteration extrapolation and
+    the same-algorithm figure are stated."""
     import json
     import subprocess
     import sys
 
     import bench
-    out = subprocess.run([sys.executable, bench.__file__, "--impl", "reference", "--steps", "1", "--warmup", "1",
+    out = subprocess.run([sys.executable, bench.__file__, "--impl", "reference", "--steps", "2", "--warmup", "1",
                           "--n", "16"], capture_output=True, text=True, timeout=600, check=True)
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["unit"] == "cells/s" and line["higher_is_better"] is True
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"] == bench.workload_config(16, 64, 1) and "solver" in line
+    assert line["extrapolation"]["iterations_timed_per_process"] == 2
+    assert line["cpu_same_algorithm"]["value"] > line["value"]
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "port" and cpu["value"] == line["value"]
     assert cpu["cores"] == min(bench.cpu_processes(16), 64)  # one per core, at most one per cell
-    assert cpu["sample"].startswith(f"{cpu['cores']} cells, one per single-threaded process")
+    assert cpu["sample"].startswith(f"{cpu['cores']} cells of 16^3 x 6 cases, one per single-threaded process")
 
 
-def test_cpu_reference_parallel_sums_the_processes():
-    """Two processes, one 16^3 cell each, two rounds of a one-iteration sample: one positive summed rate per
-    round, with the slowest process's wall time and its sample text."""
+def test_bench_reference_arm_loads_no_library():
+    """The reference arm runs the oracle only: generating its cells and timing them loads no libnlf.so."""
+    import subprocess
+    import sys
+
     import bench
-    res, procs = bench.cpu_reference_parallel(8, [1, 1], procs=2)
-    assert procs == 2 and len(res) == 2
-    for v, wall, sample in res:
-        assert v > 0 and wall > 0 and "1 FP64 PCG iterations" in sample
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', "
+            "'--n', '16']; runpy.run_path(%r, run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); print('LIBNLF' if 'libnlf' in maps else 'CLEAN')" % bench.__file__)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, check=True)
+    assert out.stdout.strip().splitlines()[-1] == "CLEAN"
+
+
+def test_cpu_reference_parallel_rounds():
+    """Two processes, one 16^3 cell each, two rounds (the first also running the node-scaled preconditioner):
+    per round one row per process with positive setup and per-iteration times."""
+    import bench
+    res = bench.cpu_reference_parallel(8, [(1, True), (1, False)], procs=2)
+    assert len(res) == 2 and all(len(r) == 2 for r in res)
+    for k, rows in enumerate(res):
+        for setup, t_ref, t_sc in rows:
+            assert setup > 0 and t_ref > 0
+            assert (t_sc is not None and t_sc > 0) if k == 0 else t_sc is None
+    assert bench.cpu_rate(res[1], 100) > 0
+
+
+def test_bench_generator_matches_the_oracle_generator():
+    """bench.synth_phi / synth_volume draw the seeded pre-densities the oracle's restatement of the reference
+    generator draws (nlfiber/fiber.py:103-121): equal to rounding, same volumes."""
+    import bench
+    from oracle import density_ref as OD
+    for seed, n_o in ((0, 8), (5, 16), (12, 32)):
+        a, b = bench.synth_phi(seed, n_o), OD.random_start(n_o, 3, seed=seed, kmax=2)
+        assert np.abs(a - b).max() < 1e-13
+        assert bench.synth_volume(seed) == float(np.random.default_rng(10_000 + seed).uniform(0.2, 0.5))

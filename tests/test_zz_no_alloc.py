@@ -4,8 +4,9 @@ regular entry point (nlf_bilinear), on two calls in a row through the C ABI.
 The no-allocation variant exists for callers that may not call cudaMalloc while they run (a handler inside a
 framework that owns all device memory, code inside another library's callback, a service with pre-reserved
 memory). They pass device arrays; the variant keeps its partial sums in a fixed device array shared by all
-calls. Two calls in a row with different inputs check that the second call does not see the first call's
-leftovers. This file is collected last on purpose."""
+calls. Two calls in a row check that the second call does not see the first call's leftovers: the first is the
+larger one (5 cells of 16^3, 6 cases), so it fills partial-sum slots with nonzero values that the second, smaller
+call (2 cells of 8^3, 4 cases) reads again after writing its own. This file is collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -16,9 +17,8 @@ from oracle import density_ref as OD
 pytestmark = pytest.mark.gpu
 
 
-def _case(seed, shape, m):
+def _case(seed, shape, m, ncell):
     rng = np.random.default_rng(seed)
-    ncell = 3
     rho = np.stack([OD.random_cell(seed + i, n_o=shape[0] // 2, beta=8.0)[0] for i in range(ncell)])
     s = 1e-3 + (1 - 1e-3) * np.clip(rho, 0, 1) ** 3
     u = rng.standard_normal((ncell, m) + shape + (3,)) * 0.1
@@ -31,11 +31,10 @@ def test_noalloc_matches_regular_entry_point_twice():
     from nlfiber_b200 import _lib
     from nlfiber_b200 import linear as L
 
-    shape, E, nu = (8, 8, 8), 1.0, 0.3
-    lh = L.LinearHomogenization(shape, E=E, nu=nu)
-    for seed, m in ((11, 6), (23, 4)):
-        s, Es, u = _case(seed, shape, m)
-        ncell = s.shape[0]
+    E, nu = 1.0, 0.3
+    for seed, shape, m, ncell in ((11, (16, 16, 16), 6, 5), (23, (8, 8, 8), 4, 2)):
+        lh = L.LinearHomogenization(shape, E=E, nu=nu)
+        s, Es, u = _case(seed, shape, m, ncell)
         C_ref = np.stack([lh.bilinear(s[i], Es, u[i]) for i in range(ncell)])  # nlf_bilinear
         s_d = torch.from_numpy(s).cuda()
         u_d = torch.from_numpy(u).cuda()
