@@ -888,6 +888,8 @@ def main():
                     help="time the third-order elastic constants of two benchmark cells instead of the default")
     ap.add_argument("--density", action="store_true",
                     help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
+    ap.add_argument("--tune", action="store_true",
+                    help="time every tile variant of the FP64 apply at --n^3 on the batch's vectors and exit")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
                     help="CG preconditioner of the Newton steps: the reference's (fft) or the node-scaled one")
     args = ap.parse_args()
@@ -966,6 +968,22 @@ def main():
                 lh.C_full_batched(rho_d, out_C=C_d)
         torch.cuda.synchronize()
         print(json.dumps({"ncu_case": f"{B} cells {n}^3, {args.iters} PCG iterations, fp64 and mixed"}))
+        return
+
+    if args.tune:
+        lh = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
+        lh.stream = stream
+        res = {}
+        for nv in (24, 6 * FAST["slots"]):
+            res[nv] = lh.autotune(nvec=nv, reps=5, force=True, report=True)["fp64"]
+        from nlfiber_b200 import _lib as LB
+        tiles = [LB.lib.nlf_apply_variants(LB.PREC_FP64)]
+        for v in range(tiles[0]):
+            lh.set_apply_tile(v)
+            tiles.append(lh.apply_tile()[1:])
+        print(json.dumps({"tune": f"apply_f64 at {n}^3", "tiles (TY, TZ, min CTAs/SM)": tiles[1:],
+                          "ms_per_launch": res,
+                          "us_per_vector": {k: [round(1e3 * t / k, 3) for t in v] for k, v in res.items()}}))
         return
 
     # C*: FP64, scaled preconditioner, tight residual

@@ -158,6 +158,20 @@ NLF_API int nlf_C_full(nlf_linear* h, int ncell, const double* rho, const double
  * out (nx, ny, nz/2+1, 6) in the order xx yy zz yz xz xy. */
 NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
 
+/* ---- tile autotuner (no counterpart in the reference, whose operator is a dense einsum that XLA compiles) ------
+ * The stiffness apply has several tile variants (TY x TZ output tile of the (y, z) plane, minimum resident CTAs
+ * per SM); variant 0 is the default. nlf_linear_autotune times every variant of one precision on `nvec`
+ * synthetic vectors of the handle's grid (`reps` launches each, CUDA events on `stream`) and keeps the fastest
+ * for this handle. Its choice is cached per (grid, precision) for the process, so later handles of the same grid
+ * take it without timing unless `force` is set or `ms_out` (one time per variant, milliseconds per launch) is
+ * given. Results of different variants agree to rounding (the apply's partial sums follow the tile), and one
+ * handle's results do not depend on the batch. Synchronizes the stream. */
+NLF_API int nlf_apply_variants(int precision);
+NLF_API int nlf_linear_set_apply_variant(nlf_linear* h, int precision, int variant);
+NLF_API int nlf_linear_get_apply_variant(nlf_linear* h, int precision, int* variant, int* ty, int* tz, int* minb);
+NLF_API int nlf_linear_autotune(nlf_linear* h, int precision, int nvec, int reps, int force, double* ms_out,
+                                void* stream);
+
 /* ---- finite-strain homogenization (nlfiber/mech.py) ------------------------------------------------------- */
 
 /* nlfiber/mech.py:91-103 Cell(rho, E, nu, material, wls, emin, p) without the density: material 0 = linear,

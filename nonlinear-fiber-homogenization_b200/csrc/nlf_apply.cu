@@ -29,10 +29,12 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   constexpr int NP = HY * HZ;
   constexpr int PF = (3 * NP + NT - 1) / NT;  // plane values each thread prefetches per layer
   // One barrier per layer: node plane j lives in pl[j % 3] (written three layers ahead, after the barrier of
-  // the layer that last read the slot), element forces and scales alternate between two buffers.
-  __shared__ T pl[3][3][NP];
-  __shared__ T sl[2][NE];
-  __shared__ T g[2][4][3][NE];
+  // the layer that last read the slot), element forces and scales alternate between two buffers. Dynamic
+  // shared memory (ApplyTiles<TY, TZ, T>::smem() bytes): pl [3][3][NP], g [2][4][3][NE], sl [2][NE].
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*pl)[3][NP] = reinterpret_cast<T(*)[3][NP]>(smem_raw);
+  T(*g)[4][3][NE] = reinterpret_cast<T(*)[4][3][NE]>(smem_raw + sizeof(T) * 9 * NP);
+  T(*sl)[NE] = reinterpret_cast<T(*)[NE]>(smem_raw + sizeof(T) * (9 * NP + 24 * NE));
   __shared__ int gys[HY], gzs[HZ];
   __shared__ double red[32 * 4];
   (void)EY;
@@ -176,36 +178,83 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   }
 }
 
-template <typename T>
-struct ApplyTile;
-template <>
-struct ApplyTile<float> {
-  static constexpr int TY = 8, TZ = 32, MINB = 2;
-};
-template <>
-struct ApplyTile<double> {
-  static constexpr int TY = 8, TZ = 16, MINB = 3;
-};
+// Shared-memory bytes of a k_apply tile.
+template <typename T, int TY, int TZ>
+constexpr size_t apply_smem() {
+  constexpr int NP = (TY + 2) * (TZ + 2), NE = (TY + 1) * (TZ + 1);
+  return sizeof(T) * (9 * NP + 24 * NE + 2 * NE);
+}
+
+template <typename T, int TY, int TZ, int MINB>
+static int launch_apply_tile(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y,
+                             const CellState* cs, double* partial, int* nblk_out, cudaStream_t st) {
+  constexpr int NT = ((TY + 1) * (TZ + 1) + 31) / 32 * 32;
+  constexpr size_t smem = apply_smem<T, TY, TZ>();
+  const Geom& g = h.g;
+  const int tiles = ((g.n2 + TZ - 1) / TZ) * ((g.n1 + TY - 1) / TY);
+  // marches of 16 planes (one halo plane per 16 re-read). The split depends on the grid and the handle's tile
+  // alone, so that the partial sums of a vector, and with them every PCG scalar, are the same whatever else is in
+  // the batch.
+  const int lx = g.n0 >= 32 ? 16 : g.n0;
+  const int chunks = (g.n0 + lx - 1) / lx;
+  if (tiles * chunks > kApplyMaxBlocks) {
+    set_error("apply: %d blocks per vector exceed the partial-sum buffer (%d)", tiles * chunks, kApplyMaxBlocks);
+    return NLF_EBADARG;
+  }
+  if (nblk_out) *nblk_out = tiles * chunks;
+  dim3 grid(tiles, chunks, nvec);
+  const int kind = sizeof(T) == 4 ? PK_APPLY32 : PK_APPLY64;
+  NLF_CUDA_TRY(raise_dyn_smem(k_apply<T, TY, TZ, MINB>, (int)smem));
+  ProfScope ps(kind, st);
+  k_apply<T, TY, TZ, MINB><<<grid, NT, smem, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs, make_modec<T>(h.lam, h.mu),
+                                                    partial, prof_units(), kind);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// The tile variants of the apply (output tile TY x TZ of the (y, z) plane, minimum resident CTAs per SM, which
+// caps the registers): variant 0 is the default; the autotuner (nlf_linear_autotune) may pick another per handle.
+#define NLF_APPLY_VARIANTS_F64(X) X(0, 8, 16, 3) X(1, 4, 16, 5) X(2, 8, 8, 5) X(3, 16, 8, 3) X(4, 4, 32, 2) \
+  X(5, 8, 16, 4) X(6, 2, 32, 4) X(7, 8, 32, 1)
+#define NLF_APPLY_VARIANTS_F32(X) X(0, 8, 32, 2) X(1, 8, 16, 3) X(2, 4, 32, 4) X(3, 16, 32, 1) X(4, 16, 16, 2)
+
+int apply_variants(bool fp64) {
+#define NLF_COUNT(i, ty, tz, mb) +1
+  return fp64 ? (0 NLF_APPLY_VARIANTS_F64(NLF_COUNT)) : (0 NLF_APPLY_VARIANTS_F32(NLF_COUNT));
+#undef NLF_COUNT
+}
+
+void apply_variant_tile(bool fp64, int v, int* ty, int* tz, int* minb) {
+#define NLF_TILE(i, a, b, c) \
+  if (v == i) {             \
+    *ty = a;                \
+    *tz = b;                \
+    *minb = c;              \
+  }
+  *ty = *tz = *minb = 0;
+  if (fp64) {
+    NLF_APPLY_VARIANTS_F64(NLF_TILE)
+  } else {
+    NLF_APPLY_VARIANTS_F32(NLF_TILE)
+  }
+#undef NLF_TILE
+}
 
 template <typename T>
 int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y, const CellState* cs,
                  double* partial, int* nblk_out, cudaStream_t st) {
-  constexpr int TY = ApplyTile<T>::TY, TZ = ApplyTile<T>::TZ, MINB = ApplyTile<T>::MINB;
-  constexpr int NT = ((TY + 1) * (TZ + 1) + 31) / 32 * 32;
-  const Geom& g = h.g;
-  const int tiles = ((g.n2 + TZ - 1) / TZ) * ((g.n1 + TY - 1) / TY);
-  // marches of 16 planes (one halo plane per 16 re-read). The split depends on the grid alone, so that the
-  // partial sums of a vector, and with them every PCG scalar, are the same whatever else is in the batch.
-  const int lx = g.n0 >= 32 ? 16 : g.n0;
-  const int chunks = (g.n0 + lx - 1) / lx;
-  if (nblk_out) *nblk_out = tiles * chunks;
-  dim3 grid(tiles, chunks, nvec);
-  const int kind = sizeof(T) == 4 ? PK_APPLY32 : PK_APPLY64;
-  ProfScope ps(kind, st);
-  k_apply<T, TY, TZ, MINB><<<grid, NT, 0, st>>>(s, x, y, g.n0, g.n1, g.n2, m, lx, cs,
-                                          make_modec<T>(h.lam, h.mu), partial, prof_units(), kind);
-  NLF_CHECK_LAUNCH();
-  return NLF_OK;
+  const int v = h.apply_variant[sizeof(T) == 8 ? 1 : 0];
+#define NLF_CASE(i, ty, tz, mb) \
+  case i:                       \
+    return launch_apply_tile<T, ty, tz, mb>(h, s, m, nvec, x, y, cs, partial, nblk_out, st);
+  if constexpr (sizeof(T) == 8) {
+    switch (v) { NLF_APPLY_VARIANTS_F64(NLF_CASE) default: break; }
+  } else {
+    switch (v) { NLF_APPLY_VARIANTS_F32(NLF_CASE) default: break; }
+  }
+#undef NLF_CASE
+  set_error("apply: no tile variant %d", v);
+  return NLF_EBADARG;
 }
 
 template int launch_apply<float>(const LinearHandle&, const float*, int, int, const float*, float*,

@@ -34,6 +34,9 @@ struct Ede {
 };
 constexpr int kEnergyWindow = 32;
 
+// apply partial sums: at most this many blocks (tiles x x-chunks) per vector
+constexpr int kApplyMaxBlocks = 4096;
+
 // exponent of the node scaling of the scaled preconditioner, w = S^-kNodeScaleExp
 constexpr double kNodeScaleExp = 0.47;
 
@@ -96,6 +99,8 @@ struct LinearHandle {
   // caller's stream by events (capture is not possible on the legacy default stream)
   cudaStream_t gst = nullptr;
   cudaEvent_t gev[2] = {nullptr, nullptr};
+  // apply tile variant per precision ([0] FP32, [1] FP64); 0 = default, set by nlf_linear_autotune
+  int apply_variant[2] = {0, 0};
 };
 
 // ---- launchers (all asynchronous on `st`) ----
@@ -103,6 +108,9 @@ struct LinearHandle {
 template <typename T>
 int launch_apply(const LinearHandle& h, const T* s, int m, int nvec, const T* x, T* y,
                  const CellState* cs, double* partial, int* nblk_out, cudaStream_t st);
+// tile variants of the apply: how many there are, and the tile (TY, TZ, minimum CTAs per SM) of variant v
+int apply_variants(bool fp64);
+void apply_variant_tile(bool fp64, int v, int* ty, int* tz, int* minb);
 int launch_load(const LinearHandle& h, const double* s, const double* fe /*(m,24) on device*/, int m,
                 int ncell, double* f, double sign, cudaStream_t st);
 int launch_bilinear(const LinearHandle& h, const double* s, const double* Es /*device (m,6)*/, int m,

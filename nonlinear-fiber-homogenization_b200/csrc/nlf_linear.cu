@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -233,8 +235,8 @@ static void carve_pcg(Arena& A, const LinearHandle& h, PcgSet<T>& P, int ncell, 
   P.spec = A.take<cplx<T>>((size_t)P.nvec * 3 * h.g.NS);
   P.vs = A.take<VecState>(P.nvec);
   P.cs = A.take<CellState>(ncell);
-  // apply partials: tiles * x-chunks <= 4096 blocks per vec
-  P.part_ap = A.take<double>((size_t)P.nvec * 4096 * 4);
+  // apply partials: tiles * x-chunks <= kApplyMaxBlocks blocks per vec
+  P.part_ap = A.take<double>((size_t)P.nvec * kApplyMaxBlocks * 4);
   P.part_pc = A.take<double>((size_t)P.nvec * 3 * h.g.n0 * 4);
   P.part_b = A.take<double>((size_t)P.nvec * h.g.n1 * h.g.n2h);  // pass-B chunks <= n2h per ky
   P.part_st = A.take<double>((size_t)P.nvec * 3 * kStatsBlocks * 2);
@@ -595,7 +597,7 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       ax64 = A.take<double>(V);
       vs_o = A.take<VecState>(nvec);
       cs_o = A.take<CellState>(ncell);
-      part_ap = A.take<double>((size_t)nvec * 4096 * 4);
+      part_ap = A.take<double>((size_t)nvec * kApplyMaxBlocks * 4);
       part_st = A.take<double>((size_t)nvec * 3 * kStatsBlocks * 2);
       mask = A.take<int>(ncell);
     }
@@ -917,6 +919,143 @@ NLF_API int nlf_apply_K_ex(nlf_linear* H, const double* s, int nvec, const doubl
   }
   if (yd != y) NLF_TRY(copy_out(y, yd, V, st));
   NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  return NLF_OK;
+}
+
+// ---- autotuner of the apply tile -----------------------------------------------------------------------------
+namespace {
+// deterministic pseudo-random fill: a[i] = lo + (hi - lo) * u_i, u_i in [0, 1) from a hash of (seed, i)
+__global__ void k_tune_fill(double* __restrict__ a, long n, unsigned seed, double lo, double hi, int logscale) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ull + seed;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    a[i] = logscale ? exp(log(lo) + (log(hi) - log(lo)) * u) : lo + (hi - lo) * u;
+  }
+}
+__global__ void k_tune_f32(const double* __restrict__ a, float* __restrict__ b, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+std::mutex g_tune_mu;
+std::map<std::array<int, 4>, int> g_tune_cache;  // (n0, n1, n2, fp64) -> variant
+}  // namespace
+
+NLF_API int nlf_apply_variants(int precision) {
+  return apply_variants(precision == NLF_PREC_FP64);
+}
+
+NLF_API int nlf_linear_set_apply_variant(nlf_linear* H, int precision, int variant) {
+  if (bad_handle(H) || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) || variant < 0 ||
+      variant >= apply_variants(precision == NLF_PREC_FP64)) {
+    set_error("nlf_linear_set_apply_variant: bad arguments");
+    return NLF_EBADARG;
+  }
+  H->h.apply_variant[precision == NLF_PREC_FP64 ? 1 : 0] = variant;
+  return NLF_OK;
+}
+
+NLF_API int nlf_linear_get_apply_variant(nlf_linear* H, int precision, int* variant, int* ty, int* tz, int* minb) {
+  if (bad_handle(H) || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) || !variant) {
+    set_error("nlf_linear_get_apply_variant: bad arguments");
+    return NLF_EBADARG;
+  }
+  const bool f64 = precision == NLF_PREC_FP64;
+  *variant = H->h.apply_variant[f64 ? 1 : 0];
+  int a, b, c;
+  apply_variant_tile(f64, *variant, &a, &b, &c);
+  if (ty) *ty = a;
+  if (tz) *tz = b;
+  if (minb) *minb = c;
+  return NLF_OK;
+}
+
+NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps, int force, double* ms_out,
+                                void* stream) {
+  if (bad_handle(H) || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) || nvec < 1 || reps < 1) {
+    set_error("nlf_linear_autotune: bad arguments");
+    return NLF_EBADARG;
+  }
+  LinearHandle& h = H->h;
+  const bool f64 = precision == NLF_PREC_FP64;
+  const int nv = apply_variants(f64);
+  const std::array<int, 4> key{h.g.n0, h.g.n1, h.g.n2, f64 ? 1 : 0};
+  if (!force && !ms_out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      h.apply_variant[f64 ? 1 : 0] = it->second;
+      return NLF_OK;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long N = h.g.N;
+  const size_t V = (size_t)nvec * 3 * N;
+  const size_t w = f64 ? 8 : 4;
+  // s, x, y and the partials in the staging buffer (FP64 s and x are filled, then converted for FP32)
+  NLF_TRY(h.io.reserve(al(N * 8) + 2 * al(V * 8) + al((size_t)nvec * kApplyMaxBlocks * 4 * 8)));
+  char* b = (char*)h.io.ptr;
+  double* s64 = reinterpret_cast<double*>(b);
+  double* x64 = reinterpret_cast<double*>(b + al(N * 8));
+  double* y64 = reinterpret_cast<double*>(b + al(N * 8) + al(V * 8));
+  double* part = reinterpret_cast<double*>(b + al(N * 8) + 2 * al(V * 8));
+  k_tune_fill<<<256, 256, 0, st>>>(s64, N, 1u, h.emin > 0 ? h.emin : 1e-9, 1.0, 1);
+  k_tune_fill<<<1024, 256, 0, st>>>(x64, (long)V, 2u, -1.0, 1.0, 0);
+  NLF_CHECK_LAUNCH();
+  void* sv = s64;
+  void* xv = x64;
+  void* yv = y64;
+  if (!f64) {  // FP32 copies in the upper halves of the FP64 buffers
+    float* s32 = reinterpret_cast<float*>(y64);
+    float* x32 = reinterpret_cast<float*>(x64) + V;
+    k_tune_f32<<<256, 256, 0, st>>>(s64, s32, N);
+    k_tune_f32<<<1024, 256, 0, st>>>(x64, x32, (long)V);
+    NLF_CHECK_LAUNCH();
+    sv = s32;
+    xv = x32;
+    yv = reinterpret_cast<float*>(y64) + N;
+  }
+  (void)w;
+  cudaEvent_t e0, e1;
+  NLF_CUDA_TRY(cudaEventCreate(&e0));
+  NLF_CUDA_TRY(cudaEventCreate(&e1));
+  const int keep = h.apply_variant[f64 ? 1 : 0];
+  int best = keep, rc = NLF_OK;
+  float best_ms = 0.0f;
+  for (int v = 0; v < nv && rc == NLF_OK; ++v) {
+    h.apply_variant[f64 ? 1 : 0] = v;
+    auto run = [&]() {
+      return f64 ? launch_apply<double>(h, (const double*)sv, 6, nvec, (const double*)xv, (double*)yv, nullptr,
+                                        part, nullptr, st)
+                 : launch_apply<float>(h, (const float*)sv, 6, nvec, (const float*)xv, (float*)yv, nullptr, part,
+                                       nullptr, st);
+    };
+    rc = run();  // warm-up
+    if (rc != NLF_OK) break;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && rc == NLF_OK; ++r) rc = run();
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = NLF_ECUDA;
+      set_error("nlf_linear_autotune: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= (float)reps;
+    if (ms_out) ms_out[v] = ms;
+    if (v == 0 || ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h.apply_variant[f64 ? 1 : 0] = rc == NLF_OK ? best : keep;
+  if (rc != NLF_OK) return rc;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best;
   return NLF_OK;
 }
 

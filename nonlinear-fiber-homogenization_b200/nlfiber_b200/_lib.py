@@ -28,6 +28,7 @@ EXPORTS = (
     "nlf_unet_forward", "nlf_unet_backward", "nlf_unet_adam_step",
     "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
     "nlf_correctors_vjp", "nlf_mech_toec",
+    "nlf_apply_variants", "nlf_linear_set_apply_variant", "nlf_linear_get_apply_variant", "nlf_linear_autotune",
 )
 
 
@@ -99,6 +100,10 @@ def _load():
         "nlf_density_vjp": (I, [P, I, I, P, P, D, P, P, P]),
         "nlf_correctors_vjp": (I, [P, I, P, P, P, I, P, P, P, P, P, P, P]),
         "nlf_mech_toec": (I, [P, P, P, P, P]),
+        "nlf_apply_variants": (I, [I]),
+        "nlf_linear_set_apply_variant": (I, [P, I, I]),
+        "nlf_linear_get_apply_variant": (I, [P, I, P, P, P, P]),
+        "nlf_linear_autotune": (I, [P, I, I, I, I, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -98,7 +98,7 @@ class LinearHomogenization:
 
     def __init__(self, shape, E=1.0, nu=0.3, emin=1e-3, p=3.0, dtype=np.float64, tol=1e-9, maxit=4000,
                  precision="fp64", precond="fft", inner_tol=1e-3, inner_maxit=200, max_sweeps=20, check_every=8,
-                 slots=0, use_graphs=False, scale_x0=False, energy_tol=0.0):
+                 slots=0, use_graphs=False, scale_x0=False, energy_tol=0.0, autotune=False):
         shape = tuple(int(n) for n in shape)
         self.plane = len(shape) == 2
         self.shape = shape + (1,) if self.plane else shape
@@ -121,6 +121,33 @@ class LinearHomogenization:
         self._h = h
         self._Kinv = None
         self.stream = None  # cudaStream_t handle (int) used by every call; None = the legacy default stream
+        if autotune:
+            self.autotune()
+
+    def autotune(self, nvec=24, reps=3, force=False, report=False):
+        """Pick the fastest tile of the stiffness apply for this grid (nlf_linear_autotune) in the solver's
+        precision(s): FP64, and FP32 too for precision="mixed". The choice is cached per grid for the process.
+        With report=True every variant is timed and {precision: [ms per launch of each variant]} is returned."""
+        out = {}
+        precs = ["fp64"] + (["mixed"] if self.precision == "mixed" else [])
+        for pr in precs:
+            code = _PREC[pr]
+            ms = np.zeros(lib.nlf_apply_variants(code)) if report else None
+            check(lib.nlf_linear_autotune(self._h, code, int(nvec), int(reps), int(force), ptr(ms), self.stream))
+            if report:
+                out[pr] = ms.tolist()
+        return out
+
+    def apply_tile(self, precision="fp64"):
+        """(variant, TY, TZ, min CTAs per SM) of the apply tile this handle uses."""
+        v, ty, tz, mb = (ctypes.c_int() for _ in range(4))
+        check(lib.nlf_linear_get_apply_variant(self._h, _PREC[precision], ctypes.byref(v), ctypes.byref(ty),
+                                               ctypes.byref(tz), ctypes.byref(mb)))
+        return v.value, ty.value, tz.value, mb.value
+
+    def set_apply_tile(self, variant, precision="fp64"):
+        """Use apply tile variant `variant` (0 = default) for this handle."""
+        check(lib.nlf_linear_set_apply_variant(self._h, _PREC[precision], int(variant)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

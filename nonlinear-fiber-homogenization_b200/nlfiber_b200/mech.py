@@ -64,20 +64,44 @@ def _dot(a, b):
     return float(a @ b)
 
 
-def _linesearch(E, gnorm, x, dx, E0, slope, gn):
-    """mech.py:73-85: halve from t = 1 until Armijo (1e-4) holds, or the energy is flat to rounding and the
-    gradient norm drops; None below t = 1e-6."""
-    tol = 64 * np.finfo(np.float64).eps * max(abs(E0), 1e-300)
-    t = 1.0
-    while t > 1e-6:
-        Et = E(x + t * dx)
-        if np.isfinite(Et):
-            if Et <= E0 + 1e-4 * t * slope:
-                return t
-            if Et <= E0 + tol and gnorm(x + t * dx) < gn:
-                return t
-        t *= 0.5
+def _backtrack(energy_at, gnorm_at, E0, slope, gn, c1=1e-4, t_min=1e-6):
+    """Step length along a descent direction (the rule of nlfiber/mech.py:73-85). Trial steps t = 1, 1/2, 1/4, ...
+    while t > t_min; a trial is accepted when its energy is finite and either meets the sufficient-decrease
+    (Armijo) condition E(t) <= E0 + c1 t slope, or lies within 64 ulps of E0 (the energy is flat to rounding)
+    while the gradient norm at t is below gn. Returns the accepted t, or None."""
+    flat = E0 + 64 * np.finfo(np.float64).eps * max(abs(E0), 1e-300)
+    trials = 1.0 / 2.0 ** np.arange(64)
+    for t in trials[trials > t_min]:
+        e = energy_at(float(t))
+        if not np.isfinite(e):
+            continue
+        if e <= E0 + c1 * t * slope or (e <= flat and gnorm_at(float(t)) < gn):
+            return float(t)
     return None
+
+
+class _Forcing:
+    """CG tolerance per Newton step (the rule of nlfiber/mech.py:310-322). With Eisenstat-Walker forcing
+    (Eisenstat & Walker 1996, choice 2 with gamma 0.9 and exponent 2): eta = 0.1 at the first step, then
+    0.9 (||g|| / ||g_prev||)^2, kept at least 0.9 eta_prev^2 when that exceeds 0.1, and capped at 0.1; the
+    tolerance is max(eta, cg_tol), and from the second step on also at least 1/2 rtol g0 / ||g|| (no tighter than
+    the outer test needs). Without it, the fixed cg_tol."""
+
+    def __init__(self, ew):
+        self.ew = ew
+        self.g_last = None
+        self.eta = None
+
+    def tolerance(self, gn, g0, rtol, cg_tol):
+        first = self.g_last is None
+        tol = cg_tol
+        if self.ew:
+            eta = 0.1 if first else 0.9 * (gn / self.g_last) ** 2
+            floor = 0.9 * self.eta ** 2 if self.eta is not None else 0.0
+            self.eta = min(max(eta, floor) if floor > 0.1 else eta, 0.1)
+            tol = max(self.eta, cg_tol) if first else max(self.eta, cg_tol, 0.5 * rtol * g0 / gn)
+        self.g_last = gn
+        return tol
 
 
 class Cell:
@@ -388,41 +412,45 @@ class Mixed:
                                         maxiter)
         return vals, (vecs * dsc[:, None]).cpu().numpy(), its
 
+    def _direction(self, z, Fb, g, tol, cg_maxit, sws, log):
+        """Newton direction at z: CG on the tangent for H dz = -g (counted in the log); when it is not a descent
+        direction (g . dz >= 0, e.g. after negative curvature), the preconditioned steepest descent
+        -proj(M g) instead (nlfiber/mech.py:323-331). Returns (dz, g . dz)."""
+        A = self.tangent(z, Fb)
+        dmac = self.macro_diag(A, Fb) if self.k else np.zeros(0)
+        dz, its, _ok, neg = self._cgA(A, -g, dmac, sws, tol, int(cg_maxit))
+        log["cg"] += int(its)
+        log["negative_curvature"] |= bool(neg)
+        slope = _dot(g, dz)
+        if slope >= 0:
+            dz = -self.proj(self.precond(g, dmac, sws))
+            slope = _dot(g, dz)
+        return dz, slope
+
     def solve(self, Fbar, z0=None, rtol=1e-9, maxnewton=30, cg_tol=1e-6, cg_maxit=20000, g_ref=None):
-        """mech.py:302-346: Newton-CG. Returns (w, Fbar_full, log) with log['z'] the state."""
+        """mech.py:302-346: Newton-CG on the energy in z = (w, free Fbar entries). Each step: the projected
+        gradient g and its norm (logged); stop when ||g|| <= rtol max(g0, 1e-300) or ||g|| < 1e-14, with g0 =
+        g_ref or the first norm; else a CG direction to the forcing tolerance, a backtracking step, and the
+        update. A failed line search ends the solve, as converged at the round-off floor when ||g|| <=
+        STALL_RTOL g0. Returns (w, Fbar_full, log) with the reference's log keys and log['z'] the state."""
         Fb = np.asarray(Fbar, dtype=np.float64)
         z = self.z0(Fb) if z0 is None else self._as_state(z0)
-        g0, log = g_ref, dict(newton=0, cg=0, converged=False, gnorm=[], negative_curvature=False)
-        eta, gprev = None, None
+        log = {"newton": 0, "cg": 0, "converged": False, "gnorm": [], "negative_curvature": False}
+        forcing = _Forcing(self.forcing == "ew")
         sws = self._sws()
-        for k in range(maxnewton):
+        g0 = g_ref
+        for step in range(maxnewton):
             g = self.proj(self._g(z, Fb))
             gn = _norm(g)
-            g0 = gn if g0 is None else g0
             log["gnorm"].append(gn)
+            g0 = gn if g0 is None else g0
             if gn <= rtol * max(g0, 1e-300) or gn < 1e-14:
                 log["converged"] = True
                 break
-            tol = cg_tol
-            if self.forcing == "ew":
-                e_new = 0.1 if gprev is None else 0.9 * (gn / gprev) ** 2
-                if eta is not None and 0.9 * eta ** 2 > 0.1:
-                    e_new = max(e_new, 0.9 * eta ** 2)
-                eta = min(e_new, 0.1)
-                tol = max(eta, cg_tol, 0.5 * rtol * g0 / gn) if gprev is not None else max(eta, cg_tol)
-            gprev = gn
-            A = self.tangent(z, Fb)
-            dmac = self.macro_diag(A, Fb) if self.k else np.zeros(0)
-            dz, its, ok, neg = self._cgA(A, -g, dmac, sws, tol, int(cg_maxit))
-            log["cg"] += int(its)
-            log["negative_curvature"] |= bool(neg)
-            E0, slope = float(self._E(z, Fb)), _dot(g, dz)
-            if slope >= 0:
-                dz = -self.proj(self.precond(g, dmac, sws))
-                slope = _dot(g, dz)
-            t = _linesearch(lambda x: self._E(x, Fb), lambda x: _norm(self.proj(self._g(x, Fb))),
-                            z, dz, E0, slope, gn)
-            log["newton"] = k + 1
+            dz, slope = self._direction(z, Fb, g, forcing.tolerance(gn, g0, rtol, cg_tol), cg_maxit, sws, log)
+            t = _backtrack(lambda t: self._E(z + t * dz, Fb), lambda t: _norm(self.proj(self._g(z + t * dz, Fb))),
+                           float(self._E(z, Fb)), slope, gn)
+            log["newton"] = step + 1
             if t is None:
                 log["linesearch_failed"] = True
                 if gn <= STALL_RTOL * g0:

@@ -1,0 +1,117 @@
+"""GPU: the measured path of the throughput benchmark against the NumPy oracle, on the benchmark's own cells.
+
+The measured path: FP64 PCG with the node-scaled FFT preconditioner on 64^3 cells at a 1e-9 void floor, the fused
+FFT pass C that updates x and p and leaves z unprojected, the energy guard, slot refill and CUDA-graph replay of
+the iterations. Two checks:
+  - its iterates: 8 iterations (tol 0) equal the oracle's PCG with the restated scaled preconditioner, in the
+    energy norm of the problem (1e-6) and in the C they give (1e-10). On these cells PCG amplifies rounding
+    fast: in the oracle alone, a relative perturbation of 1e-15 of each preconditioned residual moves the
+    iterate of the island cell (seed 0) by 4e-10 in the energy norm after 8 iterations and by 3e-2 after 20, so
+    later iterates of two correct FP64 implementations are not comparable; the converged C is;
+  - its C: the benchmark settings give every C entry within 1e-8 (the metric's bound) of the oracle's C solved
+    to a relative residual of 1e-12 on the host (tests/golden/bench_golden.npz, made by
+    tests/golden/make_bench_golden.py), on 64^3 cells with floating solid islands, a clean cell and a long
+    shear plateau, on the 32^3 batched workload, and on the Schwarz-P cell (with dC/drho).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import density_ref as OD
+from oracle import linear_ref as OL
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bench_golden.npz")
+MAT = dict(E=1.0, nu=0.3, emin=1e-9, p=3.0)
+# the benchmark's solver settings (bench.FAST) with graph replay
+FAST = dict(precision="fp64", precond="scaled", tol=1e-9, energy_tol=1e-10, maxit=4000, check_every=16,
+            slots=24, use_graphs=True)
+C_TOL = 1e-8  # the metric's relative C error
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def cerr(C, Co):
+    """Per-cell max_IJ |C - C_o| / max |C_o|."""
+    C, Co = np.asarray(C), np.asarray(Co)
+    return np.abs(C - Co).reshape(len(C), -1).max(1) / np.abs(Co).reshape(len(Co), -1).max(1)
+
+
+@pytest.fixture(scope="module")
+def L():
+    from nlfiber_b200 import linear
+    return linear
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+def test_measured_path_iterates_match_oracle_64(L):
+    """Two 64^3 benchmark cells (seed 0: three floating solid islands; seed 12: clean) through one slot, so the
+    second starts when the first stops (slot refill), graphs on, tol 0 and maxit 8: each cell's projected
+    correctors after 8 iterations equal the oracle's PCG with the scaled preconditioner (nlfiber/linear.py:173-203
+    with M = ScaledPrecond): ||u - u_o||_K <= 1e-6 ||u_o||_K summed over the 6 cases, with K = K(s) the cell's
+    stiffness, and the C of the iterates (bilinear, nlfiber/linear.py:220-229) within 1e-10."""
+    seeds = (0, 12)
+    rho = np.stack([OD.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, tol=0.0, maxit=8, slots=1))
+    res = lh.C_full_batched(rho, want_u=True)
+    assert list(res["it"]) == [8, 8]
+    oh = OL.LinearHomogenization(rho.shape[1:], **MAT, tol=0.0)
+    for k in range(len(seeds)):
+        s = oh.stiffness_scale(rho[k])
+        uo, ito = oh.solve(s, np.eye(6), maxit=8, M=OL.ScaledPrecond(oh, s))
+        assert ito == 8
+        u = res["u"][k]
+        d = u - uo
+        eK = np.sqrt(sum(np.sum(di * oh.apply_K(s, di)) for di in d) / sum(np.sum(x * oh.apply_K(s, x)) for x in uo))
+        Cg, Co = oh.bilinear(s, np.eye(6), u), oh.bilinear(s, np.eye(6), uo)
+        info = dict(seed=seeds[k], energy_rel=eK, C_rel=rel(Cg, Co), max_rel=rel(u, uo))
+        assert eK < 1e-6 and rel(Cg, Co) < 1e-10, info
+
+
+def test_measured_path_C_matches_oracle_64(L, golden):
+    """The benchmark settings on the fixture's 64^3 cells (2 slots for 4 cells, so refill runs): every C entry
+    within 1e-8 of the oracle's tightly solved C."""
+    seeds = [int(v) for v in golden["b64_seeds"]]
+    rho = np.stack([OD.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    np.testing.assert_allclose(rho.sum(axis=(1, 2, 3)), golden["b64_rho_sum"], rtol=1e-13)
+    lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=2))
+    res = lh.C_full_batched(rho)
+    assert res["status"] == 0
+    err = cerr(res["C"], golden["b64_C"])
+    assert err.max() < C_TOL, dict(zip(seeds, err))
+
+
+def test_batched_32_C_matches_oracle(L, golden):
+    """The 32^3 batched workload's generator (octant 16): 8 cells through 3 slots, every C within 1e-8."""
+    seeds = [int(v) for v in golden["b32_seeds"]]
+    rho = np.stack([OD.random_cell(i, n_o=16, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=3))
+    res = lh.C_full_batched(rho)
+    assert res["status"] == 0
+    err = cerr(res["C"], golden["b32_C"])
+    assert err.max() < C_TOL, dict(zip(seeds, err))
+
+
+def test_schwarz_p_cell_C_and_dC(L, golden):
+    """The Schwarz-P cell of 32^3 (octant 16, v 0.3, r 1.5, beta 16, emin 1e-9): C from the reference algorithm
+    (unit-stiffness preconditioner, tol 1e-10 as the configuration states, enough iterations) and from the scaled
+    one both within 1e-8 of the oracle's; dC/drho at the GPU correctors equals the oracle's closed form to 1e-11."""
+    rho = OD.schwarz_p_cell(16, v=0.3, r=1.5, beta=16.0)
+    Co = golden["schwarz_C"][0]
+    ref = L.LinearHomogenization(rho.shape, **MAT, tol=1e-10, maxit=40000, check_every=64, use_graphs=True)
+    C_ref, u_ref, it_ref = ref.C_full(rho)
+    assert rel(C_ref, Co) < C_TOL, (rel(C_ref, Co), it_ref)
+    sc = L.LinearHomogenization(rho.shape, **MAT, **dict(FAST, tol=1e-10))
+    r = sc.C_full_batched(rho[None], want_u=True, want_dC=True)
+    assert rel(r["C"][0], Co) < C_TOL
+    oh = OL.LinearHomogenization(rho.shape, **MAT)
+    dCo = oh.dC_drho(rho, np.eye(6), r["u"][0])
+    assert rel(r["dC"][0], dCo) < 1e-11

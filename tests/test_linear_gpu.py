@@ -263,3 +263,24 @@ def test_correctors_vjp_matches_oracle(L, shape):
     rb, _, _ = lh.correctors_vjp(None, Es, u, ubar, rho=rho)
     rb_o = sb_o * oh.dscale_drho(rho)
     assert np.abs(rb - rb_o).max() <= 1e-8 * np.abs(rb_o).max()
+
+
+def test_apply_tile_variants_and_autotune(L):
+    """Every tile variant of the stiffness apply gives the oracle's K(s) u to rounding (FP64 1e-13, FP32 2e-6),
+    on a grid that is not a multiple of the tiles; the autotuner keeps one of them and reports a time for each."""
+    from nlfiber_b200 import _lib
+    shape = (20, 24, 36)
+    rng = np.random.default_rng(5)
+    s = 1e-9 + rng.random(shape) ** 3
+    u = rng.standard_normal((2,) + shape + (3,))
+    lh, oh = L.LinearHomogenization(shape), OL.LinearHomogenization(shape)
+    Ku = np.stack([oh.apply_K(s, x) for x in u])
+    for prec, tol in (("fp64", 1e-13), ("mixed", 2e-6)):
+        for v in range(_lib.lib.nlf_apply_variants(_lib.PREC_FP64 if prec == "fp64" else _lib.PREC_MIXED)):
+            lh.set_apply_tile(v, prec)
+            assert lh.apply_tile(prec)[0] == v
+            assert rel(lh.apply_K(s, u, precision=prec), Ku) < tol, (prec, lh.apply_tile(prec))
+    times = lh.autotune(nvec=4, reps=2, report=True)
+    v = lh.apply_tile("fp64")[0]
+    assert len(times["fp64"]) == _lib.lib.nlf_apply_variants(_lib.PREC_FP64) and min(times["fp64"]) > 0
+    assert times["fp64"][v] == min(times["fp64"])
