@@ -495,16 +495,35 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   }
   P.s = s_sl;
   P.w = w_sl;
-  PinnedBuf pin(S * sizeof(CellState) + (size_t)S * m * sizeof(VecState));
+  // Host snapshots of the slots' state, double-buffered: the host reads the snapshot taken after chunk j while
+  // chunk j + 1 is already queued, so the GPU never waits for the host between chunks. A slot refilled while
+  // reading snapshot j still shows its previous cell in snapshot j + 1 (copied before the refill was queued), so
+  // it is read again from snapshot j + 2 on. A stopped cell's slot therefore idles for one extra chunk, which
+  // costs no GPU time: the kernels skip inactive cells.
+  const size_t snap = S * sizeof(CellState) + (size_t)S * m * sizeof(VecState);
+  PinnedBuf pin(2 * snap);
   if (!pin.p) {
     set_error("cudaMallocHost failed");
     return NLF_ECUDA;
   }
-  CellState* cs_h = static_cast<CellState*>(pin.p);
-  VecState* vs_h = reinterpret_cast<VecState*>(cs_h + S);
+  CellState* csb[2];
+  VecState* vsb[2];
+  for (int k = 0; k < 2; ++k) {
+    csb[k] = reinterpret_cast<CellState*>(static_cast<char*>(pin.p) + k * snap);
+    vsb[k] = reinterpret_cast<VecState*>(csb[k] + S);
+  }
+  struct Events {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  for (int k = 0; k < 2; ++k) NLF_CUDA_TRY(cudaEventCreateWithFlags(&ev.e[k], cudaEventDisableTiming));
   NLF_CUDA_TRY(cudaMemsetAsync(P.cs, 0, S * sizeof(CellState), st));  // every slot empty and inactive
   const PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede};
   std::vector<int> slot_cell(S, -1);
+  std::vector<long> valid_from(S, 0);  // first snapshot index that shows the slot's current cell
   int next = 0;
   auto start = [&](int sl) -> int {
     const int c = next++;
@@ -527,19 +546,29 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
     if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, m, in.x0 + (size_t)c * Vc, v.x, 1.0, st)));
     return pcg_init<double, double>(h, v, bs, xg, ctl, nullptr, st);
   };
+  auto take_snapshot = [&](long k) -> int {
+    const int b = (int)(k & 1);
+    NLF_CUDA_TRY(cudaMemcpyAsync(csb[b], P.cs, S * sizeof(CellState), cudaMemcpyDeviceToHost, st));
+    NLF_CUDA_TRY(cudaMemcpyAsync(vsb[b], P.vs, (size_t)S * m * sizeof(VecState), cudaMemcpyDeviceToHost, st));
+    NLF_CUDA_TRY(cudaEventRecord(ev.e[b], st));
+    return NLF_OK;
+  };
   for (int sl = 0; sl < S && next < ncell; ++sl) NLF_TRY(start(sl));
   const int every = ctl.check_every > 0 ? ctl.check_every : 1;
   IterGraph G;
   int status = NLF_OK;
-  for (;;) {
-    NLF_CUDA_TRY(cudaMemcpyAsync(cs_h, P.cs, S * sizeof(CellState), cudaMemcpyDeviceToHost, st));
-    NLF_CUDA_TRY(cudaMemcpyAsync(vs_h, P.vs, (size_t)S * m * sizeof(VecState), cudaMemcpyDeviceToHost, st));
-    NLF_CUDA_TRY(cudaStreamSynchronize(st));
+  NLF_TRY(take_snapshot(0));  // the state after the starts (cells may stop before their first iteration)
+  for (long j = 0;; ++j) {
+    NLF_TRY(run_iterations<double>(h, P, ctl, every, o.use_graphs != 0, G, st));
+    NLF_TRY(take_snapshot(j + 1));
+    NLF_CUDA_TRY(cudaEventSynchronize(ev.e[j & 1]));
+    const CellState* cs_h = csb[j & 1];
+    const VecState* vs_h = vsb[j & 1];
     int nact = 0;
     for (int sl = 0; sl < S; ++sl) {
       const int c = slot_cell[sl];
       if (c < 0) continue;
-      if (cs_h[sl].active) {
+      if (valid_from[sl] > j || cs_h[sl].active) {
         ++nact;
         continue;
       }
@@ -552,11 +581,14 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
       slot_cell[sl] = -1;
       if (next < ncell) {
         NLF_TRY(start(sl));
+        valid_from[sl] = j + 2;
         ++nact;
       }
     }
-    if (nact == 0) break;
-    NLF_TRY(run_iterations<double>(h, P, ctl, every, o.use_graphs != 0, G, st));
+    if (nact == 0) {
+      NLF_CUDA_TRY(cudaEventSynchronize(ev.e[(j + 1) & 1]));  // the last snapshot's copy into pinned memory
+      break;
+    }
   }
   return status;
 }

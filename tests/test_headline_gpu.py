@@ -28,6 +28,12 @@ MAT = dict(E=1.0, nu=0.3, emin=1e-9, p=3.0)
 FAST = dict(precision="fp64", precond="scaled", tol=1e-9, energy_tol=1e-10, maxit=4000, check_every=16,
             slots=24, use_graphs=True)
 C_TOL = 1e-8  # the metric's relative C error
+# Absolute floor of the C comparison (E = 1). C is a mean over the elements of s_e times a bracket whose terms are
+# O(E) and cancel in an element that moves rigidly. In cells whose solid floats in the void (seed 5 of the
+# generator: max |C| = 3.5e-8 at 64^3, 6.2e-8 at 32^3) that cancellation leaves C at 1e-8 E, and the FP64
+# assembly of either implementation rounds it at ~1e-14 E, i.e. 2e-7 of max |C|: the GPU and the oracle then
+# agree to 6e-15 whatever the iteration count (500 to 32000), which no relative test at 1e-8 can see.
+C_FLOOR = 1e-13
 
 
 def rel(a, b):
@@ -39,6 +45,13 @@ def cerr(C, Co):
     """Per-cell max_IJ |C - C_o| / max |C_o|."""
     C, Co = np.asarray(C), np.asarray(Co)
     return np.abs(C - Co).reshape(len(C), -1).max(1) / np.abs(Co).reshape(len(Co), -1).max(1)
+
+
+def c_agrees(C, Co):
+    """Per cell: every entry within the metric's relative bound of max |C_o| or within the absolute FP64 floor."""
+    C, Co = np.asarray(C), np.asarray(Co)
+    bound = C_TOL * np.abs(Co).reshape(len(Co), -1).max(1)[:, None, None] + C_FLOOR
+    return (np.abs(C - Co) <= bound).reshape(len(C), -1).all(1)
 
 
 @pytest.fixture(scope="module")
@@ -78,7 +91,7 @@ def test_measured_path_iterates_match_oracle_64(L):
 
 def test_measured_path_C_matches_oracle_64(L, golden):
     """The benchmark settings on the fixture's 64^3 cells (2 slots for 4 cells, so refill runs): every C entry
-    within 1e-8 of the oracle's tightly solved C."""
+    within 1e-8 max |C_o| (or the FP64 floor 1e-13 E) of the oracle's tightly solved C."""
     seeds = [int(v) for v in golden["b64_seeds"]]
     rho = np.stack([OD.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
     np.testing.assert_allclose(rho.sum(axis=(1, 2, 3)), golden["b64_rho_sum"], rtol=1e-13)
@@ -86,18 +99,21 @@ def test_measured_path_C_matches_oracle_64(L, golden):
     res = lh.C_full_batched(rho)
     assert res["status"] == 0
     err = cerr(res["C"], golden["b64_C"])
-    assert err.max() < C_TOL, dict(zip(seeds, err))
+    absd = np.abs(res["C"] - golden["b64_C"]).reshape(len(seeds), -1).max(1)
+    assert c_agrees(res["C"], golden["b64_C"]).all(), dict(zip(seeds, zip(err, absd)))
 
 
 def test_batched_32_C_matches_oracle(L, golden):
-    """The 32^3 batched workload's generator (octant 16): 8 cells through 3 slots, every C within 1e-8."""
+    """The 32^3 batched workload's generator (octant 16): 8 cells through 3 slots, every C entry within
+    1e-8 max |C_o| (or the FP64 floor 1e-13 E)."""
     seeds = [int(v) for v in golden["b32_seeds"]]
     rho = np.stack([OD.random_cell(i, n_o=16, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
     lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=3))
     res = lh.C_full_batched(rho)
     assert res["status"] == 0
     err = cerr(res["C"], golden["b32_C"])
-    assert err.max() < C_TOL, dict(zip(seeds, err))
+    absd = np.abs(res["C"] - golden["b32_C"]).reshape(len(seeds), -1).max(1)
+    assert c_agrees(res["C"], golden["b32_C"]).all(), dict(zip(seeds, zip(err, absd)))
 
 
 def test_schwarz_p_cell_C_and_dC(L, golden):
