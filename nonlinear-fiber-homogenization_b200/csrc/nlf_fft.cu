@@ -873,12 +873,50 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// The inverse preconditioner symbol at one wavenumber in closed form (the same values as the Kinv table, to
+// rounding). For the Q1 element with exact (2x2x2 Gauss) integration the unit-stiffness symbol factorises into the
+// 1D symbols of the linear hat, m = (2 + cos t) / 3 (mass), s = 2 - 2 cos t (stiffness) and g = sin t (gradient):
+// S_aa = s_a m_b m_c, S_ab = g_a g_b m_c, K = lam S + mu (tr S I + S); then (K + 1e-12 |tr K| I)^-1, and 0 at k = 0
+// (nlfiber/linear.py:154-165). The y and z factors are per thread; (mx, sx, gx) per x frequency.
+struct SymYZ {
+  double my, sy, gy, mz, sz, gz;
+};
+__device__ __forceinline__ SymYZ sym_yz(const cplx<double>* __restrict__ tw, int ky, int kz) {
+  const double cy = tw[ky].x, cz = tw[kz].x;
+  return {(2.0 + cy) * (1.0 / 3.0), 2.0 - 2.0 * cy, -tw[ky].y, (2.0 + cz) * (1.0 / 3.0), 2.0 - 2.0 * cz, -tw[kz].y};
+}
+__device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx, double lam, double mu,
+                                            double (&out)[6]) {
+  const double mx = (2.0 + cx) * (1.0 / 3.0), sx = 2.0 - 2.0 * cx;
+  const double Sxx = sx * q.my * q.mz, Syy = mx * q.sy * q.mz, Szz = mx * q.my * q.sz;
+  const double Syz = mx * q.gy * q.gz, Sxz = gx * q.gz * q.my, Sxy = gx * q.gy * q.mz;
+  const double lm = lam + mu, tr = Sxx + Syy + Szz;
+  double a = lm * Sxx + mu * tr, b = lm * Syy + mu * tr, c = lm * Szz + mu * tr;
+  const double d = lm * Syz, e = lm * Sxz, f = lm * Sxy;
+  const double reg = 1e-12 * fabs(a + b + c);
+  a += reg;
+  b += reg;
+  c += reg;
+  // inverse of [[a f e] [f b d] [e d c]]
+  const double cxx = b * c - d * d, cxy = d * e - c * f, cxz = d * f - b * e;
+  const double cyy = a * c - e * e, cyz = e * f - a * d, czz = a * b - f * f;
+  const double id = 1.0 / (a * cxx + f * cxy + e * cxz);
+  out[0] = cxx * id;
+  out[1] = cyy * id;
+  out[2] = czz * id;
+  out[3] = cyz * id;
+  out[4] = cxz * id;
+  out[5] = cxy * id;
+}
+
 // Pass B: x FFT of the three components of each (ky, kz) column, 3x3 Kinv, Parseval (r, z) partial, inverse.
-template <int N>
-__global__ void __launch_bounds__(Fast<N>::NTB, 2)
+// CLOSED: the Kinv entries are computed in closed form from the twiddles and the medium's (lam, mu) instead of
+// read from the table.
+template <int N, bool CLOSED>
+__global__ void __maxnreg__(112)
     k_fb_fast(cplx<double>* __restrict__ spec, const double* __restrict__ kinv, int m,
               const cplx<double>* __restrict__ tw_x, const CellState* __restrict__ cs,
-              unsigned long long* __restrict__ units, int ukind, PcgFuse fu) {
+              unsigned long long* __restrict__ units, int ukind, PcgFuse fu, double lam, double mu) {
   using F = Fast<N>;
   constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN;
   __shared__ double red[32];
@@ -904,10 +942,25 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   double dot[1] = {0.0};
   const double wt = (kz == 0 || kz == M) ? 1.0 : 2.0;
   const int kb = 4 * brevL<L>(l);
+  SymYZ q{};
+  if constexpr (CLOSED) q = sym_yz(tw_x, ky, ok ? kz : 0);
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) {
-    const double* K = kinv + (((long)(k1 + kb) * N + ky) * H + (ok ? kz : 0)) * 6;
-    const double kxx = K[0], kyy = K[1], kzz = K[2], kyz = K[3], kxz = K[4], kxy = K[5];
+    double Kv[6];
+    if constexpr (CLOSED) {
+      const int kx = k1 + kb;
+      if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) Kv[i] = 0.0;
+      } else {
+        kinv_closed(q, tw_x[kx].x, -tw_x[kx].y, lam, mu, Kv);
+      }
+    } else {
+      const double* K = kinv + (((long)(k1 + kb) * N + ky) * H + (ok ? kz : 0)) * 6;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) Kv[i] = K[i];
+    }
+    const double kxx = Kv[0], kyy = Kv[1], kzz = Kv[2], kyz = Kv[3], kxz = Kv[4], kxy = Kv[5];
     const cplx<double> A = a[0][k1], B = a[1][k1], C = a[2][k1];
     const cplx<double> ua{kxx * A.x + kxy * B.x + kxz * C.x, kxx * A.y + kxy * B.y + kxz * C.y};
     const cplx<double> ub{kxy * A.x + kyy * B.x + kyz * C.x, kxy * A.y + kyy * B.y + kyz * C.y};
@@ -1267,9 +1320,15 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   if (stages & 2) {
     ProfScope ps(PK_FFTB64, st);
     // the scaled preconditioner (w given) inverts its own reference medium
-    k_fb_fast<N><<<dim3(N / F::KY, F::KZC, nvec), F::NTB, 0, st>>>(spec, w ? h.t64s.kinv : h.t64.kinv, m, twx, cs,
-                                                                     units, PK_FFTB64,
-                                                                     fu);
+    const double* kinv = w ? h.t64s.kinv : h.t64.kinv;
+    // the medium of the inverse: the scaled preconditioner's reference medium, else the material
+    const double nu0 = w ? h.scaled_ref_nu : h.nu;
+    const double lam0 = h.E * nu0 / ((1.0 + nu0) * (1.0 - 2.0 * nu0)), mu0 = h.E / (2.0 * (1.0 + nu0));
+    const dim3 grid(N / F::KY, F::KZC, nvec);
+    if (h.pcb_closed)
+      k_fb_fast<N, true><<<grid, F::NTB, 0, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
+    else
+      k_fb_fast<N, false><<<grid, F::NTB, 0, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
     NLF_CHECK_LAUNCH();
   }
   if (stages & 4) {

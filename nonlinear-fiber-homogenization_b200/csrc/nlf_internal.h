@@ -101,6 +101,8 @@ struct LinearHandle {
   cudaEvent_t gev[2] = {nullptr, nullptr};
   // apply tile variant per precision ([0] FP32, [1] FP64); 0 = default, set by nlf_linear_autotune
   int apply_variant[2] = {0, 0};
+  // FP64 cube pass B: 1 = Kinv entries in closed form (no table reads), 0 = from the table
+  int pcb_closed = 0;
 };
 
 // ---- launchers (all asynchronous on `st`) ----

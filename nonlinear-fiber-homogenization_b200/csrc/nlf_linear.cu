@@ -1003,6 +1003,17 @@ NLF_API int nlf_linear_get_apply_variant(nlf_linear* H, int precision, int* vari
   return NLF_OK;
 }
 
+NLF_API int nlf_linear_set_kinv_mode(nlf_linear* H, int mode) {
+  if (bad_handle(H) || (mode != 0 && mode != 1)) {
+    set_error("nlf_linear_set_kinv_mode: bad arguments");
+    return NLF_EBADARG;
+  }
+  H->h.pcb_closed = mode;
+  return NLF_OK;
+}
+
+NLF_API int nlf_linear_get_kinv_mode(nlf_linear* H) { return bad_handle(H) ? NLF_EBADARG : H->h.pcb_closed; }
+
 NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps, int force, double* ms_out,
                                 void* stream) {
   if (bad_handle(H) || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) || nvec < 1 || reps < 1) {
@@ -1017,7 +1028,8 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      h.apply_variant[f64 ? 1 : 0] = it->second;
+      h.apply_variant[f64 ? 1 : 0] = it->second % 1000;
+      if (f64) h.pcb_closed = it->second / 1000;
       return NLF_OK;
     }
   }
@@ -1082,12 +1094,47 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
       best = v;
     }
   }
+  h.apply_variant[f64 ? 1 : 0] = rc == NLF_OK ? best : keep;
+  // FP64 cubes with the register-resident FFT passes: pass B with the Kinv table or in closed form, timed on the
+  // scaled preconditioner of the same vectors (node scaling from s)
+  int pcb = h.pcb_closed;
+  if (rc == NLF_OK && f64 && precond_fuses_px(h)) {
+    DevBuf& tb = h.io2;
+    rc = tb.reserve(al(N * 8) + al((size_t)nvec * 3 * h.g.NS * 16));
+    double* w64 = rc == NLF_OK ? static_cast<double*>(tb.ptr) : nullptr;
+    cplx<double>* spec = rc == NLF_OK ? reinterpret_cast<cplx<double>*>(static_cast<char*>(tb.ptr) + al(N * 8))
+                                      : nullptr;
+    if (rc == NLF_OK) rc = launch_node_scaling(h, 1, s64, nullptr, w64, nullptr, st);
+    float best_pc = 0.0f;
+    for (int v = 0; v < 2 && rc == NLF_OK; ++v) {
+      h.pcb_closed = v;
+      rc = launch_precond<double>(h, nvec, 6, x64, y64, spec, w64, nullptr, part, st);
+      if (rc != NLF_OK) break;
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps && rc == NLF_OK; ++r) rc = launch_precond<double>(h, nvec, 6, x64, y64, spec, w64,
+                                                                              nullptr, part, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = NLF_ECUDA;
+        set_error("nlf_linear_autotune: %s", cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= (float)reps;
+      if (ms_out) ms_out[nv + v] = ms;
+      if (v == 0 || ms < best_pc) {
+        best_pc = ms;
+        pcb = v;
+      }
+    }
+    h.pcb_closed = rc == NLF_OK ? pcb : 0;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  h.apply_variant[f64 ? 1 : 0] = rc == NLF_OK ? best : keep;
   if (rc != NLF_OK) return rc;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = best;
+  g_tune_cache[key] = best + 1000 * h.pcb_closed;
   return NLF_OK;
 }
 

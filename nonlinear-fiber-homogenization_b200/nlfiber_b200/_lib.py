@@ -29,6 +29,7 @@ EXPORTS = (
     "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
     "nlf_correctors_vjp", "nlf_mech_toec",
     "nlf_apply_variants", "nlf_linear_set_apply_variant", "nlf_linear_get_apply_variant", "nlf_linear_autotune",
+    "nlf_linear_set_kinv_mode", "nlf_linear_get_kinv_mode",
 )
 
 
@@ -104,6 +105,8 @@ def _load():
         "nlf_linear_set_apply_variant": (I, [P, I, I]),
         "nlf_linear_get_apply_variant": (I, [P, I, P, P, P, P]),
         "nlf_linear_autotune": (I, [P, I, I, I, I, P, P]),
+        "nlf_linear_set_kinv_mode": (I, [P, I]),
+        "nlf_linear_get_kinv_mode": (I, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -126,13 +126,15 @@ class LinearHomogenization:
 
     def autotune(self, nvec=24, reps=3, force=False, report=False):
         """Pick the fastest tile of the stiffness apply for this grid (nlf_linear_autotune) in the solver's
-        precision(s): FP64, and FP32 too for precision="mixed". The choice is cached per grid for the process.
-        With report=True every variant is timed and {precision: [ms per launch of each variant]} is returned."""
+        precision(s): FP64, and FP32 too for precision="mixed"; on FP64 cubes of 32 or 64 also the Kinv mode of the
+        preconditioner (table or closed form). The choice is cached per grid for the process. With report=True
+        every variant is timed and {precision: [ms per launch of each apply variant, then for FP64 cubes the
+        preconditioner with the table and in closed form]} is returned."""
         out = {}
         precs = ["fp64"] + (["mixed"] if self.precision == "mixed" else [])
         for pr in precs:
             code = _PREC[pr]
-            ms = np.zeros(lib.nlf_apply_variants(code)) if report else None
+            ms = np.zeros(lib.nlf_apply_variants(code) + (2 if pr == "fp64" else 0)) if report else None
             check(lib.nlf_linear_autotune(self._h, code, int(nvec), int(reps), int(force), ptr(ms), self.stream))
             if report:
                 out[pr] = ms.tolist()
@@ -144,6 +146,15 @@ class LinearHomogenization:
         check(lib.nlf_linear_get_apply_variant(self._h, _PREC[precision], ctypes.byref(v), ctypes.byref(ty),
                                                ctypes.byref(tz), ctypes.byref(mb)))
         return v.value, ty.value, tz.value, mb.value
+
+    @property
+    def kinv_mode(self):
+        """0: the FP64 cube preconditioner reads its Kinv table; 1: it computes the entries in closed form."""
+        return int(lib.nlf_linear_get_kinv_mode(self._h))
+
+    @kinv_mode.setter
+    def kinv_mode(self, mode):
+        check(lib.nlf_linear_set_kinv_mode(self._h, int(mode)))
 
     def set_apply_tile(self, variant, precision="fp64"):
         """Use apply tile variant `variant` (0 = default) for this handle."""

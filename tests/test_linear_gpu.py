@@ -284,3 +284,19 @@ def test_apply_tile_variants_and_autotune(L):
     v = lh.apply_tile("fp64")[0]
     assert len(times["fp64"]) == _lib.lib.nlf_apply_variants(_lib.PREC_FP64) and min(times["fp64"]) > 0
     assert times["fp64"][v] == min(times["fp64"])
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64)])
+def test_preconditioner_kinv_closed_form(L, shape):
+    """The register-resident preconditioner with its Kinv entries in closed form (kinv_mode 1) equals the oracle's
+    table-based inverse symbol (nlfiber/linear.py:154-170) to FP64 rounding, unscaled and scaled."""
+    rng = np.random.default_rng(3)
+    s = 1e-9 + rng.random(shape) ** 3
+    u = rng.standard_normal((2,) + shape + (3,))
+    lh, oh = L.LinearHomogenization(shape), OL.LinearHomogenization(shape)
+    lh.kinv_mode = 1
+    assert lh.kinv_mode == 1
+    assert rel(lh.precond(u), oh.precond(u)) < 1e-12
+    assert rel(lh.precond(u, precond="scaled", s=s), _scaled_oracle(oh, s, u)) < 1e-12
+    lh.kinv_mode = 0
+    assert rel(lh.precond(u, precond="scaled", s=s), _scaled_oracle(oh, s, u)) < 1e-12
