@@ -41,8 +41,9 @@ MATERIAL = dict(E=1.0, nu=0.3, emin=1e-9, p=3.0)
 # near-mechanism cells with C still 1e-3 off. C* (CSTAR) runs to a relative residual of 1e-14 or 10000
 # iterations. (The FP32-in-FP64-refinement path cannot reach 1e-8 on cells with solid islands held only by the
 # 1e-9 void: their rigid motions are below FP32 resolution.)
-FAST = dict(precision="fp64", precond="scaled", tol=1e-9, energy_tol=1e-10, maxit=4000, check_every=16, slots=24)
-CSTAR = dict(precision="fp64", precond="scaled", tol=1e-14, maxit=10000, check_every=32, slots=24)
+FAST = dict(precision="fp64", precond="scaled", tol=1e-9, energy_tol=1e-10, maxit=4000, check_every=16, slots=24,
+            autotune=True)
+CSTAR = dict(precision="fp64", precond="scaled", tol=1e-14, maxit=10000, check_every=32, slots=24, autotune=True)
 # iterations the reference algorithm (FP64 PCG, unit-stiffness FFT preconditioner, nlfiber/linear.py:154-203)
 # needs per 64^3 cell of this workload to bring C within 1e-8 of C*, from `--calibrate-plain` on B200 (the plain
 # FP64 GPU path runs the reference's iterates): cells 0-3 needed > 32000, 4000, 32000 and 16000; the mean,
@@ -893,6 +894,8 @@ def main():
                     help="time the third-order elastic constants of two benchmark cells instead of the default")
     ap.add_argument("--density", action="store_true",
                     help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
+    ap.add_argument("--per-case", type=int, default=None,
+                    help="per-case stopping probation for the measured solve (0 = lock-step per cell)")
     ap.add_argument("--tune", action="store_true",
                     help="time every tile variant of the FP64 apply at --n^3 on the batch's vectors and exit")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
@@ -976,7 +979,7 @@ def main():
         return
 
     if args.tune:
-        lh = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
+        lh = L.LinearHomogenization((n, n, n), **MATERIAL, **dict(FAST, autotune=False))
         lh.stream = stream
         res = {}
         for nv in (24, 6 * FAST["slots"]):
@@ -1007,7 +1010,8 @@ def main():
             print(json.dumps(dict(res, workload=f"{B} seeded synthetic {n}^3 cells x 6 unit strains")), flush=True)
         return
 
-    lh = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
+    fast = dict(FAST) if args.per_case is None else dict(FAST, per_case=args.per_case)
+    lh = L.LinearHomogenization((n, n, n), **MATERIAL, **fast)
     lh.stream = stream
     for _ in range(args.warmup):
         lh.C_full_batched(rho_d, out_C=C_d)
@@ -1087,8 +1091,11 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, B, world),
         "solver": "FP64 PCG, node-scaled FFT preconditioner, "
-                  f"{FAST['slots']} cells in flight, a converged cell's slot refilled from the queue, "
-                  f"stop at residual {FAST['tol']} and energy guard {FAST['energy_tol']}",
+                  f"{fast['slots']} cells in flight, a converged cell's slot refilled from the queue, "
+                  f"stop at residual {fast['tol']} and energy guard {fast['energy_tol']}" +
+                  (f", per-case stopping after {fast['per_case']} iterations of both rules holding"
+                   if fast.get("per_case") else ", lock-step per cell"),
+        "tuning": {"apply_tile (variant, TY, TZ, min CTAs/SM)": list(lh.apply_tile()), "kinv_mode": lh.kinv_mode},
         "c_err_max": float(err.max()), "c_err_entries": ent,
         "c_err_vs_oracle": vs_oracle,
         "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},

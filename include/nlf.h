@@ -65,6 +65,12 @@ typedef struct nlf_solve_opts {
                         N (C_II(u) - C_II*) (Hestenes-Stiefel), which bounds every |C_IJ(u) - C*_IJ|; C_JJ comes
                         from the same recurrences. It keeps cells whose residual is small but whose C is not
                         (near-mechanisms of the solid) running; it never stops a cell earlier. 0: residual rule only. */
+  int per_case;      /* > 0 (FP64 cubes of 32 or 64): per-case stopping. A load case stops on its own once the
+                        residual rule (and the energy guard, if on) has held for this many consecutive iterations;
+                        its corrector is then frozen while the cell's other cases go on, and the cell stops when all
+                        its cases have (or by the lock-step rule). The probation guards against cases whose
+                        residual dips below tol before a slow mode of the cell surfaces. 0: lock-step per cell, the
+                        reference's rule (nlfiber/linear.py:185-188). */
 } nlf_solve_opts;
 
 NLF_API const char* nlf_last_error(void);

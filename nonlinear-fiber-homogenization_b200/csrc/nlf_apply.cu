@@ -40,7 +40,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   (void)EY;
 
   const int vec = blockIdx.z, cell = vec / m;
-  if (cs && !cs[cell].active) return;
+  if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
   const long N = (long)n0 * n1 * n2;
   const long P = (long)n1 * n2;

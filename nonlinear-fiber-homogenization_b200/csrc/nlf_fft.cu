@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(256, 2)
   cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);  // [P][N rows][H]
   __shared__ double red[32 * 2 * P];
   const int c = blockIdx.y, vec = blockIdx.z;
-  if (cs && !cs[vec / m].active) return;
+  if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
   const int t = threadIdx.x;
   const int p = t / (N * Lz), rem = t - p * (N * Lz), y = rem / Lz, l = rem - y * Lz;
@@ -921,7 +921,7 @@ __global__ void __maxnreg__(112)
   constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN;
   __shared__ double red[32];
   const int vec = blockIdx.z;
-  if (cs && !cs[vec / m].active) return;
+  if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
   const int t = threadIdx.x, task = t / L, l = t - task * L;
   const int kyl = task / KZN, kzl = task - kyl * KZN;
@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(256, 2)
   cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);
   __shared__ double red[32 * 4];
   const int c = blockIdx.y, vec = blockIdx.z;
-  if (cs && !(fu.p ? (cs[vec / m].status & 2) : cs[vec / m].active)) return;
+  if (!(fu.p ? vec_ran(cs, vec, m) : vec_live(cs, vec, m))) return;
   prof_count(units, ukind);
   const int t = threadIdx.x;
   const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
@@ -1167,8 +1167,8 @@ __global__ void __launch_bounds__(256, 2)
   const long nplanes = (long)nvec * 3 * N;
   auto active = [&](long j) {
     if (!cs) return true;
-    const CellState& s = cs[(int)(j / (3 * N)) / m];
-    return fu.p ? (s.status & 2) != 0 : s.active != 0;
+    const int vec = (int)(j / (3 * N));
+    return fu.p ? vec_ran(cs, vec, m) : vec_live(cs, vec, m);
   };
   auto next_active = [&](long j) {
     while (j < nplanes && !active(j)) j += gridDim.x;

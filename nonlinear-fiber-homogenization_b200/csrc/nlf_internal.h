@@ -26,6 +26,8 @@ struct VecState {
   double x0scale;  // energy-optimal multiple of the initial guess (scale_x0)
   double ebase;    // N C_II at the start: (E D E) sum(s) + x0.K x0 - 2 (b, x0)   (energy stopping rule)
   double esum;     // sum over the iterations so far of alpha_j (r_j, z_j)
+  int streak;      // per-case stopping: consecutive iterations in which this case met both stopping rules
+  int pad_;
 };
 
 // energy stopping rule: E_I D E_I of the cases (m <= 6) and the window of alpha (r, z) terms it sums
@@ -45,13 +47,26 @@ constexpr double kNodeScaleExp = 0.47;
 // material's own (E, nu), as the reference does.
 constexpr double kScaledRefNu = 0.0;
 
-// Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188).
+// Per-cell PCG control. `active` follows the reference's lock-step cond (nlfiber/linear.py:185-188). With
+// per-case stopping, `stopped` has bit I set once load case I stopped on its own; `status` bit 1 says the cell
+// runs the current iteration, bit 4 + I that case I does (both set by the mark at the start of the iteration).
 struct CellState {
   int it;
   int active;
   int status;
-  int pad;
+  int stopped;
 };
+
+// vector vec = cell m + case takes part in the current iteration (its cell is active, the case has not stopped)
+__host__ __device__ inline bool vec_live(const CellState* cs, int vec, int m) {
+  if (!cs) return true;
+  const CellState& c = cs[vec / m];
+  return c.active && !((c.stopped >> (vec % m)) & 1);
+}
+// vector vec ran the current iteration (marked live at its start)
+__host__ __device__ inline bool vec_ran(const CellState* cs, int vec, int m) {
+  return !cs || ((cs[vec / m].status >> (4 + vec % m)) & 1);
+}
 
 // Grow-only device buffer.
 struct DevBuf {

@@ -197,6 +197,7 @@ struct PcgCtl {
   int scale_x0;
   double energy_tol;  // > 0: energy stopping rule (needs ede)
   Ede ede;
+  int per_case = 0;   // > 0: per-case stopping with this probation (fused FP64 iterations only)
 };
 
 template <typename T>
@@ -258,7 +259,7 @@ static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl,
       // r update, (r, r) and (r, z) ride on passes A and B; the control sets beta; pass C updates x and p
       NLF_TRY(launch_precond_pcg_ab(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.spec, P.w, P.cs, partA, P.part_b, &nchunk, st));
       NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, nullptr, nchunk, P.vs, P.cs,
-                                  ctl.tol, ctl.maxit, P.ring, ctl.energy_tol, st));
+                                  ctl.tol, ctl.maxit, P.ring, ctl.energy_tol, ctl.per_case, st));
       return launch_precond_pcg_cpx(h, P.nvec, P.m, P.spec, P.w, P.vs, P.cs, P.x, P.p, st);
     }
   }
@@ -267,7 +268,7 @@ static int pcg_iteration(const LinearHandle& h, PcgSet<T>& P, const PcgCtl& ctl,
   NLF_TRY(launch_precond_pcg<T>(h, P.nvec, P.m, P.r, P.Ap, P.vs, P.z, P.spec, P.w, P.cs, partA, P.part_b, partC,
                                 &nchunk, st));
   NLF_TRY(launch_fin_pc_fused(P.ncell, P.m, h.g.n0, h.g.n1, N, partA, P.part_b, partC, nchunk, P.vs, P.cs, ctl.tol,
-                              ctl.maxit, P.ring, ctl.energy_tol, st));
+                              ctl.maxit, P.ring, ctl.energy_tol, 0, st));
   NLF_TRY(launch_px<T>(N, P.nvec, P.m, P.x, P.p, P.z, P.vs, P.cs, st));
   return NLF_OK;
 }
@@ -521,7 +522,8 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   } ev;
   for (int k = 0; k < 2; ++k) NLF_CUDA_TRY(cudaEventCreateWithFlags(&ev.e[k], cudaEventDisableTiming));
   NLF_CUDA_TRY(cudaMemsetAsync(P.cs, 0, S * sizeof(CellState), st));  // every slot empty and inactive
-  const PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede};
+  const PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede,
+                   precond_fuses_px(h) ? o.per_case : 0};
   std::vector<int> slot_cell(S, -1);
   std::vector<long> valid_from(S, 0);  // first snapshot index that shows the slot's current cell
   int next = 0;
@@ -661,7 +663,8 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       if (scaled) NLF_TRY(launch_node_scaling(h, ncell, in.s64, nullptr, w64, nullptr, st));
       const bool xg = in.x0 != nullptr;
       if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, P64.x, 1.0, st)));
-      PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede};
+      PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede,
+                 precond_fuses_px(h) ? o.per_case : 0};
       if (o.slots > 0 && o.slots < ncell) return solve_slots(h, in, o, xout, iters_h, st);
       NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, o.use_graphs != 0, st)));
       NLF_CUDA_TRY(cudaMemcpyAsync(xout, P64.x, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -831,6 +834,7 @@ NLF_API void nlf_default_opts(nlf_solve_opts* o) {
   o->max_sweeps = 20;
   o->check_every = 8;
   o->use_graphs = 0;
+  o->per_case = 0;
   o->slots = 0;
   o->scale_x0 = 0;
   o->energy_tol = 0.0;

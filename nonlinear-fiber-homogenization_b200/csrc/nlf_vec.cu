@@ -215,7 +215,7 @@ __global__ void k_fin_apply(const double* __restrict__ partial, int nblk, long N
   const int vec = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
   if (vec >= nvec) return;
-  if (cs && !cs[vec / m].active) return;
+  if (!vec_live(cs, vec, m)) return;
   double a[4] = {0, 0, 0, 0};
   for (int b = lane; b < nblk; b += 32) {
     const double* o = partial + ((long)vec * nblk + b) * 4;
@@ -293,6 +293,7 @@ __global__ void k_fin_pc(const double* __restrict__ partial, int n0, long N, Vec
         rr += a[c][3];
       }
       if (!init) v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
+      if (init) v.streak = 0;
       v.rz = rz1;
       v.rr = rr;
       if (sqrt(rr) > tol * v.bn) atomicOr(&go, 1);
@@ -334,81 +335,104 @@ __global__ void k_p(long N, T* __restrict__ p, const T* __restrict__ z, const Ve
 __global__ void k_fin_pc_fused(const double* __restrict__ partA, const double* __restrict__ partB,
                                const double* __restrict__ partC, int nchunk, int n0, int n1, long N,
                                VecState* __restrict__ vs, CellState* __restrict__ cs, int m, double tol, int maxit,
-                               double* __restrict__ ring, double etol) {
-  __shared__ int go;
+                               double* __restrict__ ring, double etol, int probation) {
   __shared__ double s_nc[8], s_w[8];
+  __shared__ int s_res[8];
   const int cell = blockIdx.x;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (!cs[cell].active) return;
   const int itk = cs[cell].it;  // index of the iteration that just ran
-  if (threadIdx.x == 0) go = 0;
-  __syncthreads();
+  const int stopped = cs[cell].stopped;
   if (wid < m) {
     const int vec = cell * m + wid;
-    double sr[3] = {0, 0, 0}, sz[3] = {0, 0, 0}, rr = 0.0, dot = 0.0;
-    for (int c = 0; c < 3; ++c)
-      for (int x = lane; x < n0; x += 32) {
-        const long i = ((long)vec * 3 + c) * n0 + x;
-        sr[c] += partA[2 * i];
-        rr += partA[2 * i + 1];
-        if (partC) sz[c] += partC[i];
-      }
-    for (int i = lane; i < n1 * nchunk; i += 32) dot += partB[(long)vec * n1 * nchunk + i];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        sr[c] += __shfl_down_sync(0xffffffffu, sr[c], o);
-        sz[c] += __shfl_down_sync(0xffffffffu, sz[c], o);
-      }
-      rr += __shfl_down_sync(0xffffffffu, rr, o);
-      dot += __shfl_down_sync(0xffffffffu, dot, o);
-    }
-    if (etol > 0.0) {
-      // energy rule: the error energy ||x* - x_k||_K^2 = sum_{j >= k} alpha_j (r_j, z_j) (Hestenes-Stiefel),
-      // estimated by the last kEnergyWindow terms; N C_II(x_k) = ebase - esum
-      const double term = vs[vec].alpha * vs[vec].rz;
-      double* rg = ring + (long)vec * kEnergyWindow;
-      const int nw = min(itk + 1, kEnergyWindow), slot = itk % kEnergyWindow;
-      double w = (lane < nw && lane != slot) ? rg[lane] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if ((stopped >> wid) & 1) {
+      // a case that stopped on its own keeps its state; it counts as holding both rules, and its error-energy
+      // base N C_II enters the cell's scale as before
       if (lane == 0) {
-        rg[slot] = term;
-        VecState& v = vs[vec];
-        v.esum += term;
-        s_w[wid] = w + term;
-        s_nc[wid] = v.ebase - v.esum;
+        s_res[wid] = 1;
+        s_w[wid] = 0.0;
+        s_nc[wid] = vs[vec].ebase - vs[vec].esum;
       }
-    }
-    if (lane == 0) {
-      VecState& v = vs[vec];
-      double rz1 = dot / (double)N;
-      if (partC)
-        for (int c = 0; c < 3; ++c) {
-          const double mz = sz[c] / (double)N;
-          v.mean[c] = mz;
-          rz1 -= mz * sr[c];
+    } else {
+      double sr[3] = {0, 0, 0}, sz[3] = {0, 0, 0}, rr = 0.0, dot = 0.0;
+      for (int c = 0; c < 3; ++c)
+        for (int x = lane; x < n0; x += 32) {
+          const long i = ((long)vec * 3 + c) * n0 + x;
+          sr[c] += partA[2 * i];
+          rr += partA[2 * i + 1];
+          if (partC) sz[c] += partC[i];
         }
-      v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
-      v.rz = rz1;
-      v.rr = rr;
-      if (sqrt(rr) > tol * v.bn) atomicOr(&go, 1);
+      for (int i = lane; i < n1 * nchunk; i += 32) dot += partB[(long)vec * n1 * nchunk + i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          sr[c] += __shfl_down_sync(0xffffffffu, sr[c], o);
+          sz[c] += __shfl_down_sync(0xffffffffu, sz[c], o);
+        }
+        rr += __shfl_down_sync(0xffffffffu, rr, o);
+        dot += __shfl_down_sync(0xffffffffu, dot, o);
+      }
+      if (etol > 0.0) {
+        // energy rule: the error energy ||x* - x_k||_K^2 = sum_{j >= k} alpha_j (r_j, z_j) (Hestenes-Stiefel),
+        // estimated by the last kEnergyWindow terms; N C_II(x_k) = ebase - esum
+        const double term = vs[vec].alpha * vs[vec].rz;
+        double* rg = ring + (long)vec * kEnergyWindow;
+        const int nw = min(itk + 1, kEnergyWindow), slot = itk % kEnergyWindow;
+        double w = (lane < nw && lane != slot) ? rg[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+        if (lane == 0) {
+          rg[slot] = term;
+          VecState& v = vs[vec];
+          v.esum += term;
+          s_w[wid] = w + term;
+          s_nc[wid] = v.ebase - v.esum;
+        }
+      }
+      if (lane == 0) {
+        VecState& v = vs[vec];
+        double rz1 = dot / (double)N;
+        if (partC)
+          for (int c = 0; c < 3; ++c) {
+            const double mz = sz[c] / (double)N;
+            v.mean[c] = mz;
+            rz1 -= mz * sr[c];
+          }
+        v.beta = rz1 / (v.rz == 0.0 ? 1.0 : v.rz);
+        v.rz = rz1;
+        v.rr = rr;
+        s_res[wid] = sqrt(rr) <= tol * v.bn;
+      }
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    bool eok = false;
-    if (etol > 0.0 && itk + 1 >= kEnergyWindow) {
-      double cmax = 0.0;
-      for (int I = 0; I < m; ++I) cmax = fmax(cmax, s_nc[I]);
-      eok = cmax > 0.0;
-      for (int I = 0; I < m; ++I) eok = eok && s_w[I] <= etol * cmax;
+    // the energy rule of case I: its window sum at most etol times the cell's largest N C_JJ (after a full window)
+    bool eok[8];
+    double cmax = 0.0;
+    for (int I = 0; I < m; ++I) cmax = fmax(cmax, s_nc[I]);
+    for (int I = 0; I < m; ++I)
+      eok[I] = etol <= 0.0 || (itk + 1 >= kEnergyWindow && cmax > 0.0 && s_w[I] <= etol * cmax);
+    bool go = false, eall = true;
+    for (int I = 0; I < m; ++I) {
+      go = go || !s_res[I];
+      eall = eall && eok[I];
     }
-    // with the energy rule a cell stops only when both the residual rule and the energy rule hold
     CellState& s = cs[cell];
+    int stop = stopped;
+    if (probation > 0)
+      for (int I = 0; I < m; ++I) {
+        if ((stopped >> I) & 1) continue;
+        VecState& v = vs[cell * m + I];
+        v.streak = (s_res[I] && eok[I]) ? v.streak + 1 : 0;
+        if (v.streak >= probation) stop |= 1 << I;
+      }
+    s.stopped = stop;
     s.it += 1;
-    s.active = (s.it < maxit) && (go || (etol > 0.0 && !eok));
+    // lock-step: the cell stops when every case meets the residual rule and (with the energy guard) the energy
+    // rule in the same iteration; with per-case stopping also when every case has stopped on its own
+    s.active = (s.it < maxit) && (go || (etol > 0.0 && !eall)) && stop != (1 << m) - 1;
   }
 }
 
@@ -531,7 +555,10 @@ __global__ void k_x0_apply(long N, T* __restrict__ x, T* __restrict__ Ax, const 
 // status bit 1 <- active (marks the cells that run the current iteration, for k_p after k_fin_pc)
 __global__ void k_mark(CellState* cs, int ncell) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < ncell) cs[c].status = (cs[c].status & ~2) | (cs[c].active ? 2 : 0);
+  if (c < ncell) {
+    const int live = cs[c].active ? (2 | (((~cs[c].stopped) & 0x3F) << 4)) : 0;
+    cs[c].status = (cs[c].status & ~(2 | (0x3F << 4))) | live;
+  }
 }
 
 __global__ void k_cs_init(CellState* cs, int ncell, const int* __restrict__ mask) {
@@ -539,7 +566,8 @@ __global__ void k_cs_init(CellState* cs, int ncell, const int* __restrict__ mask
   if (c < ncell) {
     cs[c].it = 0;
     cs[c].active = mask ? mask[c] : 1;
-    cs[c].status = cs[c].active ? 2 : 0;
+    cs[c].status = cs[c].active ? (2 | (0x3F << 4)) : 0;
+    cs[c].stopped = 0;
   }
 }
 
@@ -617,10 +645,10 @@ int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, cons
 }
 int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
                         const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
-                        double* ring, double etol, cudaStream_t st) {
+                        double* ring, double etol, int probation, cudaStream_t st) {
   ProfScope ps_(PK_FIN, st);
   k_fin_pc_fused<<<ncell, 32 * m, 0, st>>>(partA, partB, partC, nchunk, n0, n1, N, vs, cs, m, tol, maxit, ring,
-                                           etol);
+                                           etol, probation);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }

@@ -25,10 +25,12 @@ int launch_fin_pc(int ncell, int m, int n0, long N, const double* partial, VecSt
 template <typename T>
 int launch_p(long N, int nvec, int m, T* p, const T* z, const VecState* vs, const CellState* cs, int init,
              cudaStream_t st);
-// fused iteration: (r, z), sums and the lock-step control from the FFT passes' partials; x and p updates together
+// fused iteration: (r, z), sums and the lock-step control from the FFT passes' partials; x and p updates together.
+// probation > 0 (per-case stopping): a load case stops on its own once both stopping rules have held for that many
+// consecutive iterations (CellState::stopped); the cell stops when all its cases have, or by the lock-step rule.
 int launch_fin_pc_fused(int ncell, int m, int n0, int n1, long N, const double* partA, const double* partB,
                         const double* partC, int nchunk, VecState* vs, CellState* cs, double tol, int maxit,
-                        double* ring, double etol, cudaStream_t st);
+                        double* ring, double etol, int probation, cudaStream_t st);
 // energy stopping rule, at the start of a solve: ebase = ede[I] sum(s of the cell) (+ x0.K x0 - 2 (b, x0) when
 // x_given; Ax holds K x0 and its means), esum = 0
 template <typename Tb, typename T>

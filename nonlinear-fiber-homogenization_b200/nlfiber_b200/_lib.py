@@ -40,6 +40,7 @@ class SolveOpts(ctypes.Structure):
         ("maxit", ctypes.c_int), ("inner_tol", ctypes.c_double), ("inner_maxit", ctypes.c_int),
         ("max_sweeps", ctypes.c_int), ("check_every", ctypes.c_int), ("use_graphs", ctypes.c_int),
         ("slots", ctypes.c_int), ("scale_x0", ctypes.c_int), ("energy_tol", ctypes.c_double),
+        ("per_case", ctypes.c_int),
     ]
 
 

@@ -98,7 +98,7 @@ class LinearHomogenization:
 
     def __init__(self, shape, E=1.0, nu=0.3, emin=1e-3, p=3.0, dtype=np.float64, tol=1e-9, maxit=4000,
                  precision="fp64", precond="fft", inner_tol=1e-3, inner_maxit=200, max_sweeps=20, check_every=8,
-                 slots=0, use_graphs=False, scale_x0=False, energy_tol=0.0, autotune=False):
+                 slots=0, use_graphs=False, scale_x0=False, energy_tol=0.0, per_case=0, autotune=False):
         shape = tuple(int(n) for n in shape)
         self.plane = len(shape) == 2
         self.shape = shape + (1,) if self.plane else shape
@@ -109,6 +109,7 @@ class LinearHomogenization:
         self.check_every = check_every
         self.slots, self.use_graphs, self.scale_x0 = int(slots), bool(use_graphs), bool(scale_x0)
         self.energy_tol = float(energy_tol)
+        self.per_case = int(per_case)
         B = B_matrices()
         D = iso_D(E, nu)
         self.Dm = D
@@ -173,7 +174,7 @@ class LinearHomogenization:
             tol=self.tol if tol is None else float(tol), maxit=self.maxit if maxit is None else int(maxit),
             inner_tol=float(self.inner_tol), inner_maxit=int(self.inner_maxit), max_sweeps=int(self.max_sweeps),
             check_every=int(self.check_every), slots=self.slots, use_graphs=int(self.use_graphs),
-            scale_x0=int(self.scale_x0), energy_tol=self.energy_tol)
+            scale_x0=int(self.scale_x0), energy_tol=self.energy_tol, per_case=self.per_case)
 
     def _cell(self, a, extra=()):
         """Coerce a per-cell field to (nx, ny, nz) + extra, adding the plane-strain axis where needed."""

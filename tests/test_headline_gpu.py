@@ -131,3 +131,24 @@ def test_schwarz_p_cell_C_and_dC(L, golden):
     oh = OL.LinearHomogenization(rho.shape, **MAT)
     dCo = oh.dC_drho(rho, np.eye(6), r["u"][0])
     assert rel(r["dC"][0], dCo) < 1e-11
+
+
+@pytest.mark.parametrize("key,n_o,slots", [("b64", 32, 2), ("b32", 16, 3)])
+def test_per_case_stopping_keeps_C(L, golden, key, n_o, slots):
+    """Per-case stopping (a load case stops on its own after both rules held for 64 consecutive iterations) on the
+    fixture's cells: every C entry within 1e-8 max |C_o| (or the FP64 floor) of the oracle's, no cell iterating
+    longer than under the lock-step rule, and the stopped cases' corrector frozen at a residual within the rule."""
+    seeds = [int(v) for v in golden[f"{key}_seeds"]]
+    rho = np.stack([OD.random_cell(i, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    lock = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=slots)).C_full_batched(rho)
+    pc = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=slots, per_case=64))
+    res = pc.C_full_batched(rho, want_u=True)
+    assert res["status"] == 0
+    assert c_agrees(res["C"], golden[f"{key}_C"]).all(), dict(zip(seeds, cerr(res["C"], golden[f"{key}_C"])))
+    assert (res["it"] <= lock["it"]).all(), (res["it"], lock["it"])
+    oh = OL.LinearHomogenization(rho.shape[1:], **MAT)
+    s = oh.stiffness_scale(rho[0])
+    r = oh.residual(s, np.eye(6), res["u"][0])
+    b = OL.proj(oh.load(s, np.eye(6)))
+    rel_res = np.sqrt((r ** 2).sum(axis=(1, 2, 3, 4)) / (b ** 2).sum(axis=(1, 2, 3, 4)))
+    assert rel_res.max() < 1e-8, rel_res
