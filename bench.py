@@ -967,7 +967,7 @@ def main():
     C_d = torch.empty((B, 6, 6), dtype=torch.float64, device="cuda")
 
     if args.ncu:
-        kw = dict(FAST, tol=0.0, maxit=args.iters)
+        kw = dict(FAST, tol=0.0, maxit=args.iters, autotune=False)
         for prec in ("fp64", "mixed"):
             lh = L.LinearHomogenization((n, n, n), **MATERIAL, **dict(kw, precision=prec, inner_maxit=args.iters,
                                                                         inner_tol=0.0, max_sweeps=1))
@@ -1095,7 +1095,8 @@ def main():
                   f"stop at residual {fast['tol']} and energy guard {fast['energy_tol']}" +
                   (f", per-case stopping after {fast['per_case']} iterations of both rules holding"
                    if fast.get("per_case") else ", lock-step per cell"),
-        "tuning": {"apply_tile (variant, TY, TZ, min CTAs/SM)": list(lh.apply_tile()), "kinv_mode": lh.kinv_mode},
+        "tuning": {"apply_tile (variant, TY, TZ, min CTAs/SM)": list(lh.apply_tile()), "kinv_mode": lh.kinv_mode,
+                   "fft_shared_twiddles": lh.fft_twiddles},
         "c_err_max": float(err.max()), "c_err_entries": ent,
         "c_err_vs_oracle": vs_oracle,
         "iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},

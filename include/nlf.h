@@ -171,12 +171,16 @@ NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
  * for this handle. Its choice is cached per (grid, precision) for the process, so later handles of the same grid
  * take it without timing unless `force` is set or `ms_out` (one time per variant, milliseconds per launch) is
  * given. On FP64 cubes of 32 or 64 it also times the preconditioner with its Kinv entries read from the table
- * (mode 0) or computed in closed form (mode 1; nlf_linear_set_kinv_mode), ms_out[nvariants + mode]. Results of
+ * (mode 0) or computed in closed form (mode 1; nlf_linear_set_kinv_mode), and passes A and C with their
+ * twiddles in registers (0) or read from a shared-memory copy of the tables at 3 CTAs per SM (1;
+ * nlf_linear_set_fft_twiddles): ms_out[nvariants + mode + 2 twiddles], four entries. Results of
  * different variants agree to rounding (the apply's partial sums follow the tile), and one handle's results do not
  * depend on the batch. Synchronizes the stream. */
 NLF_API int nlf_apply_variants(int precision);
 NLF_API int nlf_linear_set_kinv_mode(nlf_linear* h, int mode);
 NLF_API int nlf_linear_get_kinv_mode(nlf_linear* h);
+NLF_API int nlf_linear_set_fft_twiddles(nlf_linear* h, int shared);
+NLF_API int nlf_linear_get_fft_twiddles(nlf_linear* h);
 NLF_API int nlf_linear_set_apply_variant(nlf_linear* h, int precision, int variant);
 NLF_API int nlf_linear_get_apply_variant(nlf_linear* h, int precision, int* variant, int* ty, int* tz, int* minb);
 NLF_API int nlf_linear_autotune(nlf_linear* h, int precision, int nvec, int reps, int force, double* ms_out,

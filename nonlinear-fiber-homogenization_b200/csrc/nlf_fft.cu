@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include "nlf_internal.h"
 #include "nlf_prof.cuh"
 
@@ -651,23 +652,63 @@ struct LaneTw {
       st[j] = (L > 1) ? tw[(l & (s - 1)) * (n / (2 * s))] : cplx<double>{1.0, 0.0};
     }
   }
+  __device__ __forceinline__ cplx<double> rr(int k1) const { return r[k1]; }
+  __device__ __forceinline__ cplx<double> ss(int j) const { return st[j]; }
 };
+// The same twiddles read on use from a shared-memory copy of the table (fewer registers, more CTAs per SM).
+template <int L, int R>
+struct LaneTwS {
+  const cplx<double>* tw;  // shared, length R L
+  int l;
+  __device__ __forceinline__ void load(const cplx<double>* t, int lane) {
+    tw = t;
+    l = lane;
+  }
+  __device__ __forceinline__ cplx<double> rr(int k1) const {
+    return (l && k1) ? tw[l * k1] : cplx<double>{1.0, 0.0};
+  }
+  __device__ __forceinline__ cplx<double> ss(int j) const {
+    constexpr int n = R * L;
+    const int s = 1 << j;
+    return (L > 1) ? tw[(l & (s - 1)) * (n / (2 * s))] : cplx<double>{1.0, 0.0};
+  }
+};
+template <int L, int R, bool SMT>
+using TwT = typename std::conditional<SMT, LaneTwS<L, R>, LaneTw<L, R>>::type;
+
+// Copies of the y, z and post-processing twiddle tables (N, N/2 and N entries) in shared memory, for the
+// shared-twiddle variants of passes A and C; ends with a barrier.
+template <int N>
+struct SmTw {
+  cplx<double> y[N], z[N / 2], n2[N];
+};
+template <int N>
+__device__ __forceinline__ void stage_tw(SmTw<N>& st, const cplx<double>* __restrict__ tw_y,
+                                         const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2) {
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    st.y[i] = tw_y[i];
+    st.n2[i] = tw_n2[i];
+    if (i < N / 2) st.z[i] = tw_z[i];
+  }
+  __syncthreads();
+}
+
 template <bool INV>
 __device__ __forceinline__ cplx<double> cj(cplx<double> w) {
   return INV ? cplx<double>{w.x, -w.y} : w;
 }
 
-template <int L, int R, bool INV>
-__device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const LaneTw<L, R>& T) {
+template <int L, int R, bool INV, class TW>
+__device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW& T) {
   dft_reg<R, INV>(a);
   if (L == 1) return;
 #pragma unroll
-  for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.r[k1]));
+  for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.rr(k1)));
 #pragma unroll
   for (int j = ilog2c(L) - 1; j >= 0; --j) {
     const int s = 1 << j;
     const bool up = (l & s) != 0;
-    const cplx<double> w = cj<INV>(T.st[j]);
+    const cplx<double> w = cj<INV>(T.ss(j));
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const cplx<double> pv = shfl_xor_c(a[k1], s);
@@ -676,14 +717,14 @@ __device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const La
   }
 }
 
-template <int L, int R, bool INV>
-__device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const LaneTw<L, R>& T) {
+template <int L, int R, bool INV, class TW>
+__device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const TW& T) {
   if (L > 1) {
 #pragma unroll
     for (int j = 0; j < ilog2c(L); ++j) {
       const int s = 1 << j;
       const bool up = (l & s) != 0;
-      const cplx<double> w = cj<INV>(T.st[j]);
+      const cplx<double> w = cj<INV>(T.ss(j));
 #pragma unroll
       for (int k1 = 0; k1 < R; ++k1) {
         const cplx<double> pv = shfl_xor_c(a[k1], s);
@@ -691,7 +732,7 @@ __device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const Lan
       }
     }
 #pragma unroll
-    for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.r[k1]));
+    for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.rr(k1)));
   }
   dft_reg<R, INV>(a);
 }
@@ -736,8 +777,9 @@ __device__ __forceinline__ void block_sum_ordered(double (&v)[K], double* red /*
 }
 
 // Pass A: (fused) r update and sums; w r; packed real z FFT + real post-processing per row; y FFT per column.
-template <int N>
-__global__ void __launch_bounds__(256, 2)
+// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2.
+template <int N, bool SMT>
+__global__ void __launch_bounds__(256, SMT ? 3 : 2)
     k_fa_fast(double* __restrict__ r, const double* __restrict__ w, cplx<double>* __restrict__ spec, int m,
               const cplx<double>* __restrict__ tw_y, const cplx<double>* __restrict__ tw_z,
               const cplx<double>* __restrict__ tw_n2, const CellState* __restrict__ cs,
@@ -751,6 +793,13 @@ __global__ void __launch_bounds__(256, 2)
   const int c = blockIdx.y, vec = blockIdx.z;
   if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
+  __shared__ SmTw<N> stw;
+  if constexpr (SMT) {
+    stage_tw<N>(stw, tw_y, tw_z, tw_n2);
+    tw_y = stw.y;
+    tw_z = stw.z;
+    tw_n2 = stw.n2;
+  }
   const int t = threadIdx.x;
   const int p = t / (N * Lz), rem = t - p * (N * Lz), y = rem / Lz, l = rem - y * Lz;
   const int x = blockIdx.x * P + p;
@@ -795,7 +844,7 @@ __global__ void __launch_bounds__(256, 2)
   }
   // packed z FFT: a[k1] = Z[k1 + 8 brev(l)]
   {
-    LaneTw<Lz, 8> T;
+    TwT<Lz, 8, SMT> T;
     T.load(tw_z, l);
     fft_nat_in<Lz, 8, false>(a, l, T);
   }
@@ -853,7 +902,7 @@ __global__ void __launch_bounds__(256, 2)
   constexpr int G = 256 / Ly, TASKS = P * H, IT = (TASKS + G - 1) / G;
   const int g = t / Ly, ly = t - g * Ly;
   cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
-  LaneTw<Ly, 8> Ty;
+  TwT<Ly, 8, SMT> Ty;
   Ty.load(tw_y, ly);
 #pragma unroll 1
   for (int it = 0; it < IT; ++it) {
@@ -1014,8 +1063,9 @@ __device__ __forceinline__ void px_row(const cplx<double> (&a)[8], double norm, 
 
 // Pass C: inverse y FFT per column; real pre-processing + inverse packed z FFT per row; scale, w; sums (or the
 // fused x/p update, fu.p set).
-template <int N>
-__global__ void __launch_bounds__(256, 2)
+// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2.
+template <int N, bool SMT>
+__global__ void __launch_bounds__(256, SMT ? 3 : 2)
     k_fc_fast(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
               double* __restrict__ z, int m, const cplx<double>* __restrict__ tw_y,
               const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2,
@@ -1030,12 +1080,19 @@ __global__ void __launch_bounds__(256, 2)
   const int c = blockIdx.y, vec = blockIdx.z;
   if (!(fu.p ? vec_ran(cs, vec, m) : vec_live(cs, vec, m))) return;
   prof_count(units, ukind);
+  __shared__ SmTw<N> stw;
+  if constexpr (SMT) {
+    stage_tw<N>(stw, tw_y, tw_z, tw_n2);
+    tw_y = stw.y;
+    tw_z = stw.z;
+    tw_n2 = stw.n2;
+  }
   const int t = threadIdx.x;
   const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
   {
     constexpr int G = 256 / Ly, TASKS = P * H, IT = (TASKS + G - 1) / G;
     const int g = t / Ly, ly = t - g * Ly;
-    LaneTw<Ly, 8> Ty;
+    TwT<Ly, 8, SMT> Ty;
     Ty.load(tw_y, ly);
 #pragma unroll 1
     for (int it = 0; it < IT; ++it) {
@@ -1078,7 +1135,7 @@ __global__ void __launch_bounds__(256, 2)
     }
   }
   {
-    LaneTw<Lz, 8> T;
+    TwT<Lz, 8, SMT> T;
     T.load(tw_z, l);
     fft_tr_in<Lz, 8, true>(a, l, T);
   }
@@ -1304,8 +1361,11 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   using F = Fast<N>;
   const cplx<double>* tw = h.t64.tw;
   const size_t plane = F::smem_plane();
-  NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N>, (int)plane));
-  NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N>, (int)plane));
+  const bool smt = h.fft_smt != 0;
+  NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N, false>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N, false>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N, true>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N, true>, (int)plane));
   if (nchunk) *nchunk = F::KZC;
   unsigned long long* units = prof_units();
   const cplx<double>* twx = tw + h.tw.off0;
@@ -1314,7 +1374,11 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   const cplx<double>* twz = tw + h.tw.off2h;
   if (stages & 1) {
     ProfScope ps(PK_FFTA64, st);
-    k_fa_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
+    const dim3 grid(N / F::P, 3, nvec);
+    if (smt)
+      k_fa_fast<N, true><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
+    else
+      k_fa_fast<N, false><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
     NLF_CHECK_LAUNCH();
   }
   if (stages & 2) {
@@ -1333,15 +1397,18 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   }
   if (stages & 4) {
     ProfScope ps(PK_FFTC64, st);
-    if constexpr (N == 64) {
+    if (smt) {
+      k_fc_fast<N, true><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial,
+                                                                     units, PK_FFTC64, fu);
+    } else if constexpr (N == 64) {
       const size_t pipe = (size_t)3 * N * F::H * sizeof(cplx<double>);  // two staging planes and the transpose
       NLF_CUDA_TRY(raise_dyn_smem(k_fc_pipe<N>, (int)pipe));
       const long planes = (long)nvec * 3 * N;
       const int grid = (int)std::min<long>(planes, 2L * h.nsm);
       k_fc_pipe<N><<<grid, 256, pipe, st>>>(spec, w, r, z, m, nvec, twy, twz, twn2, cs, partial, units, PK_FFTC64, fu);
     } else {
-      k_fc_fast<N><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial,
-                                                               units, PK_FFTC64, fu);
+      k_fc_fast<N, false><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs,
+                                                                      partial, units, PK_FFTC64, fu);
     }
     NLF_CHECK_LAUNCH();
   }

@@ -1018,6 +1018,17 @@ NLF_API int nlf_linear_set_kinv_mode(nlf_linear* H, int mode) {
 
 NLF_API int nlf_linear_get_kinv_mode(nlf_linear* H) { return bad_handle(H) ? NLF_EBADARG : H->h.pcb_closed; }
 
+NLF_API int nlf_linear_set_fft_twiddles(nlf_linear* H, int shared) {
+  if (bad_handle(H) || (shared != 0 && shared != 1)) {
+    set_error("nlf_linear_set_fft_twiddles: bad arguments");
+    return NLF_EBADARG;
+  }
+  H->h.fft_smt = shared;
+  return NLF_OK;
+}
+
+NLF_API int nlf_linear_get_fft_twiddles(nlf_linear* H) { return bad_handle(H) ? NLF_EBADARG : H->h.fft_smt; }
+
 NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps, int force, double* ms_out,
                                 void* stream) {
   if (bad_handle(H) || (precision != NLF_PREC_FP64 && precision != NLF_PREC_MIXED) || nvec < 1 || reps < 1) {
@@ -1033,7 +1044,10 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
       h.apply_variant[f64 ? 1 : 0] = it->second % 1000;
-      if (f64) h.pcb_closed = it->second / 1000;
+      if (f64) {
+        h.pcb_closed = (it->second / 1000) & 1;
+        h.fft_smt = (it->second / 1000) >> 1;
+      }
       return NLF_OK;
     }
   }
@@ -1101,7 +1115,7 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
   h.apply_variant[f64 ? 1 : 0] = rc == NLF_OK ? best : keep;
   // FP64 cubes with the register-resident FFT passes: pass B with the Kinv table or in closed form, timed on the
   // scaled preconditioner of the same vectors (node scaling from s)
-  int pcb = h.pcb_closed;
+  int pcb = h.pcb_closed + 2 * h.fft_smt;
   if (rc == NLF_OK && f64 && precond_fuses_px(h)) {
     DevBuf& tb = h.io2;
     rc = tb.reserve(al(N * 8) + al((size_t)nvec * 3 * h.g.NS * 16));
@@ -1110,8 +1124,9 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
                                       : nullptr;
     if (rc == NLF_OK) rc = launch_node_scaling(h, 1, s64, nullptr, w64, nullptr, st);
     float best_pc = 0.0f;
-    for (int v = 0; v < 2 && rc == NLF_OK; ++v) {
-      h.pcb_closed = v;
+    for (int v = 0; v < 4 && rc == NLF_OK; ++v) {  // v = Kinv mode + 2 x shared twiddles
+      h.pcb_closed = v & 1;
+      h.fft_smt = v >> 1;
       rc = launch_precond<double>(h, nvec, 6, x64, y64, spec, w64, nullptr, part, st);
       if (rc != NLF_OK) break;
       cudaEventRecord(e0, st);
@@ -1132,13 +1147,14 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
         pcb = v;
       }
     }
-    h.pcb_closed = rc == NLF_OK ? pcb : 0;
+    h.pcb_closed = rc == NLF_OK ? (pcb & 1) : 0;
+    h.fft_smt = rc == NLF_OK ? (pcb >> 1) : 0;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != NLF_OK) return rc;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = best + 1000 * h.pcb_closed;
+  g_tune_cache[key] = best + 1000 * (h.pcb_closed + 2 * h.fft_smt);
   return NLF_OK;
 }
 

@@ -29,7 +29,8 @@ EXPORTS = (
     "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
     "nlf_correctors_vjp", "nlf_mech_toec",
     "nlf_apply_variants", "nlf_linear_set_apply_variant", "nlf_linear_get_apply_variant", "nlf_linear_autotune",
-    "nlf_linear_set_kinv_mode", "nlf_linear_get_kinv_mode",
+    "nlf_linear_set_kinv_mode", "nlf_linear_get_kinv_mode", "nlf_linear_set_fft_twiddles",
+    "nlf_linear_get_fft_twiddles",
 )
 
 
@@ -108,6 +109,8 @@ def _load():
         "nlf_linear_autotune": (I, [P, I, I, I, I, P, P]),
         "nlf_linear_set_kinv_mode": (I, [P, I]),
         "nlf_linear_get_kinv_mode": (I, [P]),
+        "nlf_linear_set_fft_twiddles": (I, [P, I]),
+        "nlf_linear_get_fft_twiddles": (I, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

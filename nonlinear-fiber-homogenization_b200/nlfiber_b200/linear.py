@@ -130,12 +130,12 @@ class LinearHomogenization:
         precision(s): FP64, and FP32 too for precision="mixed"; on FP64 cubes of 32 or 64 also the Kinv mode of the
         preconditioner (table or closed form). The choice is cached per grid for the process. With report=True
         every variant is timed and {precision: [ms per launch of each apply variant, then for FP64 cubes the
-        preconditioner with the table and in closed form]} is returned."""
+        preconditioner for Kinv mode + 2 x shared twiddles = 0, 1, 2, 3]} is returned."""
         out = {}
         precs = ["fp64"] + (["mixed"] if self.precision == "mixed" else [])
         for pr in precs:
             code = _PREC[pr]
-            ms = np.zeros(lib.nlf_apply_variants(code) + (2 if pr == "fp64" else 0)) if report else None
+            ms = np.zeros(lib.nlf_apply_variants(code) + (4 if pr == "fp64" else 0)) if report else None
             check(lib.nlf_linear_autotune(self._h, code, int(nvec), int(reps), int(force), ptr(ms), self.stream))
             if report:
                 out[pr] = ms.tolist()
@@ -156,6 +156,16 @@ class LinearHomogenization:
     @kinv_mode.setter
     def kinv_mode(self, mode):
         check(lib.nlf_linear_set_kinv_mode(self._h, int(mode)))
+
+    @property
+    def fft_twiddles(self):
+        """0: passes A and C of the FP64 cube preconditioner keep their twiddles in registers; 1: in shared
+        memory (fewer registers, 3 CTAs per SM)."""
+        return int(lib.nlf_linear_get_fft_twiddles(self._h))
+
+    @fft_twiddles.setter
+    def fft_twiddles(self, shared):
+        check(lib.nlf_linear_set_fft_twiddles(self._h, int(shared)))
 
     def set_apply_tile(self, variant, precision="fp64"):
         """Use apply tile variant `variant` (0 = default) for this handle."""

@@ -152,3 +152,17 @@ def test_per_case_stopping_keeps_C(L, golden, key, n_o, slots):
     b = OL.proj(oh.load(s, np.eye(6)))
     rel_res = np.sqrt((r ** 2).sum(axis=(1, 2, 3, 4)) / (b ** 2).sum(axis=(1, 2, 3, 4)))
     assert rel_res.max() < 1e-8, rel_res
+
+
+def test_tuned_variants_keep_C(L, golden):
+    """The measured path with every tuned variant switched away from its default (apply tile 1, closed-form Kinv,
+    shared-memory twiddles in passes A and C) on the 32^3 fixture cells: C agrees with the oracle as before."""
+    seeds = [int(v) for v in golden["b32_seeds"]]
+    rho = np.stack([OD.random_cell(i, n_o=16, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=3))
+    lh.set_apply_tile(1)
+    lh.kinv_mode = 1
+    lh.fft_twiddles = 1
+    res = lh.C_full_batched(rho)
+    assert res["status"] == 0
+    assert c_agrees(res["C"], golden["b32_C"]).all(), dict(zip(seeds, cerr(res["C"], golden["b32_C"])))

@@ -284,7 +284,7 @@ def test_apply_tile_variants_and_autotune(L):
     v = lh.apply_tile("fp64")[0]
     nv = _lib.lib.nlf_apply_variants(_lib.PREC_FP64)
     ta = times["fp64"][:nv]  # then the preconditioner's two Kinv modes, timed on cubes of 32 and 64 only
-    assert len(times["fp64"]) == nv + 2 and min(ta) > 0 and times["fp64"][nv:] == [0.0, 0.0]
+    assert len(times["fp64"]) == nv + 4 and min(ta) > 0 and times["fp64"][nv:] == [0.0] * 4
     assert ta[v] == min(ta)
 
 
@@ -301,4 +301,8 @@ def test_preconditioner_kinv_closed_form(L, shape):
     assert rel(lh.precond(u), oh.precond(u)) < 1e-12
     assert rel(lh.precond(u, precond="scaled", s=s), _scaled_oracle(oh, s, u)) < 1e-12
     lh.kinv_mode = 0
+    assert rel(lh.precond(u, precond="scaled", s=s), _scaled_oracle(oh, s, u)) < 1e-12
+    lh.fft_twiddles = 1  # passes A and C with shared-memory twiddles
+    assert lh.fft_twiddles == 1
+    assert rel(lh.precond(u), oh.precond(u)) < 1e-12
     assert rel(lh.precond(u, precond="scaled", s=s), _scaled_oracle(oh, s, u)) < 1e-12
