@@ -448,36 +448,55 @@ def unet_flops(widths, n, nb):
     return sum(2.0 * v * t * ci * co for v, ci, co, t in layers)
 
 
-def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
+def solver_pairs(L, seeds, n_o, stream, chunk):
+    """Training pairs from the solver: rho (ncell, n, n, n) float32, the converged correctors as the network's
+    18 target channels (float32) and the loss weights, all on the GPU, solved `chunk` cells at a time."""
+    import torch
+    from nlfiber_b200 import learned as LN
+    n = 2 * n_o
+    seeds = list(seeds)
+    rho_all = torch.empty((len(seeds), n, n, n), dtype=torch.float32, device="cuda")
+    tgt = torch.empty((len(seeds), n, n, n, 18), dtype=torch.float32, device="cuda")
+    h = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST)
+    h.stream = stream
+    for k in range(0, len(seeds), chunk):
+        part = seeds[k:k + chunk]
+        rho = gpu_cells(part, n_o, stream=stream)
+        u = torch.empty((len(part), 6, n, n, n, 3), dtype=torch.float64, device="cuda")
+        h.C_full_batched(rho, out_u=u)
+        rho_all[k:k + len(part)] = rho.float()
+        tgt[k:k + len(part)] = LN.corrector_channels(u)
+        del u, rho
+    w = LN.loss_weights(rho_all, MATERIAL["emin"], MATERIAL["p"]) + 0.05
+    return rho_all, tgt, w
+
+
+def learned_arm(args, L, n, stream, peaks, peak_kind):
     """The learned warm start: solver-generated training pairs (32^3 and n^3 cells of the same generator, other
-    seeds), Adam training of the U-Net on the GPU, then the measured workload solved cold and warm (u0 = the
-    network's prediction, scaled energy-optimally) with the same stopping rule."""
+    seeds), Adam training of the U-Net on the GPU, then held-out n^3 cells (seeds from 1,000,000) solved cold and
+    warm (u0 = the network's prediction, scaled energy-optimally) with the same stopping rule, against C* of the
+    same cells. Also the prediction error of the trained and the untrained network on the held-out cells: what
+    training gains in the fit, beside what it does to the solve."""
     import torch
     from nlfiber_b200 import _lib
     from nlfiber_b200 import learned as LN
     t0 = time.perf_counter()
-    c32 = gpu_cells(range(10_000, 10_000 + args.train_cells32), 16, stream=stream)
-    cbig = gpu_cells(range(20_000, 20_000 + args.train_cells64), n // 2, stream=stream)
-    sets = []
-    for rho in (c32, cbig):
-        m = rho.shape[1]
-        h = L.LinearHomogenization((m, m, m), **MATERIAL, **FAST)
-        h.stream = stream
-        r = h.C_full_batched(rho, want_u=True)
-        sets.append((rho.float(), LN.corrector_channels(torch.from_numpy(r["u"])).cuda(),
-                     LN.loss_weights(rho, MATERIAL["emin"], MATERIAL["p"]).cuda() + 0.05))
-        del r
+    sets = [solver_pairs(L, range(10_000, 10_000 + args.train_cells32), 16, stream, 512),
+            solver_pairs(L, range(200_000, 200_000 + args.train_cells64), n // 2, stream, 64)]
+    torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     widths = (16, 32, 64)
     net = LN.UNet(widths, seed=0)
     net.stream = stream
+    untrained = LN.UNet(widths, seed=0)
+    untrained.stream = stream
     rng = np.random.default_rng(0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     losses = []
     e0.record()
     for it in range(args.train_steps):
-        rho, tgt, w = sets[it % 2]
-        b = min(8, rho.shape[0]) if it % 2 == 0 else min(2, rho.shape[0])
+        rho, tgt, w = sets[it % 2] if sets[1][0].shape[0] else sets[0]
+        b = min(8, rho.shape[0]) if rho.shape[1] < n else min(2, rho.shape[0])
         idx = torch.as_tensor(rng.choice(rho.shape[0], size=b, replace=False), device="cuda")
         ww = w[idx]
         loss, _ = net.loss_grad(rho[idx], tgt[idx], ww / ww.sum())
@@ -486,8 +505,31 @@ def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
     e1.record()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
-    # convolution throughput: one profiled forward over the measured cells
-    rho32 = rho_d.float()
+    del sets
+    # held-out cells and their reference C*
+    ev = list(range(1_000_000, 1_000_000 + args.eval_cells))
+    rho_e = gpu_cells(ev, n // 2, stream=stream)
+    ref = L.LinearHomogenization((n, n, n), **MATERIAL, **CSTAR)
+    ref.stream = stream
+    u_e = torch.empty((len(ev), 6, n, n, n, 3), dtype=torch.float64, device="cuda")
+    Cs_e = ref.C_full_batched(rho_e, out_u=u_e, out_C=torch.empty((len(ev), 6, 6), dtype=torch.float64,
+                                                                   device="cuda"))["C"].cpu().numpy()
+    del ref
+    # prediction error on the held-out cells (stiffness-weighted relative L2 of u / n, 8 cells at a time)
+    def pred_err(model):
+        num = den = 0.0
+        for k in range(0, len(ev), 8):
+            r = rho_e[k:k + 8]
+            t = LN.corrector_channels(u_e[k:k + 8])
+            wt = LN.loss_weights(r, MATERIAL["emin"], MATERIAL["p"])[..., None]
+            y = model.forward(r.float()) if model is not None else torch.zeros_like(t)
+            num += float((wt * (y - t) ** 2).sum())
+            den += float((wt * t ** 2).sum())
+        return (num / den) ** 0.5
+    errs = {"trained": pred_err(net), "untrained": pred_err(untrained), "zero": pred_err(None)}
+    del u_e
+    # convolution throughput: one profiled forward over 64 held-out cells
+    rho32 = rho_e[:64].float()
     net.forward(rho32[:2])
     _lib.profile(True)
     net.forward(rho32)
@@ -495,32 +537,40 @@ def learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind):
     prof = _lib.profile_report()
     _lib.profile(False)
     conv_ms, conv_la = prof["unet_conv"][0], prof["unet_conv"][1]
-    flops = unet_flops(widths, n, rho_d.shape[0])
+    flops = unet_flops(widths, n, rho32.shape[0])
     peak = float(peaks.get("bf16_tflops", 1590.0))
     conv = {"kernel": "unet_conv (k_conv_tc)", "bound": "tensor", "achieved": round(flops / (conv_ms * 1e-3) / 1e12, 2),
             "peak": peak, "unit": "TFLOP/s", "frac": round(flops / (conv_ms * 1e-3) / 1e12 / peak, 4),
             "peak_kind": "of measured cuBLAS bf16 (burst)" if peak_kind == "measured" else "of fallback 1590",
             "launches": conv_la, "ms": round(conv_ms, 3), "flops": flops}
+    del rho32
     out = {}
     for name, kw in (("cold", {}), ("warm", {"scale_x0": True})):
         h = L.LinearHomogenization((n, n, n), **MATERIAL, **FAST, **kw)
         h.stream = stream
-        C = torch.empty((rho_d.shape[0], 6, 6), dtype=torch.float64, device="cuda")
-        torch.cuda.synchronize()
-        e0.record()
-        u0 = LN.WarmStart(net).u0(rho_d) if name == "warm" else None
-        r = h.C_full_batched(rho_d, u0=u0, out_C=C)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        out[name] = {"cells_per_s": round(rho_d.shape[0] / (ms / 1e3), 3), "it_mean": float(np.mean(r["it"])),
-                     "it_max": int(np.max(r["it"])), "c_err_max": float(rel_err(C.cpu().numpy(), Cstar).max()),
-                     "status": int(r["status"])}
-        del u0
-    return {"mode": "learned", "widths": widths, "train_pairs": [args.train_cells32, args.train_cells64],
-            "train_steps": args.train_steps, "train_s": round(train_ms / 1e3, 2), "data_s": round(t_data, 1),
-            "loss_first": float(np.mean(losses[:20])) if losses else None,
-            "loss_last": float(np.mean(losses[-20:])) if losses else None, "conv_roofline": conv, **out}
+        C = torch.empty((len(ev), 6, 6), dtype=torch.float64, device="cuda")
+        its, st, ms = [], 0, 0.0
+        for k in range(0, len(ev), 64):
+            r = rho_e[k:k + 64]
+            torch.cuda.synchronize()
+            e0.record()
+            u0 = LN.WarmStart(net).u0(r.float()) if name == "warm" else None
+            res = h.C_full_batched(r, u0=u0, out_C=C[k:k + 64])
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            its += list(res["it"])
+            st = max(st, int(res["status"]))
+            del u0
+        out[name] = {"cells_per_s": round(len(ev) / (ms / 1e3), 3), "it_mean": float(np.mean(its)),
+                     "it_max": int(np.max(its)), "c_err_max": float(rel_err(C.cpu().numpy(), Cs_e).max()),
+                     "status": st}
+    return {"mode": "learned", "widths": widths, "train_pairs": {"32^3": args.train_cells32, f"{n}^3": args.train_cells64},
+            "eval_cells": args.eval_cells, "train_steps": args.train_steps, "train_s": round(train_ms / 1e3, 2),
+            "data_s": round(t_data, 1), "loss_first": float(np.mean(losses[:20])) if losses else None,
+            "loss_last": float(np.mean(losses[-20:])) if losses else None,
+            "prediction_error_heldout": errs, "conv_roofline": conv, **out,
+            "iterations_saved_mean": out["cold"]["it_mean"] - out["warm"]["it_mean"]}
 
 
 def mech_arm(args, stream):
@@ -880,6 +930,10 @@ def main():
     ap.add_argument("--train-cells32", type=int, default=256)
     ap.add_argument("--train-cells64", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--eval-cells", type=int, default=64, help="held-out cells of the learned arm")
+    ap.add_argument("--config5", action="store_true",
+                    help="the learned arm at its stated size: 18000 + 2000 training pairs at 32^3 / 64^3, 6000 "
+                         "Adam steps, 512 held-out 64^3 cells")
     ap.add_argument("--mech", action="store_true",
                     help="finite-strain compression path (Newton-CG on the GPU) instead of the default measurement")
     ap.add_argument("--mech-cells", type=int, default=2)
@@ -894,6 +948,11 @@ def main():
                     help="time the third-order elastic constants of two benchmark cells instead of the default")
     ap.add_argument("--density", action="store_true",
                     help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
+    ap.add_argument("--slots", type=int, default=None,
+                    help="cells in flight for the measured solve (0 = all cells in one lock-step batch)")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="solver precision of the measured solve (mixed: FP32 PCG inside FP64 refinement)")
+    ap.add_argument("--graphs", action="store_true", help="replay the PCG iterations from CUDA graphs")
     ap.add_argument("--per-case", type=int, default=None,
                     help="per-case stopping probation for the measured solve (0 = lock-step per cell)")
     ap.add_argument("--tune", action="store_true",
@@ -901,6 +960,9 @@ def main():
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
                     help="CG preconditioner of the Newton steps: the reference's (fft) or the node-scaled one")
     args = ap.parse_args()
+    if args.config5:
+        args.learned = True
+        args.train_cells32, args.train_cells64, args.train_steps, args.eval_cells = 18000, 2000, 6000, 512
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -994,6 +1056,14 @@ def main():
                           "us_per_vector": {k: [round(1e3 * t / k, 3) for t in v] for k, v in res.items()}}))
         return
 
+    if args.learned:
+        peaks, peak_kind = measured_peaks()
+        res = learned_arm(args, L, n, stream, peaks, peak_kind)
+        if rank == 0:
+            print(json.dumps(dict(res, workload=f"held-out seeded synthetic {n}^3 cells x 6 unit strains")),
+                  flush=True)
+        return
+
     # C*: FP64, scaled preconditioner, tight residual
     ref = L.LinearHomogenization((n, n, n), **MATERIAL, **CSTAR)
     ref.stream = stream
@@ -1003,14 +1073,13 @@ def main():
         if rank == 0:
             print(json.dumps({"calibrate_plain": calibrate_plain(L, rho_d, Cstar, n, stream)}), flush=True)
         return
-    if args.learned:
-        peaks, peak_kind = measured_peaks()
-        res = learned_arm(args, L, rho_d, Cstar, n, stream, peaks, peak_kind)
-        if rank == 0:
-            print(json.dumps(dict(res, workload=f"{B} seeded synthetic {n}^3 cells x 6 unit strains")), flush=True)
-        return
 
-    fast = dict(FAST) if args.per_case is None else dict(FAST, per_case=args.per_case)
+    fast = dict(FAST)
+    for key, val in (("per_case", args.per_case), ("slots", args.slots), ("precision", args.precision)):
+        if val is not None:
+            fast[key] = val
+    if args.graphs:
+        fast["use_graphs"] = True
     lh = L.LinearHomogenization((n, n, n), **MATERIAL, **fast)
     lh.stream = stream
     for _ in range(args.warmup):
@@ -1090,8 +1159,11 @@ def main():
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, B, world),
-        "solver": "FP64 PCG, node-scaled FFT preconditioner, "
-                  f"{fast['slots']} cells in flight, a converged cell's slot refilled from the queue, "
+        "solver": ("FP64 PCG" if fast["precision"] == "fp64" else "FP32 PCG inside FP64 refinement") +
+                  ", node-scaled FFT preconditioner, " +
+                  (f"{fast['slots']} cells in flight, a converged cell's slot refilled from the queue, "
+                   if 0 < fast["slots"] < B else "all cells in one lock-step batch, ") +
+                  ("graph-replayed iterations, " if fast.get("use_graphs") else "") +
                   f"stop at residual {fast['tol']} and energy guard {fast['energy_tol']}" +
                   (f", per-case stopping after {fast['per_case']} iterations of both rules holding"
                    if fast.get("per_case") else ", lock-step per cell"),

@@ -329,14 +329,15 @@ class LinearHomogenization:
         check(lib.nlf_dC_drho(self._h, 1, ptr(rho), ptr(Es), m, ptr(u), ptr(out), self.stream))
         return out
 
-    def C_full_batched(self, rho, u0=None, want_u=False, want_dC=False, out_C=None, **opt):
+    def C_full_batched(self, rho, u0=None, want_u=False, want_dC=False, out_C=None, out_u=None, **opt):
         """C (ncell, 6, 6) of ncell cells of this shape in one batched solve. Returns a dict with C, it, status
-        and, when asked, u (ncell, 6, nx, ny, nz, 3) and dC (ncell, 6, 6, nx, ny, nz). rho and out_C may be
-        CUDA float64 torch tensors (device resident) or pinned host tensors."""
+        and, when asked, u (ncell, 6, nx, ny, nz, 3) and dC (ncell, 6, 6, nx, ny, nz). rho, out_C and out_u (the
+        correctors' buffer, implies want_u) may be CUDA float64 torch tensors (device resident) or pinned host
+        tensors."""
         rho = as_f64(rho)
         ncell = int(np.prod(rho.shape)) // self.N
         C = np.empty((ncell, 6, 6)) if out_C is None else out_C
-        u = np.empty((ncell, 6) + self.shape + (3,)) if want_u else None
+        u = out_u if out_u is not None else (np.empty((ncell, 6) + self.shape + (3,)) if want_u else None)
         dC = np.empty((ncell, 6, 6) + self.shape) if want_dC else None
         it = np.zeros(ncell, dtype=np.int32)
         u0 = None if u0 is None else as_f64(u0)
