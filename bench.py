@@ -42,8 +42,9 @@ MATERIAL = dict(E=1.0, nu=0.3, emin=1e-9, p=3.0)
 # iterations. (The FP32-in-FP64-refinement path cannot reach 1e-8 on cells with solid islands held only by the
 # 1e-9 void: their rigid motions are below FP32 resolution.)
 FAST = dict(precision="fp64", precond="scaled", tol=1e-9, energy_tol=1e-10, maxit=4000, check_every=16, slots=24,
-            autotune=True)
-CSTAR = dict(precision="fp64", precond="scaled", tol=1e-14, maxit=10000, check_every=32, slots=24, autotune=True)
+            use_graphs=True, autotune=True)
+CSTAR = dict(precision="fp64", precond="scaled", tol=1e-14, maxit=10000, check_every=32, slots=24, use_graphs=True,
+             autotune=True)
 # iterations the reference algorithm (FP64 PCG, unit-stiffness FFT preconditioner, nlfiber/linear.py:154-203)
 # needs per 64^3 cell of this workload to bring C within 1e-8 of C*, from `--calibrate-plain` on B200 (the plain
 # FP64 GPU path runs the reference's iterates): cells 0-3 needed > 32000, 4000, 32000 and 16000; the mean,
