@@ -574,6 +574,33 @@ def learned_arm(args, L, n, stream, peaks, peak_kind):
             "iterations_saved_mean": out["cold"]["it_mean"] - out["warm"]["it_mean"]}
 
 
+def path_step(mix, Fb, z, Fprev, depth=0):
+    """One load step of a path, as the reference's driver takes it (nlfiber/qoi.py:26-46): Newton from z; while
+    it has not converged and its line search has not failed, up to 3 restarts from where it stopped (gradient
+    scale kept); if it still fails, up to 3 levels of splitting: the midpoint between the previous and this
+    macroscopic F first, then this F from the midpoint's state. Returns (w, F, log, counts)."""
+    w, F, log = mix.solve(Fb, z0=z)
+    tot = {"newton": int(log["newton"]), "cg": int(log["cg"]), "restarts": 0, "splits": 0}
+    while not log["converged"] and not log.get("linesearch_failed") and tot["restarts"] < 3:
+        w, F, log = mix.solve(Fb, z0=log["z"], g_ref=log["g0"])
+        tot["newton"] += int(log["newton"])
+        tot["cg"] += int(log["cg"])
+        tot["restarts"] += 1
+    if log["converged"] or depth >= 3 or Fprev is None:
+        return w, F, log, tot
+    mid = 0.5 * (np.asarray(Fprev) + np.asarray(Fb))
+    _, _, lm, tm = path_step(mix, mid, z, Fprev, depth + 1)
+    sub = [tm]
+    if lm["converged"]:
+        w, F, log, t2 = path_step(mix, Fb, lm["z"], mid, depth + 1)
+        sub.append(t2)
+    for t in sub:
+        for key in tot:
+            tot[key] += t[key]
+    tot["splits"] += 1
+    return w, F, log, tot
+
+
 def mech_arm(args, stream):
     """Finite-strain compression (the reference's qoi.run_path "compression" driver, nlfiber/qoi.py:49-115):
     compressible neo-Hookean cells (E 1, nu 0.3, void rho^3 with floor 1e-6, WLS (500, 0.01)), Fbar_xx = 1 - e
@@ -592,23 +619,36 @@ def mech_arm(args, stream):
     for i in range(len(cells)):
         cell = MH.Cell(cells[i], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
         mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
-        z = None
+        rng = np.random.default_rng(i)
+        void = torch.as_tensor(cells[i] < 0.5, device="cuda")
+        z, Fprev = None, np.eye(3)
         for k in range(1, args.mech_steps + 1):
             e = -0.01 * k
             Fb = np.eye(3)
             if z is not None:
                 Fb = mix.unpack(z, Fb)[1]
             Fb[0, 0] = 1.0 + e
-            w, F, log = mix.solve(Fb, z0=z)
+            w, F, log, tot = path_step(mix, Fb, z, Fprev)
             P = np.asarray(cell.mean_stress(w, F))
+            # contact: share of the void voxels whose Gauss-point Jacobians fall below 0.1 (nearly inverted)
+            H = torch.as_tensor(cell.grad_w(w), device="cuda") + torch.as_tensor(F - np.eye(3), device="cuda")
+            J = torch.linalg.det(torch.eye(3, dtype=torch.float64, device="cuda") + H)
+            inverted = float((J < 0.1)[:, void].double().mean()) if bool(void.any()) else 0.0
             rows.append({"cell": i, "e": e, "P_xx": float(P[0, 0]), "nu": [float(-(F[j, j] - 1) / e) for j in (1, 2)],
-                         "newton": int(log["newton"]), "cg": int(log["cg"]), "converged": bool(log["converged"])})
-            newton += int(log["newton"])
-            cg += int(log["cg"])
+                         "newton": tot["newton"], "cg": tot["cg"], "restarts": tot["restarts"], "splits": tot["splits"],
+                         "converged": bool(log["converged"]), "void_inverted": inverted})
+            newton += tot["newton"]
+            cg += tot["cg"]
             steps += 1
-            z = log["z"]
-            if not log["converged"]:
+            if not log["converged"] or inverted > 0.01:
                 break
+            # the next step starts from this state plus a seeded kick of 1e-3 max |w| on w, so the path can
+            # leave a symmetric branch
+            z = log["z"]
+            nw = mix.nw
+            kick = torch.as_tensor(rng.standard_normal(nw), device=z.device) * (1e-3 * float(z[:nw].abs().max()) + 1e-15)
+            z = torch.cat([z[:nw] + kick, z[nw:]])
+            Fprev = F
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)

@@ -603,6 +603,8 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
   const size_t V = (size_t)nvec * 3 * N;
   const bool mixed = o.precision == NLF_PREC_MIXED;
   const bool scaled = o.precond == NLF_PC_FFT_SCALED;
+  // slot refill holds only `slots` cells of PCG state: dispatch before sizing the all-cells workspace
+  if (!mixed && o.slots > 0 && o.slots < ncell) return solve_slots(h, in, o, xout, iters_h, st);
   Pinned pin;
   if (!pin.count) {
     set_error("cudaMallocHost failed");
@@ -665,7 +667,6 @@ static int solve_core(LinearHandle& h, const SolveIn& in, const nlf_solve_opts& 
       if (xg) NLF_TRY((launch_aos_to_soa<double, double>(N, nvec, in.x0, P64.x, 1.0, st)));
       PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede,
                  precond_fuses_px(h) ? o.per_case : 0};
-      if (o.slots > 0 && o.slots < ncell) return solve_slots(h, in, o, xout, iters_h, st);
       NLF_TRY((pcg<double, double>(h, P64, b64, xg, ctl, nullptr, pin.count, o.use_graphs != 0, st)));
       NLF_CUDA_TRY(cudaMemcpyAsync(xout, P64.x, V * sizeof(double), cudaMemcpyDeviceToDevice, st));
       NLF_CUDA_TRY(cudaMemcpyAsync(csh.data(), P64.cs, ncell * sizeof(CellState), cudaMemcpyDeviceToHost, st));
