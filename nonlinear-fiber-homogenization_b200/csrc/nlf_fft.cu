@@ -960,18 +960,25 @@ __device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx
 
 // Pass B: x FFT of the three components of each (ky, kz) column, 3x3 Kinv, Parseval (r, z) partial, inverse.
 // CLOSED: the Kinv entries are computed in closed form from the twiddles and the medium's (lam, mu) instead of
-// read from the table.
+// read from the table; the x twiddles are then read from a shared-memory copy of the table, which keeps the CTA
+// (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps).
 template <int N, bool CLOSED>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(Fast<N>::NTB, 2)
     k_fb_fast(cplx<double>* __restrict__ spec, const double* __restrict__ kinv, int m,
               const cplx<double>* __restrict__ tw_x, const CellState* __restrict__ cs,
               unsigned long long* __restrict__ units, int ukind, PcgFuse fu, double lam, double mu) {
   using F = Fast<N>;
   constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN;
   __shared__ double red[32];
+  __shared__ cplx<double> twsh[N];
   const int vec = blockIdx.z;
   if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
+  if constexpr (CLOSED) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) twsh[i] = tw_x[i];
+    __syncthreads();
+    tw_x = twsh;
+  }
   const int t = threadIdx.x, task = t / L, l = t - task * L;
   const int kyl = task / KZN, kzl = task - kyl * KZN;
   const int kz = blockIdx.y * KZN + kzl;
@@ -984,7 +991,7 @@ __global__ void __maxnreg__(112)
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
-  LaneTw<L, 4> T;
+  TwT<L, 4, CLOSED> T;
   T.load(tw_x, l);
 #pragma unroll
   for (int c = 0; c < 3; ++c) fft_nat_in<L, 4, false>(a[c], l, T);
