@@ -496,31 +496,32 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   }
   P.s = s_sl;
   P.w = w_sl;
-  // Host snapshots of the slots' state, double-buffered: the host reads the snapshot taken after chunk j while
-  // chunk j + 1 is already queued, so the GPU never waits for the host between chunks. A slot refilled while
-  // reading snapshot j still shows its previous cell in snapshot j + 1 (copied before the refill was queued), so
-  // it is read again from snapshot j + 2 on. A stopped cell's slot therefore idles for one extra chunk, which
-  // costs no GPU time: the kernels skip inactive cells.
+  // Host snapshots of the slots' state, kLook chunks ahead: the host reads the snapshot taken after chunk j while
+  // chunks up to j + kLook are already queued, so the GPU does not wait for a busy host between chunks. A slot
+  // refilled while reading snapshot j still shows its previous cell in the snapshots up to j + kLook (copied
+  // before the refill was queued), so it is read again from snapshot j + kLook + 1 on. A stopped cell's slot
+  // therefore idles for kLook extra chunks, which costs no GPU time: the kernels skip inactive cells.
+  constexpr int kLook = 2, kRing = kLook + 1;
   const size_t snap = S * sizeof(CellState) + (size_t)S * m * sizeof(VecState);
-  PinnedBuf pin(2 * snap);
+  PinnedBuf pin(kRing * snap);
   if (!pin.p) {
     set_error("cudaMallocHost failed");
     return NLF_ECUDA;
   }
-  CellState* csb[2];
-  VecState* vsb[2];
-  for (int k = 0; k < 2; ++k) {
+  CellState* csb[kRing];
+  VecState* vsb[kRing];
+  for (int k = 0; k < kRing; ++k) {
     csb[k] = reinterpret_cast<CellState*>(static_cast<char*>(pin.p) + k * snap);
     vsb[k] = reinterpret_cast<VecState*>(csb[k] + S);
   }
   struct Events {
-    cudaEvent_t e[2] = {nullptr, nullptr};
+    cudaEvent_t e[kRing] = {};
     ~Events() {
       for (cudaEvent_t x : e)
         if (x) cudaEventDestroy(x);
     }
   } ev;
-  for (int k = 0; k < 2; ++k) NLF_CUDA_TRY(cudaEventCreateWithFlags(&ev.e[k], cudaEventDisableTiming));
+  for (int k = 0; k < kRing; ++k) NLF_CUDA_TRY(cudaEventCreateWithFlags(&ev.e[k], cudaEventDisableTiming));
   NLF_CUDA_TRY(cudaMemsetAsync(P.cs, 0, S * sizeof(CellState), st));  // every slot empty and inactive
   const PcgCtl ctl{o.tol, o.maxit, o.check_every, o.scale_x0, in.has_ede ? o.energy_tol : 0.0, in.ede,
                    precond_fuses_px(h) ? o.per_case : 0};
@@ -549,7 +550,7 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
     return pcg_init<double, double>(h, v, bs, xg, ctl, nullptr, st);
   };
   auto take_snapshot = [&](long k) -> int {
-    const int b = (int)(k & 1);
+    const int b = (int)(k % kRing);
     NLF_CUDA_TRY(cudaMemcpyAsync(csb[b], P.cs, S * sizeof(CellState), cudaMemcpyDeviceToHost, st));
     NLF_CUDA_TRY(cudaMemcpyAsync(vsb[b], P.vs, (size_t)S * m * sizeof(VecState), cudaMemcpyDeviceToHost, st));
     NLF_CUDA_TRY(cudaEventRecord(ev.e[b], st));
@@ -560,12 +561,16 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   IterGraph G;
   int status = NLF_OK;
   NLF_TRY(take_snapshot(0));  // the state after the starts (cells may stop before their first iteration)
+  for (long k = 1; k < kLook; ++k) {
+    NLF_TRY(run_iterations<double>(h, P, ctl, every, o.use_graphs != 0, G, st));
+    NLF_TRY(take_snapshot(k));
+  }
   for (long j = 0;; ++j) {
     NLF_TRY(run_iterations<double>(h, P, ctl, every, o.use_graphs != 0, G, st));
-    NLF_TRY(take_snapshot(j + 1));
-    NLF_CUDA_TRY(cudaEventSynchronize(ev.e[j & 1]));
-    const CellState* cs_h = csb[j & 1];
-    const VecState* vs_h = vsb[j & 1];
+    NLF_TRY(take_snapshot(j + kLook));
+    NLF_CUDA_TRY(cudaEventSynchronize(ev.e[j % kRing]));
+    const CellState* cs_h = csb[j % kRing];
+    const VecState* vs_h = vsb[j % kRing];
     int nact = 0;
     for (int sl = 0; sl < S; ++sl) {
       const int c = slot_cell[sl];
@@ -583,12 +588,12 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
       slot_cell[sl] = -1;
       if (next < ncell) {
         NLF_TRY(start(sl));
-        valid_from[sl] = j + 2;
+        valid_from[sl] = j + kLook + 1;
         ++nact;
       }
     }
     if (nact == 0) {
-      NLF_CUDA_TRY(cudaEventSynchronize(ev.e[(j + 1) & 1]));  // the last snapshot's copy into pinned memory
+      NLF_CUDA_TRY(cudaEventSynchronize(ev.e[(j + kLook) % kRing]));  // the last snapshot's copy
       break;
     }
   }
