@@ -172,8 +172,9 @@ NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
  * take it without timing unless `force` is set or `ms_out` (one time per variant, milliseconds per launch) is
  * given. On FP64 cubes of 32 or 64 it also times the preconditioner with its Kinv entries read from the table
  * (mode 0) or computed in closed form (mode 1; nlf_linear_set_kinv_mode), and passes A and C with their
- * twiddles in registers (0) or read from a shared-memory copy of the tables at 3 CTAs per SM (1;
- * nlf_linear_set_fft_twiddles): ms_out[nvariants + mode + 2 twiddles], four entries. Results of
+ * twiddles in registers (0), read from a shared-memory copy of the tables at 3 CTAs per SM (1), or that with
+ * their spectrum rows staged through shared memory for coalesced transfers (2; nlf_linear_set_fft_twiddles):
+ * ms_out[nvariants + mode + 2 twiddles], six entries. Results of
  * different variants agree to rounding (the apply's partial sums follow the tile), and one handle's results do not
  * depend on the batch. Synchronizes the stream. */
 NLF_API int nlf_apply_variants(int precision);

@@ -693,6 +693,14 @@ __device__ __forceinline__ void stage_tw(SmTw<N>& st, const cplx<double>* __rest
   __syncthreads();
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, L2 only)
+__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 template <bool INV>
 __device__ __forceinline__ cplx<double> cj(cplx<double> w) {
   return INV ? cplx<double>{w.x, -w.y} : w;
@@ -777,8 +785,10 @@ __device__ __forceinline__ void block_sum_ordered(double (&v)[K], double* red /*
 }
 
 // Pass A: (fused) r update and sums; w r; packed real z FFT + real post-processing per row; y FFT per column.
-// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2.
-template <int N, bool SMT>
+// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2. STG (with SMT): the y
+// transforms write back into the plane buffer, and the plane leaves in whole 528-byte kz rows (coalesced)
+// instead of 16-byte pieces scattered over 8 ky rows per warp.
+template <int N, bool SMT, bool STG = false>
 __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     k_fa_fast(double* __restrict__ r, const double* __restrict__ w, cplx<double>* __restrict__ spec, int m,
               const cplx<double>* __restrict__ tw_y, const cplx<double>* __restrict__ tw_z,
@@ -916,8 +926,21 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     fft_nat_in<Ly, 8, false>(b, ly, Ty);
     if (ok) {
       const int xx = blockIdx.x * P + pp, kb = 8 * brevL<Ly>(ly);
+      if constexpr (STG) {
+        // in place: this group alone reads and writes column (pp, kz), and its reads precede the shuffles
 #pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
+        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + kb) * H + swz<M>(kz)] = b[k1];
+      } else {
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
+      }
+    }
+  }
+  if constexpr (STG) {
+    __syncthreads();
+    for (int i = t; i < P * N * H; i += 256) {
+      const int pp = i / (N * H), rr = i - pp * (N * H), ky = rr / H, kz = rr - ky * H;
+      sp[((long)ky * N + blockIdx.x * P + pp) * H + kz] = sm[((long)pp * N + ky) * H + swz<M>(kz)];
     }
   }
 }
@@ -1070,8 +1093,10 @@ __device__ __forceinline__ void px_row(const cplx<double> (&a)[8], double norm, 
 
 // Pass C: inverse y FFT per column; real pre-processing + inverse packed z FFT per row; scale, w; sums (or the
 // fused x/p update, fu.p set).
-// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2.
-template <int N, bool SMT>
+// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2. STG (with SMT): the plane's
+// spectrum rows are first copied whole into the plane buffer by cp.async (coalesced 16-byte pieces), and the y
+// transforms run in place there.
+template <int N, bool SMT, bool STG = false>
 __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     k_fc_fast(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
               double* __restrict__ z, int m, const cplx<double>* __restrict__ tw_y,
@@ -1096,6 +1121,15 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   }
   const int t = threadIdx.x;
   const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
+  if constexpr (STG) {
+    for (int i = t; i < P * N * H; i += 256) {
+      const int pp = i / (N * H), rr = i - pp * (N * H), ky = rr / H, kz = rr - ky * H;
+      cp16_async(sm + ((long)pp * N + ky) * H + swz<M>(kz), sp + ((long)ky * N + blockIdx.x * P + pp) * H + kz);
+    }
+    cp_async_commit();
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+  }
   {
     constexpr int G = 256 / Ly, TASKS = P * H, IT = (TASKS + G - 1) / G;
     const int g = t / Ly, ly = t - g * Ly;
@@ -1110,8 +1144,12 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
       const int xx = blockIdx.x * P + pp;
       cplx<double> b[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
-        b[q] = ok ? sp[((long)(ly + Ly * q) * N + xx) * H + kz] : cplx<double>{0.0, 0.0};
+      for (int q = 0; q < 8; ++q) {
+        if constexpr (STG)
+          b[q] = sm[((long)pp * N + ly + Ly * q) * H + swz<M>(kz)];
+        else
+          b[q] = ok ? sp[((long)(ly + Ly * q) * N + xx) * H + kz] : cplx<double>{0.0, 0.0};
+      }
       fft_nat_in<Ly, 8, true>(b, ly, Ty);
       if (ok) {
         const int yb = 8 * brevL<Ly>(ly);
@@ -1201,13 +1239,6 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   }
 }
 
-// 16-byte asynchronous global -> shared copy (cp.async, L2 only)
-__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Pass C, persistent and pipelined (cubes of 64): each CTA walks the planes (vec, comp, x) blockIdx.x,
 // blockIdx.x + gridDim.x, ... of active cells; while it transforms one plane, the spectrum rows of its next
@@ -1373,6 +1404,8 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N, false>, (int)plane));
   NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N, true>, (int)plane));
   NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N, true>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fa_fast<N, true, true>, (int)plane));
+  NLF_CUDA_TRY(raise_dyn_smem(k_fc_fast<N, true, true>, (int)plane));
   if (nchunk) *nchunk = F::KZC;
   unsigned long long* units = prof_units();
   const cplx<double>* twx = tw + h.tw.off0;
@@ -1382,7 +1415,9 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   if (stages & 1) {
     ProfScope ps(PK_FFTA64, st);
     const dim3 grid(N / F::P, 3, nvec);
-    if (smt)
+    if (h.fft_smt == 2)
+      k_fa_fast<N, true, true><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
+    else if (smt)
       k_fa_fast<N, true><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
     else
       k_fa_fast<N, false><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
@@ -1404,7 +1439,10 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   }
   if (stages & 4) {
     ProfScope ps(PK_FFTC64, st);
-    if (smt) {
+    if (h.fft_smt == 2) {
+      k_fc_fast<N, true, true><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs,
+                                                                           partial, units, PK_FFTC64, fu);
+    } else if (smt) {
       k_fc_fast<N, true><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs, partial,
                                                                      units, PK_FFTC64, fu);
     } else if constexpr (N == 64) {

@@ -118,7 +118,8 @@ struct LinearHandle {
   int apply_variant[2] = {0, 0};
   // FP64 cube pass B: 1 = Kinv entries in closed form (no table reads), 0 = from the table
   int pcb_closed = 0;
-  // FP64 cube passes A and C: 1 = twiddles from shared memory (3 CTAs per SM), 0 = in registers (2 per SM)
+  // FP64 cube passes A and C: 0 = twiddles in registers (2 CTAs per SM), 1 = from shared memory (3 per SM),
+  // 2 = as 1 with the spectrum staged through shared memory in whole rows (coalesced)
   int fft_smt = 0;
 };
 

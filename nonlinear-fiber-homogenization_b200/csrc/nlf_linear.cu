@@ -1025,7 +1025,7 @@ NLF_API int nlf_linear_set_kinv_mode(nlf_linear* H, int mode) {
 NLF_API int nlf_linear_get_kinv_mode(nlf_linear* H) { return bad_handle(H) ? NLF_EBADARG : H->h.pcb_closed; }
 
 NLF_API int nlf_linear_set_fft_twiddles(nlf_linear* H, int shared) {
-  if (bad_handle(H) || (shared != 0 && shared != 1)) {
+  if (bad_handle(H) || shared < 0 || shared > 2) {
     set_error("nlf_linear_set_fft_twiddles: bad arguments");
     return NLF_EBADARG;
   }
@@ -1130,7 +1130,7 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
                                       : nullptr;
     if (rc == NLF_OK) rc = launch_node_scaling(h, 1, s64, nullptr, w64, nullptr, st);
     float best_pc = 0.0f;
-    for (int v = 0; v < 4 && rc == NLF_OK; ++v) {  // v = Kinv mode + 2 x shared twiddles
+    for (int v = 0; v < 6 && rc == NLF_OK; ++v) {  // v = Kinv mode + 2 x twiddle / staging mode (0, 1, 2)
       h.pcb_closed = v & 1;
       h.fft_smt = v >> 1;
       rc = launch_precond<double>(h, nvec, 6, x64, y64, spec, w64, nullptr, part, st);

@@ -162,7 +162,8 @@ def test_tuned_variants_keep_C(L, golden):
     lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=3))
     lh.set_apply_tile(1)
     lh.kinv_mode = 1
-    lh.fft_twiddles = 1
-    res = lh.C_full_batched(rho)
-    assert res["status"] == 0
-    assert c_agrees(res["C"], golden["b32_C"]).all(), dict(zip(seeds, cerr(res["C"], golden["b32_C"])))
+    for mode in (1, 2):
+        lh.fft_twiddles = mode
+        res = lh.C_full_batched(rho)
+        assert res["status"] == 0
+        assert c_agrees(res["C"], golden["b32_C"]).all(), dict(zip(seeds, cerr(res["C"], golden["b32_C"])))
