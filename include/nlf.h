@@ -171,10 +171,12 @@ NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
  * for this handle. Its choice is cached per (grid, precision) for the process, so later handles of the same grid
  * take it without timing unless `force` is set or `ms_out` (one time per variant, milliseconds per launch) is
  * given. On FP64 cubes of 32 or 64 it also times the preconditioner with its Kinv entries read from the table
- * (mode 0) or computed in closed form (mode 1; nlf_linear_set_kinv_mode), and passes A and C with their
- * twiddles in registers (0), read from a shared-memory copy of the tables at 3 CTAs per SM (1), or that with
- * their spectrum rows staged through shared memory for coalesced transfers (2; nlf_linear_set_fft_twiddles):
- * ms_out[nvariants + mode + 2 twiddles], six entries. Results of
+ * (mode 0), computed in closed form (mode 1), or that with pass B's slabs staged through shared memory (mode 2,
+ * 64^3 only; nlf_linear_set_kinv_mode), and passes A and C with their
+ * twiddles in registers (0), read from a shared-memory copy of the tables at 3 CTAs per SM (1), that with pass
+ * C's spectrum rows staged through shared memory for coalesced transfers (2), or pass A's too (3;
+ * nlf_linear_set_fft_twiddles): ms_out[nvariants + kinv mode + nk twiddle mode], nk = 3 Kinv modes at 64^3
+ * and 2 at 32^3, so at most twelve entries. Results of
  * different variants agree to rounding (the apply's partial sums follow the tile), and one handle's results do not
  * depend on the batch. Synchronizes the stream. */
 NLF_API int nlf_apply_variants(int precision);

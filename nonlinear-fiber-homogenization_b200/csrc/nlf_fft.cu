@@ -985,15 +985,21 @@ __device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx
 // CLOSED: the Kinv entries are computed in closed form from the twiddles and the medium's (lam, mu) instead of
 // read from the table; the x twiddles are then read from a shared-memory copy of the table, which keeps the CTA
 // (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps).
-template <int N, bool CLOSED>
+// STG (cubes of 64, with CLOSED): the CTA's three [x][kz-chunk] slabs are copied whole into shared memory by
+// cp.async (272-byte row pieces instead of 16-byte pieces over 16 x rows per warp), transformed from there, and
+// written back the same way; rows padded to KZN + 1 entries spread the column reads over all banks.
+template <int N, bool CLOSED, bool STG = false>
 __global__ void __launch_bounds__(Fast<N>::NTB, 2)
     k_fb_fast(cplx<double>* __restrict__ spec, const double* __restrict__ kinv, int m,
               const cplx<double>* __restrict__ tw_x, const CellState* __restrict__ cs,
               unsigned long long* __restrict__ units, int ukind, PcgFuse fu, double lam, double mu) {
   using F = Fast<N>;
-  constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN;
+  constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN, KP = KZN + 1;
+  static_assert(!STG || KY == 1, "staged pass B takes one ky row per CTA");
   __shared__ double red[32];
   __shared__ cplx<double> twsh[N];
+  extern __shared__ __align__(16) unsigned char fb_raw[];
+  cplx<double>* sb = reinterpret_cast<cplx<double>*>(fb_raw);  // STG: [3][N][KP]
   const int vec = blockIdx.z;
   if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
@@ -1008,12 +1014,27 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   const bool ok = kyl < KY && kz < H;
   const int ky = blockIdx.x * KY + (ok ? kyl : 0);
   const long NS = (long)N * N * H;
+  const int kz0 = blockIdx.y * KZN, nkz = min(KZN, H - kz0);
+  if constexpr (STG) {
+    for (int i = t; i < 3 * N * KZN; i += blockDim.x) {
+      const int c = i / (N * KZN), rr = i - c * (N * KZN), x = rr / KZN, kk = rr - x * KZN;
+      if (kk < nkz)
+        cp16_async(sb + (c * N + x) * KP + kk, spec + ((long)vec * 3 + c) * NS + ((long)blockIdx.x * N + x) * H + kz0 + kk);
+    }
+    cp_async_commit();
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+  }
   cplx<double> a[3][4];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-      a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
+    for (int q = 0; q < 4; ++q) {
+      if constexpr (STG)
+        a[c][q] = ok ? sb[(c * N + l + L * q) * KP + kzl] : cplx<double>{0.0, 0.0};
+      else
+        a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
+    }
   TwT<L, 4, CLOSED> T;
   T.load(tw_x, l);
 #pragma unroll
@@ -1055,7 +1076,19 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] = a[c][q];
+      for (int q = 0; q < 4; ++q) {
+        if constexpr (STG)
+          sb[(c * N + l + L * q) * KP + kzl] = a[c][q];
+        else
+          spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] = a[c][q];
+      }
+  if constexpr (STG) {
+    __syncthreads();
+    for (int i = t; i < 3 * N * KZN; i += blockDim.x) {
+      const int c = i / (N * KZN), rr = i - c * (N * KZN), x = rr / KZN, kk = rr - x * KZN;
+      if (kk < nkz) spec[((long)vec * 3 + c) * NS + ((long)blockIdx.x * N + x) * H + kz0 + kk] = sb[(c * N + x) * KP + kk];
+    }
+  }
   if (fu.partB) {
     if (!ok) dot[0] = 0.0;
     block_sum_ordered<1>(dot, red);
@@ -1391,6 +1424,23 @@ __global__ void __launch_bounds__(256, 2)
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Pass B with staged slabs (cubes of 64 only; other grids have no such variant)
+template <int N>
+static int launch_fb_staged(dim3 grid, cplx<double>* spec, const double* kinv, int m, const cplx<double>* twx,
+                            const CellState* cs, unsigned long long* units, const PcgFuse& fu, double lam0,
+                            double mu0, cudaStream_t st) {
+  if constexpr (N == 64) {
+    constexpr size_t sbb = (size_t)3 * N * (Fast<N>::KZN + 1) * sizeof(cplx<double>);
+    NLF_CUDA_TRY(raise_dyn_smem(k_fb_fast<N, true, true>, (int)sbb));
+    k_fb_fast<N, true, true><<<grid, Fast<N>::NTB, sbb, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
+    NLF_CHECK_LAUNCH();
+    return NLF_OK;
+  } else {
+    set_error("pass B: no staged variant for n = %d", N);
+    return NLF_EBADARG;
+  }
+}
+
 // stages: bit 0 pass A, bit 1 pass B, bit 2 pass C
 template <int N>
 static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double* z, cplx<double>* spec,
@@ -1415,7 +1465,7 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
   if (stages & 1) {
     ProfScope ps(PK_FFTA64, st);
     const dim3 grid(N / F::P, 3, nvec);
-    if (h.fft_smt == 2)
+    if (h.fft_smt == 3)
       k_fa_fast<N, true, true><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
     else if (smt)
       k_fa_fast<N, true><<<grid, 256, plane, st>>>(r, w, spec, m, twy, twz, twn2, cs, units, PK_FFTA64, fu);
@@ -1431,15 +1481,18 @@ static int launch_fast(const LinearHandle& h, int nvec, int m, double* r, double
     const double nu0 = w ? h.scaled_ref_nu : h.nu;
     const double lam0 = h.E * nu0 / ((1.0 + nu0) * (1.0 - 2.0 * nu0)), mu0 = h.E / (2.0 * (1.0 + nu0));
     const dim3 grid(N / F::KY, F::KZC, nvec);
-    if (h.pcb_closed)
+    if (N == 64 && h.pcb_closed == 2) {
+      NLF_TRY(launch_fb_staged<N>(grid, spec, kinv, m, twx, cs, units, fu, lam0, mu0, st));
+    } else if (h.pcb_closed) {
       k_fb_fast<N, true><<<grid, F::NTB, 0, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
-    else
+    } else {
       k_fb_fast<N, false><<<grid, F::NTB, 0, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
+    }
     NLF_CHECK_LAUNCH();
   }
   if (stages & 4) {
     ProfScope ps(PK_FFTC64, st);
-    if (h.fft_smt == 2) {
+    if (h.fft_smt >= 2) {
       k_fc_fast<N, true, true><<<dim3(N / F::P, 3, nvec), 256, plane, st>>>(spec, w, r, z, m, twy, twz, twn2, cs,
                                                                            partial, units, PK_FFTC64, fu);
     } else if (smt) {

@@ -1014,7 +1014,7 @@ NLF_API int nlf_linear_get_apply_variant(nlf_linear* H, int precision, int* vari
 }
 
 NLF_API int nlf_linear_set_kinv_mode(nlf_linear* H, int mode) {
-  if (bad_handle(H) || (mode != 0 && mode != 1)) {
+  if (bad_handle(H) || mode < 0 || mode > 2 || (mode == 2 && H->h.g.n0 != 64)) {
     set_error("nlf_linear_set_kinv_mode: bad arguments");
     return NLF_EBADARG;
   }
@@ -1025,7 +1025,7 @@ NLF_API int nlf_linear_set_kinv_mode(nlf_linear* H, int mode) {
 NLF_API int nlf_linear_get_kinv_mode(nlf_linear* H) { return bad_handle(H) ? NLF_EBADARG : H->h.pcb_closed; }
 
 NLF_API int nlf_linear_set_fft_twiddles(nlf_linear* H, int shared) {
-  if (bad_handle(H) || shared < 0 || shared > 2) {
+  if (bad_handle(H) || shared < 0 || shared > 3) {
     set_error("nlf_linear_set_fft_twiddles: bad arguments");
     return NLF_EBADARG;
   }
@@ -1051,8 +1051,8 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
     if (it != g_tune_cache.end()) {
       h.apply_variant[f64 ? 1 : 0] = it->second % 1000;
       if (f64) {
-        h.pcb_closed = (it->second / 1000) & 1;
-        h.fft_smt = (it->second / 1000) >> 1;
+        h.pcb_closed = (it->second / 1000) % 4;
+        h.fft_smt = (it->second / 1000) / 4;
       }
       return NLF_OK;
     }
@@ -1121,7 +1121,7 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
   h.apply_variant[f64 ? 1 : 0] = rc == NLF_OK ? best : keep;
   // FP64 cubes with the register-resident FFT passes: pass B with the Kinv table or in closed form, timed on the
   // scaled preconditioner of the same vectors (node scaling from s)
-  int pcb = h.pcb_closed + 2 * h.fft_smt;
+  int pcb = 0;
   if (rc == NLF_OK && f64 && precond_fuses_px(h)) {
     DevBuf& tb = h.io2;
     rc = tb.reserve(al(N * 8) + al((size_t)nvec * 3 * h.g.NS * 16));
@@ -1130,9 +1130,10 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
                                       : nullptr;
     if (rc == NLF_OK) rc = launch_node_scaling(h, 1, s64, nullptr, w64, nullptr, st);
     float best_pc = 0.0f;
-    for (int v = 0; v < 6 && rc == NLF_OK; ++v) {  // v = Kinv mode + 2 x twiddle / staging mode (0, 1, 2)
-      h.pcb_closed = v & 1;
-      h.fft_smt = v >> 1;
+    const int nk = h.g.n0 == 64 ? 3 : 2;  // Kinv modes: table, closed form, closed form with staged slabs (64^3)
+    for (int v = 0; v < 4 * nk && rc == NLF_OK; ++v) {  // v = Kinv mode + nk x twiddle / staging mode (0 .. 3)
+      h.pcb_closed = v % nk;
+      h.fft_smt = v / nk;
       rc = launch_precond<double>(h, nvec, 6, x64, y64, spec, w64, nullptr, part, st);
       if (rc != NLF_OK) break;
       cudaEventRecord(e0, st);
@@ -1153,14 +1154,14 @@ NLF_API int nlf_linear_autotune(nlf_linear* H, int precision, int nvec, int reps
         pcb = v;
       }
     }
-    h.pcb_closed = rc == NLF_OK ? (pcb & 1) : 0;
-    h.fft_smt = rc == NLF_OK ? (pcb >> 1) : 0;
+    h.pcb_closed = rc == NLF_OK ? pcb % nk : 0;
+    h.fft_smt = rc == NLF_OK ? pcb / nk : 0;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != NLF_OK) return rc;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache[key] = best + 1000 * (h.pcb_closed + 2 * h.fft_smt);
+  g_tune_cache[key] = best + 1000 * (h.pcb_closed + 4 * h.fft_smt);
   return NLF_OK;
 }
 

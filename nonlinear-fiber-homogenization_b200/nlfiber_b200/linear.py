@@ -130,12 +130,13 @@ class LinearHomogenization:
         precision(s): FP64, and FP32 too for precision="mixed"; on FP64 cubes of 32 or 64 also the Kinv mode of the
         preconditioner (table or closed form). The choice is cached per grid for the process. With report=True
         every variant is timed and {precision: [ms per launch of each apply variant, then for FP64 cubes the
-        preconditioner for Kinv mode + 2 x twiddle mode = 0 .. 5]} is returned."""
+        preconditioner, entry Kinv mode + nk x twiddle mode with nk = 3 Kinv modes at 64^3 (2 at 32^3; zeros
+        elsewhere)]} is returned."""
         out = {}
         precs = ["fp64"] + (["mixed"] if self.precision == "mixed" else [])
         for pr in precs:
             code = _PREC[pr]
-            ms = np.zeros(lib.nlf_apply_variants(code) + (6 if pr == "fp64" else 0)) if report else None
+            ms = np.zeros(lib.nlf_apply_variants(code) + (12 if pr == "fp64" else 0)) if report else None
             check(lib.nlf_linear_autotune(self._h, code, int(nvec), int(reps), int(force), ptr(ms), self.stream))
             if report:
                 out[pr] = ms.tolist()
@@ -150,7 +151,8 @@ class LinearHomogenization:
 
     @property
     def kinv_mode(self):
-        """0: the FP64 cube preconditioner reads its Kinv table; 1: it computes the entries in closed form."""
+        """0: the FP64 cube preconditioner reads its Kinv table; 1: it computes the entries in closed form; 2 (64^3):
+        closed form with pass B's slabs staged through shared memory."""
         return int(lib.nlf_linear_get_kinv_mode(self._h))
 
     @kinv_mode.setter
@@ -160,7 +162,8 @@ class LinearHomogenization:
     @property
     def fft_twiddles(self):
         """0: passes A and C of the FP64 cube preconditioner keep their twiddles in registers; 1: in shared
-        memory (fewer registers, 3 CTAs per SM); 2: as 1, with the spectrum rows staged through shared memory."""
+        memory (fewer registers, 3 CTAs per SM); 2: as 1, with pass C's spectrum rows staged through shared
+        memory; 3: pass A's too."""
         return int(lib.nlf_linear_get_fft_twiddles(self._h))
 
     @fft_twiddles.setter

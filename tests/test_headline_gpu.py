@@ -162,8 +162,23 @@ def test_tuned_variants_keep_C(L, golden):
     lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=3))
     lh.set_apply_tile(1)
     lh.kinv_mode = 1
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
+        if mode == 3:
+            lh.kinv_mode = 0
         lh.fft_twiddles = mode
         res = lh.C_full_batched(rho)
         assert res["status"] == 0
         assert c_agrees(res["C"], golden["b32_C"]).all(), dict(zip(seeds, cerr(res["C"], golden["b32_C"])))
+
+
+def test_tuned_variants_keep_C_64(L, golden):
+    """The 64^3 variants chosen on the B200 (closed-form Kinv with staged pass B slabs, shared twiddles, staged
+    pass C) on two fixture cells through one slot: C agrees with the oracle."""
+    seeds = [int(v) for v in golden["b64_seeds"]][:2]
+    rho = np.stack([OD.random_cell(i, n_o=32, r=1.5, beta=16.0, kmax=2)[0] for i in seeds])
+    lh = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, slots=1))
+    lh.kinv_mode = 2
+    lh.fft_twiddles = 2
+    res = lh.C_full_batched(rho)
+    assert res["status"] == 0
+    assert c_agrees(res["C"], golden["b64_C"][:2]).all(), dict(zip(seeds, cerr(res["C"], golden["b64_C"][:2])))
