@@ -785,9 +785,9 @@ __device__ __forceinline__ void block_sum_ordered(double (&v)[K], double* red /*
 }
 
 // Pass A: (fused) r update and sums; w r; packed real z FFT + real post-processing per row; y FFT per column.
-// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2. STG (with SMT): the y
-// transforms write back into the plane buffer, and the plane leaves in whole 528-byte kz rows (coalesced)
-// instead of 16-byte pieces scattered over 8 ky rows per warp.
+// SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2. STG (with SMT, one plane
+// per CTA): the r update, the sums and the node scaling run over the plane in whole 512-byte rows (coalesced)
+// and reach the FFT's layout through the plane buffer.
 template <int N, bool SMT, bool STG = false>
 __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     k_fa_fast(double* __restrict__ r, const double* __restrict__ w, cplx<double>* __restrict__ spec, int m,
@@ -819,7 +819,42 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
   cplx<double> a[8];
   double sr = 0.0, srr = 0.0;
-  {
+  if constexpr (STG && P == 1) {
+    // the plane in whole 512-byte rows: each warp takes one row of r, Ap and w per step (coalesced) for the r
+    // update, the sums and the scaling; w r goes through the plane buffer to the FFT's layout
+    double2* vs2 = reinterpret_cast<double2*>(sm);  // [N rows][N / 2 pairs]
+    const long poff = ((long)vec * 3 + c) * NN + (long)x * N * N;
+    double2* rq = reinterpret_cast<double2*>(r + poff);
+    const double2* aq = fu.Ap ? reinterpret_cast<const double2*>(static_cast<const double*>(fu.Ap) + poff) : nullptr;
+    const double2* wq = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + (long)x * N * N) : nullptr;
+    const double al = aq ? fu.vs[vec].alpha : 0.0, mu = aq ? fu.vs[vec].mean[c] : 0.0;
+    constexpr int PAIRS = N * N / 2;
+#pragma unroll 4
+    for (int j = t; j < PAIRS; j += 256) {
+      double2 v = rq[j];
+      if (aq) {
+        const double2 u = aq[j];
+        v.x -= al * (u.x - mu);
+        v.y -= al * (u.y - mu);
+        rq[j] = v;
+      }
+      sr += v.x + v.y;
+      srr += v.x * v.x + v.y * v.y;
+      if (wq) {
+        const double2 ww = wq[j];
+        v.x *= ww.x;
+        v.y *= ww.y;
+      }
+      vs2[j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double2 v = vs2[y * (N / 2) + l + Lz * q];
+      a[q] = {v.x, v.y};
+    }
+    __syncthreads();  // the plane buffer takes the rows' spectra next
+  } else {
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = rp2[l + Lz * q];
@@ -926,21 +961,8 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     fft_nat_in<Ly, 8, false>(b, ly, Ty);
     if (ok) {
       const int xx = blockIdx.x * P + pp, kb = 8 * brevL<Ly>(ly);
-      if constexpr (STG) {
-        // in place: this group alone reads and writes column (pp, kz), and its reads precede the shuffles
 #pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + kb) * H + swz<M>(kz)] = b[k1];
-      } else {
-#pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
-      }
-    }
-  }
-  if constexpr (STG) {
-    __syncthreads();
-    for (int i = t; i < P * N * H; i += 256) {
-      const int pp = i / (N * H), rr = i - pp * (N * H), ky = rr / H, kz = rr - ky * H;
-      sp[((long)ky * N + blockIdx.x * P + pp) * H + kz] = sm[((long)pp * N + ky) * H + swz<M>(kz)];
+      for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
     }
   }
 }
@@ -1221,6 +1243,30 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   constexpr double norm = 2.0 / (double)NN;
   const long roff = ((long)vec * 3 + c) * NN + ((long)x * N + y) * N;
   const double2* wp2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + ((long)x * N + y) * N) : nullptr;
+  if constexpr (STG) {
+    if (fu.p && P == 1) {
+      // the x/p update in whole 512-byte rows: z goes through the plane buffer (after every row's reads of it)
+      // and each warp then updates one row of x and p per step (coalesced), w, x and p read the same way
+      double2* zs = reinterpret_cast<double2*>(sm);  // [N rows][N / 2 pairs]
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 8; ++q) zs[y * (N / 2) + l + Lz * q] = make_double2(a[q].x * norm, a[q].y * norm);
+      __syncthreads();
+      const long poff = ((long)vec * 3 + c) * NN + (long)x * N * N;
+      const double2* wq2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + (long)x * N * N) : nullptr;
+      double2* xq2 = reinterpret_cast<double2*>(fu.x + poff);
+      double2* pq2 = reinterpret_cast<double2*>(fu.p + poff);
+      const double al = fu.vs[vec].alpha, be = fu.vs[vec].beta;
+      constexpr int PAIRS = N * N / 2;
+#pragma unroll 4
+      for (int j = t; j < PAIRS; j += 256) {
+        const double2 ww = wq2 ? wq2[j] : make_double2(1.0, 1.0), po = pq2[j], xo = xq2[j], zz = zs[j];
+        xq2[j] = make_double2(xo.x + al * po.x, xo.y + al * po.y);
+        pq2[j] = make_double2(zz.x * ww.x + be * po.x, zz.y * ww.y + be * po.y);
+      }
+      return;
+    }
+  }
   if (fu.p) {  // partial and partC are null here, so no thread reaches the barrier below
     px_row<Lz>(a, norm, wp2, reinterpret_cast<double2*>(fu.x + roff), reinterpret_cast<double2*>(fu.p + roff), l,
                fu.vs[vec].alpha, fu.vs[vec].beta);

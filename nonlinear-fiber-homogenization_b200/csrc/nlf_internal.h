@@ -119,7 +119,8 @@ struct LinearHandle {
   // FP64 cube pass B: 1 = Kinv entries in closed form (no table reads), 0 = from the table
   int pcb_closed = 0;
   // FP64 cube passes A and C: 0 = twiddles in registers (2 CTAs per SM), 1 = from shared memory (3 per SM),
-  // 2 = as 1 with pass C's spectrum rows staged through shared memory (coalesced), 3 = pass A's too
+  // 2 = as 1 with pass C's spectrum rows staged through shared memory and its x/p update in whole rows
+  // (coalesced), 3 = as 2 with pass A's row inputs coalesced too
   int fft_smt = 0;
 };
 
