@@ -1137,14 +1137,18 @@ def main():
     clocks = ClockSampler(vis.split(",")[local] if vis else torch.cuda.current_device())
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     torch.cuda.synchronize()
     e0.record()
+    marks[0].record()
     its = None
-    for _ in range(args.steps):
+    for k in range(args.steps):
         its = lh.C_full_batched(rho_d, out_C=C_d)["it"]
+        marks[k + 1].record()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    step_ms = [round(marks[k].elapsed_time(marks[k + 1]), 1) for k in range(args.steps)]
     clk = clocks.stop()
     # one more step with the library's per-launch CUDA events on (they cost a few per cent, so the timed
     # steps above run without them): the per-kernel times and the roofline come from this step
@@ -1202,7 +1206,7 @@ def main():
         return
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "step_ms": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(n, B, world),
         "solver": ("FP64 PCG" if fast["precision"] == "fp64" else "FP32 PCG inside FP64 refinement") +
