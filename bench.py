@@ -994,6 +994,10 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="solver precision of the measured solve (mixed: FP32 PCG inside FP64 refinement)")
     ap.add_argument("--graphs", action="store_true", help="replay the PCG iterations from CUDA graphs")
+    ap.add_argument("--fft-mode", type=int, default=None,
+                    help="force the preconditioner passes' twiddle / staging mode (0-3) instead of the tuner's")
+    ap.add_argument("--kinv-mode", type=int, default=None,
+                    help="force the Kinv mode (0 table, 1 closed form, 2 closed form with staged pass B)")
     ap.add_argument("--per-case", type=int, default=None,
                     help="per-case stopping probation for the measured solve (0 = lock-step per cell)")
     ap.add_argument("--tune", action="store_true",
@@ -1128,6 +1132,10 @@ def main():
         fast["use_graphs"] = True
     lh = L.LinearHomogenization((n, n, n), **MATERIAL, **fast)
     lh.stream = stream
+    if args.fft_mode is not None:
+        lh.fft_twiddles = args.fft_mode
+    if args.kinv_mode is not None:
+        lh.kinv_mode = args.kinv_mode
     for _ in range(args.warmup):
         lh.C_full_batched(rho_d, out_C=C_d)
     torch.cuda.synchronize()
