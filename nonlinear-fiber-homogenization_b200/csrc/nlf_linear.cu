@@ -501,7 +501,7 @@ static int solve_slots(LinearHandle& h, const SolveIn& in, const nlf_solve_opts&
   // refilled while reading snapshot j still shows its previous cell in the snapshots up to j + kLook (copied
   // before the refill was queued), so it is read again from snapshot j + kLook + 1 on. A stopped cell's slot
   // therefore idles for kLook extra chunks, which costs no GPU time: the kernels skip inactive cells.
-  constexpr int kLook = 2, kRing = kLook + 1;
+  constexpr int kLook = 3, kRing = kLook + 1;
   const size_t snap = S * sizeof(CellState) + (size_t)S * m * sizeof(VecState);
   PinnedBuf pin(kRing * snap);
   if (!pin.p) {
