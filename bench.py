@@ -208,10 +208,13 @@ def unit_bytes(kind, N, NS, m):
 
 
 # DRAM bytes per vector of a kernel class at 64^3, from one ncu --set full capture on the small profiling case
-# (`bench.py --ncu --cells 4 --iters 8`, one launch of 24 vectors; the full workload is too large to capture),
-# scaled to a launch by the vectors it processes: k_fc_pipe<64> (fused pass C) read 466.1 MB and wrote
-# 247.3 MB for 24 vectors.
-NCU_TRAFFIC_PER_VECTOR_64 = {"fft_c_f64": (466.139904e6 + 247.341312e6) / 24}
+# (`bench.py --ncu --cells 4 --iters 8`, one launch of 24 vectors per kernel with the tuned variants; the full
+# workload is too large to capture), scaled to a launch by the vectors it processes
+# (profiles/pcg_kernels_64cubed_fp64_ncu.md): read + write MB per 24-vector launch.
+NCU_TRAFFIC_PER_VECTOR_64 = {"apply_f64": (159.546368e6 + 115.603200e6) / 24,
+                             "fft_a_f64": (310.692608e6 + 251.151360e6) / 24,
+                             "fft_b_f64": (155.786752e6 + 102.791680e6) / 24,
+                             "fft_c_f64": (466.180096e6 + 248.286208e6) / 24}
 
 
 def roofline(prof, N, NS, m, peaks, peak_kind):
