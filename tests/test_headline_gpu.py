@@ -182,3 +182,15 @@ def test_tuned_variants_keep_C_64(L, golden):
     res = lh.C_full_batched(rho)
     assert res["status"] == 0
     assert c_agrees(res["C"], golden["b64_C"][:2]).all(), dict(zip(seeds, cerr(res["C"], golden["b64_C"][:2])))
+
+
+def test_per_case_stopping_survives_the_slow_mode_of_cell_10(L):
+    """Cell 10 of the 64^3 workload: its normal cases meet both stopping rules near iteration 310, then a slow
+    mode of the near-mechanism brings their residual back up (a CPU replay stopped them there with C 1.9e-4 off).
+    With the 64-iteration probation, per-case stopping keeps C within 1e-8 of the cell's C* (residual 1e-14)."""
+    rho = OD.random_cell(10, n_o=32, r=1.5, beta=16.0, kmax=2)[0][None]
+    ref = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, tol=1e-14, energy_tol=0.0, maxit=10000))
+    Cs = ref.C_full_batched(rho)["C"]
+    pc = L.LinearHomogenization(rho.shape[1:], **MAT, **dict(FAST, per_case=64)).C_full_batched(rho)
+    assert pc["status"] == 0
+    assert cerr(pc["C"], Cs).max() < C_TOL, cerr(pc["C"], Cs)
