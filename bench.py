@@ -709,6 +709,43 @@ def mech_arm(args, stream):
             "converged_all": all(r["converged"] for r in rows), "rows": rows, "kernels": kernels}
 
 
+def schwarz_arm(args, stream):
+    """Configuration 1: the Schwarz-P cell of 32^3 (pre-density -(cos X + cos Y + cos Z) on a 16^3 octant, cone filter
+    r 1.5, beta 16, exact volume 0.3, cubic symmetry), E 1, nu 0.3, emin 1e-9, six unit strains, PCG tol 1e-10;
+    C and dC/drho by the reference algorithm (unit-stiffness preconditioner) and by the node-scaled one, timed
+    with CUDA events, each C against the oracle's C in the committed fixture."""
+    import torch
+    from nlfiber_b200 import linear as L
+    from nlfiber_b200.density import GpuDensityMap
+    n_o = 16
+    xs = 2 * np.pi * (np.arange(n_o) + 0.5) / (2 * n_o)
+    phi = -sum(np.cos(g) for g in np.meshgrid(xs, xs, xs, indexing="ij"))
+    dm = GpuDensityMap(n_o, 3, r=1.5, v=0.3)
+    dm.stream = stream
+    rho = dm.run(phi, 16.0, eta=False)["rho"]
+    g = np.load(GOLDEN)
+    Co = g["schwarz_C"][0]
+    out = {}
+    for name, kw in (("reference algorithm (unit-stiffness FFT preconditioner)", dict(precond="fft", maxit=40000)),
+                     ("node-scaled preconditioner", dict(precond="scaled", maxit=4000))):
+        lh = L.LinearHomogenization(rho.shape[1:], **MATERIAL, tol=1e-10, check_every=64, use_graphs=True, **kw)
+        lh.stream = stream
+        lh.C_full_batched(rho)  # warm-up (graph capture, workspace)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = lh.C_full_batched(rho, want_u=True, want_dC=True)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = {"ms": round(e0.elapsed_time(e1), 2), "iterations": int(r["it"][0]), "status": int(r["status"]),
+                     "c_err_vs_oracle": float(rel_err(r["C"], Co[None])[0]),
+                     "C_11_12_44": [float(r["C"][0][0, 0]), float(r["C"][0][0, 1]), float(r["C"][0][3, 3])],
+                     "dC_drho_sum_11": float(np.asarray(r["dC"])[0, 0, 0].sum())}
+    return {"mode": "schwarz", "workload": "Schwarz-P cell 32^3, v 0.3, emin 1e-9, tol 1e-10, C and dC/drho",
+            "timing": "CUDA events around one C_full call with dC/drho (rho on the device, C, u, dC to the host)",
+            **out}
+
+
 def uneven_beta(i):
     """Sharpness of cell i of the uneven batch: drawn from {4, 8, 16} by default_rng(20000 + i)."""
     return float(np.random.default_rng(20_000 + i).choice([4.0, 8.0, 16.0]))
@@ -1003,6 +1040,8 @@ def main():
                     help="force the Kinv mode (0 table, 1 closed form, 2 closed form with staged pass B)")
     ap.add_argument("--per-case", type=int, default=None,
                     help="per-case stopping probation for the measured solve (0 = lock-step per cell)")
+    ap.add_argument("--schwarz", action="store_true",
+                    help="configuration 1: the Schwarz-P 32^3 cell's C and dC/drho by both preconditioners")
     ap.add_argument("--tune", action="store_true",
                     help="time every tile variant of the FP64 apply at --n^3 on the batch's vectors and exit")
     ap.add_argument("--mech-precond", default="scaled", choices=["fft", "scaled"],
@@ -1020,6 +1059,13 @@ def main():
         import torch
         torch.cuda.set_device(local)
         res = uneven_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+    if args.schwarz:
+        import torch
+        torch.cuda.set_device(local)
+        res = schwarz_arm(args, torch.cuda.current_stream().cuda_stream)
         if rank == 0:
             print(json.dumps(res), flush=True)
         return
