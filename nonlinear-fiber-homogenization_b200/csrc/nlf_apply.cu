@@ -37,7 +37,6 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   T(*sl)[NE] = reinterpret_cast<T(*)[NE]>(smem_raw + sizeof(T) * (9 * NP + 24 * NE));
   __shared__ int gys[HY], gzs[HZ];
   __shared__ double red[32 * 4];
-  (void)EY;
 
   const int vec = blockIdx.z, cell = vec / m;
   if (!vec_live(cs, vec, m)) return;
@@ -68,8 +67,14 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
       poff[i] = c * N + (long)gys[hy] * n2 + gzs[hz];
     }
   }
+  // thread -> element: the EY x TZ elements right of the halo column run along rows of TZ threads, so that a
+  // half-warp's 8-byte accesses (node corners, forces, scales) fall on 16 consecutive words of one row (no bank
+  // conflicts when TZ is a multiple of 16); the EY halo-column elements follow. e = ey EZ + ez indexes the
+  // element's force and scale slots.
   const bool ev = tid < NE;
-  const int ey = tid / EZ, ez = tid - (tid / EZ) * EZ;
+  const int ey = tid < EY * TZ ? tid / TZ : tid - EY * TZ;
+  const int ez = tid < EY * TZ ? 1 + (tid - (tid / TZ) * TZ) : 0;
+  const int e = ey * EZ + ez;
   const long soff = ev ? (long)gys[ey] * n2 + gzs[ez] : 0;
   int cidx[4];  // in-plane corner q = ay + 2 az of this element, in node-plane coordinates
 #pragma unroll
@@ -87,7 +92,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 #pragma unroll
       for (int j = -1; j <= 1; ++j) pl[slot(xb + j)][0][idx] = __ldg(xv + (long)wrap(xb + j, n0) * P + poff[i]);
     }
-  if (ev) sl[(xb - 1) & 1][tid] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
+  if (ev) sl[(xb - 1) & 1][e] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
   __syncthreads();
 
   T ft[3][4];  // top-corner forces carried to the next layer
@@ -122,19 +127,19 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
           v[c][2 * q] = lo[c][cidx[q]];
           v[c][2 * q + 1] = hi[c][cidx[q]];
         }
-      const ModeC<T> ks = scale_modec(kc, sl[k & 1][tid]);
+      const ModeC<T> ks = scale_modec(kc, sl[k & 1][e]);
       element_force(v, ks, f);
       if (k >= xb) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) gk[q][c][tid] = ft[c][q] + f[c][2 * q];
+          for (int q = 0; q < 4; ++q) gk[q][c][e] = ft[c][q] + f[c][2 * q];
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) ft[c][q] = f[c][2 * q + 1];
-      if (snext) sl[(k + 1) & 1][tid] = pres;  // layer k + 1's scales; sl[(k+1)&1] was last read by layer k - 1
+      if (snext) sl[(k + 1) & 1][e] = pres;  // layer k + 1's scales; sl[(k+1)&1] was last read by layer k - 1
     }
     if (partial && outp && k >= xb) {
 #pragma unroll

@@ -656,7 +656,9 @@ struct LaneTw {
   __device__ __forceinline__ cplx<double> ss(int j) const { return st[j]; }
 };
 // The same twiddles read on use from a shared-memory copy of the table (fewer registers, more CTAs per SM).
-template <int L, int R>
+// SWZ: the copy holds entry i at tw_slot(i) (pass B's table; see there).
+__device__ __forceinline__ int tw_slot(int i) { return i ^ ((i >> 3) & 7); }
+template <int L, int R, bool SWZ = false>
 struct LaneTwS {
   const cplx<double>* tw;  // shared, length R L
   int l;
@@ -664,20 +666,24 @@ struct LaneTwS {
     tw = t;
     l = lane;
   }
+  __device__ __forceinline__ cplx<double> at(int i) const { return tw[SWZ ? tw_slot(i) : i]; }
   __device__ __forceinline__ cplx<double> rr(int k1) const {
-    return (l && k1) ? tw[l * k1] : cplx<double>{1.0, 0.0};
+    return (l && k1) ? at(l * k1) : cplx<double>{1.0, 0.0};
   }
   __device__ __forceinline__ cplx<double> ss(int j) const {
     constexpr int n = R * L;
     const int s = 1 << j;
-    return (L > 1) ? tw[(l & (s - 1)) * (n / (2 * s))] : cplx<double>{1.0, 0.0};
+    return (L > 1) ? at((l & (s - 1)) * (n / (2 * s))) : cplx<double>{1.0, 0.0};
   }
 };
 template <int L, int R, bool SMT>
 using TwT = typename std::conditional<SMT, LaneTwS<L, R>, LaneTw<L, R>>::type;
 
 // Copies of the y, z and post-processing twiddle tables (N, N/2 and N entries) in shared memory, for the
-// shared-twiddle variants of passes A and C; ends with a barrier.
+// shared-twiddle variants of passes A and C; ends with a barrier. The post-processing table is stored permuted
+// within aligned runs of 8 (entry k at swz_tw(k)): the 4 lanes of a row read entries k1 + 8 k2, which then fall in
+// different bank groups.
+__device__ __forceinline__ int swz_tw(int k) { return (k & ~7) | ((k ^ (k >> 3)) & 7); }
 template <int N>
 struct SmTw {
   cplx<double> y[N], z[N / 2], n2[N];
@@ -687,7 +693,7 @@ __device__ __forceinline__ void stage_tw(SmTw<N>& st, const cplx<double>* __rest
                                          const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2) {
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     st.y[i] = tw_y[i];
-    st.n2[i] = tw_n2[i];
+    st.n2[swz_tw(i)] = tw_n2[i];
     if (i < N / 2) st.z[i] = tw_z[i];
   }
   __syncthreads();
@@ -763,8 +769,28 @@ struct Fast {
   static constexpr int KZC = (N == 64) ? 2 : 1;            // kz chunks per ky row (one CTA each)
   static constexpr int KZN = (H + KZC - 1) / KZC;          // kz per chunk
   static constexpr int NTB = ((KY * KZN * Lb) + 31) / 32 * 32;
-  static constexpr size_t smem_plane() { return (size_t)P * N * H * sizeof(cplx<double>); }
+  // row stride (16-byte entries) of pass B's staged slabs: KZN is odd, so the 8 x rows a quarter-warp reads or
+  // writes at one kz land in 8 different bank groups
+  static constexpr int KPB = KZN;
+  // plane buffer of passes A and C: [P][N rows][HS] (16-byte entries), bin kz of row y at slot(y, kz). For N = 64
+  // the rows are padded to 40 entries and the bins permuted within each aligned run of 8 by the row and the run
+  // index, so that a quarter-warp's 16-byte accesses hit 8 different bank groups in every access pattern of the
+  // passes: 8 rows of one column (y = l + 8 q, and y = k1 + 8 brev(l) when the y transform writes back), and 4 bins
+  // k1 + 8 k2 (or their mirrors M - k) of 2 adjacent rows. For N = 32 the rows stay at H entries (swz only).
+  static constexpr int HS = (N == 64) ? 40 : H;
+  // row stride, in double pairs, of the real-row views of the same buffer (staged variants, one plane per CTA)
+  static constexpr int PS = (N == 64) ? N / 2 + 4 : N / 2;
+  static constexpr size_t smem_plane() { return (size_t)P * N * HS * sizeof(cplx<double>); }
+  __device__ static __forceinline__ int slot(int y, int kz) {
+    if constexpr (N == 64) {
+      const int h = ((((y & 1) << 2) | ((y & 7) >> 1)) ^ (y >> 3)) & 7;
+      return (kz & ~7) | ((kz ^ (kz >> 3) ^ h) & 7);
+    } else {
+      return swz<M>(kz);
+    }
+  }
 };
+static_assert(Fast<64>::PS * 64 <= Fast<64>::P * 64 * Fast<64>::HS, "real-row view fits the plane buffer");
 
 // deterministic block sum of K values: warp shuffles, per-warp slots, thread 0 adds the warps in order
 template <int K>
@@ -822,7 +848,7 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   if constexpr (STG && P == 1) {
     // the plane in whole 512-byte rows: each warp takes one row of r, Ap and w per step (coalesced) for the r
     // update, the sums and the scaling; w r goes through the plane buffer to the FFT's layout
-    double2* vs2 = reinterpret_cast<double2*>(sm);  // [N rows][N / 2 pairs]
+    double2* vs2 = reinterpret_cast<double2*>(sm);  // [N rows][PS] (N / 2 pairs used)
     const long poff = ((long)vec * 3 + c) * NN + (long)x * N * N;
     double2* rq = reinterpret_cast<double2*>(r + poff);
     const double2* aq = fu.Ap ? reinterpret_cast<const double2*>(static_cast<const double*>(fu.Ap) + poff) : nullptr;
@@ -845,12 +871,12 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
         v.x *= ww.x;
         v.y *= ww.y;
       }
-      vs2[j] = v;
+      vs2[(j / (N / 2)) * F::PS + (j % (N / 2))] = v;
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const double2 v = vs2[y * (N / 2) + l + Lz * q];
+      const double2 v = vs2[y * F::PS + l + Lz * q];
       a[q] = {v.x, v.y};
     }
     __syncthreads();  // the plane buffer takes the rows' spectra next
@@ -894,7 +920,7 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     fft_nat_in<Lz, 8, false>(a, l, T);
   }
   const int k2 = brevL<Lz>(l);
-  cplx<double>* row = sm + ((long)p * N + y) * H;
+  cplx<double>* row = sm + ((long)p * N + y) * F::HS;
   {
     // k1 = 0 partner: bin M - 8 k2 = 8 ((Lz - k2) mod Lz)
     const int lane0 = (t & 31) - l;
@@ -909,14 +935,14 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
       cplx<double> R;
       if (k == 0) {
         R = {a[0].x + a[0].y, 0.0};
-        row[swz<M>(M)] = {a[0].x - a[0].y, 0.0};
+        row[F::slot(y, M)] = {a[0].x - a[0].y, 0.0};
       } else {
         const cplx<double> A = a[k1], B = bz[k1];  // X_k, X_{M-k}
         const cplx<double> E{(A.x + B.x) * 0.5, (A.y - B.y) * 0.5};
         const cplx<double> O{(A.y + B.y) * 0.5, -(A.x - B.x) * 0.5};
-        R = cadd(E, cmul(tw_n2[k], O));
+        R = cadd(E, cmul(tw_n2[SMT ? swz_tw(k) : k], O));
       }
-      row[swz<M>(k)] = R;
+      row[F::slot(y, k)] = R;
     }
   }
   if (fu.partA) {
@@ -957,7 +983,7 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     const int pp = ok ? task / H : 0, kz = ok ? task - pp * H : 0;
     cplx<double> b[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) b[q] = sm[((long)pp * N + ly + Ly * q) * H + swz<M>(kz)];
+    for (int q = 0; q < 8; ++q) b[q] = sm[((long)pp * N + ly + Ly * q) * F::HS + F::slot(ly + Ly * q, kz)];
     fft_nat_in<Ly, 8, false>(b, ly, Ty);
     if (ok) {
       const int xx = blockIdx.x * P + pp, kb = 8 * brevL<Ly>(ly);
@@ -975,9 +1001,9 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
 struct SymYZ {
   double my, sy, gy, mz, sz, gz;
 };
-__device__ __forceinline__ SymYZ sym_yz(const cplx<double>* __restrict__ tw, int ky, int kz) {
-  const double cy = tw[ky].x, cz = tw[kz].x;
-  return {(2.0 + cy) * (1.0 / 3.0), 2.0 - 2.0 * cy, -tw[ky].y, (2.0 + cz) * (1.0 / 3.0), 2.0 - 2.0 * cz, -tw[kz].y};
+__device__ __forceinline__ SymYZ sym_yz(cplx<double> ty, cplx<double> tz) {
+  const double cy = ty.x, cz = tz.x;
+  return {(2.0 + cy) * (1.0 / 3.0), 2.0 - 2.0 * cy, -ty.y, (2.0 + cz) * (1.0 / 3.0), 2.0 - 2.0 * cz, -tz.y};
 }
 __device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx, double lam, double mu,
                                             double (&out)[6]) {
@@ -1006,17 +1032,20 @@ __device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx
 // Pass B: x FFT of the three components of each (ky, kz) column, 3x3 Kinv, Parseval (r, z) partial, inverse.
 // CLOSED: the Kinv entries are computed in closed form from the twiddles and the medium's (lam, mu) instead of
 // read from the table; the x twiddles are then read from a shared-memory copy of the table, which keeps the CTA
-// (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps).
+// (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps). The copy holds entry i
+// at tw_slot(i) = i ^ ((i >> 3) & 7): the 8 lanes of a quarter-warp then read the entries kx = k1 + 4 brev(l) of
+// the inverse symbol, and the stage and most of the register-DFT twiddles of the x transform, from 8 different
+// bank groups (in table order the kx reads alone took 8 wavefronts each).
 // STG (cubes of 64, with CLOSED): the CTA's three [x][kz-chunk] slabs are copied whole into shared memory by
 // cp.async (272-byte row pieces instead of 16-byte pieces over 16 x rows per warp), transformed from there, and
-// written back the same way; rows padded to KZN + 1 entries spread the column reads over all banks.
+// written back the same way; rows of KZN (odd) entries spread the column accesses over all bank groups.
 template <int N, bool CLOSED, bool STG = false>
 __global__ void __launch_bounds__(Fast<N>::NTB, 2)
     k_fb_fast(cplx<double>* __restrict__ spec, const double* __restrict__ kinv, int m,
               const cplx<double>* __restrict__ tw_x, const CellState* __restrict__ cs,
               unsigned long long* __restrict__ units, int ukind, PcgFuse fu, double lam, double mu) {
   using F = Fast<N>;
-  constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN, KP = KZN + 1;
+  constexpr int M = F::M, H = F::H, L = F::Lb, KY = F::KY, KZC = F::KZC, KZN = F::KZN, KP = F::KPB;
   static_assert(!STG || KY == 1, "staged pass B takes one ky row per CTA");
   __shared__ double red[32];
   __shared__ cplx<double> twsh[N];
@@ -1026,7 +1055,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
   if constexpr (CLOSED) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x) twsh[i] = tw_x[i];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) twsh[tw_slot(i)] = tw_x[i];
     __syncthreads();
     tw_x = twsh;
   }
@@ -1057,7 +1086,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
       else
         a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
     }
-  TwT<L, 4, CLOSED> T;
+  typename std::conditional<CLOSED, LaneTwS<L, 4, true>, LaneTw<L, 4>>::type T;
   T.load(tw_x, l);
 #pragma unroll
   for (int c = 0; c < 3; ++c) fft_nat_in<L, 4, false>(a[c], l, T);
@@ -1065,7 +1094,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   const double wt = (kz == 0 || kz == M) ? 1.0 : 2.0;
   const int kb = 4 * brevL<L>(l);
   SymYZ q{};
-  if constexpr (CLOSED) q = sym_yz(tw_x, ky, ok ? kz : 0);
+  if constexpr (CLOSED) q = sym_yz(tw_x[tw_slot(ky)], tw_x[tw_slot(ok ? kz : 0)]);
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) {
     double Kv[6];
@@ -1075,7 +1104,8 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
 #pragma unroll
         for (int i = 0; i < 6; ++i) Kv[i] = 0.0;
       } else {
-        kinv_closed(q, tw_x[kx].x, -tw_x[kx].y, lam, mu, Kv);
+        const cplx<double> tx = tw_x[tw_slot(kx)];
+        kinv_closed(q, tx.x, -tx.y, lam, mu, Kv);
       }
     } else {
       const double* K = kinv + (((long)(k1 + kb) * N + ky) * H + (ok ? kz : 0)) * 6;
@@ -1177,9 +1207,14 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   const int t = threadIdx.x;
   const cplx<double>* sp = spec + ((long)vec * 3 + c) * ((long)N * N * H);
   if constexpr (STG) {
-    for (int i = t; i < P * N * H; i += 256) {
-      const int pp = i / (N * H), rr = i - pp * (N * H), ky = rr / H, kz = rr - ky * H;
-      cp16_async(sm + ((long)pp * N + ky) * H + swz<M>(kz), sp + ((long)ky * N + blockIdx.x * P + pp) * H + kz);
+    // walked in slot order (8 consecutive threads fill one aligned run of 8 slots: no bank conflicts); the pad
+    // slots of a row are skipped
+    constexpr int HS = F::HS;
+    for (int i = t; i < P * N * HS; i += 256) {
+      const int pp = i / (N * HS), rr = i - pp * (N * HS), ky = rr / HS, sl = rr - ky * HS;
+      const int kz = F::slot(ky, sl);  // slot() permutes each aligned run of 8 as an involution
+      if (kz < H && F::slot(ky, kz) == sl)
+        cp16_async(sm + ((long)pp * N + ky) * HS + sl, sp + ((long)ky * N + blockIdx.x * P + pp) * H + kz);
     }
     cp_async_commit();
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -1201,7 +1236,7 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         if constexpr (STG)
-          b[q] = sm[((long)pp * N + ly + Ly * q) * H + swz<M>(kz)];
+          b[q] = sm[((long)pp * N + ly + Ly * q) * F::HS + F::slot(ly + Ly * q, kz)];
         else
           b[q] = ok ? sp[((long)(ly + Ly * q) * N + xx) * H + kz] : cplx<double>{0.0, 0.0};
       }
@@ -1209,14 +1244,14 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
       if (ok) {
         const int yb = 8 * brevL<Ly>(ly);
 #pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + yb) * H + swz<M>(kz)] = b[k1];
+        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + yb) * F::HS + F::slot(k1 + yb, kz)] = b[k1];
       }
     }
   }
   __syncthreads();
   const int p = t / (N * Lz), rem = t - p * (N * Lz), y = rem / Lz, l = rem - y * Lz;
   const int x = blockIdx.x * P + p;
-  const cplx<double>* row = sm + ((long)p * N + y) * H;
+  const cplx<double>* row = sm + ((long)p * N + y) * F::HS;
   cplx<double> a[8];
   const int k2 = brevL<Lz>(l);
 #pragma unroll
@@ -1224,13 +1259,13 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     const int k = k1 + 8 * k2;
     if (k == 0) {
       // X_0 and X_M of a real signal are real: their imaginary parts are rounding and are dropped
-      const double A = row[swz<M>(0)].x, B = row[swz<M>(M)].x;
+      const double A = row[F::slot(y, 0)].x, B = row[F::slot(y, M)].x;
       a[k1] = {(A + B) * 0.5, (A - B) * 0.5};
     } else {
-      const cplx<double> A = row[swz<M>(k)], B = row[swz<M>(M - k)];
+      const cplx<double> A = row[F::slot(y, k)], B = row[F::slot(y, M - k)];
       const cplx<double> E{(A.x + B.x) * 0.5, (A.y - B.y) * 0.5};
       const cplx<double> D{(A.x - B.x) * 0.5, (A.y + B.y) * 0.5};
-      const cplx<double> O = cmul(D, cconj(tw_n2[k]));
+      const cplx<double> O = cmul(D, cconj(tw_n2[SMT ? swz_tw(k) : k]));
       a[k1] = {E.x - O.y, E.y + O.x};
     }
   }
@@ -1247,10 +1282,10 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     if (fu.p && P == 1) {
       // the x/p update in whole 512-byte rows: z goes through the plane buffer (after every row's reads of it)
       // and each warp then updates one row of x and p per step (coalesced), w, x and p read the same way
-      double2* zs = reinterpret_cast<double2*>(sm);  // [N rows][N / 2 pairs]
+      double2* zs = reinterpret_cast<double2*>(sm);  // [N rows][PS] (N / 2 pairs used)
       __syncthreads();
 #pragma unroll
-      for (int q = 0; q < 8; ++q) zs[y * (N / 2) + l + Lz * q] = make_double2(a[q].x * norm, a[q].y * norm);
+      for (int q = 0; q < 8; ++q) zs[y * F::PS + l + Lz * q] = make_double2(a[q].x * norm, a[q].y * norm);
       __syncthreads();
       const long poff = ((long)vec * 3 + c) * NN + (long)x * N * N;
       const double2* wq2 = w ? reinterpret_cast<const double2*>(w + (long)(vec / m) * NN + (long)x * N * N) : nullptr;
@@ -1260,7 +1295,8 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
       constexpr int PAIRS = N * N / 2;
 #pragma unroll 4
       for (int j = t; j < PAIRS; j += 256) {
-        const double2 ww = wq2 ? wq2[j] : make_double2(1.0, 1.0), po = pq2[j], xo = xq2[j], zz = zs[j];
+        const double2 ww = wq2 ? wq2[j] : make_double2(1.0, 1.0), po = pq2[j], xo = xq2[j],
+                      zz = zs[(j / (N / 2)) * F::PS + (j % (N / 2))];
         xq2[j] = make_double2(xo.x + al * po.x, xo.y + al * po.y);
         pq2[j] = make_double2(zz.x * ww.x + be * po.x, zz.y * ww.y + be * po.y);
       }
@@ -1476,7 +1512,7 @@ static int launch_fb_staged(dim3 grid, cplx<double>* spec, const double* kinv, i
                             const CellState* cs, unsigned long long* units, const PcgFuse& fu, double lam0,
                             double mu0, cudaStream_t st) {
   if constexpr (N == 64) {
-    constexpr size_t sbb = (size_t)3 * N * (Fast<N>::KZN + 1) * sizeof(cplx<double>);
+    constexpr size_t sbb = (size_t)3 * N * Fast<N>::KPB * sizeof(cplx<double>);
     NLF_CUDA_TRY(raise_dyn_smem(k_fb_fast<N, true, true>, (int)sbb));
     k_fb_fast<N, true, true><<<grid, Fast<N>::NTB, sbb, st>>>(spec, kinv, m, twx, cs, units, PK_FFTB64, fu, lam0, mu0);
     NLF_CHECK_LAUNCH();
