@@ -655,47 +655,59 @@ struct LaneTw {
   __device__ __forceinline__ cplx<double> rr(int k1) const { return r[k1]; }
   __device__ __forceinline__ cplx<double> ss(int j) const { return st[j]; }
 };
-// The same twiddles read on use from a shared-memory copy of the table (fewer registers, more CTAs per SM).
-// SWZ: the copy holds entry i at tw_slot(i) (pass B's table; see there).
-__device__ __forceinline__ int tw_slot(int i) { return i ^ ((i >> 3) & 7); }
-template <int L, int R, bool SWZ = false>
+// The same twiddles read on use from a lane-major shared-memory table (fewer registers, more CTAs per SM): row
+// k1 - 1 (k1 = 1..R-1) holds W_n^{l k1} and row R - 1 + j the stage-j factor, for lanes l = 0..L-1 side by side.
+// The L lanes of a line read L consecutive entries of one row (no bank conflicts, no index arithmetic beyond the
+// lane's base). Entries equal those LaneTw reads from the table, (1, 0) for l = 0.
+template <int L, int R>
+struct LaneTab {
+  static constexpr int NS = ilog2c(L) > 0 ? ilog2c(L) : 1;
+  static constexpr int ROWS = (R - 1) + NS;
+  static constexpr int SIZE = ROWS * L;
+};
+// Fills a lane-major table from a twiddle table of n = R L entries (tw[k] = e^{-2 pi i k / n}); no barrier.
+template <int L, int R>
+__device__ __forceinline__ void stage_lane_tab(cplx<double>* __restrict__ dst, const cplx<double>* __restrict__ tw) {
+  constexpr int n = R * L;
+  for (int i = threadIdx.x; i < LaneTab<L, R>::SIZE; i += blockDim.x) {
+    const int row = i / L, l = i - row * L;
+    int k;
+    if (row < R - 1) {
+      k = l * (row + 1);
+    } else {
+      const int s = 1 << (row - (R - 1));
+      k = (l & (s - 1)) * (n / (2 * s));
+    }
+    dst[i] = (L > 1 && k) ? tw[k] : cplx<double>{1.0, 0.0};
+  }
+}
+template <int L, int R>
 struct LaneTwS {
-  const cplx<double>* tw;  // shared, length R L
-  int l;
-  __device__ __forceinline__ void load(const cplx<double>* t, int lane) {
-    tw = t;
-    l = lane;
-  }
-  __device__ __forceinline__ cplx<double> at(int i) const { return tw[SWZ ? tw_slot(i) : i]; }
-  __device__ __forceinline__ cplx<double> rr(int k1) const {
-    return (l && k1) ? at(l * k1) : cplx<double>{1.0, 0.0};
-  }
+  const cplx<double>* b;  // the lane's column of a LaneTab<L, R> table in shared memory
+  __device__ __forceinline__ void load(const cplx<double>* tab, int lane) { b = tab + lane; }
+  __device__ __forceinline__ cplx<double> rr(int k1) const { return k1 ? b[(k1 - 1) * L] : cplx<double>{1.0, 0.0}; }
   __device__ __forceinline__ cplx<double> ss(int j) const {
-    constexpr int n = R * L;
-    const int s = 1 << j;
-    return (L > 1) ? at((l & (s - 1)) * (n / (2 * s))) : cplx<double>{1.0, 0.0};
+    return (L > 1) ? b[(R - 1 + j) * L] : cplx<double>{1.0, 0.0};
   }
 };
 template <int L, int R, bool SMT>
 using TwT = typename std::conditional<SMT, LaneTwS<L, R>, LaneTw<L, R>>::type;
 
-// Copies of the y, z and post-processing twiddle tables (N, N/2 and N entries) in shared memory, for the
-// shared-twiddle variants of passes A and C; ends with a barrier. The post-processing table is stored permuted
+// Shared-memory twiddles of the shared-twiddle variants of passes A and C: lane-major tables of the y lines (N / 8
+// lanes of 8) and of the z lines (N / 16 lanes of 8), and the post-processing table (N entries) stored permuted
 // within aligned runs of 8 (entry k at swz_tw(k)): the 4 lanes of a row read entries k1 + 8 k2, which then fall in
-// different bank groups.
+// different bank groups. stage_tw ends with a barrier.
 __device__ __forceinline__ int swz_tw(int k) { return (k & ~7) | ((k ^ (k >> 3)) & 7); }
 template <int N>
 struct SmTw {
-  cplx<double> y[N], z[N / 2], n2[N];
+  cplx<double> y[LaneTab<N / 8, 8>::SIZE], z[LaneTab<N / 16, 8>::SIZE], n2[N];
 };
 template <int N>
 __device__ __forceinline__ void stage_tw(SmTw<N>& st, const cplx<double>* __restrict__ tw_y,
                                          const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    st.y[i] = tw_y[i];
-    st.n2[swz_tw(i)] = tw_n2[i];
-    if (i < N / 2) st.z[i] = tw_z[i];
-  }
+  stage_lane_tab<N / 8, 8>(st.y, tw_y);
+  stage_lane_tab<N / 16, 8>(st.z, tw_z);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) st.n2[swz_tw(i)] = tw_n2[i];
   __syncthreads();
 }
 
@@ -1029,13 +1041,15 @@ __device__ __forceinline__ void kinv_closed(const SymYZ& q, double cx, double gx
   out[5] = cxy * id;
 }
 
+__device__ __forceinline__ int tw_slot(int i) { return i ^ ((i >> 3) & 7); }
+
 // Pass B: x FFT of the three components of each (ky, kz) column, 3x3 Kinv, Parseval (r, z) partial, inverse.
 // CLOSED: the Kinv entries are computed in closed form from the twiddles and the medium's (lam, mu) instead of
 // read from the table; the x twiddles are then read from a shared-memory copy of the table, which keeps the CTA
-// (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps). The copy holds entry i
-// at tw_slot(i) = i ^ ((i >> 3) & 7): the 8 lanes of a quarter-warp then read the entries kx = k1 + 4 brev(l) of
-// the inverse symbol, and the stage and most of the register-DFT twiddles of the x transform, from 8 different
-// bank groups (in table order the kx reads alone took 8 wavefronts each).
+// (9 warps) at 96 registers, the most for 2 CTAs per SM (an SMSP takes 5 of the 18 warps). The x transforms read
+// their twiddles from a lane-major copy (LaneTab); the symbol's entries kx = k1 + 4 brev(l), ky and kz come from a
+// copy of the table that holds entry i at tw_slot(i) = i ^ ((i >> 3) & 7), so that the 8 lanes of a quarter-warp
+// read their kx entries from 8 different bank groups (8 wavefronts each in table order).
 // STG (cubes of 64, with CLOSED): the CTA's three [x][kz-chunk] slabs are copied whole into shared memory by
 // cp.async (272-byte row pieces instead of 16-byte pieces over 16 x rows per warp), transformed from there, and
 // written back the same way; rows of KZN (odd) entries spread the column accesses over all bank groups.
@@ -1049,6 +1063,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   static_assert(!STG || KY == 1, "staged pass B takes one ky row per CTA");
   __shared__ double red[32];
   __shared__ cplx<double> twsh[N];
+  __shared__ cplx<double> twl[CLOSED ? LaneTab<L, 4>::SIZE : 1];
   extern __shared__ __align__(16) unsigned char fb_raw[];
   cplx<double>* sb = reinterpret_cast<cplx<double>*>(fb_raw);  // STG: [3][N][KP]
   const int vec = blockIdx.z;
@@ -1056,6 +1071,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
   prof_count(units, ukind);
   if constexpr (CLOSED) {
     for (int i = threadIdx.x; i < N; i += blockDim.x) twsh[tw_slot(i)] = tw_x[i];
+    stage_lane_tab<L, 4>(twl, tw_x);
     __syncthreads();
     tw_x = twsh;
   }
@@ -1086,8 +1102,8 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
       else
         a[c][q] = ok ? spec[((long)vec * 3 + c) * NS + ((long)ky * N + l + L * q) * H + kz] : cplx<double>{0.0, 0.0};
     }
-  typename std::conditional<CLOSED, LaneTwS<L, 4, true>, LaneTw<L, 4>>::type T;
-  T.load(tw_x, l);
+  typename std::conditional<CLOSED, LaneTwS<L, 4>, LaneTw<L, 4>>::type T;
+  T.load(CLOSED ? twl : tw_x, l);
 #pragma unroll
   for (int c = 0; c < 3; ++c) fft_nat_in<L, 4, false>(a[c], l, T);
   double dot[1] = {0.0};
