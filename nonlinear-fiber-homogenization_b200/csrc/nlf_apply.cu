@@ -13,6 +13,8 @@
 // to shared memory; each output node then sums its 4 in-plane element contributions. Node planes are
 // prefetched three layers ahead into a three-slot ring, so one barrier per layer suffices. Every output node is
 // written once, with a fixed summation order (deterministic), and the whole 27-point stencil stays on chip.
+#include <climits>
+
 #include "nlf_internal.h"
 #include "nlf_prof.cuh"
 
@@ -28,21 +30,23 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   constexpr int NT = (NE + 31) / 32 * 32;
   constexpr int NP = HY * HZ;
   constexpr int PF = (3 * NP + NT - 1) / NT;  // plane values each thread prefetches per layer
-  // One barrier per layer: node plane j lives in pl[j % 3] (written three layers ahead, after the barrier of
-  // the layer that last read the slot), element forces and scales alternate between two buffers. Dynamic
-  // shared memory (ApplyTiles<TY, TZ, T>::smem() bytes): pl [3][3][NP], g [2][4][3][NE], sl [2][NE].
+  constexpr int PFF = (3 * NP) / NT;          // ... of which the first PFF exist for every thread
+  // One barrier per layer. Dynamic shared memory (apply_smem<T, TY, TZ>() bytes): a ring of three node planes
+  // [3][3 comps][NP] (plane k + 3 is written into the slot of plane k after the barrier of layer k, the last layer
+  // that reads plane k), element forces [2][4 corners][3 comps][NE] and scales [2][NE], each alternating between
+  // its two buffers. The slots are tracked as offsets that rotate every layer (no index arithmetic mod 3), and
+  // every offset into a vector is 32-bit (the host bounds 3 N below 2^31).
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T(*pl)[3][NP] = reinterpret_cast<T(*)[3][NP]>(smem_raw);
-  T(*g)[4][3][NE] = reinterpret_cast<T(*)[4][3][NE]>(smem_raw + sizeof(T) * 9 * NP);
-  T(*sl)[NE] = reinterpret_cast<T(*)[NE]>(smem_raw + sizeof(T) * (9 * NP + 24 * NE));
+  T* const pl = reinterpret_cast<T*>(smem_raw);
+  T* const g = pl + 9 * NP;
+  T* const sl = g + 24 * NE;
   __shared__ int gys[HY], gzs[HZ];
   __shared__ double red[32 * 4];
 
   const int vec = blockIdx.z, cell = vec / m;
   if (!vec_live(cs, vec, m)) return;
   prof_count(units, ukind);
-  const long N = (long)n0 * n1 * n2;
-  const long P = (long)n1 * n2;
+  const int P = n1 * n2, N = n0 * P;
   const int ntz = (n2 + TZ - 1) / TZ;
   const int z0 = (blockIdx.x % ntz) * TZ, y0 = (blockIdx.x / ntz) * TY;
   const int xb = blockIdx.y * lx, xe = min(xb + lx, n0);
@@ -55,8 +59,8 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   for (int i = tid; i < HZ; i += NT) gzs[i] = wrap(z0 - 1 + i, n2);
   __syncthreads();
 
-  // per-thread offsets (within a node plane) of the plane values this thread loads, and of its element's s
-  long poff[PF];
+  // per-thread offsets (within a node plane of the vector) of the plane values this thread loads
+  int poff[PF];
 #pragma unroll
   for (int i = 0; i < PF; ++i) {
     const int idx = tid + i * NT;
@@ -64,7 +68,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
     if (idx < 3 * NP) {
       const int c = idx / NP, r = idx - c * NP;
       const int hy = r / HZ, hz = r - hy * HZ;
-      poff[i] = c * N + (long)gys[hy] * n2 + gzs[hz];
+      poff[i] = c * N + gys[hy] * n2 + gzs[hz];
     }
   }
   // thread -> element: the EY x TZ elements right of the halo column run along rows of TZ threads, so that a
@@ -75,24 +79,26 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   const int ey = tid < EY * TZ ? tid / TZ : tid - EY * TZ;
   const int ez = tid < EY * TZ ? 1 + (tid - (tid / TZ) * TZ) : 0;
   const int e = ey * EZ + ez;
-  const long soff = ev ? (long)gys[ey] * n2 + gzs[ez] : 0;
+  const int soff = ev ? gys[ey] * n2 + gzs[ez] : 0;
   int cidx[4];  // in-plane corner q = ay + 2 az of this element, in node-plane coordinates
 #pragma unroll
   for (int q = 0; q < 4; ++q) cidx[q] = (ey + (q & 1)) * HZ + ez + (q >> 1);
-  const bool outp = tid < TY * TZ;
   const int ty = tid / TZ, tz = tid - (tid / TZ) * TZ;
-  const int own = (ty + 1) * HZ + tz + 1;  // the output node in node-plane coordinates
-  auto slot = [](int j) { return ((j % 3) + 3) % 3; };
+  const bool outp = tid < TY * TZ;
+  const bool ownv = outp && y0 + ty < n1 && z0 + tz < n2;  // this thread writes output node (y0 + ty, z0 + tz)
+  const int own = (ty + 1) * HZ + tz + 1;                   // the output node in node-plane coordinates
+  const int inpl = (y0 + ty) * n2 + z0 + tz;               // ... and within a plane of the vector
+  const int e00 = (ty + 1) * EZ + (tz + 1);  // node (ty+1, tz+1) is corner q = ay + 2az of element (ty+1-ay, tz+1-az)
 
-  // prologue: node planes xb - 1, xb, xb + 1 and the element scales of layer xb - 1
+  // prologue: node planes xb - 1, xb, xb + 1 into ring slots 0, 1, 2 and the element scales of layer xb - 1
 #pragma unroll
   for (int i = 0; i < PF; ++i)
-    if (poff[i] >= 0) {
+    if (i < PFF || poff[i] >= 0) {
       const int idx = tid + i * NT;
 #pragma unroll
-      for (int j = -1; j <= 1; ++j) pl[slot(xb + j)][0][idx] = __ldg(xv + (long)wrap(xb + j, n0) * P + poff[i]);
+      for (int j = 0; j < 3; ++j) pl[j * 3 * NP + idx] = __ldg(xv + (wrap(xb - 1 + j, n0) * P + poff[i]));
     }
-  if (ev) sl[(xb - 1) & 1][e] = __ldg(sv + (long)wrap(xb - 1, n0) * P + soff);
+  if (ev) sl[e] = __ldg(sv + (wrap(xb - 1, n0) * P + soff));
   __syncthreads();
 
   T ft[3][4];  // top-corner forces carried to the next layer
@@ -102,20 +108,24 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
     for (int q = 0; q < 4; ++q) ft[c][q] = T(0);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
+  int r0 = 0, r1 = 3 * NP, r2 = 6 * NP;  // ring slots of planes k, k + 1, k + 2
+  int gc = 0, sc = 0;                    // this layer's force and scale buffers (the others: 12 NE - gc, NE - sc)
+  int pofs = wrap(xb + 2, n0) * P;       // plane k + 3 within the vector
+  int sofs = wrap(xb, n0) * P + soff;    // this element's scale in layer k + 1
+  int kofs = (xb - 1) * P;               // plane k
   for (int k = xb - 1; k < xe; ++k) {
     // prefetch node plane k + 3 and the scales of layer k + 1 into registers
     T pre[PF];
     T pres = T(0);
     const bool pnext = k + 3 <= xe, snext = k + 1 < xe;
     if (pnext) {
-      const long base = (long)wrap(k + 3, n0) * P;
 #pragma unroll
-      for (int i = 0; i < PF; ++i) pre[i] = poff[i] >= 0 ? __ldg(xv + base + poff[i]) : T(0);
+      for (int i = 0; i < PF; ++i) pre[i] = (i < PFF || poff[i] >= 0) ? __ldg(xv + (pofs + poff[i])) : T(0);
     }
-    if (snext && ev) pres = __ldg(sv + (long)wrap(k + 1, n0) * P + soff);
-    const T(*lo)[NP] = pl[slot(k)];
-    const T(*hi)[NP] = pl[slot(k + 1)];
-    T(*gk)[3][NE] = g[k & 1];
+    if (snext && ev) pres = __ldg(sv + sofs);
+    const T* lo = pl + r0;
+    const T* hi = pl + r1;
+    T* gk = g + gc;
     T xo[3] = {T(0), T(0), T(0)};
     if (ev) {
       // (carrying the lower corners in registers instead of re-reading them measured slower: register pressure)
@@ -124,50 +134,56 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          v[c][2 * q] = lo[c][cidx[q]];
-          v[c][2 * q + 1] = hi[c][cidx[q]];
+          v[c][2 * q] = lo[c * NP + cidx[q]];
+          v[c][2 * q + 1] = hi[c * NP + cidx[q]];
         }
-      const ModeC<T> ks = scale_modec(kc, sl[k & 1][e]);
+      const ModeC<T> ks = scale_modec(kc, sl[sc + e]);
       element_force(v, ks, f);
       if (k >= xb) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) gk[q][c][e] = ft[c][q] + f[c][2 * q];
+          for (int q = 0; q < 4; ++q) gk[(q * 3 + c) * NE + e] = ft[c][q] + f[c][2 * q];
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) ft[c][q] = f[c][2 * q + 1];
-      if (snext) sl[(k + 1) & 1][e] = pres;  // layer k + 1's scales; sl[(k+1)&1] was last read by layer k - 1
+      if (snext) sl[(NE - sc) + e] = pres;  // layer k + 1's scales; that buffer was last read by layer k - 1
     }
-    if (partial && outp && k >= xb) {
+    if (partial && ownv && k >= xb) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xo[c] = lo[c][own];
+      for (int c = 0; c < 3; ++c) xo[c] = lo[c * NP + own];
     }
     __syncthreads();  // gk complete; every read of plane k is done
-    if (k >= xb && outp) {
-      const int yy = y0 + ty, zz = z0 + tz;
-      if (yy < n1 && zz < n2) {
-        // node (ty+1, tz+1) is corner q = ay + 2az of element (ty+1-ay, tz+1-az)
-        const int e00 = (ty + 1) * EZ + (tz + 1);
-        const long idx = (long)k * P + (long)yy * n2 + zz;
+    if (k >= xb && ownv) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T o = (gk[0][c][e00] + gk[1][c][e00 - EZ]) + (gk[2][c][e00 - 1] + gk[3][c][e00 - EZ - 1]);
-          yv[c * N + idx] = o;
-          if (partial) {
-            acc[c] += (double)o;
-            acc[3] += (double)xo[c] * (double)o;
-          }
+      for (int c = 0; c < 3; ++c) {
+        const T* gc0 = gk + c * NE;
+        const T o = (gc0[e00] + gc0[3 * NE + e00 - EZ]) + (gc0[6 * NE + e00 - 1] + gc0[9 * NE + e00 - EZ - 1]);
+        yv[c * N + kofs + inpl] = o;
+        if (partial) {
+          acc[c] += (double)o;
+          acc[3] += (double)xo[c] * (double)o;
         }
       }
     }
     if (pnext) {
 #pragma unroll
       for (int i = 0; i < PF; ++i)
-        if (poff[i] >= 0) pl[slot(k + 3)][0][tid + i * NT] = pre[i];  // plane k + 3 replaces plane k
+        if (i < PFF || poff[i] >= 0) pl[r0 + tid + i * NT] = pre[i];  // plane k + 3 replaces plane k
     }
+    const int rt = r0;
+    r0 = r1;
+    r1 = r2;
+    r2 = rt;
+    gc = 12 * NE - gc;
+    sc = NE - sc;
+    pofs += P;
+    if (pofs == N) pofs = 0;
+    sofs += P;
+    if (sofs >= N) sofs -= N;
+    kofs += P;
   }
   if (partial) {
     block_sum<4>(acc, red);
@@ -202,6 +218,10 @@ static int launch_apply_tile(const LinearHandle& h, const T* s, int m, int nvec,
   // the batch.
   const int lx = g.n0 >= 32 ? 16 : g.n0;
   const int chunks = (g.n0 + lx - 1) / lx;
+  if (3 * g.N > (long)INT_MAX) {
+    set_error("apply: 3 n0 n1 n2 = %ld exceeds the 32-bit offsets of the kernel", 3 * g.N);
+    return NLF_EBADARG;
+  }
   if (tiles * chunks > kApplyMaxBlocks) {
     set_error("apply: %d blocks per vector exceed the partial-sum buffer (%d)", tiles * chunks, kApplyMaxBlocks);
     return NLF_EBADARG;
