@@ -724,6 +724,12 @@ __device__ __forceinline__ cplx<double> cj(cplx<double> w) {
   return INV ? cplx<double>{w.x, -w.y} : w;
 }
 
+// The cross-lane butterflies run the same arithmetic on both lanes of a pair, with no per-element selects: a lane
+// of the upper half (up) takes the sign -1 and its stage twiddle w, a lane of the lower half +1 and w = 1 (a
+// product by (1, 0) is exact). The results equal those of the two-sided form
+//   natural in:    lower a + pv, upper (pv - a) w
+//   transposed in: lower a + w pv, upper pv - w a
+// (the pair's lanes share w, so in the transposed form the upper lane forms w a and hands it to the lower one).
 template <int L, int R, bool INV, class TW>
 __device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW& T) {
   dft_reg<R, INV>(a);
@@ -735,10 +741,13 @@ __device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW
     const int s = 1 << j;
     const bool up = (l & s) != 0;
     const cplx<double> w = cj<INV>(T.ss(j));
+    const cplx<double> wl = up ? w : cplx<double>{1.0, 0.0};
+    const double sg = up ? -1.0 : 1.0;
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const cplx<double> pv = shfl_xor_c(a[k1], s);
-      a[k1] = up ? cmul(csub(pv, a[k1]), w) : cadd(a[k1], pv);
+      const cplx<double> d{fma(sg, a[k1].x, pv.x), fma(sg, a[k1].y, pv.y)};  // a + pv, or pv - a
+      a[k1] = cmul(d, wl);
     }
   }
 }
@@ -751,10 +760,13 @@ __device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const TW&
       const int s = 1 << j;
       const bool up = (l & s) != 0;
       const cplx<double> w = cj<INV>(T.ss(j));
+      const cplx<double> wl = up ? w : cplx<double>{1.0, 0.0};
+      const double sg = up ? -1.0 : 1.0;
 #pragma unroll
       for (int k1 = 0; k1 < R; ++k1) {
-        const cplx<double> pv = shfl_xor_c(a[k1], s);
-        a[k1] = up ? csub(pv, cmul(w, a[k1])) : cadd(a[k1], cmul(w, pv));
+        const cplx<double> c = cmul(wl, a[k1]);  // the upper element times w, or the lower one as it is
+        const cplx<double> pv = shfl_xor_c(c, s);
+        a[k1] = {fma(sg, c.x, pv.x), fma(sg, c.y, pv.y)};  // a + w pv, or pv - w a
       }
     }
 #pragma unroll
