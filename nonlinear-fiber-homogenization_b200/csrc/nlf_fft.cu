@@ -847,8 +847,11 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
   using F = Fast<N>;
   constexpr int M = F::M, H = F::H, Lz = F::Lz, Ly = F::Ly, P = F::P;
   constexpr long NN = (long)N * N * N;
+  // SOUT (shared twiddles, one plane per CTA): the y transforms write back into the plane buffer, and the plane's
+  // spectrum goes out in whole rows afterwards (instead of 64-byte pieces of 8 rows per warp store)
+  constexpr bool SOUT = SMT && P == 1;
   extern __shared__ unsigned char smem_raw[];
-  cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);  // [P][N rows][H]
+  cplx<double>* sm = reinterpret_cast<cplx<double>*>(smem_raw);  // [P][N rows][HS]
   __shared__ double red[32 * 2 * P];
   const int c = blockIdx.y, vec = blockIdx.z;
   if (!vec_live(cs, vec, m)) return;
@@ -1011,8 +1014,23 @@ __global__ void __launch_bounds__(256, SMT ? 3 : 2)
     fft_nat_in<Ly, 8, false>(b, ly, Ty);
     if (ok) {
       const int xx = blockIdx.x * P + pp, kb = 8 * brevL<Ly>(ly);
+      if constexpr (SOUT) {
+        // back into the column's slots (every lane of the group has read the column: the shuffles order it)
 #pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
+        for (int k1 = 0; k1 < 8; ++k1) sm[((long)pp * N + k1 + kb) * F::HS + F::slot(k1 + kb, kz)] = b[k1];
+      } else {
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) sp[((long)(k1 + kb) * N + xx) * H + kz] = b[k1];
+      }
+    }
+  }
+  if constexpr (SOUT) {
+    // the plane's spectrum rows [ky][x][0, H) out in whole rows, walked in slot order (the pad slots skipped)
+    __syncthreads();
+    for (int i = t; i < N * F::HS; i += 256) {
+      const int ky = i / F::HS, sl = i - ky * F::HS;
+      const int kz = F::slot(ky, sl);  // slot() permutes each aligned run of 8 as an involution
+      if (kz < H && F::slot(ky, kz) == sl) sp[((long)ky * N + blockIdx.x) * H + kz] = sm[(long)ky * F::HS + sl];
     }
   }
 }
@@ -1208,9 +1226,10 @@ __device__ __forceinline__ void px_row(const cplx<double> (&a)[8], double norm, 
 // fused x/p update, fu.p set).
 // SMT: twiddles from a shared-memory copy of the tables, 3 CTAs per SM instead of 2. STG (with SMT): the plane's
 // spectrum rows are first copied whole into the plane buffer by cp.async (coalesced 16-byte pieces), and the y
-// transforms run in place there.
+// transforms run in place there; at N = 64 it runs 4 CTAs per SM (64 registers, a few spilled: measured 7.2 -> 6.5
+// us per vector in the fused iteration, where pass A at 4 CTAs per SM loses).
 template <int N, bool SMT, bool STG = false>
-__global__ void __launch_bounds__(256, SMT ? 3 : 2)
+__global__ void __launch_bounds__(256, SMT ? ((STG && N == 64) ? 4 : 3) : 2)
     k_fc_fast(const cplx<double>* __restrict__ spec, const double* __restrict__ w, const double* __restrict__ r,
               double* __restrict__ z, int m, const cplx<double>* __restrict__ tw_y,
               const cplx<double>* __restrict__ tw_z, const cplx<double>* __restrict__ tw_n2,
