@@ -211,10 +211,10 @@ def unit_bytes(kind, N, NS, m):
 # (`bench.py --ncu --cells 4 --iters 8`, one launch of 24 vectors per kernel with the tuned variants; the full
 # workload is too large to capture), scaled to a launch by the vectors it processes
 # (profiles/pcg_kernels_64cubed_fp64_ncu.md): read + write MB per 24-vector launch.
-NCU_TRAFFIC_PER_VECTOR_64 = {"apply_f64": (159.546368e6 + 115.603200e6) / 24,
-                             "fft_a_f64": (310.692608e6 + 251.151360e6) / 24,
-                             "fft_b_f64": (155.786752e6 + 102.791680e6) / 24,
-                             "fft_c_f64": (466.180096e6 + 248.286208e6) / 24}
+NCU_TRAFFIC_PER_VECTOR_64 = {"apply_f64": (159.616512e6 + 112.823808e6) / 24,
+                             "fft_a_f64": (311.123200e6 + 252.546048e6) / 24,
+                             "fft_b_f64": (155.782144e6 + 105.678848e6) / 24,
+                             "fft_c_f64": (466.286336e6 + 267.508224e6) / 24}
 
 
 def roofline(prof, N, NS, m, peaks, peak_kind):
