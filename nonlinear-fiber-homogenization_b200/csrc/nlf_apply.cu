@@ -20,6 +20,18 @@
 
 namespace nlf {
 
+// Asynchronous global -> shared copy of one element (4 or 8 bytes, through L1), and a wait for this thread's
+// copies in flight.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src),
+               "n"((int)sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_none() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename T, int TY, int TZ, int MINB>
 __global__ void __launch_bounds__(((TY + 1) * (TZ + 1) + 31) / 32 * 32, MINB)
 k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int n0, int n1, int n2, int m,
@@ -32,14 +44,15 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   constexpr int PF = (3 * NP + NT - 1) / NT;  // plane values each thread prefetches per layer
   constexpr int PFF = (3 * NP) / NT;          // ... of which the first PFF exist for every thread
   // One barrier per layer. Dynamic shared memory (apply_smem<T, TY, TZ>() bytes): a ring of three node planes
-  // [3][3 comps][NP] (plane k + 3 is written into the slot of plane k after the barrier of layer k, the last layer
-  // that reads plane k), element forces [2][4 corners][3 comps][NE] and scales [2][NE], each alternating between
-  // its two buffers. The slots are tracked as offsets that rotate every layer (no index arithmetic mod 3), and
-  // every offset into a vector is 32-bit (the host bounds 3 N below 2^31).
+  // [3][3 comps][NP] and element forces [2][4 corners][3 comps][NE] (alternating buffers). Plane k + 3 is copied
+  // into the slot of plane k by cp.async after the barrier of layer k (the last layer that reads plane k); each
+  // thread waits for its copies before the barrier of layer k + 1, which publishes the plane before layer k + 2
+  // reads it. An element's stiffness scale is read by its own thread only and stays in a register. The slots are
+  // tracked as offsets that rotate every layer (no index arithmetic mod 3), and every offset into a vector is
+  // 32-bit (the host bounds 3 N below 2^31).
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* const pl = reinterpret_cast<T*>(smem_raw);
   T* const g = pl + 9 * NP;
-  T* const sl = g + 24 * NE;
   __shared__ int gys[HY], gzs[HZ];
   __shared__ double red[32 * 4];
 
@@ -98,7 +111,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 #pragma unroll
       for (int j = 0; j < 3; ++j) pl[j * 3 * NP + idx] = __ldg(xv + (wrap(xb - 1 + j, n0) * P + poff[i]));
     }
-  if (ev) sl[e] = __ldg(sv + (wrap(xb - 1, n0) * P + soff));
+  T s_cur = ev ? __ldg(sv + (wrap(xb - 1, n0) * P + soff)) : T(0);  // scale of this element in layer k
   __syncthreads();
 
   T ft[3][4];  // top-corner forces carried to the next layer
@@ -109,20 +122,13 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
   int r0 = 0, r1 = 3 * NP, r2 = 6 * NP;  // ring slots of planes k, k + 1, k + 2
-  int gc = 0, sc = 0;                    // this layer's force and scale buffers (the others: 12 NE - gc, NE - sc)
+  int gc = 0;                            // this layer's force buffer (the other: 12 NE - gc)
   int pofs = wrap(xb + 2, n0) * P;       // plane k + 3 within the vector
   int sofs = wrap(xb, n0) * P + soff;    // this element's scale in layer k + 1
   int kofs = (xb - 1) * P;               // plane k
   for (int k = xb - 1; k < xe; ++k) {
-    // prefetch node plane k + 3 and the scales of layer k + 1 into registers
-    T pre[PF];
-    T pres = T(0);
     const bool pnext = k + 3 <= xe, snext = k + 1 < xe;
-    if (pnext) {
-#pragma unroll
-      for (int i = 0; i < PF; ++i) pre[i] = (i < PFF || poff[i] >= 0) ? __ldg(xv + (pofs + poff[i])) : T(0);
-    }
-    if (snext && ev) pres = __ldg(sv + sofs);
+    const T s_nxt = (snext && ev) ? __ldg(sv + sofs) : T(0);  // the element's scale in layer k + 1
     const T* lo = pl + r0;
     const T* hi = pl + r1;
     T* gk = g + gc;
@@ -137,7 +143,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
           v[c][2 * q] = lo[c * NP + cidx[q]];
           v[c][2 * q + 1] = hi[c * NP + cidx[q]];
         }
-      const ModeC<T> ks = scale_modec(kc, sl[sc + e]);
+      const ModeC<T> ks = scale_modec(kc, s_cur);
       element_force(v, ks, f);
       if (k >= xb) {
 #pragma unroll
@@ -149,13 +155,13 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < 4; ++q) ft[c][q] = f[c][2 * q + 1];
-      if (snext) sl[(NE - sc) + e] = pres;  // layer k + 1's scales; that buffer was last read by layer k - 1
     }
     if (partial && ownv && k >= xb) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) xo[c] = lo[c * NP + own];
     }
-    __syncthreads();  // gk complete; every read of plane k is done
+    cp_async_wait_none();  // this thread's copies of plane k + 2 (issued in layer k - 1)
+    __syncthreads();       // gk complete; every read of plane k is done; plane k + 2 visible
     if (k >= xb && ownv) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -171,14 +177,16 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
     if (pnext) {
 #pragma unroll
       for (int i = 0; i < PF; ++i)
-        if (i < PFF || poff[i] >= 0) pl[r0 + tid + i * NT] = pre[i];  // plane k + 3 replaces plane k
+        if (i < PFF || poff[i] >= 0)
+          cp_async_elem(pl + (r0 + tid + i * NT), xv + (pofs + poff[i]));  // plane k + 3 replaces plane k
+      cp_async_commit_all();
     }
     const int rt = r0;
     r0 = r1;
     r1 = r2;
     r2 = rt;
     gc = 12 * NE - gc;
-    sc = NE - sc;
+    s_cur = s_nxt;
     pofs += P;
     if (pofs == N) pofs = 0;
     sofs += P;
@@ -203,7 +211,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
 template <typename T, int TY, int TZ>
 constexpr size_t apply_smem() {
   constexpr int NP = (TY + 2) * (TZ + 2), NE = (TY + 1) * (TZ + 1);
-  return sizeof(T) * (9 * NP + 24 * NE + 2 * NE);
+  return sizeof(T) * (9 * NP + 24 * NE);
 }
 
 template <typename T, int TY, int TZ, int MINB>
