@@ -730,12 +730,19 @@ __device__ __forceinline__ cplx<double> cj(cplx<double> w) {
 //   natural in:    lower a + pv, upper (pv - a) w
 //   transposed in: lower a + w pv, upper pv - w a
 // (the pair's lanes share w, so in the transposed form the upper lane forms w a and hands it to the lower one).
-template <int L, int R, bool INV, class TW>
-__device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW& T) {
-  dft_reg<R, INV>(a);
+// NL lines at once (the same lanes and twiddles, e.g. the three components of a column): each stage's sign,
+// twiddle and lane twiddle are formed once, and the lines' butterflies interleave (NL independent chains).
+template <int L, int R, bool INV, class TW, int NL>
+__device__ __forceinline__ void fft_nat_in_n(cplx<double> (&a)[NL][R], int l, const TW& T) {
+#pragma unroll
+  for (int n = 0; n < NL; ++n) dft_reg<R, INV>(a[n]);
   if (L == 1) return;
 #pragma unroll
-  for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.rr(k1)));
+  for (int k1 = 1; k1 < R; ++k1) {
+    const cplx<double> t = cj<INV>(T.rr(k1));
+#pragma unroll
+    for (int n = 0; n < NL; ++n) a[n][k1] = cmul(a[n][k1], t);
+  }
 #pragma unroll
   for (int j = ilog2c(L) - 1; j >= 0; --j) {
     const int s = 1 << j;
@@ -744,16 +751,17 @@ __device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW
     const cplx<double> wl = up ? w : cplx<double>{1.0, 0.0};
     const double sg = up ? -1.0 : 1.0;
 #pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) {
-      const cplx<double> pv = shfl_xor_c(a[k1], s);
-      const cplx<double> d{fma(sg, a[k1].x, pv.x), fma(sg, a[k1].y, pv.y)};  // a + pv, or pv - a
-      a[k1] = cmul(d, wl);
-    }
+    for (int k1 = 0; k1 < R; ++k1)
+#pragma unroll
+      for (int n = 0; n < NL; ++n) {
+        const cplx<double> pv = shfl_xor_c(a[n][k1], s);
+        const cplx<double> d{fma(sg, a[n][k1].x, pv.x), fma(sg, a[n][k1].y, pv.y)};  // a + pv, or pv - a
+        a[n][k1] = cmul(d, wl);
+      }
   }
 }
-
-template <int L, int R, bool INV, class TW>
-__device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const TW& T) {
+template <int L, int R, bool INV, class TW, int NL>
+__device__ __forceinline__ void fft_tr_in_n(cplx<double> (&a)[NL][R], int l, const TW& T) {
   if (L > 1) {
 #pragma unroll
     for (int j = 0; j < ilog2c(L); ++j) {
@@ -763,16 +771,31 @@ __device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const TW&
       const cplx<double> wl = up ? w : cplx<double>{1.0, 0.0};
       const double sg = up ? -1.0 : 1.0;
 #pragma unroll
-      for (int k1 = 0; k1 < R; ++k1) {
-        const cplx<double> c = cmul(wl, a[k1]);  // the upper element times w, or the lower one as it is
-        const cplx<double> pv = shfl_xor_c(c, s);
-        a[k1] = {fma(sg, c.x, pv.x), fma(sg, c.y, pv.y)};  // a + w pv, or pv - w a
-      }
+      for (int k1 = 0; k1 < R; ++k1)
+#pragma unroll
+        for (int n = 0; n < NL; ++n) {
+          const cplx<double> c = cmul(wl, a[n][k1]);  // the upper element times w, or the lower one as it is
+          const cplx<double> pv = shfl_xor_c(c, s);
+          a[n][k1] = {fma(sg, c.x, pv.x), fma(sg, c.y, pv.y)};  // a + w pv, or pv - w a
+        }
     }
 #pragma unroll
-    for (int k1 = 1; k1 < R; ++k1) a[k1] = cmul(a[k1], cj<INV>(T.rr(k1)));
+    for (int k1 = 1; k1 < R; ++k1) {
+      const cplx<double> t = cj<INV>(T.rr(k1));
+#pragma unroll
+      for (int n = 0; n < NL; ++n) a[n][k1] = cmul(a[n][k1], t);
+    }
   }
-  dft_reg<R, INV>(a);
+#pragma unroll
+  for (int n = 0; n < NL; ++n) dft_reg<R, INV>(a[n]);
+}
+template <int L, int R, bool INV, class TW>
+__device__ __forceinline__ void fft_nat_in(cplx<double> (&a)[R], int l, const TW& T) {
+  fft_nat_in_n<L, R, INV, TW, 1>(reinterpret_cast<cplx<double>(&)[1][R]>(a), l, T);
+}
+template <int L, int R, bool INV, class TW>
+__device__ __forceinline__ void fft_tr_in(cplx<double> (&a)[R], int l, const TW& T) {
+  fft_tr_in_n<L, R, INV, TW, 1>(reinterpret_cast<cplx<double>(&)[1][R]>(a), l, T);
 }
 
 // shared plane index of bin kz in a row: within each run of 8 bins the low 3 bits are xor-ed with the run index
@@ -1134,8 +1157,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
     }
   typename std::conditional<CLOSED, LaneTwS<L, 4>, LaneTw<L, 4>>::type T;
   T.load(CLOSED ? twl : tw_x, l);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) fft_nat_in<L, 4, false>(a[c], l, T);
+  fft_nat_in_n<L, 4, false>(a, l, T);
   double dot[1] = {0.0};
   const double wt = (kz == 0 || kz == M) ? 1.0 : 2.0;
   const int kb = 4 * brevL<L>(l);
@@ -1168,8 +1190,7 @@ __global__ void __launch_bounds__(Fast<N>::NTB, 2)
     a[1][k1] = ub;
     a[2][k1] = uc;
   }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) fft_tr_in<L, 4, true>(a[c], l, T);
+  fft_tr_in_n<L, 4, true>(a, l, T);
   if (ok)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
