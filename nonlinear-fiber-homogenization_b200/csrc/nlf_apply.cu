@@ -126,6 +126,7 @@ k_apply(const T* __restrict__ s, const T* __restrict__ x, T* __restrict__ y, int
   int pofs = wrap(xb + 2, n0) * P;       // plane k + 3 within the vector
   int sofs = wrap(xb, n0) * P + soff;    // this element's scale in layer k + 1
   int kofs = (xb - 1) * P;               // plane k
+#pragma unroll 2
   for (int k = xb - 1; k < xe; ++k) {
     const bool pnext = k + 3 <= xe, snext = k + 1 < xe;
     const T s_nxt = (snext && ev) ? __ldg(sv + sofs) : T(0);  // the element's scale in layer k + 1
