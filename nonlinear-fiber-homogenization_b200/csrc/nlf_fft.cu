@@ -819,18 +819,23 @@ struct Fast {
   // row stride (16-byte entries) of pass B's staged slabs: KZN is odd, so the 8 x rows a quarter-warp reads or
   // writes at one kz land in 8 different bank groups
   static constexpr int KPB = KZN;
-  // plane buffer of passes A and C: [P][N rows][HS] (16-byte entries), bin kz of row y at slot(y, kz). For N = 64
-  // the rows are padded to 40 entries and the bins permuted within each aligned run of 8 by the row and the run
-  // index, so that a quarter-warp's 16-byte accesses hit 8 different bank groups in every access pattern of the
-  // passes: 8 rows of one column (y = l + 8 q, and y = k1 + 8 brev(l) when the y transform writes back), and 4 bins
-  // k1 + 8 k2 (or their mirrors M - k) of 2 adjacent rows. For N = 32 the rows stay at H entries (swz only).
-  static constexpr int HS = (N == 64) ? 40 : H;
+  // plane buffer of passes A and C: [P][N rows][HS] (16-byte entries), bin kz of row y at slot(y, kz): the rows
+  // are padded (N = 64: 40 entries, N = 32: 24) and the bins permuted within each aligned run of 8 by the row and
+  // the run index, so that a quarter-warp's 16-byte accesses hit 8 different bank groups in every access pattern
+  // of the passes. N = 64: 8 rows of one column (y = l + 8 q, and y = k1 + 8 brev(l) when the y transform writes
+  // back), and 4 bins k1 + 8 k2 (or their mirrors M - k) of 2 adjacent rows. N = 32: 4 rows of 2 adjacent columns
+  // (y = l + 4 q, and k1 + 8 brev(l)), and 2 bins k1 + 8 k2 of 4 adjacent rows. The row term of the N = 32 map
+  // was found by an exhaustive search over maps of this form.
+  static constexpr int HS = (N == 64) ? 40 : (N == 32) ? 24 : H;
   // row stride, in double pairs, of the real-row views of the same buffer (staged variants, one plane per CTA)
   static constexpr int PS = (N == 64) ? N / 2 + 4 : N / 2;
   static constexpr size_t smem_plane() { return (size_t)P * N * HS * sizeof(cplx<double>); }
   __device__ static __forceinline__ int slot(int y, int kz) {
     if constexpr (N == 64) {
       const int h = ((((y & 1) << 2) | ((y & 7) >> 1)) ^ (y >> 3)) & 7;
+      return (kz & ~7) | ((kz ^ (kz >> 3) ^ h) & 7);
+    } else if constexpr (N == 32) {
+      const int h = (2 * (y & 7) + 2 * (y >> 3)) & 7;
       return (kz & ~7) | ((kz ^ (kz >> 3) ^ h) & 7);
     } else {
       return swz<M>(kz);
