@@ -203,11 +203,12 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
   const long N = a.N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < N; e += (long)gridDim.x * blockDim.x) {
     const int k = (int)(e % a.n2), j = (int)((e / a.n2) % a.n1), i = (int)(e / ((long)a.n1 * a.n2));
+    // the element's 8 nodes e + (ax, ay, az): periodic neighbours by a compare, not a modulo
+    const long ip = (i + 1 == a.n0 ? 0 : i + 1), jp = (j + 1 == a.n1 ? 0 : j + 1), kp = (k + 1 == a.n2 ? 0 : k + 1);
     long nid[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-      nid[q] = ((long)wrap(i + (q & 1), a.n0) * a.n1 + wrap(j + ((q >> 1) & 1), a.n1)) * a.n2 +
-               wrap(k + (q >> 2), a.n2);
+      nid[q] = (((q & 1) ? ip : i) * a.n1 + (((q >> 1) & 1) ? jp : j)) * a.n2 + ((q >> 2) ? kp : k);
     double wn[3][8];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -286,10 +287,11 @@ __global__ void k_mech_gather(long N, int n0, int n1, int n2, const double* __re
   const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int k = (int)(n % n2), j = (int)((n / n2) % n1), i = (int)(n / ((long)n1 * n2));
+  const long im = (i == 0 ? n0 - 1 : i - 1), jm = (j == 0 ? n1 - 1 : j - 1), km = (k == 0 ? n2 - 1 : k - 1);
   double o[3] = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    const long e = ((long)wrap(i - (q & 1), n0) * n1 + wrap(j - ((q >> 1) & 1), n1)) * n2 + wrap(k - (q >> 2), n2);
+    const long e = (((q & 1) ? im : i) * n1 + (((q >> 1) & 1) ? jm : j)) * n2 + ((q >> 2) ? km : k);
 #pragma unroll
     for (int c = 0; c < 3; ++c) o[c] += fe[(long)(3 * q + c) * N + e];
   }
