@@ -615,12 +615,12 @@ def mech_arm(args, stream):
     from nlfiber_b200 import mech as MH
     n = args.n
     cells = gpu_cells(range(args.mech_cells), n // 2, stream=stream).cpu().numpy()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    rows, newton, cg, steps = [], 0, 0, 0
-    torch.cuda.synchronize()
-    e0.record()
-    for i in range(len(cells)):
-        cell = MH.Cell(cells[i], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
+
+    def run_path(i):
+        """The compression path of cell i on the calling thread's CUDA stream: its rows."""
+        out = []
+        cell = handles[i]
+        cell.stream = torch.cuda.current_stream().cuda_stream
         mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
         rng = np.random.default_rng(i)
         void = torch.as_tensor(cells[i] < 0.5, device="cuda")
@@ -637,12 +637,9 @@ def mech_arm(args, stream):
             H = torch.as_tensor(cell.grad_w(w), device="cuda") + torch.as_tensor(F - np.eye(3), device="cuda")
             J = torch.linalg.det(torch.eye(3, dtype=torch.float64, device="cuda") + H)
             inverted = float((J < 0.1)[:, void].double().mean()) if bool(void.any()) else 0.0
-            rows.append({"cell": i, "e": e, "P_xx": float(P[0, 0]), "nu": [float(-(F[j, j] - 1) / e) for j in (1, 2)],
-                         "newton": tot["newton"], "cg": tot["cg"], "restarts": tot["restarts"], "splits": tot["splits"],
-                         "converged": bool(log["converged"]), "void_inverted": inverted})
-            newton += tot["newton"]
-            cg += tot["cg"]
-            steps += 1
+            out.append({"cell": i, "e": e, "P_xx": float(P[0, 0]), "nu": [float(-(F[j, j] - 1) / e) for j in (1, 2)],
+                        "newton": tot["newton"], "cg": tot["cg"], "restarts": tot["restarts"], "splits": tot["splits"],
+                        "converged": bool(log["converged"]), "void_inverted": inverted})
             if not log["converged"] or inverted > 0.01:
                 break
             # the next step starts from this state plus a seeded kick of 1e-3 max |w| on w, so the path can
@@ -652,9 +649,39 @@ def mech_arm(args, stream):
             kick = torch.as_tensor(rng.standard_normal(nw), device=z.device) * (1e-3 * float(z[:nw].abs().max()) + 1e-15)
             z = torch.cat([z[:nw] + kick, z[nw:]])
             Fprev = F
-    e1.record()
+        torch.cuda.current_stream().synchronize()
+        return out
+
+    def worker(idx):
+        """Host thread idx: its own CUDA stream, cells idx, idx + workers, ... one after the other."""
+        torch.cuda.set_device(torch.cuda.current_device())
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            return [r for i in range(idx, len(cells), workers) for r in run_path(i)]
+
+    # cells run concurrently from `workers` host threads, each on its own stream and handles (the Newton loop's
+    # host work and small kernels of one cell leave most of the GPU idle); per-cell results do not depend on it
+    workers = max(1, min(args.mech_workers, len(cells)))
+    # every cell's handle made (and sized) here, before the threads: making or freeing one synchronizes the
+    # device, which a CUDA graph capture running in another thread does not permit; freed after the threads
+    handles = [MH.Cell(cells[i], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0) for i in range(len(cells))]
+    # torch initialises its linear-algebra backends lazily and once: do it here, before any thread needs them
+    torch.linalg.det(torch.eye(3, dtype=torch.float64, device="cuda")[None])
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    if workers == 1:
+        rows = worker(0)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(workers) as ex:
+            rows = [r for part in ex.map(worker, range(workers)) for r in part]
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    del handles
+    rows.sort(key=lambda r: (r["cell"], -r["e"]))
+    newton = sum(r["newton"] for r in rows)
+    cg = sum(r["cg"] for r in rows)
+    steps = len(rows)
     # kernel classes from one more first step of cell 0 with per-launch events on (and no graph replay)
     cell = MH.Cell(cells[0], E=1.0, nu=0.3, material="neohooke", emin=1e-6, p=3.0)
     mix = MH.Mixed(cell, ((1, 1), (2, 2)), precond=args.mech_precond, device="cuda")
@@ -701,6 +728,7 @@ def mech_arm(args, stream):
                           "(the 3m x 3m projected eigenproblems too, through torch)"}
     return {"mode": "mech", "stability": stab, "workload": f"{len(cells)} seeded synthetic {n}^3 cells, compression to "
             f"{0.01 * args.mech_steps:.2f} in steps of 0.01, lateral stresses free", "precond": args.mech_precond,
+            "workers": workers, "timing": "host wall clock around the synchronized paths of all cells",
             "steps": steps, "seconds": round(ms / 1e3, 2), "steps_per_s": round(steps / (ms / 1e3), 3),
             "newton_per_step": round(newton / max(steps, 1), 2), "cg_per_step": round(cg / max(steps, 1), 1),
             "ms_per_cg_iteration": round(ms / max(cg, 1), 3),
@@ -1021,6 +1049,8 @@ def main():
     ap.add_argument("--mech-stability", action="store_true",
                     help="with --mech: also time the effective tangent and the lowest eigenvalues of cell 0")
     ap.add_argument("--mech-steps", type=int, default=3)
+    ap.add_argument("--mech-workers", type=int, default=4,
+                    help="host threads (each with its own CUDA stream) running the mech cells concurrently")
     ap.add_argument("--uneven", default=None,
                     help="uneven batch 'n1,count1,n2,count2,...' (e.g. 32,128,64,64,128,16) instead of the default")
     ap.add_argument("--cufft", action="store_true",

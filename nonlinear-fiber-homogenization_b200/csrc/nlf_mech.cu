@@ -857,6 +857,21 @@ NLF_API int nlf_mech_set_rho(nlf_mech* H, const double* rho, double* s_out, doub
   for (long i = 0; i < N; ++i) a += lg[i];
   H->sws = std::exp(a / (double)N);
   if (sws_out) *sws_out = H->sws;
+  // the handle's work buffers at the largest size any of its calls takes (energy, hvp, grad_w, toec, and the CG
+  // with the 9 macro unknowns at most), so that no later call allocates or frees device memory: a free while
+  // another host thread captures a CUDA graph would invalidate that capture
+  {
+    const size_t V = al(3 * N * 8), part = al(4096 * 10 * 8);
+    const size_t Lz = al((3 * N + 9) * 8);
+    const size_t eh = 4 * V + al(24 * N * 8) + 256 + part + 256;  // energy and hvp
+    const size_t gw = V + al(72 * N * 8);                         // grad_w
+    const int nblk = (int)std::min<long>(4 * 148, (N + kToecWarps - 1) / kToecWarps);
+    const size_t te = al(18 * N * 8) + al((size_t)nblk * kToecOut * 8) + al(kToecOut * 8);
+    const size_t cgw = V + 5 * Lz + V + al(24 * N * 8) + al(3 * lin_of(H).g.NS * 16) + part +
+                       al(3 * (size_t)H->d.n0 * 4 * 8) + al(256) + al(sizeof(MechCG));
+    NLF_TRY(H->ws.reserve(std::max(std::max(eh, gw), std::max(te, cgw))));
+    NLF_TRY(H->io.reserve(std::max(al(18 * N * 8), 2 * Lz)));
+  }
   H->rho_set = true;
   return NLF_OK;
 }
@@ -1145,6 +1160,9 @@ NLF_API int nlf_mech_toec(nlf_mech* H, const double* chi, double* C, double* T, 
 // (w (nx, ny, nz, 3) flattened, then the k macro unknowns Fbar[free[2j], free[2j+1]]).
 // dmac: (k,) macro preconditioner diagonal; sws: stiffness scale of the w preconditioner.
 // Outputs x (3N + k), *it, *conv, *neg (negative curvature met).
+// graph captures of nlf_mech_cg (and the destruction of their executables) one at a time in the process
+static std::mutex g_capture_mu;
+
 NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k, const int* free_idx,
                         const double* b, const double* dmac, double sws, double tol, int maxit, double* x, int* it,
                         int* conv, int* neg, int check_every, void* stream) {
@@ -1256,6 +1274,9 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
       NLF_CUDA_TRY(cudaEventCreateWithFlags(&H->gev[1], cudaEventDisableTiming));
     }
     cudaGraph_t graph = nullptr;
+    // one capture at a time in the process, and no graph destroyed meanwhile: solves of different cells may run
+    // from several host threads
+    std::lock_guard<std::mutex> capture_lock(g_capture_mu);
     NLF_CUDA_TRY(cudaStreamBeginCapture(H->gst, cudaStreamCaptureModeThreadLocal));
     const int rc = chunk(H->gst);
     const cudaError_t e = cudaStreamEndCapture(H->gst, &graph);
@@ -1271,7 +1292,10 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
   struct ExecGuard {
     cudaGraphExec_t g;
     ~ExecGuard() {
-      if (g) cudaGraphExecDestroy(g);
+      if (g) {
+        std::lock_guard<std::mutex> lock(g_capture_mu);
+        cudaGraphExecDestroy(g);
+      }
     }
   } guard{gexec};
   int host_done = hs.done, iters = 0;

@@ -107,7 +107,7 @@ class _Forcing:
 class Cell:
     """mech.py:88-192: a periodic voxel cell; rho (nx, ny, nz) or (n, n) in [0, 1]."""
 
-    def __init__(self, rho, E=1.0, nu=0.3, material="neohooke", wls=(500.0, 0.01), emin=1e-3, p=3.0):
+    def __init__(self, rho, E=1.0, nu=0.3, material="neohooke", wls=(500.0, 0.01), emin=1e-3, p=3.0, stream=None):
         rho = np.ascontiguousarray(np.asarray(rho, dtype=np.float64))
         if rho.ndim == 2:
             rho = rho[..., None]
@@ -123,11 +123,11 @@ class Cell:
         check(lib.nlf_mech_create(ctypes.byref(h), *self.shape, float(E), float(nu), MATERIALS.index(material), b,
                                   r0, float(emin), float(p)))
         self._h = h
-        self.stream = None
+        self.stream = stream  # CUDA stream (cudaStream_t as an int) of every call of this cell; None: the default
         self.s = np.empty(self.shape)
         gam = np.empty(self.shape) if wls is not None else None
         sws = ctypes.c_double()
-        check(lib.nlf_mech_set_rho(h, ptr(rho), ptr(self.s), ptr(gam), ctypes.byref(sws), None))
+        check(lib.nlf_mech_set_rho(h, ptr(rho), ptr(self.s), ptr(gam), ctypes.byref(sws), self.stream))
         self.gamma = gam if wls is not None else None
         self.sws = sws.value
 
