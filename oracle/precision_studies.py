@@ -1,5 +1,6 @@
-"""CPU studies behind two design decisions of the solver, on the oracle's PCG. TEST INFRASTRUCTURE ONLY: nothing
-in the library imports this file; it restates variants of the oracle's node-scaled PCG to measure them.
+"""CPU studies behind three design decisions of the solvers, on the oracle's PCG and Newton-CG. TEST
+INFRASTRUCTURE ONLY: nothing in the library imports this file; it restates variants of the oracle's node-scaled
+PCG and of its finite-strain tangent to measure them.
 
 1. Mixed precision (the solver stays FP64). Three variants of the FP64 PCG with the node-scaled preconditioner on
    cells of the benchmark generator at a 1e-9 void floor, each run to the residual rule 1e-9:
@@ -19,8 +20,17 @@ in the library imports this file; it restates variants of the oracle's node-scal
    after 20 (emin 1e-9; 1e-4 after 20 at emin 1e-3). Two correct FP64 implementations therefore agree in their
    early iterates only; their converged C agree to rounding.
 
+3. An FP32 tangent inside the FP64 Newton-CG of the finite-strain step (nlfiber/mech.py:199-346). The oracle's
+   Newton (FP64 gradient, energy and line search) with the node-scaled CG preconditioner, its tangent matvec
+   either FP64 or FP32 (element tangent, element forces and nodal sums in float32), one compression step of 1 %
+   (Fbar_xx = 0.99, lateral stresses free) at emin 1e-6 (the finite-strain configuration's floor).
+   Measured (32^3): seed 1 (one solid piece) FP64 4 Newton / 105 CG, FP32 4 / 113, the same lateral F to 1e-10;
+   seed 5 (13 pieces) FP64 15 / 1043 and FP32 14 / 766, both stopping by the gradient rule but at lateral strains
+   0.0021061 and 0.0021020: the floating pieces settle differently.
+
     python -m oracle.precision_studies mixed 16 0,1,2,3     # octant size and seeds
     python -m oracle.precision_studies sensitivity 32 0 8 1e-9
+    python -m oracle.precision_studies tangent32 16 1,5
 """
 import sys
 
@@ -131,8 +141,73 @@ def sensitivity_study(n_o, seed, iters, emin, noise=1e-15):
             "C_rel": OL.rel_C_error(oh.bilinear(s, np.eye(6), u2), oh.bilinear(s, np.eye(6), u1))}
 
 
+def hvp_f32(cell):
+    """The tangent matvec of mech_ref.Cell.hvp in float32: F and dF from the float32 state and direction, the
+    neo-Hookean dP with the WLS void interpolation, the element forces and their nodal sums all in float32."""
+    from . import mech_ref as OM
+    f = np.float32
+    DN = OM.DN.astype(f)
+    s32, g32 = cell.s.astype(f), cell.gamma.astype(f)
+    I3 = np.eye(3, dtype=f)
+    lam, mu, wq = f(cell.lam), f(cell.mu), f(cell.wq)
+
+    def gw(w):
+        nod = np.stack([np.roll(w, shift=tuple(-o for o in off), axis=(0, 1, 2)) for off in OM.NODES])
+        return np.einsum("aijkc,gad->gijkcd", nod, DN)
+
+    def dP_nh(F, dF):
+        Fit = np.swapaxes(np.linalg.inv(F), -1, -2)
+        lnJ = np.log(np.linalg.det(F))
+        t = Fit @ np.swapaxes(dF, -1, -2) @ Fit
+        return mu * dF + (mu - lam * lnJ)[..., None, None] * t + lam * np.sum(Fit * dF, axis=(-2, -1))[..., None, None] * Fit
+
+    def dsig(dF):
+        e = f(0.5) * (dF + np.swapaxes(dF, -1, -2))
+        return lam * np.trace(e, axis1=-2, axis2=-1)[..., None, None] * I3 + f(2) * mu * e
+
+    def hvp(w, Fbar, v, dFmac):
+        F = np.asarray(Fbar, f)[None, None, None, None] + gw(w.astype(f))
+        dF = np.asarray(dFmac, f)[None, None, None, None] + gw(v.astype(f))
+        g = g32[None][..., None, None]
+        Fg = I3 + g * (F - I3)
+        dP = wq * s32[None, ..., None, None] * (g * g * (dP_nh(Fg, dF) - dsig(dF)) + dsig(dF))
+        out = np.zeros(cell.shape + (3,), f)
+        for a, off in enumerate(OM.NODES):
+            out = out + np.roll(np.einsum("gijkcd,gd->ijkc", dP, DN[:, a]), shift=tuple(off), axis=(0, 1, 2))
+        return out.astype(np.float64), dP.sum(axis=(0, 1, 2, 3)).astype(np.float64)
+
+    return hvp
+
+
+def tangent32_study(n_o, seeds, e=0.01):
+    """One compression step per cell, FP64 and FP32 tangent: Newton and CG iterations, convergence, lateral F."""
+    from . import mech_ref as OM
+    out = []
+    for seed in seeds:
+        rho = OD.random_cell(seed, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0]
+        for fp32 in (False, True):
+            cell = OM.Cell(rho, E=1.0, nu=0.3, emin=1e-6)
+            if fp32:
+                cell.hvp = hvp_f32(cell)
+            mx = OM.Mixed(cell)
+            wn = OL.node_scaling(cell.s)[..., None]
+
+            def precond(r, dmac, sws, mx=mx, cell=cell, wn=wn):
+                z = wn * cell.precond_w(wn * r[: mx.nw].reshape(cell.shape + (3,)))
+                return np.concatenate([z.ravel(), r[mx.nw:] / dmac])
+
+            mx.precond = precond
+            _, F, log = mx.solve(np.diag([1.0 - e, 1.0, 1.0]), rtol=1e-9, cg_tol=1e-6)
+            out.append({"seed": seed, "fp32": fp32, "newton": log["newton"], "cg": log["cg"],
+                        "converged": log["converged"], "F_lateral": [float(F[1, 1]), float(F[2, 2])]})
+    return out
+
+
 if __name__ == "__main__":
-    if sys.argv[1] == "mixed":
+    if sys.argv[1] == "tangent32":
+        for row in tangent32_study(int(sys.argv[2]), [int(v) for v in sys.argv[3].split(",")]):
+            print(row, flush=True)
+    elif sys.argv[1] == "mixed":
         for row in mixed_study(int(sys.argv[2]), [int(v) for v in sys.argv[3].split(",")]):
             print(row, flush=True)
     else:
