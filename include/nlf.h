@@ -174,7 +174,8 @@ NLF_API int nlf_precond_symbol(nlf_linear* h, double* kinv6);
  * (mode 0), computed in closed form (mode 1), or that with pass B's slabs staged through shared memory (mode 2,
  * 64^3 only; nlf_linear_set_kinv_mode), and passes A and C with their
  * twiddles in registers (0), read from a shared-memory copy of the tables at 3 CTAs per SM (1), that with pass
- * C's spectrum rows and x/p update moved in whole rows through shared memory (2), or with pass A's row inputs
+ * C's spectrum rows and x/p update moved in whole rows through shared memory (2; pass C at 4 CTAs per SM at
+ * 64^3), or with pass A's row inputs
  * coalesced the same way too (3;
  * nlf_linear_set_fft_twiddles): ms_out[nvariants + kinv mode + nk twiddle mode], nk = 3 Kinv modes at 64^3
  * and 2 at 32^3, so at most twelve entries. Results of

@@ -163,7 +163,8 @@ class LinearHomogenization:
     def fft_twiddles(self):
         """0: passes A and C of the FP64 cube preconditioner keep their twiddles in registers; 1: in shared
         memory (fewer registers, 3 CTAs per SM); 2: as 1, with pass C's spectrum rows and x/p update moved in
-        whole rows through shared memory; 3: as 2, with pass A's row inputs coalesced too."""
+        whole rows through shared memory (4 CTAs per SM at 64^3); 3: as 2, with pass A's row inputs coalesced
+        too."""
         return int(lib.nlf_linear_get_fft_twiddles(self._h))
 
     @fft_twiddles.setter
