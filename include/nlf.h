@@ -263,15 +263,18 @@ NLF_API int nlf_unet_adam_step(nlf_unet* net, double lr, double beta1, double be
 
 /* ---- density map (nlfiber/density.py, nlfiber/symmetry.py) ------------------------------------------------
  * The input side of the solve: a pre-density phi on the symmetric octant (n_o)^3 becomes the physical density
- * rho of the full periodic cell (2 n_o)^3 with mean(rho) = v exactly. Cubes (d = 3) only. */
+ * rho of the full periodic cell (2 n_o)^3 with mean(rho) = v exactly; on squares (d = 2) the quadrant (n_o)^2
+ * becomes the cell (2 n_o)^2. Below, read (n_o, n_o, n_o) and (n, n, n) as (n_o, n_o) and (n, n) for squares. */
 typedef struct nlf_density nlf_density;
 
-/* nlfiber/density.py:75-82 DensityMap.__init__(n_o, d=3, r, v) without v: the periodic cone filter of radius r
- * voxels (density.py:23-31; at most 8192 nonzero taps) and the symmetry orbits of the octant
- * (symmetry.py:74-96). */
+/* nlfiber/density.py:75-82 DensityMap.__init__(n_o, d, r, v) without v: the periodic cone filter of radius r
+ * voxels (density.py:23-31; at most 8192 nonzero taps) and the symmetry orbits of the octant (quadrant)
+ * (symmetry.py:74-96). nlf_density_create is nlf_density_create_d with d = 3. */
 NLF_API int nlf_density_create(nlf_density** out, int n_o, double r);
+NLF_API int nlf_density_create_d(nlf_density** out, int n_o, int d, double r);
 NLF_API int nlf_density_destroy(nlf_density* dm);
-/* Number of symmetry orbits of the octant (sorted index triples, symmetry.py:20-22 n_free); -1 for NULL. */
+/* Number of symmetry orbits of the octant (sorted index triples; pairs on squares; symmetry.py:20-22 n_free);
+ * -1 for NULL. */
 NLF_API int nlf_density_orbits(const nlf_density* dm);
 /* nlfiber/density.py:84-94 DensityMap.smooth and rho (threshold / solve_eta, density.py:43-72) for ncell cells:
  * phi (ncell, n_o, n_o, n_o) octant pre-densities (symmetrized here, as sym_perm does in smooth); v (ncell,) the

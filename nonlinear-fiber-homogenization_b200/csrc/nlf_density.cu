@@ -1,6 +1,7 @@
 // Density map on the GPU: pre-density phi (octant) -> physical density rho (full periodic cell) with an exact
 // volume fraction (nlfiber/density.py:23-91 DensityMap.smooth / rho, threshold, solve_eta; nlfiber/symmetry.py
-// sym_perm, mirror, fold, exact_symmetrize). Cubes only (d = 3), batched over cells:
+// sym_perm, mirror, fold, exact_symmetrize). Cubes (d = 3), batched over cells, as below; squares (d = 2) take the
+// same steps with kernels of their own (k2_*: quadrant, 2 permutations, 4 mirror images, orbits of sorted pairs):
 //
 //   phis = sym_perm(phi)                 octant (n_o)^3: mean of the 6 axis permutations, numpy's order
 //   u    = k * mirror(phis)              periodic cone filter of radius r on the full cell (n = 2 n_o)^3, as a
@@ -35,6 +36,7 @@ constexpr int kEtaThreads = 1024;
 constexpr int kEtaCta = 2;  // CTAs (one cluster) per cell in the volume bisection
 
 struct DensityHandle {
+  int d = 3;  // 3: cubes, octant (n_o)^3; 2: squares, quadrant (n_o)^2 (tables and kernels of their own)
   int n_o = 0, n = 0, R = 0, ntap = 0, halo = 0;
   double r = 0.0;
   int* tap_off = nullptr;     // [ntap][3] kernel offsets g (-n / 2 < g <= n / 2) with k(g) > 0
@@ -331,7 +333,7 @@ __device__ __forceinline__ double cluster_total(cg::cluster_group& cl, double v,
 // ro = sigmoid(beta (o - eta)). A cluster of kEtaCta CTAs per cell: CTA q takes the orbits q B + t + k kEtaCta B
 // (B threads) and the per-step sums are combined across the cluster, so every CTA takes the same decisions.
 __global__ void __cluster_dims__(kEtaCta, 1, 1) __launch_bounds__(kEtaThreads)
-    k_dens_eta(int n_o, int R, const double* __restrict__ o, const double* __restrict__ mult,
+    k_dens_eta(double NO, int R, const double* __restrict__ o, const double* __restrict__ mult,
                const double* __restrict__ vol, double beta, double* __restrict__ eta_out, double* __restrict__ ro) {
   __shared__ double red[33];
   __shared__ double slots[2];
@@ -339,7 +341,7 @@ __global__ void __cluster_dims__(kEtaCta, 1, 1) __launch_bounds__(kEtaThreads)
   const int cell = blockIdx.x / kEtaCta, rank = (int)cl.block_rank();
   const int r0 = rank * blockDim.x + threadIdx.x, rs = kEtaCta * blockDim.x;
   const double* x = o + (long)cell * R;
-  const double NO = (double)n_o * n_o * n_o, v = vol[cell];
+  const double v = vol[cell];  // NO: points of the octant (quadrant), each orbit holding mult of them
   int buf = 0;
   double mn = INFINITY, mxv = -INFINITY;
   for (int r = r0; r < R; r += rs) {
@@ -559,6 +561,191 @@ __global__ void k_dv_filter_tile(int n_o, int H, int ntap, int nrow, int R, cons
   }
 }
 
+// ---- square cells (d = 2): quadrant (n_o)^2 -> full cell (2 n_o)^2, the same steps with 2 permutations, 4 mirror
+// images and orbits of sorted pairs a <= b (multiplicity 1 or 2); one thread per point, as small as these cells are
+
+// phis = sym_perm(phi): numpy adds transpose(x, (0, 1)) then transpose(x, (1, 0)), then divides by 2
+__global__ void k2_symphi(int n_o, const double* __restrict__ phi, double* __restrict__ phis) {
+  const long NO = (long)n_o * n_o;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= NO) return;
+  const int cell = blockIdx.y, b = (int)(t % n_o), a = (int)(t / n_o);
+  const double* x = phi + (long)cell * NO;
+  phis[(long)cell * NO + t] = (x[(long)a * n_o + b] + x[(long)b * n_o + a]) / 2.0;
+}
+
+// u(y) = sum_g k(g) f(y - g), f = mirror(phis); psum[cell][blk] = the CTA's partial sum of u
+__global__ void k2_filter(int n_o, int ntap, const int* __restrict__ tap_off, const double* __restrict__ tap_w,
+                          const double* __restrict__ phis, double* __restrict__ u, double* __restrict__ psum) {
+  __shared__ double red[32];
+  const int n = 2 * n_o;
+  const long N = (long)n * n, NO = (long)n_o * n_o;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int cell = blockIdx.y;
+  double acc = 0.0;
+  if (t < N) {
+    const int j = (int)(t % n), i = (int)(t / n);
+    const double* f = phis + (long)cell * NO;
+    for (int q = 0; q < ntap; ++q) {
+      const int ii = wrap_fold(i, tap_off[3 * q], n, n_o), jj = wrap_fold(j, tap_off[3 * q + 1], n, n_o);
+      acc += tap_w[q] * f[(long)ii * n_o + jj];
+    }
+    u[(long)cell * N + t] = acc;
+  }
+  double a[1] = {acc};
+  block_sum<1>(a, red);
+  if (threadIdx.x == 0) psum[(long)cell * gridDim.x + blockIdx.x] = a[0];
+}
+
+// F = fold(u / den) on the quadrant (x, then y: 0.5 (a + b) each), den = std(u) + 1e-12 from the k_dens_var partials
+__global__ void k2_fold(int n_o, const double* __restrict__ u, int nvar, const double* __restrict__ pvar,
+                        double* __restrict__ F) {
+  __shared__ double s_den;
+  const int cell = blockIdx.y, n = 2 * n_o;
+  const long N = (long)n * n, NO = (long)n_o * n_o;
+  const double tot = warp0_sum(pvar + (long)cell * nvar, nvar);
+  if (threadIdx.x == 0) s_den = sqrt(tot / (double)N) + 1e-12;
+  __syncthreads();
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= NO) return;
+  const int j = (int)(t % n_o), i = (int)(t / n_o);
+  const double* x = u + (long)cell * N;
+  const double dd = s_den;
+  auto us = [&](int ii, int jj) { return x[(long)ii * n + jj] / dd; };
+  auto f0 = [&](int ii, int jj) { return 0.5 * (us(ii, jj) + us(n - 1 - ii, jj)); };
+  F[(long)cell * NO + t] = 0.5 * (f0(i, j) + f0(i, n - 1 - j));
+}
+
+// o[orbit] = sym_perm(F) at the orbit's sorted pair
+__global__ void k2_orbits(int n_o, int R, const int* __restrict__ orbit_abc, const double* __restrict__ F,
+                          double* __restrict__ o) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  const int cell = blockIdx.y;
+  const double* x = F + (long)cell * n_o * n_o;
+  const int a = orbit_abc[3 * r], b = orbit_abc[3 * r + 1];
+  o[(long)cell * R + r] = (x[(long)a * n_o + b] + x[(long)b * n_o + a]) / 2.0;
+}
+
+// rho and the smoothed field on the full cell: copies of the orbit values
+__global__ void k2_rho(int n_o, int R, const int* __restrict__ orbit_of, const double* __restrict__ o,
+                       const double* __restrict__ ro, double* __restrict__ rho, double* __restrict__ u_out) {
+  const int n = 2 * n_o;
+  const long N = (long)n * n;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  const int cell = blockIdx.y, j = (int)(t % n), i = (int)(t / n);
+  const int q = orbit_of[(long)fold_idx(i, n_o) * n_o + fold_idx(j, n_o)];
+  if (rho) rho[(long)cell * N + t] = ro[(long)cell * R + q];
+  if (u_out) u_out[(long)cell * N + t] = o[(long)cell * R + q];
+}
+
+// go[p] = sum of g over the 4 mirror images of quadrant point p (x, then y)
+__global__ void k2_mirror_t(int n_o, const double* __restrict__ g, double* __restrict__ go) {
+  const int n = 2 * n_o;
+  const long NO = (long)n_o * n_o, N = (long)n * n;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= NO) return;
+  const int vec = blockIdx.y, b = (int)(t % n_o), a = (int)(t / n_o);
+  const double* x = g + (long)vec * N;
+  auto x1 = [&](int j) { return x[(long)a * n + j] + x[(long)(n - 1 - a) * n + j]; };
+  go[(long)vec * NO + t] = x1(b) + x1(n - 1 - b);
+}
+
+// Per orbit r: W_r = beta d_r gs_r (gs_r the orbit's sum of go, d_r = s_r (1 - s_r)), then the orbit mean of the
+// threshold's transpose, ubs_r = W_r / (4 mult_r) - d_r (sum W) / (4 sum mult d). One CTA per vector.
+__global__ void __launch_bounds__(1024) k2_dv_orbits(int n_o, int R, int nrow, const int* __restrict__ orbit_abc,
+                                                     const double* __restrict__ mult, const double* __restrict__ ro,
+                                                     const double* __restrict__ go, double beta,
+                                                     double* __restrict__ ubs) {
+  __shared__ double red[32 * 2];
+  __shared__ double s_w, s_d;
+  const int vec = blockIdx.x, cell = vec / nrow;
+  const double* G = go + (long)vec * n_o * n_o;
+  const double* sr = ro + (long)cell * R;
+  double* out = ubs + (long)vec * R;
+  double acc[2] = {0.0, 0.0};
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const int a = orbit_abc[3 * r], b = orbit_abc[3 * r + 1];
+    double gs = G[(long)a * n_o + b];
+    if (a != b) gs = gs + G[(long)b * n_o + a];
+    const double d = sr[r] * (1.0 - sr[r]);
+    const double W = beta * d * gs;
+    out[r] = W;
+    acc[0] += W;
+    acc[1] += mult[r] * d;
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) {
+    s_w = acc[0];
+    s_d = 4.0 * acc[1];
+  }
+  __syncthreads();
+  const double k = s_w / s_d;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const double d = sr[r] * (1.0 - sr[r]);
+    out[r] = out[r] / (4.0 * mult[r]) - d * k;
+  }
+}
+
+// pdot[vec][blk] = partial sum over the cell of ubs[orbit(x)] u(x)
+__global__ void k2_dv_dot(int n_o, int R, int nrow, const int* __restrict__ orbit_of, const double* __restrict__ ubs,
+                          const double* __restrict__ u, double* __restrict__ pdot) {
+  __shared__ double red[32];
+  const int n = 2 * n_o, vec = blockIdx.y, cell = vec / nrow;
+  const long N = (long)n * n;
+  const double* uc = u + (long)cell * N;
+  const double* ub = ubs + (long)vec * R;
+  double a[1] = {0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(i % n), x = (int)(i / n);
+    a[0] += ub[orbit_of[(long)fold_idx(x, n_o) * n_o + fold_idx(j, n_o)]] * uc[i];
+  }
+  block_sum<1>(a, red);
+  if (threadIdx.x == 0) pdot[(long)vec * gridDim.x + blockIdx.x] = a[0];
+}
+
+// uf[vec] = the cone filter of ubar(x) = ubs[orbit(x)] / D - cc (u(x) - mean) / (N sd) (the transpose of the
+// unit-std scaling applied to the orbit-mean cotangent; D = sd + 1e-12, cc = sum ubs u / D^2)
+__global__ void k2_dv_filter(int n_o, int ntap, int nrow, int R, const int* __restrict__ tap_off,
+                             const double* __restrict__ tap_w, const int* __restrict__ orbit_of,
+                             const double* __restrict__ ubs, const double* __restrict__ u, int nsum,
+                             const double* __restrict__ psum, int nvar, const double* __restrict__ pvar, int ndot,
+                             const double* __restrict__ pdot, double* __restrict__ uf) {
+  __shared__ double sc[4];
+  const int n = 2 * n_o, vec = blockIdx.y, cell = vec / nrow;
+  const long N = (long)n * n;
+  {
+    const double t0 = warp0_sum(psum + (long)cell * nsum, nsum);
+    const double t1 = warp0_sum(pvar + (long)cell * nvar, nvar);
+    const double t2 = warp0_sum(pdot + (long)vec * ndot, ndot);
+    if (threadIdx.x == 0) {
+      const double sd = sqrt(t1 / (double)N), D = sd + 1e-12;
+      sc[0] = t0 / (double)N;
+      sc[1] = D;
+      sc[2] = t2 / (D * D);
+      sc[3] = (double)N * sd;
+    }
+  }
+  __syncthreads();
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  const double mean = sc[0], D = sc[1], cc = sc[2], Nsd = sc[3];
+  const double* uc = u + (long)cell * N;
+  const double* ub = ubs + (long)vec * R;
+  const int j = (int)(t % n), i = (int)(t / n);
+  double acc = 0.0;
+  for (int q = 0; q < ntap; ++q) {
+    int ii = i - tap_off[3 * q], jj = j - tap_off[3 * q + 1];
+    ii = ii < 0 ? ii + n : (ii >= n ? ii - n : ii);
+    jj = jj < 0 ? jj + n : (jj >= n ? jj - n : jj);
+    const double ubar = ub[orbit_of[(long)fold_idx(ii, n_o) * n_o + fold_idx(jj, n_o)]] / D -
+                        cc * (uc[(long)ii * n + jj] - mean) / Nsd;
+    acc += tap_w[q] * ubar;
+  }
+  uf[(long)vec * N + t] = acc;
+}
+
 bool dens_on_dev(const void* p) {
   if (!p) return false;
   cudaPointerAttributes at;
@@ -578,12 +765,13 @@ size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 static int density_tables(DensityHandle& h) {
   const int n = h.n, n_o = h.n_o;
   // the cone kernel on the periodic grid: k(g) = max(0, r - |min-image g|), normalised (a delta if all zero)
-  std::vector<int> off;
+  std::vector<int> off;  // [ntap][3]; the third offset is 0 on squares
   std::vector<double> w;
   double sum = 0.0;
+  const int nz = h.d == 3 ? n : 1;
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) {
+      for (int k = 0; k < nz; ++k) {
         const double gi = std::min(i, n - i), gj = std::min(j, n - j), gk = std::min(k, n - k);
         const double val = std::max(0.0, h.r - std::sqrt(gi * gi + gj * gj + gk * gk));
         if (val > 0.0) {
@@ -605,18 +793,30 @@ static int density_tables(DensityHandle& h) {
   h.ntap = (int)w.size();
   h.halo = 0;
   for (int x : off) h.halo = std::max(h.halo, std::abs(x));
-  // orbits: sorted triples in lexicographic order, their multiplicity, and the orbit of every octant point
-  std::vector<int> abc, of((size_t)n_o * n_o * n_o, -1);
+  // orbits: sorted triples (pairs on squares) in lexicographic order, their multiplicity, and the orbit of every
+  // octant (quadrant) point
+  std::vector<int> abc, of(h.d == 3 ? (size_t)n_o * n_o * n_o : (size_t)n_o * n_o, -1);
   std::vector<double> mult;
-  for (int a = 0; a < n_o; ++a)
-    for (int b = a; b < n_o; ++b)
-      for (int c = b; c < n_o; ++c) {
+  if (h.d == 2) {
+    for (int a = 0; a < n_o; ++a)
+      for (int b = a; b < n_o; ++b) {
         const int id = (int)mult.size();
-        abc.insert(abc.end(), {a, b, c});
-        mult.push_back((a == b && b == c) ? 1.0 : (a == b || b == c) ? 3.0 : 6.0);
-        const int p[6][3] = {{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a}, {c, a, b}, {c, b, a}};
-        for (auto& q : p) of[((size_t)q[0] * n_o + q[1]) * n_o + q[2]] = id;
+        abc.insert(abc.end(), {a, b, 0});
+        mult.push_back(a == b ? 1.0 : 2.0);
+        of[(size_t)a * n_o + b] = id;
+        of[(size_t)b * n_o + a] = id;
       }
+  } else {
+    for (int a = 0; a < n_o; ++a)
+      for (int b = a; b < n_o; ++b)
+        for (int c = b; c < n_o; ++c) {
+          const int id = (int)mult.size();
+          abc.insert(abc.end(), {a, b, c});
+          mult.push_back((a == b && b == c) ? 1.0 : (a == b || b == c) ? 3.0 : 6.0);
+          const int p[6][3] = {{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a}, {c, a, b}, {c, b, a}};
+          for (auto& q : p) of[((size_t)q[0] * n_o + q[1]) * n_o + q[2]] = id;
+        }
+  }
   h.R = (int)mult.size();
   NLF_CUDA_TRY(cudaMalloc(&h.tap_off, off.size() * sizeof(int)));
   NLF_CUDA_TRY(cudaMalloc(&h.tap_w, w.size() * sizeof(double)));
@@ -645,7 +845,8 @@ static void density_free(DensityHandle& h) {
 static int density_run(DensityHandle& h, int ncell, const double* phi, const double* vol, double beta, double* rho,
                        double* u_out, double* eta_out, cudaStream_t st, DensWs* keep = nullptr) {
   const int n_o = h.n_o, n = h.n;
-  const long NO = (long)n_o * n_o * n_o, N = (long)n * n * n;
+  const bool sq = h.d == 2;
+  const long NO = sq ? (long)n_o * n_o : (long)n_o * n_o * n_o, N = sq ? (long)n * n : (long)n * n * n;
   // the tiled filter when its staged region fits in shared memory (cone radii up to ~6 at 64^3), else the gather
   // (NLF_DENSITY_GATHER=1 forces the gather)
   const size_t tsm = tile_smem(n, h.halo, h.ntap);
@@ -653,7 +854,7 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
     const char* e = std::getenv("NLF_DENSITY_GATHER");
     return e && e[0] == '1';
   }();
-  const bool tiled = tsm <= 200 * 1024 && !force_gather;
+  const bool tiled = !sq && tsm <= 200 * 1024 && !force_gather;
   const int ntile = ((n + kTX - 1) / kTX) * ((n + kTY - 1) / kTY);
   const int nsum = tiled ? ntile : (int)((N + 255) / 256), nvar = (int)std::min<long>(128, (N + 2047) / 2048);
   const size_t o_phis = 0, o_u = al256(o_phis + (size_t)ncell * NO * 8),
@@ -679,6 +880,38 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
     keep->eta = eta;
     keep->nsum = nsum;
     keep->nvar = nvar;
+  }
+  if (sq) {
+    {
+      ProfScope ps(PK_DENS_FILTER, st);
+      k2_symphi<<<dim3((unsigned)((NO + 255) / 256), ncell), 256, 0, st>>>(n_o, phi, phis);
+      NLF_CHECK_LAUNCH();
+      k2_filter<<<dim3((unsigned)nsum, ncell), 256, 0, st>>>(n_o, h.ntap, h.tap_off, h.tap_w, phis, u, psum);
+      NLF_CHECK_LAUNCH();
+    }
+    {
+      ProfScope ps(PK_DENS_VAR, st);
+      k_dens_var<<<dim3((unsigned)nvar, ncell), 256, 0, st>>>(N, nsum, u, psum, pvar);
+      NLF_CHECK_LAUNCH();
+    }
+    {
+      ProfScope ps(PK_DENS_FOLD, st);
+      k2_fold<<<dim3((unsigned)((NO + 255) / 256), ncell), 256, 0, st>>>(n_o, u, nvar, pvar, phis);
+      NLF_CHECK_LAUNCH();
+      k2_orbits<<<dim3((unsigned)((h.R + 255) / 256), ncell), 256, 0, st>>>(n_o, h.R, h.orbit_abc, phis, orb);
+      NLF_CHECK_LAUNCH();
+    }
+    {
+      ProfScope ps(PK_DENS_ETA, st);
+      k_dens_eta<<<ncell * kEtaCta, kEtaThreads, 0, st>>>((double)NO, h.R, orb, h.orbit_mult, vol, beta, eta, ro);
+      NLF_CHECK_LAUNCH();
+    }
+    {
+      ProfScope ps(PK_DENS_RHO, st);
+      k2_rho<<<dim3((unsigned)((N + 255) / 256), ncell), 256, 0, st>>>(n_o, h.R, h.orbit_of, orb, ro, rho, u_out);
+      NLF_CHECK_LAUNCH();
+    }
+    return NLF_OK;
   }
   {
     ProfScope ps(PK_DENS_FILTER, st);
@@ -710,7 +943,7 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
   }
   {
     ProfScope ps(PK_DENS_ETA, st);
-    k_dens_eta<<<ncell * kEtaCta, kEtaThreads, 0, st>>>(n_o, h.R, orb, h.orbit_mult, vol, beta, eta, ro);
+    k_dens_eta<<<ncell * kEtaCta, kEtaThreads, 0, st>>>((double)NO, h.R, orb, h.orbit_mult, vol, beta, eta, ro);
     NLF_CHECK_LAUNCH();
   }
   {
@@ -727,8 +960,9 @@ static int density_run(DensityHandle& h, int ncell, const double* phi, const dou
 static int density_vjp_run(DensityHandle& h, int ncell, int nrow, const double* phi, const double* vol, double beta,
                            const double* gbar, double* phibar, cudaStream_t st) {
   const int n_o = h.n_o, n = h.n, nvec = ncell * nrow;
-  const long NO = (long)n_o * n_o * n_o, N = (long)n * n * n;
-  const size_t tsm = tile_smem(n, h.halo, h.ntap);
+  const bool sq = h.d == 2;
+  const long NO = sq ? (long)n_o * n_o : (long)n_o * n_o * n_o, N = sq ? (long)n * n : (long)n * n * n;
+  const size_t tsm = sq ? 0 : tile_smem(n, h.halo, h.ntap);
   if (tsm > 200 * 1024) {
     set_error("nlf_density_vjp: the filter radius %g needs %zu B of shared memory per tile (at most 200 KiB)", h.r,
               tsm);
@@ -750,6 +984,23 @@ static int density_vjp_run(DensityHandle& h, int ncell, int nrow, const double* 
   double* mt = reinterpret_cast<double*>(b + o_mt);
   ProfScope ps(PK_DENS_VJP, st);
   const dim3 goct((unsigned)((NO + 255) / 256), nvec);
+  if (sq) {
+    k2_mirror_t<<<goct, 256, 0, st>>>(n_o, gbar, go);
+    NLF_CHECK_LAUNCH();
+    k2_dv_orbits<<<nvec, 1024, 0, st>>>(n_o, h.R, nrow, h.orbit_abc, h.orbit_mult, f.ro, go, beta, ubs);
+    NLF_CHECK_LAUNCH();
+    k2_dv_dot<<<dim3((unsigned)ndot, nvec), 256, 0, st>>>(n_o, h.R, nrow, h.orbit_of, ubs, f.u, pdot);
+    NLF_CHECK_LAUNCH();
+    k2_dv_filter<<<dim3((unsigned)((N + 255) / 256), nvec), 256, 0, st>>>(n_o, h.ntap, nrow, h.R, h.tap_off, h.tap_w,
+                                                                           h.orbit_of, ubs, f.u, f.nsum, f.psum,
+                                                                           f.nvar, f.pvar, ndot, pdot, uf);
+    NLF_CHECK_LAUNCH();
+    k2_mirror_t<<<goct, 256, 0, st>>>(n_o, uf, mt);
+    NLF_CHECK_LAUNCH();
+    k2_symphi<<<goct, 256, 0, st>>>(n_o, mt, phibar);
+    NLF_CHECK_LAUNCH();
+    return NLF_OK;
+  }
   k_dv_mirror_t<<<goct, 256, 0, st>>>(n_o, gbar, go);
   NLF_CHECK_LAUNCH();
   k_dv_orbits<<<nvec, 1024, 0, st>>>(n_o, h.R, nrow, h.orbit_abc, h.orbit_mult, f.ro, go, beta, ubs);
@@ -779,13 +1030,17 @@ struct nlf_density {
 
 extern "C" {
 
-NLF_API int nlf_density_create(nlf_density** out, int n_o, double r) {
-  if (!out || n_o < 1 || n_o > 512 || !(r >= 0.0) || !std::isfinite(r)) {
-    set_error("nlf_density_create: bad arguments (n_o in [1, 512], r >= 0 finite)");
+NLF_API int nlf_density_create(nlf_density** out, int n_o, double r) { return nlf_density_create_d(out, n_o, 3, r); }
+
+NLF_API int nlf_density_create_d(nlf_density** out, int n_o, int d, double r) {
+  if (!out || (d != 2 && d != 3) || n_o < 1 || n_o > (d == 3 ? 512 : 4096) || !(r >= 0.0) || !std::isfinite(r)) {
+    set_error("nlf_density_create: bad arguments (d 2 or 3, n_o in [1, 512] for cubes or [1, 4096] for squares, "
+              "r >= 0 finite)");
     return NLF_EBADARG;
   }
   *out = nullptr;
   nlf_density* H = new nlf_density();
+  H->h.d = d;
   H->h.n_o = n_o;
   H->h.n = 2 * n_o;
   H->h.r = r;
@@ -817,7 +1072,8 @@ NLF_API int nlf_density_rho(nlf_density* H, int ncell, const double* phi, const 
   }
   DensityHandle& h = H->h;
   cudaStream_t st = (cudaStream_t)stream;
-  const long NO = (long)h.n_o * h.n_o * h.n_o, N = (long)h.n * h.n * h.n;
+  const long NO = h.d == 2 ? (long)h.n_o * h.n_o : (long)h.n_o * h.n_o * h.n_o,
+             N = h.d == 2 ? (long)h.n * h.n : (long)h.n * h.n * h.n;
   const bool dphi = dens_on_dev(phi), dv = dens_on_dev(v), drho = !rho || dens_on_dev(rho),
              du = !u || dens_on_dev(u), deta = !eta || dens_on_dev(eta);
   const size_t o_phi = 0, o_v = al256(o_phi + (dphi ? 0 : (size_t)ncell * NO * 8)),
@@ -856,7 +1112,8 @@ NLF_API int nlf_density_vjp(nlf_density* H, int ncell, int nrow, const double* p
   }
   DensityHandle& h = H->h;
   cudaStream_t st = (cudaStream_t)stream;
-  const long NO = (long)h.n_o * h.n_o * h.n_o, N = (long)h.n * h.n * h.n;
+  const long NO = h.d == 2 ? (long)h.n_o * h.n_o : (long)h.n_o * h.n_o * h.n_o,
+             N = h.d == 2 ? (long)h.n * h.n : (long)h.n * h.n * h.n;
   const size_t nvec = (size_t)ncell * nrow;
   const bool dphi = dens_on_dev(phi), dv = dens_on_dev(v), dg = dens_on_dev(rho_bar), dout = dens_on_dev(phi_bar);
   const size_t o_phi = 0, o_v = al256(o_phi + (dphi ? 0 : (size_t)ncell * NO * 8)),

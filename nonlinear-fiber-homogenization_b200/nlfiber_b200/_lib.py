@@ -26,7 +26,7 @@ EXPORTS = (
     "nlf_mech_precond_w", "nlf_mech_grad_w", "nlf_mech_cg", "nlf_mech_set_precond",
     "nlf_unet_create", "nlf_unet_destroy", "nlf_unet_param_count", "nlf_unet_get_params", "nlf_unet_set_params",
     "nlf_unet_forward", "nlf_unet_backward", "nlf_unet_adam_step",
-    "nlf_density_create", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
+    "nlf_density_create", "nlf_density_create_d", "nlf_density_destroy", "nlf_density_orbits", "nlf_density_rho", "nlf_density_vjp",
     "nlf_correctors_vjp", "nlf_mech_toec",
     "nlf_apply_variants", "nlf_linear_set_apply_variant", "nlf_linear_get_apply_variant", "nlf_linear_autotune",
     "nlf_linear_set_kinv_mode", "nlf_linear_get_kinv_mode", "nlf_linear_set_fft_twiddles",
@@ -97,6 +97,7 @@ def _load():
         "nlf_unet_backward": (I, [P, I, I, I, I, P, P, P, P, P, P]),
         "nlf_unet_adam_step": (I, [P, D, D, D, D, P]),
         "nlf_density_create": (I, [ctypes.POINTER(P), I, D]),
+        "nlf_density_create_d": (I, [ctypes.POINTER(P), I, I, D]),
         "nlf_density_destroy": (I, [P]),
         "nlf_density_orbits": (I, [P]),
         "nlf_density_rho": (I, [P, I, P, P, D, P, P, P, P]),

@@ -1,5 +1,5 @@
 """Pre-density phi -> physical density rho with exact volume, on the GPU (nlfiber/density.py and
-nlfiber/symmetry.py for cubic cells, batched, in libnlf.so: nlf_density_*).
+nlfiber/symmetry.py for cubic and square cells, batched, in libnlf.so: nlf_density_*).
 
     u   = F mirror(sym_perm(phi)) / std    periodic cone filter on the full cell, unit standard deviation
     rho = sigmoid(beta (u - eta)),         eta such that mean(rho) = v (bisection, then Newton)
@@ -14,22 +14,23 @@ import numpy as np
 
 
 class GpuDensityMap:
-    """DensityMap on the GPU (nlfiber/density.py:75-94 smooth / rho / eta) for cubic cells, batched.
+    """DensityMap on the GPU (nlfiber/density.py:75-94 smooth / rho / eta) for cubic (d = 3) and square (d = 2)
+    cells, batched.
 
-    phi is an octant (n_o)^3 pre-density (or a batch (ncell, n_o, n_o, n_o)); NumPy arrays are copied in, CUDA
+    phi is an octant (n_o)^d pre-density (or a batch (ncell,) + (n_o,)*d); NumPy arrays are copied in, CUDA
     float64 tensors are used in place. Results are CUDA float64 tensors. The filter runs as a direct periodic sum
     over its taps and the volume bisection over the symmetry orbits, so values agree with `DensityMap` to
     rounding (not bitwise); symmetric voxels are bit-identical and mean(rho) = v to rounding."""
 
     def __init__(self, n_o, d=3, r=1.5, v=0.3):
-        if d != 3:
-            raise ValueError("GpuDensityMap takes cubic cells (d = 3)")
+        if d not in (2, 3):
+            raise ValueError("GpuDensityMap takes cubic (d = 3) or square (d = 2) cells")
         from ._lib import check, lib
-        self.n_o, self.d, self.r, self.v = int(n_o), d, float(r), float(v)
+        self.n_o, self.d, self.r, self.v = int(n_o), int(d), float(r), float(v)
         self.n = 2 * self.n_o
-        self.shape = (self.n,) * 3
+        self.shape = (self.n,) * self.d
         h = ctypes.c_void_p()
-        check(lib.nlf_density_create(ctypes.byref(h), self.n_o, self.r))
+        check(lib.nlf_density_create_d(ctypes.byref(h), self.n_o, self.d, self.r))
         self._h = h
         self._lib = lib  # kept for __del__, which may run while the interpreter shuts down
         self.orbits = int(lib.nlf_density_orbits(h))
@@ -48,14 +49,14 @@ class GpuDensityMap:
             phi = phi.to(device="cuda", dtype=torch.float64).contiguous()
         else:
             phi = torch.as_tensor(np.ascontiguousarray(np.asarray(phi, dtype=np.float64)), device="cuda")
-        if phi.dim() == 3:
+        if phi.dim() == self.d:
             phi = phi.unsqueeze(0)
-        if tuple(phi.shape[1:]) != (self.n_o,) * 3:
-            raise ValueError(f"phi must be (ncell, {self.n_o}, {self.n_o}, {self.n_o}), got {tuple(phi.shape)}")
+        if tuple(phi.shape[1:]) != (self.n_o,) * self.d:
+            raise ValueError(f"phi must be (ncell,) + {(self.n_o,) * self.d}, got {tuple(phi.shape)}")
         return phi
 
     def run(self, phi, beta, v=None, rho=True, smooth=False, eta=True):
-        """The map for a batch: {"rho": (ncell, n, n, n), "u": smoothed field or None, "eta": (ncell,)};
+        """The map for a batch: {"rho": (ncell,) + shape, "u": smoothed field or None, "eta": (ncell,)};
         v is a scalar or one volume fraction per cell (default: the map's v)."""
         import torch
         from ._lib import check, lib, ptr
@@ -72,11 +73,11 @@ class GpuDensityMap:
 
     def vjp(self, phi, beta, rho_bar, v=None):
         """Cotangents of phi for cotangents of rho (the reverse mode of `rho`, with the implicit d eta of
-        nlfiber/density.py:66-72). phi (n_o,)*3 with rho_bar (nrow, n, n, n), or a batch (ncell, n_o, n_o, n_o)
-        with rho_bar (ncell, nrow, n, n, n). Returns (nrow, n_o, n_o, n_o) or (ncell, nrow, n_o, n_o, n_o)."""
+        nlfiber/density.py:66-72). phi (n_o,)*d with rho_bar (nrow,) + shape, or a batch (ncell,) + (n_o,)*d with
+        rho_bar (ncell, nrow) + shape. Returns (nrow,) + (n_o,)*d or (ncell, nrow) + (n_o,)*d."""
         import torch
         from ._lib import check, lib, ptr
-        single = np.ndim(phi) == 3
+        single = (phi.dim() if torch.is_tensor(phi) else np.ndim(phi)) == self.d
         phi = self._phi(phi)
         nc = phi.shape[0]
         if torch.is_tensor(rho_bar):
@@ -85,12 +86,12 @@ class GpuDensityMap:
             g = torch.as_tensor(np.ascontiguousarray(np.asarray(rho_bar, dtype=np.float64)), device="cuda")
         if single:
             g = g.reshape((1, -1) + self.shape)
-        if g.dim() != 5 or g.shape[0] != nc or tuple(g.shape[2:]) != self.shape:
+        if g.dim() != 2 + self.d or g.shape[0] != nc or tuple(g.shape[2:]) != self.shape:
             raise ValueError(f"rho_bar must be (ncell, nrow) + {self.shape}, got {tuple(g.shape)}")
         nrow = g.shape[1]
         vv = torch.as_tensor(np.broadcast_to(np.asarray(self.v if v is None else v, dtype=np.float64), (nc,)).copy(),
                              device="cuda")
-        out = torch.empty((nc, nrow) + (self.n_o,) * 3, dtype=torch.float64, device="cuda")
+        out = torch.empty((nc, nrow) + (self.n_o,) * self.d, dtype=torch.float64, device="cuda")
         check(lib.nlf_density_vjp(self._h, nc, nrow, ptr(phi), ptr(vv), float(beta), ptr(g), ptr(out), self.stream))
         return out[0] if single else out
 

@@ -1,10 +1,11 @@
 """The constraint map of the fiber on the GPU: phi (symmetric octant) -> normalized stiffness invariants
-c(phi) = (C11, C12, C44) / E and its Jacobian (nlfiber/fiber.py:17-60).
+c(phi) = (C11, C12, C44) / E in 3D, (C11, C12, C66) / E in 2D (plane strain), and its Jacobian
+(nlfiber/fiber.py:17-60).
 
 Value: the density map (libnlf.so nlf_density_rho), the cubic two-case corrector solve and C assembly
 (nlf_linear_solve, nlf_bilinear). Jacobian rows: dc_k/drho with the correctors held fixed (nlf_dC_drho, exact
 because the correctors are stationary), pulled back through the density map (nlf_density_vjp) -- the three
-VJPs of the reference's `value_and_jac` (fiber.py:34-39), without JAX. Cubic cells (d = 3) only.
+VJPs of the reference's `value_and_jac` (fiber.py:34-39), without JAX. Cubic (d = 3) and square (d = 2) cells.
 """
 import numpy as np
 
@@ -18,8 +19,6 @@ class Fiber:
     solver (e.g. precond="scaled", energy_tol)."""
 
     def __init__(self, n_o, d=3, v=0.3, r=1.5, E=1.0, nu=0.3, emin=1e-3, p=3.0, tol=1e-9, **solver):
-        if d != 3:
-            raise ValueError("the GPU Fiber takes cubic cells (d = 3)")
         self.n_o, self.d, self.v = n_o, d, v
         self.dm = GpuDensityMap(n_o, d, r, v)
         self.lh = LinearHomogenization(self.dm.shape, E=E, nu=nu, emin=emin, p=p, tol=tol, **solver)
@@ -43,13 +42,13 @@ class Fiber:
         return self._solve(phi, beta, warm)[1]
 
     def value_jac(self, phi, beta, warm=True):
-        """nlfiber/fiber.py:53-57: (c (3,), J (3, n_o, n_o, n_o)), J[k] = dc_k / dphi."""
+        """nlfiber/fiber.py:53-57: (c (3,), J (3,) + (n_o,)*d), J[k] = dc_k / dphi."""
         rho, c, u2 = self._solve(phi, beta, warm)
         lh = self.lh
         u3 = np.ascontiguousarray(np.stack([u2[0], lh.swap_xy(u2[0]), u2[1]]))
         Es = np.stack([unit_strain(0), unit_strain(1), unit_strain(lh._shear())])
         dC = lh.dC_drho(rho, Es, u3)
-        rows = np.ascontiguousarray(np.stack([dC[0, 0], dC[1, 0], dC[2, 2]]) / lh.E)
+        rows = np.ascontiguousarray((np.stack([dC[0, 0], dC[1, 0], dC[2, 2]]) / lh.E).reshape((3,) + self.dm.shape))
         J = self.dm.vjp(phi, float(beta), rows)
         return c, J.cpu().numpy()
 

@@ -193,3 +193,77 @@ def test_fiber_value_jac_matches_oracle_chain_and_finite_differences():
     fd = (fib.value(phi + h * d, beta, warm=False) - fib.value(phi - h * d, beta, warm=False)) / (2 * h)
     jd = np.tensordot(J, d, axes=3)
     np.testing.assert_allclose(jd, fd, rtol=1e-6, atol=1e-9)
+
+
+# ---- square cells (d = 2): the same map on a quadrant (n_o)^2 and a full cell (2 n_o)^2 ----------------------
+
+def _gpu2(n_o, r, v):
+    from nlfiber_b200.density import GpuDensityMap
+    return GpuDensityMap(n_o, 2, r=r, v=v)
+
+
+@pytest.mark.parametrize("n_o,r,v,beta,seed", [(4, 1.5, 0.27, 8.0, 2), (6, 1.5, 0.3, 16.0, 5), (8, 2.5, 0.25, 32.0, 3),
+                                               (5, 1.0, 0.4, 4.0, 7), (32, 1.5, 0.3, 16.0, 11)])
+def test_square_rho_smooth_eta_match_oracle(n_o, r, v, beta, seed):
+    """DensityMap(n_o, d=2) (nlfiber/density.py:75-94, symmetry.py for d = 2) on the GPU against the oracle."""
+    phi = np.random.default_rng(seed).standard_normal((n_o,) * 2)
+    dm = OD.DensityMap(n_o, 2, r=r, v=v)
+    u_o = dm.smooth(phi)
+    eta_o = OD.solve_eta(u_o, v, beta)
+    rho_o = dm.rho(phi, beta)
+    g = _gpu2(n_o, r, v)
+    assert g.orbits == n_o * (n_o + 1) // 2
+    out = g.run(phi, beta, smooth=True)
+    rho, u, eta = (out[k].cpu().numpy() for k in ("rho", "u", "eta"))
+    assert np.abs(u[0] - u_o).max() < TOL
+    assert abs(eta[0] - eta_o) < TOL
+    assert np.abs(rho[0] - rho_o).max() < TOL
+    assert abs(rho[0].mean() - v) < 1e-12
+    for f in (rho[0], u[0]):  # the 8 symmetries of the square, exactly
+        np.testing.assert_array_equal(f, f[::-1])
+        np.testing.assert_array_equal(f, f[:, ::-1])
+        np.testing.assert_array_equal(f, f.T)
+
+
+@pytest.mark.parametrize("n_o,r,v,beta", [(4, 1.5, 0.27, 4.0), (5, 1.0, 0.4, 8.0), (16, 1.5, 0.25, 32.0)])
+def test_square_vjp_matches_oracle(n_o, r, v, beta):
+    """nlf_density_vjp on squares against the oracle's reverse mode (pinned by finite differences on the CPU), for
+    2 cells with per-cell volumes and 3 cotangent rows each."""
+    rng = np.random.default_rng(n_o)
+    phis = rng.standard_normal((2,) + (n_o,) * 2)
+    vols = np.array([v, v + 0.05])
+    g = rng.standard_normal((2, 3) + (2 * n_o,) * 2)
+    out = _gpu2(n_o, r, v).vjp(phis, beta, g, v=vols).cpu().numpy()
+    for i in range(2):
+        dm = OD.DensityMap(n_o, 2, r=r, v=float(vols[i]))
+        for k in range(3):
+            ref = OD.rho_vjp(dm, phis[i], beta, g[i, k])
+            assert np.abs(out[i, k] - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+
+
+def test_square_fiber_value_jac_matches_oracle_chain_and_finite_differences():
+    """nlfiber/fiber.py:17-60 with d = 2: c = (C11, C12, C66) / E of the plane-strain two-case solve and its
+    Jacobian rows, against the oracle's chain and central differences of the GPU value."""
+    from nlfiber_b200.fiber import Fiber
+    from oracle import linear_ref as OL
+    n_o, beta, v = 6, 8.0, 0.35
+    phi = OD.sym_perm(np.random.default_rng(5).standard_normal((n_o,) * 2))
+    fib = Fiber(n_o, d=2, v=v, r=1.5, emin=1e-3, tol=1e-13, maxit=20000)
+    c, J = fib.value_jac(phi, beta, warm=False)
+    assert J.shape == (3, n_o, n_o)
+    dm = OD.DensityMap(n_o, 2, r=1.5, v=v)
+    rho = dm.rho(phi, beta)
+    lh = OL.LinearHomogenization(rho.shape, emin=1e-3, tol=1e-13, maxit=20000)
+    c_o, u2, _ = lh.invariants(rho)
+    np.testing.assert_allclose(c, c_o, rtol=1e-10)
+    u3 = np.stack([u2[0], lh.swap_xy(u2[0]), u2[1]])
+    Es = np.stack([OL.unit_strain(0), OL.unit_strain(1), OL.unit_strain(lh._shear())])
+    dC = lh.dC_drho(rho, Es, u3)
+    for k, (I, Jx) in enumerate(((0, 0), (1, 0), (2, 2))):
+        ref = OD.rho_vjp(dm, phi, beta, dC[I, Jx].reshape(rho.shape) / lh.E)
+        assert np.abs(J[k] - ref).max() <= 1e-8 * np.abs(ref).max()
+    d = OD.sym_perm(np.random.default_rng(6).standard_normal((n_o,) * 2))
+    h = 1e-5
+    fd = (fib.value(phi + h * d, beta, warm=False) - fib.value(phi - h * d, beta, warm=False)) / (2 * h)
+    jd = np.tensordot(J, d, axes=2)
+    np.testing.assert_allclose(jd, fd, rtol=1e-6, atol=1e-9)
