@@ -931,6 +931,59 @@ def density_arm(args, stream, peaks, peak_kind):
                              "sample": f"{ns} cells through the oracle's NumPy map (FFT filter, full-cell bisection)"}}
 
 
+def binary_arm(args, stream):
+    """DensityMap.binary (nlfiber/density.py:96-122) of the benchmark cells on the GPU: smoothing, threshold at the
+    cell's volume fraction, floating-piece removal and regrowth (GpuDensityMap.binary), per cell from host phi to a
+    host bool cell (each call synchronizes: the regrowth rounds decide on the host). Checked against the oracle's
+    NumPy restatement, which is also the CPU baseline; up = 2 (the 128^3 upsampled check) on a few cells."""
+    import torch
+    from nlfiber_b200 import density as D
+    from nlfiber_b200.topology import cells
+    from oracle import density_ref as OD
+    n_o, nc = args.n // 2, min(args.cells, 16)
+    n = 2 * n_o
+    phis = [synth_phi(i, n_o) for i in range(nc)]
+    vols = [synth_volume(i) for i in range(nc)]
+    g = D.GpuDensityMap(n_o, 3, r=1.5)
+    for i in range(max(1, min(nc, args.warmup))):
+        g.binary(phis[i], v=vols[i])
+    torch.cuda.synchronize()
+    outs, rounds = [], []
+    t0 = time.perf_counter()
+    for i in range(nc):
+        outs.append(g.binary(phis[i], v=vols[i]))
+        rounds.append(cells(3, n).last_rounds)
+    gpu_s = (time.perf_counter() - t0) / nc
+    nu = min(nc, 4)
+    g.binary(phis[0], up=2, v=vols[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ups = [g.binary(phis[i], up=2, v=vols[i]) for i in range(nu)]
+    up_s = (time.perf_counter() - t0) / nu
+    ns = min(nc, 4)
+    t0 = time.perf_counter()
+    ref = [OD.DensityMap(n_o, 3, r=1.5, v=vols[i]).binary(phis[i]) for i in range(ns)]
+    cpu_s = (time.perf_counter() - t0) / ns
+    t0 = time.perf_counter()
+    ref_up = OD.DensityMap(n_o, 3, r=1.5, v=vols[0]).binary(phis[0], up=2)
+    cpu_up_s = time.perf_counter() - t0
+    equal = sum(bool(np.array_equal(outs[i], ref[i])) for i in range(ns))
+    return {"metric": f"binary cells/s at {n}^3 (DensityMap.binary: phi -> bool cell, floating pieces removed)",
+            "value": round(1.0 / gpu_s, 2), "unit": "cells/s", "n_gpus": 1, "ms_per_cell": round(gpu_s * 1e3, 3),
+            "higher_is_better": True, "dtype": "f64 field, u8 cell", "data": "synthetic",
+            "config": {"workload": f"{nc} seeded pre-densities random_start({n_o}, seed=i, kmax=2), v_i ~ U[0.2, "
+                                   f"0.5], cone filter r = 1.5", "cells": nc, "grid": n},
+            "regrowth_rounds": rounds, "solid_fraction": [round(float(b.mean()), 6) for b in outs],
+            "equal_to_oracle": f"{equal} of {ns}",
+            "up2": {"grid": 2 * n, "ms_per_cell": round(up_s * 1e3, 3), "cells": nu,
+                    "equal_to_oracle": bool(np.array_equal(ups[0], ref_up)),
+                    "cpu_ms_per_cell": round(cpu_up_s * 1e3, 1)},
+            "e2e": {"value": round(1.0 / gpu_s, 2), "unit": "cells/s", "h2d_bytes_per_step": 8 * n_o ** 3,
+                    "d2h_bytes_per_step": n ** 3},
+            "cpu_baseline": {"value": round(1.0 / cpu_s, 2), "unit": "cells/s", "cores": 1, "kind": "port",
+                             "sample": f"{ns} cells through the oracle's NumPy / SciPy binary map"}}
+
+
 def toec_arm(args, stream):
     """Third-order elastic constants (nlfiber/mech.py:458-493) of benchmark cells at --n^3: linear correctors
     from the batched solve, then nlf_mech_toec timed with CUDA events (correctors resident on the device)."""
@@ -1057,6 +1110,8 @@ def main():
                     help="time the FFT preconditioner against a cuFFT (torch) version instead of the default")
     ap.add_argument("--toec", action="store_true",
                     help="time the third-order elastic constants of two benchmark cells instead of the default")
+    ap.add_argument("--binary", action="store_true",
+                    help="time DensityMap.binary (binary cells, floating pieces removed) of the benchmark cells")
     ap.add_argument("--density", action="store_true",
                     help="time the GPU density map (phi -> rho) of the benchmark cells instead of the default")
     ap.add_argument("--slots", type=int, default=None,
@@ -1110,6 +1165,13 @@ def main():
         import torch
         torch.cuda.set_device(local)
         res = toec_arm(args, torch.cuda.current_stream().cuda_stream)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+    if args.binary:
+        import torch
+        torch.cuda.set_device(local)
+        res = binary_arm(args, torch.cuda.current_stream().cuda_stream)
         if rank == 0:
             print(json.dumps(res), flush=True)
         return

@@ -292,6 +292,40 @@ NLF_API int nlf_density_rho(nlf_density* dm, int ncell, const double* phi, const
 NLF_API int nlf_density_vjp(nlf_density* dm, int ncell, int nrow, const double* phi, const double* v, double beta,
                             const double* rho_bar, double* phi_bar, void* stream);
 
+/* ---- binary cells (nlfiber/density.py:96-149, nlfiber/topology.py:8-63) ------------------------------------
+ * The binary check of a design: the smoothed field thresholded at its volume fraction, floating solid removed
+ * and the volume grown back. A topology handle serves one cell side n (n^3 voxels, n^2 on squares, at most
+ * 2^30); b is a byte per voxel (0 void, 1 solid; NumPy bool), C order. Host or device pointers. A handle is not
+ * shared between host threads. */
+typedef struct nlf_topo nlf_topo;
+
+NLF_API int nlf_topo_create(nlf_topo** out, int d, int n);
+NLF_API int nlf_topo_destroy(nlf_topo* t);
+/* nlfiber/topology.py:8-43 periodic_label: connected components of the periodic cell, 26 neighbours (8 on
+ * squares) or, with faces = 1, the 6 faces (4 edges; the void's dual connectivity, topology.py:90). labels[i]
+ * is 1..ncomp, numbered in the order of each component's first voxel (the reference numbers them in its own
+ * scan order: the same components), 0 for void. */
+NLF_API int nlf_topo_label(nlf_topo* t, const uint8_t* b, int faces, int32_t* labels, int* ncomp, void* stream);
+/* nlfiber/topology.py:46-63 remove_floating, in place: keeps the components (26 / 8 neighbours) that touch
+ * every slice along every axis. Optional outputs: components, spanning components, solid voxels kept. */
+NLF_API int nlf_topo_remove_floating(nlf_topo* t, uint8_t* b, int* ncomp, int* nspan, long long* nsolid,
+                                     void* stream);
+/* The rank-th smallest (0-based) of u over the voxels where mask != 0 (all voxels when mask is NULL). */
+NLF_API int nlf_topo_select(nlf_topo* t, const double* u, const uint8_t* mask, long long rank, double* value,
+                            void* stream);
+/* nlfiber/density.py:96-122 DensityMap.binary after the smoothing: u (the smoothed, exactly symmetric field of
+ * nlf_density_rho, upsampled by nlf_upsample_sym when up > 1) -> b = u > quantile(u, 1 - v); with
+ * remove_floating, floating pieces are removed and the solid grown back towards v through the void voxels that
+ * touch it, highest u first (at most 500 rounds, the number run in *iters), then removed once more. */
+NLF_API int nlf_topo_binary(nlf_topo* t, const double* u, double v, int remove_floating, uint8_t* b, int* iters,
+                            void* stream);
+/* nlfiber/density.py:133-149 upsample_periodic of a cell-centred field of side n to side m, then
+ * nlfiber/symmetry.py:60-65 exact_symmetrize: out has side 2 (m / 2). Bitwise numpy's arithmetic. */
+NLF_API int nlf_upsample_sym(int d, int n, int m, const double* u, double* out, void* stream);
+/* numpy's default ("linear") quantile q of n sorted host values, with numpy's rounding: the interpolation
+ * nlf_topo_binary applies to its two order statistics. Host only. */
+NLF_API int nlf_quantile_linear(long long n, double q, const double* sorted, double* out);
+
 /* ---- kernel profiler ------------------------------------------------------------------------------------- */
 
 /* Turns the kernel-level profiler on (1) or off (0) and resets it. When on, every kernel launch of the library

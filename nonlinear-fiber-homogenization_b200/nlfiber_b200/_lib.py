@@ -31,6 +31,8 @@ EXPORTS = (
     "nlf_apply_variants", "nlf_linear_set_apply_variant", "nlf_linear_get_apply_variant", "nlf_linear_autotune",
     "nlf_linear_set_kinv_mode", "nlf_linear_get_kinv_mode", "nlf_linear_set_fft_twiddles",
     "nlf_linear_get_fft_twiddles",
+    "nlf_topo_create", "nlf_topo_destroy", "nlf_topo_label", "nlf_topo_remove_floating", "nlf_topo_select",
+    "nlf_topo_binary", "nlf_upsample_sym", "nlf_quantile_linear",
 )
 
 
@@ -112,6 +114,14 @@ def _load():
         "nlf_linear_get_kinv_mode": (I, [P]),
         "nlf_linear_set_fft_twiddles": (I, [P, I]),
         "nlf_linear_get_fft_twiddles": (I, [P]),
+        "nlf_topo_create": (I, [ctypes.POINTER(P), I, I]),
+        "nlf_topo_destroy": (I, [P]),
+        "nlf_topo_label": (I, [P, P, I, P, P, P]),
+        "nlf_topo_remove_floating": (I, [P, P, P, P, P, P]),
+        "nlf_topo_select": (I, [P, P, P, ctypes.c_longlong, P, P]),
+        "nlf_topo_binary": (I, [P, P, D, I, P, P, P]),
+        "nlf_upsample_sym": (I, [I, I, I, P, P, P]),
+        "nlf_quantile_linear": (I, [ctypes.c_longlong, D, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

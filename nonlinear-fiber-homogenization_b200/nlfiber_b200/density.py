@@ -103,3 +103,15 @@ class GpuDensityMap:
 
     def eta(self, phi, beta):
         return float(self.run(phi, beta, rho=False)["eta"][0])
+
+    def binary(self, phi, up=1, v=None, remove_floating=True):
+        """nlfiber/density.py:96-122: the binary cell of phi, a NumPy bool array of side 2 n_o (2 (m / 2) with
+        m = round(2 n_o up) when up > 1). The smoothed field u (nlf_density_rho), its periodic multilinear
+        upsampling by `up` with exact symmetrization (nlf_upsample_sym), the threshold at the volume fraction v and
+        the removal of floating pieces with regrowth towards v (nlf_topo_binary) all run on the device."""
+        from .topology import cells, upsample_sym
+        v = self.v if v is None else v
+        u = self.run(phi, 1.0, rho=False, smooth=True, eta=False)["u"][0]
+        if up > 1:
+            u = upsample_sym(u, up)
+        return cells(self.d, u.shape[0]).binary(u, v, remove_floating)

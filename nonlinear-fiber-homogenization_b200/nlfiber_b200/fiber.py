@@ -10,7 +10,7 @@ VJPs of the reference's `value_and_jac` (fiber.py:34-39), without JAX. Cubic (d 
 import numpy as np
 
 from .density import GpuDensityMap
-from .linear import LinearHomogenization, unit_strain
+from .linear import LinearHomogenization, cubic_invariants, cubic_leakage, unit_strain
 
 
 class Fiber:
@@ -21,7 +21,9 @@ class Fiber:
     def __init__(self, n_o, d=3, v=0.3, r=1.5, E=1.0, nu=0.3, emin=1e-3, p=3.0, tol=1e-9, **solver):
         self.n_o, self.d, self.v = n_o, d, v
         self.dm = GpuDensityMap(n_o, d, r, v)
-        self.lh = LinearHomogenization(self.dm.shape, E=E, nu=nu, emin=emin, p=p, tol=tol, **solver)
+        self._mat = dict(E=E, nu=nu, emin=emin, p=p, tol=tol, **solver)
+        self.lh = LinearHomogenization(self.dm.shape, **self._mat)
+        self._lh_bin = {}
         self.u = None  # warm start of the correctors
         self.solves = 0
 
@@ -55,3 +57,28 @@ class Fiber:
     def rho(self, phi, beta):
         """nlfiber/fiber.py:59-60 (a CUDA tensor)."""
         return self.dm.rho(phi, float(beta))
+
+    # --- binary check (nlfiber/fiber.py:62-81) ----------------------------------------------------------------
+    def lh_for(self, shape):
+        """The solver for binary cells of this shape (kept per shape)."""
+        shape = tuple(shape)
+        if shape not in self._lh_bin:
+            self._lh_bin[shape] = LinearHomogenization(shape, **self._mat)
+        return self._lh_bin[shape]
+
+    def binary_check(self, phi, up=1, full=False):
+        """nlfiber/fiber.py:67-81: binarize (upsampled by `up`), drop floating pieces, re-solve. Returns
+        dict(c, vol, cell[, C, leak])."""
+        b = self.dm.binary(phi, up=up)
+        lh = self.lh_for(b.shape)
+        rho = b.astype(np.float64)
+        out = dict(vol=float(b.mean()), cell=b)
+        if full:
+            C, _, _ = lh.C_full(rho)
+            C = np.asarray(C)
+            out.update(C=C, c=cubic_invariants(C) / lh.E, leak=cubic_leakage(C))
+        else:
+            c, _, _ = lh.invariants(rho)
+            out["c"] = np.asarray(c)
+        self.solves += 1
+        return out

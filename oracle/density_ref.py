@@ -157,25 +157,53 @@ class DensityMap:
     def rho(self, phi, beta):
         return threshold(self.smooth(phi), self.v, beta)
 
-    def binary(self, phi, v=None, remove_floating=True):
-        """nlfiber/density.py:96-122 with up=1."""
+    def binary(self, phi, up=1, v=None, remove_floating=True):
+        """nlfiber/density.py:96-122: smooth, upsample by `up` (periodic multilinear, then exact_symmetrize),
+        threshold at the volume fraction, remove floating pieces and grow back."""
         v = self.v if v is None else v
         u = np.asarray(self.smooth(phi), dtype=np.float64)
-        b = u > np.quantile(u, 1.0 - v)
-        if remove_floating:
-            for _ in range(500):
-                b = remove_floating_pieces(b)
-                missing = v - b.mean()
-                if missing * b.size < 1 or not b.any():
-                    break
-                front = _dilate_periodic(b) & ~b
-                cand = np.sort(u[front])[::-1]
-                if cand.size == 0:
-                    break
-                k = min(max(int(round(missing * b.size)), 1), cand.size)
-                b = b | (front & (u >= cand[k - 1]))
+        if up > 1:
+            u = exact_symmetrize(upsample_periodic(u, up))
+        return binary_from_u(u, v, remove_floating)
+
+
+def binary_from_u(u, v, remove_floating=True):
+    """nlfiber/density.py:105-122, the steps of DensityMap.binary after the smoothing (and upsampling)."""
+    u = np.asarray(u, dtype=np.float64)
+    b = u > np.quantile(u, 1.0 - v)
+    if remove_floating:
+        for _ in range(500):
             b = remove_floating_pieces(b)
-        return b
+            missing = v - b.mean()
+            if missing * b.size < 1 or not b.any():
+                break
+            front = _dilate_periodic(b) & ~b
+            cand = np.sort(u[front])[::-1]
+            if cand.size == 0:
+                break
+            k = min(max(int(round(missing * b.size)), 1), cand.size)
+            b = b | (front & (u >= cand[k - 1]))
+        b = remove_floating_pieces(b)
+    return b
+
+
+def upsample_periodic(c, f):
+    """nlfiber/density.py:133-149: periodic multilinear resampling of a cell-centred field by a factor f, axis by
+    axis (output index X samples x = (X + 0.5) n / m - 0.5 between floor(x) and floor(x) + 1, periodic)."""
+    out = np.asarray(c, dtype=np.float64)
+    for ax in range(out.ndim):
+        n = out.shape[ax]
+        m = int(round(n * f))
+        x = (np.arange(m) + 0.5) * n / m - 0.5
+        i0 = np.floor(x).astype(int)
+        w = x - i0
+        a = np.take(out, i0 % n, axis=ax)
+        b = np.take(out, (i0 + 1) % n, axis=ax)
+        shp = [1] * out.ndim
+        shp[ax] = m
+        w = w.reshape(shp)
+        out = (1 - w) * a + w * b
+    return out
 
 
 def rho_vjp(dm, phi, beta, gbar):
@@ -236,12 +264,14 @@ def _dilate_periodic(b):
 
 
 # --- topology (nlfiber/topology.py:8-63) ---------------------------------------------------------
-def periodic_label(b):
-    """Connected components of a periodic binary array (26-connectivity in 3D, 8 in 2D)."""
+def periodic_label(b, faces=False):
+    """Connected components of a periodic binary array (26-connectivity in 3D, 8 in 2D; with `faces`, the
+    face connectivity ndimage.generate_binary_structure(d, 1) that topology.py:90,116 uses for the void)."""
     b = np.asarray(b, dtype=bool)
     d = b.ndim
     p = np.pad(b, 1, mode="wrap")
-    lab, n = ndimage.label(p, structure=np.ones((3,) * d, dtype=bool))
+    st = ndimage.generate_binary_structure(d, 1) if faces else np.ones((3,) * d, dtype=bool)
+    lab, n = ndimage.label(p, structure=st)
     parent = np.arange(n + 1)
 
     def find(a):

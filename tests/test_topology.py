@@ -1,0 +1,72 @@
+"""CPU: the oracle's restatement of the binary map (nlfiber/density.py:96-149, nlfiber/topology.py:8-63) pinned to
+the reference's own tests of it (tests/test_core.py:55-75,145-157), and the host half of the GPU binarization:
+libnlf.so's numpy-"linear" quantile interpolation (nlf_quantile_linear, a host function) against np.quantile."""
+import ctypes
+
+import numpy as np
+
+from oracle import density_ref as OD
+
+
+def test_oracle_binary_volume_after_floating_removal():
+    """tests/test_core.py:55-67: the kept solid grows back to v (to one orbit of 48 voxels), nothing floats."""
+    kept = 0
+    for seed in range(8):
+        b = OD.DensityMap(8, 3, r=2.5, v=0.25).binary(OD.random_start(8, seed=seed, kmax=3), up=1)
+        if not b.any():
+            continue
+        kept += 1
+        assert abs(b.mean() - 0.25) * b.size <= 48
+        lab, n = OD.periodic_label(b)
+        assert all(OD._spanning(lab, k) for k in range(1, n + 1))
+    assert kept >= 2
+
+
+def test_oracle_binary_upsampled_volume_and_symmetry():
+    """tests/test_core.py:69-74: up = 2 doubles the side, keeps the volume to one orbit and the symmetry exact."""
+    b = OD.DensityMap(6, 3, r=1.5, v=0.3).binary(OD.schwarz_p_phi(6), up=2)
+    assert b.shape == (24,) * 3
+    assert abs(b.mean() - 0.3) < 48.0 / b.size
+    assert OD.sym_residual(b.astype(float)) < 1e-14
+
+
+def test_oracle_components():
+    """tests/test_core.py:145-157."""
+    b = np.zeros((6, 6, 6), bool)
+    b[:, 2, 2] = True
+    lab, n = OD.periodic_label(b)
+    assert n == 1 and not OD._spanning(lab, 1)
+    b[2, :, 2] = b[2, 2, :] = True
+    assert OD.remove_floating_pieces(b).sum() == b.sum()
+    b2 = b.copy()
+    b2[5, 5, 5] = True
+    assert OD.remove_floating_pieces(b2).sum() == b.sum()
+    # face connectivity splits diagonal neighbours
+    c = np.zeros((4, 4), bool)
+    c[0, 0] = c[1, 1] = True
+    assert OD.periodic_label(c)[1] == 1 and OD.periodic_label(c, faces=True)[1] == 2
+
+
+def test_oracle_upsample_keeps_linear_fields_periodic_mean():
+    """upsample_periodic is an interpolation: a constant stays constant, the mean of a cosine is kept."""
+    u = np.full((6, 6, 6), 0.7)
+    assert np.allclose(OD.upsample_periodic(u, 2), 0.7)
+    x = (np.arange(8) + 0.5) / 8
+    f = np.cos(2 * np.pi * x)[:, None] * np.ones((8, 8))
+    g = OD.upsample_periodic(f, 3)
+    assert g.shape == (24, 24) and abs(g.mean()) < 1e-12
+
+
+def test_quantile_linear_matches_numpy_bitwise():
+    from nlfiber_b200._lib import lib
+    rng = np.random.default_rng(0)
+    out = ctypes.c_double()
+    for t in range(600):
+        n = int(rng.integers(1, 400))
+        a = rng.standard_normal(n) * 10.0 ** rng.integers(-3, 4)
+        if t % 3 == 0:
+            a = np.round(a, 1)  # ties
+        a = np.sort(a)
+        for q in (0.0, 1.0, 0.5, 0.7, 0.75, float(rng.random()), 1.0 - float(rng.random()) * 1e-3):
+            assert lib.nlf_quantile_linear(n, q, a.ctypes.data, ctypes.byref(out)) == 0
+            assert out.value == np.quantile(a, q), (n, q)
