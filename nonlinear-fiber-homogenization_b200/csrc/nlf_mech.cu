@@ -11,11 +11,16 @@
 //   neo-Hookean: P = mu (F - F^-T) + lam lnJ F^-T,
 //                dP = mu dF + (mu - lam lnJ) F^-T dF^T F^-T + lam (F^-T : dF) F^-T.
 // Element forces go to a [24][N] buffer; a gather kernel sums the 8 contributions of each node in a fixed order.
+// Inside the Newton step's CG the state is fixed, so the CG computes the state-dependent part of dP once per solve
+// (k_mech_tan_cache: F_g^-T and mu - lam ln det F_g at every Gauss point, 80 doubles per element) and its matvec
+// (k_mech_hvp_tc) reads that instead of recomputing F, the inverse and the log; it also takes the direction's
+// gradients and forces in the element's mode form, and sums dP only at the free macro entries.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
+#include "nlf_element.cuh"
 #include "nlf_vec.cuh"
 #include "nlf_prof.cuh"
 
@@ -108,12 +113,10 @@ __device__ __forceinline__ void add_P_nh(const double (&F)[9], double lam, doubl
   for (int q = 0; q < 9; ++q) P[q] += c * (mu * (F[q] - G[q]) + lam * lnJ * G[q]);
 }
 
-__device__ __forceinline__ void add_dP_nh(const double (&F)[9], const double (&d)[9], double lam, double mu,
-                                          double c, double (&P)[9]) {
-  const double J = det3(F);
-  double G[9];
-  inv_t3(F, J, G);
-  const double lnJ = log(J);
+// dP += c (mu dF + cm G dF^T G + lam (G : dF) G) with G = F^-T and cm = mu - lam lnJ given (the tangent cache of
+// the CG holds them per Gauss point; add_dP_nh computes them from F)
+__device__ __forceinline__ void add_dP_nh_g(const double (&G)[9], double cm, const double (&d)[9], double lam,
+                                            double mu, double c, double (&P)[9]) {
   double GdF = 0.0;
 #pragma unroll
   for (int q = 0; q < 9; ++q) GdF += G[q] * d[q];
@@ -123,7 +126,6 @@ __device__ __forceinline__ void add_dP_nh(const double (&F)[9], const double (&d
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int l = 0; l < 3; ++l) M[i * 3 + l] = G[i * 3] * d[l * 3] + G[i * 3 + 1] * d[l * 3 + 1] + G[i * 3 + 2] * d[l * 3 + 2];
-  const double cm = mu - lam * lnJ;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -131,6 +133,20 @@ __device__ __forceinline__ void add_dP_nh(const double (&F)[9], const double (&d
       const double T = M[i * 3] * G[j] + M[i * 3 + 1] * G[3 + j] + M[i * 3 + 2] * G[6 + j];
       P[i * 3 + j] += c * (mu * d[i * 3 + j] + cm * T + lam * GdF * G[i * 3 + j]);
     }
+}
+
+// G = F^-T and cm = mu - lam ln det F
+__device__ __forceinline__ void nh_point(const double (&F)[9], double lam, double mu, double (&G)[9], double& cm) {
+  const double J = det3(F);
+  inv_t3(F, J, G);
+  cm = mu - lam * log(J);
+}
+
+__device__ __forceinline__ void add_dP_nh(const double (&F)[9], const double (&d)[9], double lam, double mu,
+                                          double c, double (&P)[9]) {
+  double G[9], cm;
+  nh_point(F, lam, mu, G, cm);
+  add_dP_nh_g(G, cm, d, lam, mu, c, P);
 }
 
 // psi_eff, P_eff, dP_eff (mech.py:134-139) at one Gauss point, scaled by c = wq s
@@ -178,10 +194,36 @@ __device__ __forceinline__ void add_dP_eff(const MechDev& a, const double (&F)[9
   add_dsig_lin(d, a.lam, a.mu, c * (1.0 - gam * gam), P);
 }
 
+// the neo-Hookean point quantities of the tangent at F: G = F_g^-T and cm = mu - lam ln det F_g of the WLS
+// argument F_g = I + gamma (F - I) (F itself without WLS)
+__device__ __forceinline__ void tan_point(const MechDev& a, const double (&F)[9], double gam, double (&G)[9],
+                                          double& cm) {
+  if (!a.use_gamma) {
+    nh_point(F, a.lam, a.mu, G, cm);
+    return;
+  }
+  double Fg[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Fg[q] = (q % 4 == 0 ? 1.0 : 0.0) + gam * (F[q] - (q % 4 == 0 ? 1.0 : 0.0));
+  nh_point(Fg, a.lam, a.mu, G, cm);
+}
+
+// add_dP_eff of the neo-Hookean material from the cached point quantities (G, cm)
+__device__ __forceinline__ void add_dP_eff_g(const MechDev& a, const double (&G)[9], double cm, const double (&d)[9],
+                                             double gam, double c, double (&P)[9]) {
+  if (!a.use_gamma) {
+    add_dP_nh_g(G, cm, d, a.lam, a.mu, c, P);
+    return;
+  }
+  add_dP_nh_g(G, cm, d, a.lam, a.mu, c * gam * gam, P);
+  add_dsig_lin(d, a.lam, a.mu, c * (1.0 - gam * gam), P);
+}
+
 // ---- element kernel ------------------------------------------------------------------------------------------
 // MODE 0: energy, element forces of P, sum of P (10 partials); 1: element forces of dP, sum of dP (9);
 // 2: energy only (1). Vectors are SoA [3][N]; fe is [24][N] (dof 3a + c of the element's node a).
 constexpr int kMechThreads = 128;
+constexpr int kTanCache = 10;  // cached doubles per Gauss point: G = F_g^-T (9), cm
 
 template <int MODE>
 __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const double* __restrict__ w,
@@ -189,7 +231,8 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
                                                             const double* __restrict__ v,
                                                             const double* __restrict__ dFm,
                                                             double* __restrict__ fe, double* __restrict__ partial) {
-  constexpr int NP = MODE == 0 ? 10 : (MODE == 1 ? 9 : 1);
+  constexpr bool TAN = MODE == 1;
+  constexpr int NP = MODE == 0 ? 10 : (TAN ? 9 : 1);
   __shared__ double red[32 * NP];
   double acc[NP];
 #pragma unroll
@@ -198,7 +241,7 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
     Fb[q] = Fbar[q];
-    dM[q] = MODE == 1 ? dFm[q] : 0.0;
+    dM[q] = TAN ? dFm[q] : 0.0;
   }
   const long N = a.N;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < N; e += (long)gridDim.x * blockDim.x) {
@@ -215,7 +258,7 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
 #pragma unroll
       for (int q = 0; q < 8; ++q) wn[c][q] = w[c * N + nid[q]];
     double vn[3][8];
-    if (MODE == 1) {
+    if (TAN) {
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -245,7 +288,7 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
       for (int q = 0; q < 9; ++q) P[q] = 0.0;
       if (MODE == 0 || MODE == 2) acc[0] += cs * psi_eff(a, F, gam);
       if (MODE == 0) add_P_eff(a, F, gam, cs, P);
-      if (MODE == 1) {
+      if (TAN) {
         double dF[9];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -279,6 +322,49 @@ __global__ void __launch_bounds__(kMechThreads) k_mech_elem(MechDev a, const dou
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < NP; ++q) partial[(long)blockIdx.x * NP + q] = acc[q];
+  }
+}
+
+// Tangent cache of a CG solve at the state (w, Fbar) of the neo-Hookean material: G = F_g^-T and
+// cm = mu - lam ln det F_g at each Gauss point of each element, tc[(g kTanCache + q) N + e], computed once instead
+// of in every matvec (F, F_g, det, the inverse and the log are fixed while the CG runs).
+__global__ void __launch_bounds__(kMechThreads) k_mech_tan_cache(MechDev a, const double* __restrict__ w,
+                                                                 const double* __restrict__ Fbar,
+                                                                 double* __restrict__ tc) {
+  double Fb[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Fb[q] = Fbar[q];
+  const long N = a.N;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < N; e += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % a.n2), j = (int)((e / a.n2) % a.n1), i = (int)(e / ((long)a.n1 * a.n2));
+    const long ip = (i + 1 == a.n0 ? 0 : i + 1), jp = (j + 1 == a.n1 ? 0 : j + 1), kp = (k + 1 == a.n2 ? 0 : k + 1);
+    double wn[3][8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long nid = (((q & 1) ? ip : i) * a.n1 + (((q >> 1) & 1) ? jp : j)) * a.n2 + ((q >> 2) ? kp : k);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) wn[c][q] = w[c * N + nid];
+    }
+    const double gam = a.use_gamma ? a.gamma[e] : 1.0;
+#pragma unroll 1
+    for (int g = 0; g < 8; ++g) {
+      double F[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double h = 0.0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h += wn[c][q] * cDN[g][q][d];
+          F[c * 3 + d] = Fb[c * 3 + d] + h;
+        }
+      double G[9], cm;
+      tan_point(a, F, gam, G, cm);
+      double* t = tc + (long)g * kTanCache * N + e;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) t[q * N] = G[q];
+      t[9 * N] = cm;
+    }
   }
 }
 
@@ -620,6 +706,132 @@ struct FreeIdx {
   int ab[9];
 };
 
+// Tangent matvec of the CG from the tangent cache (k_mech_tan_cache, neo-Hookean material): the element forces of
+// dP for the direction (v, dFm) and the sums of dP at the first KF free macro entries fi.ab (partial rows of 9, the
+// other entries 0; k_cg_aptail reads the free ones). Only the free macro entries are summed: the CG's tail needs no
+// others.
+//
+// The direction's gradient and the element forces are taken in the mode form of the trilinear element (as in the
+// linear operator, nlf_element.cuh): the butterfly c = H v of the 8 nodal values gives u = sum_p c_p 2^-z(p)
+// prod_{d in p} X_d on X in [-1/2, 1/2]^3 (z(p) the zero bits of p), so at a Gauss point X = (sx, sy, sz) h,
+// h = 1 / (2 sqrt 3):
+//   du/dx = k1 + sy k3 + sz k5 + sy sz k7,  du/dy = k2 + sx k3 + sz k6 + sx sz k7,  du/dz = k4 + sx k5 + sy k6 + sx sy k7
+// with k1,2,4 = c / 4, k3,5,6 = c h / 2, k7 = c h^2. The macro direction is the linear field dFm X, whose modes are
+// k1,2,4 += dFm[.][x, y, z]. The forces are the transpose: signed sums of P over the Gauss points per mode, scaled
+// the same way, then the transposed butterfly f = H^T m.
+template <int KF>
+__global__ void __launch_bounds__(kMechThreads, 3) k_mech_hvp_tc(MechDev a, const double* __restrict__ v,
+                                                                 const double* __restrict__ dFm, FreeIdx fi,
+                                                                 double* __restrict__ fe,
+                                                                 double* __restrict__ partial,
+                                                                 const double* __restrict__ tc) {
+  constexpr int NA = KF > 0 ? KF : 1;
+  constexpr double h = 0.28867513459481288225;  // 1 / (2 sqrt 3)
+  __shared__ double red[32 * NA];
+  double acc[NA];
+#pragma unroll
+  for (int j = 0; j < NA; ++j) acc[j] = 0.0;
+  const long N = a.N;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < N; e += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % a.n2), j = (int)((e / a.n2) % a.n1), i = (int)(e / ((long)a.n1 * a.n2));
+    const long ip = (i + 1 == a.n0 ? 0 : i + 1), jp = (j + 1 == a.n1 ? 0 : j + 1), kp = (k + 1 == a.n2 ? 0 : k + 1);
+    double km[3][8];  // scaled modes k1..k7 of each component (km[c][0] unused)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long nid = (((q & 1) ? ip : i) * a.n1 + (((q >> 1) & 1) ? jp : j)) * a.n2 + ((q >> 2) ? kp : k);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) km[c][q] = v[c * N + nid];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      butterfly8(km[c]);
+      km[c][1] = 0.25 * km[c][1] + dFm[c * 3];
+      km[c][2] = 0.25 * km[c][2] + dFm[c * 3 + 1];
+      km[c][4] = 0.25 * km[c][4] + dFm[c * 3 + 2];
+      km[c][3] *= 0.5 * h;
+      km[c][5] *= 0.5 * h;
+      km[c][6] *= 0.5 * h;
+      km[c][7] *= h * h;
+    }
+    const double cs = a.wq * a.s[e];
+    const double gam = a.use_gamma ? a.gamma[e] : 1.0;
+    double nm[3][8];  // signed sums of P per mode (nm[c][0] unused)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) nm[c][q] = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < 8; ++g) {
+      const double sx = (g & 1) ? 1.0 : -1.0, sy = ((g >> 1) & 1) ? 1.0 : -1.0, sz = (g >> 2) ? 1.0 : -1.0;
+      const double syz = sy * sz, sxz = sx * sz, sxy = sx * sy;
+      double dF[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dF[c * 3] = km[c][1] + sy * km[c][3] + sz * km[c][5] + syz * km[c][7];
+        dF[c * 3 + 1] = km[c][2] + sx * km[c][3] + sz * km[c][6] + sxz * km[c][7];
+        dF[c * 3 + 2] = km[c][4] + sx * km[c][5] + sy * km[c][6] + sxy * km[c][7];
+      }
+      const double* t = tc + (long)g * kTanCache * N + e;
+      double G[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) G[q] = t[q * N];
+      double P[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) P[q] = 0.0;
+      add_dP_eff_g(a, G, t[9 * N], dF, gam, cs, P);
+#pragma unroll
+      for (int jf = 0; jf < KF; ++jf) {
+        double pj = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) pj = (q == fi.ab[jf]) ? P[q] : pj;
+        acc[jf] += pj;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double px = P[c * 3], py = P[c * 3 + 1], pz = P[c * 3 + 2];
+        nm[c][1] += px;
+        nm[c][2] += py;
+        nm[c][4] += pz;
+        nm[c][3] += sy * px + sx * py;
+        nm[c][5] += sz * px + sx * pz;
+        nm[c][6] += sz * py + sy * pz;
+        nm[c][7] += syz * px + sxz * py + sxy * pz;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      nm[c][0] = 0.0;
+      nm[c][1] *= 0.25;
+      nm[c][2] *= 0.25;
+      nm[c][4] *= 0.25;
+      nm[c][3] *= 0.5 * h;
+      nm[c][5] *= 0.5 * h;
+      nm[c][6] *= 0.5 * h;
+      nm[c][7] *= h * h;
+      butterfly8_t(nm[c]);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) fe[(long)(3 * q + c) * N + e] = nm[c][q];
+  }
+  if constexpr (KF > 0) {
+    block_sum<NA>(acc, red);
+    if (threadIdx.x == 0) {
+      double row[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) row[q] = 0.0;
+#pragma unroll
+      for (int jf = 0; jf < KF; ++jf)
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+          if (q == fi.ab[jf]) row[q] = acc[jf];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) partial[(long)blockIdx.x * 9 + q] = row[q];
+    }
+  }
+}
+
 // dFm (9, row-major) = sum_j p_tail[j] e_(a_j b_j): the macro part of the CG direction enters the element pass
 __global__ void k_cg_dfm(const double* __restrict__ ptail, FreeIdx f, double* __restrict__ dfm) {
   const int q = threadIdx.x;
@@ -728,6 +940,33 @@ int mech_pass(nlf_mech* H, const double* w, const double* Fb, const double* v, c
   *nb = blocks;
   ProfScope ps(PK_MECH_ELEM, st);
   k_mech_elem<MODE><<<blocks, kMechThreads, 0, st>>>(H->d, w, Fb, v, dFm, fe, partial);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// the tangent cache of a CG solve at (w, Fbar) (neo-Hookean material only)
+int tan_cache(nlf_mech* H, const double* w, const double* Fb, double* tc, cudaStream_t st) {
+  const long N = H->d.N;
+  const int blocks = (int)std::min<long>((N + kMechThreads - 1) / kMechThreads, 4L * 148 * 4);
+  ProfScope ps(PK_MECH_TANC, st);
+  k_mech_tan_cache<<<blocks, kMechThreads, 0, st>>>(H->d, w, Fb, tc);
+  NLF_CHECK_LAUNCH();
+  return NLF_OK;
+}
+
+// the CG's tangent matvec from the cache; the free macro entries' sums of dP go to partial rows of 9
+int hvp_cached(nlf_mech* H, const double* v, const double* dFm, const FreeIdx& fi, double* fe, double* partial,
+               int* nb, const double* tc, cudaStream_t st) {
+  const long N = H->d.N;
+  const int blocks = (int)std::min<long>((N + kMechThreads - 1) / kMechThreads, 4L * 148 * 4);
+  *nb = blocks;
+  ProfScope ps(PK_MECH_ELEM, st);
+  if (fi.k == 0)
+    k_mech_hvp_tc<0><<<blocks, kMechThreads, 0, st>>>(H->d, v, dFm, fi, fe, partial, tc);
+  else if (fi.k <= 2)
+    k_mech_hvp_tc<2><<<blocks, kMechThreads, 0, st>>>(H->d, v, dFm, fi, fe, partial, tc);
+  else
+    k_mech_hvp_tc<9><<<blocks, kMechThreads, 0, st>>>(H->d, v, dFm, fi, fe, partial, tc);
   NLF_CHECK_LAUNCH();
   return NLF_OK;
 }
@@ -868,7 +1107,8 @@ NLF_API int nlf_mech_set_rho(nlf_mech* H, const double* rho, double* s_out, doub
     const int nblk = (int)std::min<long>(4 * 148, (N + kToecWarps - 1) / kToecWarps);
     const size_t te = al(18 * N * 8) + al((size_t)nblk * kToecOut * 8) + al(kToecOut * 8);
     const size_t cgw = V + 5 * Lz + V + al(24 * N * 8) + al(3 * lin_of(H).g.NS * 16) + part +
-                       al(3 * (size_t)H->d.n0 * 4 * 8) + al(256) + al(sizeof(MechCG));
+                       al(3 * (size_t)H->d.n0 * 4 * 8) + al(256) + al(sizeof(MechCG)) +
+                       (H->d.material == 1 ? al((size_t)8 * kTanCache * N * 8) : 0);
     NLF_TRY(H->ws.reserve(std::max(std::max(eh, gw), std::max(te, cgw))));
     NLF_TRY(H->io.reserve(std::max(al(18 * N * 8), 2 * Lz)));
   }
@@ -1185,6 +1425,8 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
                o_ap = take(Lz * 8), o_zf = take(3 * N * 8), o_z0 = take(Lz * 8), o_fe = take(24 * N * 8),
                o_sp = take(3 * L.g.NS * 16), o_pa = take(4096 * 10 * 8), o_pc = take(3 * L.g.n0 * 4 * 8),
                o_fb = take(256), o_st = take(sizeof(MechCG));
+  const bool cached = H->d.material == 1;
+  const size_t o_tc = cached ? take((size_t)8 * kTanCache * N * 8) : 0;
   NLF_TRY(H->ws.reserve(off));
   NLF_TRY(H->io.reserve(2 * al(Lz * 8)));
   char* B = (char*)H->ws.ptr;
@@ -1201,6 +1443,7 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
   double* ppc = reinterpret_cast<double*>(B + o_pc);
   double* fbd = reinterpret_cast<double*>(B + o_fb);
   MechCG* stt = reinterpret_cast<MechCG*>(B + o_st);
+  double* tc = cached ? reinterpret_cast<double*>(B + o_tc) : nullptr;
   // inputs: w -> SoA; b -> r (SoA w part + tail)
   const double *wd = nullptr, *bd = nullptr;
   NLF_TRY(stage(w, 3 * N, H->io, 0, &wd, st));
@@ -1209,6 +1452,7 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
   NLF_TRY((launch_aos_to_soa<double, double>(N, 1, bd, r, 1.0, st)));
   if (k) NLF_CUDA_TRY(cudaMemcpyAsync(r + 3 * N, bd + 3 * N, k * 8, cudaMemcpyDeviceToDevice, st));
   NLF_CUDA_TRY(cudaMemcpyAsync(fbd, Fbar, 72, on_dev(Fbar) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  if (cached) NLF_TRY(tan_cache(H, ws, fbd, tc, st));
   MechCG hs;
   std::memset(&hs, 0, sizeof(hs));
   hs.k = k;
@@ -1242,7 +1486,10 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
       k_cg_clear_ran<<<1, 1, 0, s>>>(stt);
       // Ap = H p; the macro part of p enters as dFm (fbd[9..17])
       k_cg_dfm<<<1, 32, 0, s>>>(p + 3 * N, fi, fbd + 9);
-      NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, s));
+      if (cached)
+        NLF_TRY(hvp_cached(H, p, fbd + 9, fi, fe, part, &nb, tc, s));
+      else
+        NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, s));
       double* sum9 = part + 4096 * 9;
       k_mech_sum<<<1, 32, 0, s>>>(part, nb, 9, sum9);
       NLF_TRY(gather(H, fe, Ap, s));

@@ -38,7 +38,8 @@ const char* kNames[PK_COUNT] = {"apply_f32", "apply_f64", "fft_a_f32", "fft_b_f3
                                 "fft_a_f64", "fft_b_f64", "fft_c_f64", "p_update",
                                 "stats",     "finalize",  "bilinear",  "load",      "other",
                                 "unet_conv", "unet_wgrad", "unet_misc", "mech_elem", "mech_gather",
-                                "dens_filter", "dens_var", "dens_fold", "dens_eta", "dens_rho", "dens_vjp"};
+                                "dens_filter", "dens_var", "dens_fold", "dens_eta", "dens_rho", "dens_vjp",
+                                "mech_tan_cache"};
 }  // namespace
 
 bool prof_on() { return g_on; }

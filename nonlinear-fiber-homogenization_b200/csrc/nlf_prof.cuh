@@ -9,7 +9,7 @@ namespace nlf {
 enum ProfKind {
   PK_APPLY32 = 0, PK_APPLY64, PK_FFTA32, PK_FFTB32, PK_FFTC32, PK_FFTA64, PK_FFTB64, PK_FFTC64,
   PK_P, PK_STATS, PK_FIN, PK_BILINEAR, PK_LOAD, PK_OTHER, PK_UNET_CONV, PK_UNET_WGRAD,
-  PK_UNET_MISC, PK_MECH_ELEM, PK_MECH_GATHER, PK_DENS_FILTER, PK_DENS_VAR, PK_DENS_FOLD, PK_DENS_ETA, PK_DENS_RHO, PK_DENS_VJP, PK_COUNT
+  PK_UNET_MISC, PK_MECH_ELEM, PK_MECH_GATHER, PK_DENS_FILTER, PK_DENS_VAR, PK_DENS_FOLD, PK_DENS_ETA, PK_DENS_RHO, PK_DENS_VJP, PK_MECH_TANC, PK_COUNT
 };
 
 bool prof_on();

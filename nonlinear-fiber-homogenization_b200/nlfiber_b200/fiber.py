@@ -6,6 +6,8 @@ Value: the density map (libnlf.so nlf_density_rho), the cubic two-case corrector
 (nlf_linear_solve, nlf_bilinear). Jacobian rows: dc_k/drho with the correctors held fixed (nlf_dC_drho, exact
 because the correctors are stationary), pulled back through the density map (nlf_density_vjp) -- the three
 VJPs of the reference's `value_and_jac` (fiber.py:34-39), without JAX. Cubic (d = 3) and square (d = 2) cells.
+Binary check (fiber.py:62-81): the binary cell of the density map on the GPU (GpuDensityMap.binary, floating
+pieces removed), re-solved.
 """
 import numpy as np
 
