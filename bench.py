@@ -694,9 +694,10 @@ def mech_arm(args, stream):
     _lib.profile(False)
     N = n ** 3
     el = prof.get("mech_elem", (0.0, 0, 0))
-    # tangent matvec bytes per voxel (FP64): v in and the element forces out (3 + 24 doubles: the forces of the
-    # 8 corners go to a per-element array that the gather sums), state w (3), s and gamma (2)
-    hvp_bytes = N * 8 * (3 + 24 + 3 + 2)
+    # the CG's tangent matvec (k_mech_hvp_tc) bytes per voxel (FP64): v in and the element forces out (3 + 24
+    # doubles: the forces of the 8 corners go to a per-element array that the gather sums), the tangent cache
+    # (8 Gauss points x 10 doubles), s and gamma (2)
+    hvp_bytes = N * 8 * (3 + 24 + 80 + 2)
     kernels = {k: {"ms": round(v[0], 2), "launches": v[1]} for k, v in prof.items() if v[1]}
     kernels["profiled_step_cg_iterations"] = int(plog["cg"])
     stab = None

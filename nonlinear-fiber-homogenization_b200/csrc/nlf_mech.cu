@@ -719,6 +719,17 @@ struct FreeIdx {
 // with k1,2,4 = c / 4, k3,5,6 = c h / 2, k7 = c h^2. The macro direction is the linear field dFm X, whose modes are
 // k1,2,4 += dFm[.][x, y, z]. The forces are the transpose: signed sums of P over the Gauss points per mode, scaled
 // the same way, then the transposed butterfly f = H^T m.
+// asynchronous copy of one double global -> shared (through L1), and the waits for this thread's copy groups
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
 template <int KF>
 __global__ void __launch_bounds__(kMechThreads, 3) k_mech_hvp_tc(MechDev a, const double* __restrict__ v,
                                                                  const double* __restrict__ dFm, FreeIdx fi,
@@ -728,6 +739,10 @@ __global__ void __launch_bounds__(kMechThreads, 3) k_mech_hvp_tc(MechDev a, cons
   constexpr int NA = KF > 0 ? KF : 1;
   constexpr double h = 0.28867513459481288225;  // 1 / (2 sqrt 3)
   __shared__ double red[32 * NA];
+  // the cache entries of the next Gauss point are copied into this thread's own slots while the current one is
+  // computed (each thread reads only what it copied, so its own wait suffices: no barrier)
+  __shared__ double stage[2][kTanCache][kMechThreads];
+  const int tid = threadIdx.x;
   double acc[NA];
 #pragma unroll
   for (int j = 0; j < NA; ++j) acc[j] = 0.0;
@@ -753,6 +768,12 @@ __global__ void __launch_bounds__(kMechThreads, 3) k_mech_hvp_tc(MechDev a, cons
       km[c][6] *= 0.5 * h;
       km[c][7] *= h * h;
     }
+    {
+      const double* t0 = tc + e;
+#pragma unroll
+      for (int q = 0; q < kTanCache; ++q) cp_async8(&stage[0][q][tid], t0 + (long)q * N);
+      cp_async_commit_group();
+    }
     const double cs = a.wq * a.s[e];
     const double gam = a.use_gamma ? a.gamma[e] : 1.0;
     double nm[3][8];  // signed sums of P per mode (nm[c][0] unused)
@@ -771,14 +792,23 @@ __global__ void __launch_bounds__(kMechThreads, 3) k_mech_hvp_tc(MechDev a, cons
         dF[c * 3 + 1] = km[c][2] + sx * km[c][3] + sz * km[c][6] + sxz * km[c][7];
         dF[c * 3 + 2] = km[c][4] + sx * km[c][5] + sy * km[c][6] + sxy * km[c][7];
       }
-      const double* t = tc + (long)g * kTanCache * N + e;
+      if (g + 1 < 8) {
+        const double* tn = tc + (long)(g + 1) * kTanCache * N + e;
+#pragma unroll
+        for (int q = 0; q < kTanCache; ++q) cp_async8(&stage[(g + 1) & 1][q][tid], tn + (long)q * N);
+        cp_async_commit_group();
+        cp_async_wait_group<1>();  // this Gauss point's copies are done, the next one's may still be in flight
+      } else {
+        cp_async_wait_group<0>();
+      }
       double G[9];
 #pragma unroll
-      for (int q = 0; q < 9; ++q) G[q] = t[q * N];
+      for (int q = 0; q < 9; ++q) G[q] = stage[g & 1][q][tid];
+      const double cmg = stage[g & 1][9][tid];
       double P[9];
 #pragma unroll
       for (int q = 0; q < 9; ++q) P[q] = 0.0;
-      add_dP_eff_g(a, G, t[9 * N], dF, gam, cs, P);
+      add_dP_eff_g(a, G, cmg, dF, gam, cs, P);
 #pragma unroll
       for (int jf = 0; jf < KF; ++jf) {
         double pj = 0.0;
