@@ -385,13 +385,26 @@ __global__ void k_mech_gather(long N, int n0, int n1, int n2, const double* __re
   for (int c = 0; c < 3; ++c) out[c * N + n] = o[c];
 }
 
-// sum of nb partial rows of width np into out[np] (one block, fixed order)
-__global__ void k_mech_sum(const double* __restrict__ partial, int nb, int np, double* __restrict__ out) {
-  for (int q = threadIdx.x; q < np; q += blockDim.x) {
-    double a = 0.0;
-    for (int b = 0; b < nb; ++b) a += partial[(long)b * np + q];
-    out[q] = a;
-  }
+// sum of nb partial rows of width NP into out[NP]
+// (one block of kSumThreads: thread t adds rows t, t + kSumThreads, ... of every column, then the block adds the
+// threads' sums in a fixed order, so the result does not depend on timing; a single thread per column would walk
+// the nb rows as one chain of dependent loads)
+constexpr int kSumThreads = 256;
+
+template <int NP>
+__global__ void __launch_bounds__(kSumThreads) k_mech_sum(const double* __restrict__ partial, int nb,
+                                                          double* __restrict__ out) {
+  __shared__ double red[32 * NP];
+  double a[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q) a[q] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += kSumThreads)
+#pragma unroll
+    for (int q = 0; q < NP; ++q) a[q] += partial[(long)b * NP + q];
+  block_sum<NP>(a, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < NP; ++q) out[q] = a[q];
 }
 
 __global__ void k_mech_scale(int n0, int n1, int n2, const double* __restrict__ rho, double emin, double p,
@@ -1173,10 +1186,10 @@ NLF_API int nlf_mech_energy(nlf_mech* H, const double* w, const double* Fbar, do
   const bool want_g = gw || P;
   if (want_g) {
     NLF_TRY(mech_pass<0>(H, ws, fbd, nullptr, nullptr, fe, part, &nb, st));
-    k_mech_sum<<<1, 32, 0, st>>>(part, nb, 10, sum);
+    k_mech_sum<10><<<1, kSumThreads, 0, st>>>(part, nb, sum);
   } else {
     NLF_TRY(mech_pass<2>(H, ws, fbd, nullptr, nullptr, nullptr, part, &nb, st));
-    k_mech_sum<<<1, 32, 0, st>>>(part, nb, 1, sum);
+    k_mech_sum<1><<<1, kSumThreads, 0, st>>>(part, nb, sum);
   }
   NLF_CHECK_LAUNCH();
   double h[10];
@@ -1224,7 +1237,7 @@ NLF_API int nlf_mech_hvp(nlf_mech* H, const double* w, const double* Fbar, const
   double* sum = reinterpret_cast<double*>(b + o_sum);
   int nb = 0;
   NLF_TRY(mech_pass<1>(H, ws, fbd, vs, fbd + 9, fe, part, &nb, st));
-  k_mech_sum<<<1, 32, 0, st>>>(part, nb, 9, sum);
+  k_mech_sum<9><<<1, kSumThreads, 0, st>>>(part, nb, sum);
   NLF_CHECK_LAUNCH();
   double* os = reinterpret_cast<double*>(b + o_os);
   NLF_TRY(gather(H, fe, os, st));
@@ -1521,7 +1534,7 @@ NLF_API int nlf_mech_cg(nlf_mech* H, const double* w, const double* Fbar, int k,
       else
         NLF_TRY(mech_pass<1>(H, ws, fbd, p, fbd + 9, fe, part, &nb, s));
       double* sum9 = part + 4096 * 9;
-      k_mech_sum<<<1, 32, 0, s>>>(part, nb, 9, sum9);
+      k_mech_sum<9><<<1, kSumThreads, 0, s>>>(part, nb, sum9);
       NLF_TRY(gather(H, fe, Ap, s));
       if (k) k_cg_aptail<<<1, 32, 0, s>>>(sum9, fi, Ap + 3 * N);
       // proj(Ap) and pAp
