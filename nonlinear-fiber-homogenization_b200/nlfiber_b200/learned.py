@@ -27,14 +27,16 @@ class UNet:
         h = ctypes.c_void_p()
         check(lib.nlf_unet_create(ctypes.byref(h), *(int(w) for w in widths), int(seed)))
         self._h = h
+        self._lib = lib
         self.widths = tuple(int(w) for w in widths)
         self.n_params = int(lib.nlf_unet_param_count(h))
         self.stream = None
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib.nlf_unet_destroy(h)
+        lb = getattr(self, "_lib", None)  # the module global may be gone while the interpreter shuts down
+        if h is not None and h.value and lb is not None:
+            lb.nlf_unet_destroy(h)
             self._h = None
 
     def get_params(self):

@@ -120,6 +120,7 @@ class LinearHomogenization:
         check(lib.nlf_linear_create(ctypes.byref(h), *self.shape, self.E, self.nu, self.emin, self.p, self.tol,
                                     self.maxit))
         self._h = h
+        self._lib = lib
         self._Kinv = None
         self.stream = None  # cudaStream_t handle (int) used by every call; None = the legacy default stream
         if autotune:
@@ -177,8 +178,9 @@ class LinearHomogenization:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib.nlf_linear_destroy(h)
+        lb = getattr(self, "_lib", None)  # the module global may be gone while the interpreter shuts down
+        if h is not None and h.value and lb is not None:
+            lb.nlf_linear_destroy(h)
             self._h = None
 
     # --- options ---------------------------------------------------------------------------------------------

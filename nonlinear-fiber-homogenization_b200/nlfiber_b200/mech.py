@@ -123,6 +123,7 @@ class Cell:
         check(lib.nlf_mech_create(ctypes.byref(h), *self.shape, float(E), float(nu), MATERIALS.index(material), b,
                                   r0, float(emin), float(p)))
         self._h = h
+        self._lib = lib
         self.stream = stream  # CUDA stream (cudaStream_t as an int) of every call of this cell; None: the default
         self.s = np.empty(self.shape)
         gam = np.empty(self.shape) if wls is not None else None
@@ -133,8 +134,9 @@ class Cell:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            lib.nlf_mech_destroy(h)
+        lb = getattr(self, "_lib", None)  # the module global may be gone while the interpreter shuts down
+        if h is not None and h.value and lb is not None:
+            lb.nlf_mech_destroy(h)
             self._h = None
 
     def scale_of(self, rho):
