@@ -1,6 +1,7 @@
 """CPU: the oracle's restatement of the binary map (nlfiber/density.py:96-149, nlfiber/topology.py:8-63) pinned to
 the reference's own tests of it (tests/test_core.py:55-75,145-157), and the host half of the GPU binarization:
-libnlf.so's numpy-"linear" quantile interpolation (nlf_quantile_linear, a host function) against np.quantile."""
+libnlf.so's numpy-"linear" quantile interpolation (nlf_quantile_linear, a host function) against np.quantile,
+the entry points' argument checks (before any CUDA call) and the connectivity structures periodic_label takes."""
 import ctypes
 
 import numpy as np
@@ -70,3 +71,42 @@ def test_quantile_linear_matches_numpy_bitwise():
         for q in (0.0, 1.0, 0.5, 0.7, 0.75, float(rng.random()), 1.0 - float(rng.random()) * 1e-3):
             assert lib.nlf_quantile_linear(n, q, a.ctypes.data, ctypes.byref(out)) == 0
             assert out.value == np.quantile(a, q), (n, q)
+
+
+def test_binary_entry_points_reject_bad_arguments_without_a_device():
+    """The binary-cell entry points check their arguments before any CUDA call (status -1, message set)."""
+    from nlfiber_b200._lib import NLF_EBADARG, lib
+    h = ctypes.c_void_p()
+    assert lib.nlf_topo_create(ctypes.byref(h), 4, 8) == NLF_EBADARG
+    assert lib.nlf_topo_create(ctypes.byref(h), 3, 0) == NLF_EBADARG
+    assert lib.nlf_topo_create(ctypes.byref(h), 3, 2048) == NLF_EBADARG  # 2^33 voxels
+    assert lib.nlf_topo_create(None, 3, 8) == NLF_EBADARG
+    assert b"nlf_topo_create" in lib.nlf_last_error()
+    out = ctypes.c_double()
+    assert lib.nlf_topo_binary(None, None, 0.3, 1, None, None, None) == NLF_EBADARG
+    assert lib.nlf_topo_select(None, None, None, 0, ctypes.byref(out), None) == NLF_EBADARG
+    assert lib.nlf_topo_label(None, None, 0, None, None, None) == NLF_EBADARG
+    assert lib.nlf_topo_remove_floating(None, None, None, None, None, None) == NLF_EBADARG
+    u = np.zeros(8)
+    assert lib.nlf_upsample_sym(4, 2, 4, u.ctypes.data, u.ctypes.data, None) == NLF_EBADARG
+    assert lib.nlf_upsample_sym(3, 2, 1, u.ctypes.data, u.ctypes.data, None) == NLF_EBADARG
+    assert lib.nlf_quantile_linear(0, 0.5, u.ctypes.data, ctypes.byref(out)) == NLF_EBADARG
+    assert lib.nlf_quantile_linear(3, float("nan"), u.ctypes.data, ctypes.byref(out)) == NLF_EBADARG
+
+
+def test_connectivity_structures():
+    """nlfiber/topology.py:8 periodic_label(b, connectivity): the full neighbourhood (None or all ones) or the
+    face structure; anything else is refused."""
+    from scipy import ndimage
+    from nlfiber_b200.topology import _structure_faces
+    b = np.zeros((4, 4, 4), bool)
+    assert _structure_faces(b, None) is False
+    assert _structure_faces(b, np.ones((3, 3, 3), bool)) is False
+    assert _structure_faces(b, ndimage.generate_binary_structure(3, 1)) is True
+    assert _structure_faces(np.zeros((5, 5), bool), ndimage.generate_binary_structure(2, 1)) is True
+    try:
+        _structure_faces(b, ndimage.generate_binary_structure(3, 2))
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("edge connectivity must be refused")
