@@ -203,8 +203,76 @@ def tangent32_study(n_o, seeds, e=0.01):
     return out
 
 
+def _norms(v):
+    return np.sqrt((v * v).sum(axis=(1, 2, 3, 4)))
+
+
+def _orth(V, drop=1e-14):
+    """Orthonormal basis of the vectors V[k] (a Gram eigen-decomposition; directions whose squared singular value is
+    below `drop` times the largest are dropped: the rank-revealing step of breakdown-free block CG)."""
+    k = V.shape[0]
+    Vf = V.reshape(k, -1)
+    w, Q = np.linalg.eigh(Vf @ Vf.T)
+    keep = w > drop * w.max()
+    T = Q[:, keep] / np.sqrt(w[keep])
+    return (T.T @ Vf).reshape((int(keep.sum()),) + V.shape[1:])
+
+
+def block_pcg(lh, s, b, M, tol, maxit):
+    """Breakdown-free block PCG (Ji & Li 2017, after O'Leary 1980) over the m load cases of one cell, which share
+    the operator: one block Krylov space for all cases, the search block orthonormalized (rank-revealing) every
+    iteration. Mean-free projection, preconditioner and stopping rule (every case ||r|| <= tol ||b||) as the
+    lock-step PCG. Returns (x, iterations, matvecs)."""
+    P = OL.proj
+    b = P(b)
+    m = b.shape[0]
+    bn = _norms(b)
+    x = np.zeros_like(b)
+    r = b.copy()
+    p = _orth(P(M(r)))
+    it = mv = 0
+    while it < maxit and np.any(_norms(r) > tol * bn):
+        q = P(lh._A(s, p))
+        mv += p.shape[0]
+        k = p.shape[0]
+        Pf, Qf, Rf = p.reshape(k, -1), q.reshape(k, -1), r.reshape(m, -1)
+        PQ = Pf @ Qf.T
+        alpha = np.linalg.solve(PQ, Pf @ Rf.T)  # k x m
+        x = x + (alpha.T @ Pf).reshape(x.shape)
+        r = r - (alpha.T @ Qf).reshape(r.shape)
+        it += 1
+        if not np.any(_norms(r) > tol * bn):
+            break
+        z = P(M(r))
+        beta = -np.linalg.solve(PQ, Qf @ z.reshape(m, -1).T)  # k x m
+        p = _orth(z + (beta.T @ Pf).reshape(z.shape))
+    return x, it, mv
+
+
+def block_study(n_o, seeds, emin=1e-9, tol=1e-9):
+    """Iterations of the lock-step PCG (the reference's algorithm with the library's node-scaled preconditioner)
+    against block PCG over the 6 unit strains, to the same rule; C of each against a tight lock-step solve."""
+    out = []
+    for sd in seeds:
+        rho = OD.random_cell(sd, n_o=n_o, r=1.5, beta=16.0, kmax=2)[0]
+        lh = OL.LinearHomogenization(rho.shape, **MAT, emin=emin, tol=1e-12, maxit=4000)
+        s = lh.stiffness_scale(rho)
+        E = np.eye(6)
+        us, its = lh.solve(s, E, M=OL.ScaledPrecond(lh, s))
+        Cs = lh.bilinear(s, E, us)
+        lh.tol = tol
+        u, it = lh.solve(s, E, M=OL.ScaledPrecond(lh, s))
+        ub, itb, mv = block_pcg(lh, s, -lh.load(s, E), OL.ScaledPrecond(lh, s), tol, 4000)
+        out.append({"seed": sd, "lockstep": (it, OL.rel_C_error(lh.bilinear(s, E, u), Cs)),
+                    "block": (itb, mv, OL.rel_C_error(lh.bilinear(s, E, ub), Cs)), "tight_iterations": its})
+    return out
+
+
 if __name__ == "__main__":
-    if sys.argv[1] == "tangent32":
+    if sys.argv[1] == "block":
+        for row in block_study(int(sys.argv[2]), [int(v) for v in sys.argv[3].split(",")]):
+            print(row, flush=True)
+    elif sys.argv[1] == "tangent32":
         for row in tangent32_study(int(sys.argv[2]), [int(v) for v in sys.argv[3].split(",")]):
             print(row, flush=True)
     elif sys.argv[1] == "mixed":
