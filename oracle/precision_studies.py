@@ -1,4 +1,4 @@
-"""CPU studies behind three design decisions of the solvers, on the oracle's PCG and Newton-CG. TEST
+"""CPU studies behind four design decisions of the solvers, on the oracle's PCG and Newton-CG. TEST
 INFRASTRUCTURE ONLY: nothing in the library imports this file; it restates variants of the oracle's node-scaled
 PCG and of its finite-strain tangent to measure them.
 
@@ -28,6 +28,14 @@ PCG and of its finite-strain tangent to measure them.
    seed 5 (13 pieces) FP64 15 / 1043 and FP32 14 / 766, both stopping by the gradient rule but at lateral strains
    0.0021061 and 0.0021020: the floating pieces settle differently.
 
+4. Block PCG over the 6 load cases of a cell (they share the operator), breakdown-free (Ji & Li 2017), with the
+   node-scaled preconditioner and the lock-step rule (every case residual 1e-9), at a 1e-9 void floor.
+   Measured (32^3): clean cells: seed 1, 84 lock-step iterations against 79 block iterations; seed 2, 77 against
+   71; C unchanged. Island cells: seed 0, 192 against no convergence in 4000; seed 5, 303 against no
+   convergence in 4000. The islands' near-null modes leave P^T A P and the Gram-based orthonormalization
+   ill-conditioned. The island cells are the ones that bound a batch.
+
+    python -m oracle.precision_studies block 16 0,5,1,2
     python -m oracle.precision_studies mixed 16 0,1,2,3     # octant size and seeds
     python -m oracle.precision_studies sensitivity 32 0 8 1e-9
     python -m oracle.precision_studies tangent32 16 1,5
