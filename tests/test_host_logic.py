@@ -150,3 +150,69 @@ def test_bench_generator_matches_the_oracle_generator():
         a, b = bench.synth_phi(seed, n_o), OD.random_start(n_o, 3, seed=seed, kmax=2)
         assert np.abs(a - b).max() < 1e-13
         assert bench.synth_volume(seed) == float(np.random.default_rng(10_000 + seed).uniform(0.2, 0.5))
+
+
+def _q1_gradients():
+    """Shape-function gradients of the unit-cube Q1 element at the 2x2x2 Gauss points, dN[g][a][d] (node
+    a = ax + 2 ay + 4 az, Gauss point g likewise; nlfiber/linear.py:22-41), as libnlf.so's finite-strain kernels
+    load them."""
+    h = 1.0 / (2.0 * np.sqrt(3.0))
+    g1 = (0.5 - h, 0.5 + h)
+    dN = np.zeros((8, 8, 3))
+    for g in range(8):
+        x, y, z = g1[g & 1], g1[(g >> 1) & 1], g1[(g >> 2) & 1]
+        for a in range(8):
+            i, j, k = a & 1, (a >> 1) & 1, (a >> 2) & 1
+            fx, fy, fz = (x if i else 1 - x), (y if j else 1 - y), (z if k else 1 - z)
+            dN[g, a] = [(1 if i else -1) * fy * fz, fx * (1 if j else -1) * fz, fx * fy * (1 if k else -1)]
+    return dN, h
+
+
+def _butterfly(v, transpose=False):
+    """The element's sum/difference butterfly over x, y, z (nlf_element.cuh butterfly8 / butterfly8_t)."""
+    v = np.array(v, dtype=np.float64)
+    pairs = [[(a, a + 1) for a in range(0, 8, 2)], [((q & 1) + ((q >> 1) << 2), (q & 1) + ((q >> 1) << 2) + 2)
+                                                    for q in range(4)], [(a, a + 4) for a in range(4)]]
+    for lev in (reversed(pairs) if transpose else pairs):
+        for a, b in lev:
+            if transpose:
+                v[a], v[b] = v[a] - v[b], v[a] + v[b]
+            else:
+                v[a], v[b] = v[a] + v[b], v[b] - v[a]
+    return v
+
+
+def test_mode_form_gradients_and_forces_of_the_cached_tangent_matvec():
+    """The algebra of the finite-strain CG matvec (k_mech_hvp_tc): the direction's gradient at each Gauss point
+    from the 7 scaled modes of the butterfly, with the macro direction added to the constant-strain modes, and the
+    element forces as signed mode sums then the transposed butterfly, equal the shape-function forms
+    dF_g = dFm + sum_a v_a (x) dN[g][a] and f_a = sum_g P_g dN[g][a] to rounding."""
+    dN, h = _q1_gradients()
+    rng = np.random.default_rng(3)
+    vn, dFm, P = rng.standard_normal((3, 8)), rng.standard_normal((3, 3)), rng.standard_normal((8, 3, 3))
+    km = np.array([_butterfly(vn[c]) for c in range(3)])
+    km[:, 1] = 0.25 * km[:, 1] + dFm[:, 0]
+    km[:, 2] = 0.25 * km[:, 2] + dFm[:, 1]
+    km[:, 4] = 0.25 * km[:, 4] + dFm[:, 2]
+    km[:, [3, 5, 6]] *= 0.5 * h
+    km[:, 7] *= h * h
+    nm = np.zeros((3, 8))
+    for g in range(8):
+        sx, sy, sz = (1 if g & 1 else -1), (1 if (g >> 1) & 1 else -1), (1 if g >> 2 else -1)
+        dF = np.stack([km[:, 1] + sy * km[:, 3] + sz * km[:, 5] + sy * sz * km[:, 7],
+                       km[:, 2] + sx * km[:, 3] + sz * km[:, 6] + sx * sz * km[:, 7],
+                       km[:, 4] + sx * km[:, 5] + sy * km[:, 6] + sx * sy * km[:, 7]], axis=1)
+        np.testing.assert_allclose(dF, dFm + vn @ dN[g], atol=1e-14)
+        px, py, pz = P[g][:, 0], P[g][:, 1], P[g][:, 2]
+        nm[:, 1] += px
+        nm[:, 2] += py
+        nm[:, 4] += pz
+        nm[:, 3] += sy * px + sx * py
+        nm[:, 5] += sz * px + sx * pz
+        nm[:, 6] += sz * py + sy * pz
+        nm[:, 7] += sy * sz * px + sx * sz * py + sx * sy * pz
+    nm[:, [1, 2, 4]] *= 0.25
+    nm[:, [3, 5, 6]] *= 0.5 * h
+    nm[:, 7] *= h * h
+    f = np.array([_butterfly(nm[c], transpose=True) for c in range(3)])
+    np.testing.assert_allclose(f, np.einsum("gcd,gad->ca", P, dN), atol=1e-14)

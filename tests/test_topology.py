@@ -110,3 +110,43 @@ def test_connectivity_structures():
         pass
     else:
         raise AssertionError("edge connectivity must be refused")
+
+
+def _bfs_components(b, faces=False):
+    """Periodic connected components by breadth-first search on the torus (independent of scipy's labelling and
+    of the pad-and-merge construction of nlfiber/topology.py:8-43)."""
+    d = b.ndim
+    offs = [o for o in np.ndindex(*(3,) * d) if any(x != 1 for x in o)]
+    offs = [tuple(x - 1 for x in o) for o in offs]
+    if faces:
+        offs = [o for o in offs if sum(abs(x) for x in o) == 1]
+    lab = np.zeros(b.shape, dtype=np.int64)
+    n = 0
+    for start in zip(*np.nonzero(b)):
+        if lab[start]:
+            continue
+        n += 1
+        lab[start] = n
+        queue = [start]
+        while queue:
+            cur = queue.pop()
+            for o in offs:
+                nb = tuple((c + x) % s for c, x, s in zip(cur, o, b.shape))
+                if b[nb] and not lab[nb]:
+                    lab[nb] = n
+                    queue.append(nb)
+    return lab, n
+
+
+def test_oracle_labelling_matches_breadth_first_search():
+    """The oracle's labelling (the checker of the GPU union-find) gives the components of a breadth-first search
+    on the torus, for both connectivities, cubes and squares, odd and tiny sides."""
+    rng = np.random.default_rng(11)
+    for shape, p in (((6, 6, 6), 0.3), ((5, 7, 4), 0.35), ((2, 2, 2), 0.5), ((9, 9), 0.45), ((3, 11), 0.4)):
+        b = rng.random(shape) < p
+        for faces in (False, True):
+            lab, n = OD.periodic_label(b, faces=faces)
+            ref, nr = _bfs_components(b, faces)
+            assert n == nr
+            pairs = set(zip(lab[b].tolist(), ref[b].tolist()))
+            assert len(pairs) == n and len({a for a, _ in pairs}) == n and len({c for _, c in pairs}) == n
